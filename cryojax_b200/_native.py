@@ -1,0 +1,209 @@
+"""ctypes binding of libcryojax_b200.so (the C-ABI in include/cryojax_b200.h).
+
+The library is the product: there is no CPU fallback.  Loading fails loudly
+when the shared library is missing; calls fail loudly when a tensor is not
+on a CUDA device.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from .build import LIB_PATH
+
+# ---- constants mirrored from include/cryojax_b200.h ----------------------
+CJX_OK = 0
+CJX_ERR_INVALID_ARGUMENT = 1
+CJX_ERR_UNSUPPORTED = 2
+CJX_ERR_CUDA = 3
+CJX_ERR_WORKSPACE = 4
+
+CJX_APPLY_CTF = 1 << 0
+CJX_APPLY_TRANSLATION = 1 << 1
+CJX_APPLY_ENVELOPE = 1 << 2
+CJX_ZERO_FILL_NEGATIVE = 1 << 3
+
+CJX_MAX_SIDE = 1024
+PARAMS_DOUBLES = 32  # sizeof(cjx_image_params) / 8
+
+# field offsets (in doubles) of cjx_image_params
+P_ROT = 0
+P_SHIFT_X = 9
+P_SHIFT_Y = 10
+P_DEFOCUS = 11
+P_ASTIG = 12
+P_ASTIG_ANGLE = 13
+P_CS = 14
+P_WAVELENGTH = 15
+P_PHASE_TOTAL = 16
+P_PIXEL_SIZE = 17
+P_SCALE = 18
+P_ENV_AMP = 19
+P_ENV_B = 20
+
+
+class SliceDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32),
+        ("py", ctypes.c_int32),
+        ("px", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+        ("fill_re", ctypes.c_float),
+        ("fill_im", ctypes.c_float),
+        ("images_per_chunk", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class CryojaxB200Error(RuntimeError):
+    """Raised when a C-ABI entry point returns a nonzero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"cryojax_b200 error {code}: {message}")
+        self.code = code
+
+
+# Every exported symbol of include/cryojax_b200.h with (restype, argtypes).
+_SIGNATURES = {
+    "cjx_get_version": (ctypes.c_int, []),
+    "cjx_get_last_error": (ctypes.c_char_p, []),
+    "cjx_slice_ctf_workspace_size": (
+        ctypes.c_int,
+        [ctypes.POINTER(SliceDesc), ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)],
+    ),
+    "cjx_slice_ctf_forward": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(SliceDesc),
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_int64,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_size_t,
+            ctypes.c_void_p,
+        ],
+    ),
+    "cjx_probe_read_bandwidth": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def library_path() -> str:
+    return os.environ.get("CRYOJAX_B200_LIB", LIB_PATH)
+
+
+def load_library() -> ctypes.CDLL:
+    """Load the shared library (once).  Raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = library_path()
+        if not os.path.exists(path):
+            raise ImportError(
+                f"libcryojax_b200.so not found at {path}; build it with "
+                "`python -m cryojax_b200.build` (there is no CPU fallback)"
+            )
+        lib = ctypes.CDLL(path)
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+        return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def _check(code: int) -> None:
+    if code != CJX_OK:
+        msg = load_library().cjx_get_last_error().decode(errors="replace")
+        raise CryojaxB200Error(code, msg)
+
+
+def make_desc(n, py, px, flags, fill_value=0j, images_per_chunk=0) -> SliceDesc:
+    fill = complex(fill_value)
+    return SliceDesc(int(n), int(py), int(px), int(flags), fill.real, fill.imag, int(images_per_chunk), 0)
+
+
+def workspace_size(desc: SliceDesc, n_images: int) -> int:
+    out = ctypes.c_size_t(0)
+    _check(load_library().cjx_slice_ctf_workspace_size(ctypes.byref(desc), int(n_images), ctypes.byref(out)))
+    return int(out.value)
+
+
+def _cuda_ptr(t, what):
+    if not t.is_cuda:
+        raise ValueError(f"{what} must be a CUDA tensor (no CPU fallback)")
+    if not t.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream=None) -> None:
+    """Launch cjx_slice_ctf_forward on torch CUDA tensors (stream-ordered)."""
+    import torch
+
+    n_images = params.shape[0]
+    if params.dtype != torch.float64 or params.shape[-1] != PARAMS_DOUBLES:
+        raise ValueError("params must be float64 [n_images, 32]")
+    if grid.dtype != torch.complex64:
+        raise ValueError("grid must be complex64")
+    if out.dtype != torch.complex64:
+        raise ValueError("out must be complex64")
+    ws_ptr = ctypes.c_void_p(0)
+    ws_bytes = 0
+    if workspace is not None:
+        ws_ptr = _cuda_ptr(workspace, "workspace")
+        ws_bytes = workspace.numel() * workspace.element_size()
+    _check(
+        load_library().cjx_slice_ctf_forward(
+            ctypes.byref(desc),
+            _cuda_ptr(grid, "grid"),
+            _cuda_ptr(params, "params"),
+            int(n_images),
+            _cuda_ptr(out, "out"),
+            ws_ptr,
+            ws_bytes,
+            _stream_ptr(stream),
+        )
+    )
+
+
+def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:
+    _check(
+        load_library().cjx_probe_read_bandwidth(
+            _cuda_ptr(buf, "buf"),
+            buf.numel() * buf.element_size(),
+            int(passes),
+            _cuda_ptr(sink, "sink"),
+            _stream_ptr(stream),
+        )
+    )
+
+
+def empty_params(n_images: int) -> np.ndarray:
+    p = np.zeros((n_images, PARAMS_DOUBLES), np.float64)
+    p[:, P_SCALE] = 1.0
+    p[:, P_ENV_AMP] = 1.0
+    return p

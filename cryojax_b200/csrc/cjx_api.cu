@@ -1,0 +1,80 @@
+// extern "C" entry points of libcryojax_b200 (declared in include/cryojax_b200.h).
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "cjx_common.cuh"
+
+namespace cjx {
+
+int make_geom(const cjx_slice_desc* d, SliceGeom* g);
+bool needs_resize(const SliceGeom& g);
+size_t workspace_per_image(const SliceGeom& g);
+int64_t default_chunk(const SliceGeom& g, int64_t n_images);
+int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, int64_t n_images,
+                   float2* out, void* workspace, int64_t chunk, cudaStream_t stream);
+int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return CJX_OK;
+  return fail(CJX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static int64_t chunk_for(const SliceGeom& g, const cjx_slice_desc* d, int64_t n_images) {
+  if (d->images_per_chunk > 0) return std::min<int64_t>(d->images_per_chunk, std::max<int64_t>(n_images, 1));
+  return default_chunk(g, n_images);
+}
+
+}  // namespace cjx
+
+using namespace cjx;
+
+extern "C" {
+
+int cjx_get_version(void) { return CJX_ABI_VERSION; }
+
+const char* cjx_get_last_error(void) { return g_last_error.c_str(); }
+
+int cjx_slice_ctf_workspace_size(const cjx_slice_desc* desc, int64_t n_images, size_t* bytes) {
+  if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
+  SliceGeom g;
+  if (int e = make_geom(desc, &g)) return e;
+  *bytes = needs_resize(g) ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
+  return CJX_OK;
+}
+
+int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cjx_image_params* params,
+                          int64_t n_images, void* out, void* workspace, size_t workspace_bytes, void* stream) {
+  SliceGeom g;
+  if (int e = make_geom(desc, &g)) return e;
+  if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
+  if (n_images == 0) return CJX_OK;
+  if (!grid || !params || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params and out must be non-NULL");
+  int64_t chunk = 0;
+  if (needs_resize(g)) {
+    chunk = chunk_for(g, desc, n_images);
+    const size_t need = (size_t)chunk * workspace_per_image(g);
+    if (!workspace || workspace_bytes < need)
+      return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_workspace_size()");
+  }
+  return launch_forward(g, static_cast<const float2*>(grid), params, n_images, static_cast<float2*>(out),
+                        workspace, chunk, static_cast<cudaStream_t>(stream));
+}
+
+int cjx_probe_read_bandwidth(const void* buf, size_t bytes, int passes, void* sink, void* stream) {
+  if (!buf || !sink || bytes < 16 || passes < 1)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "need buf, sink, bytes >= 16, passes >= 1");
+  return launch_read_probe(buf, bytes, passes, sink, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

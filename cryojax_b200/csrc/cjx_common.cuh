@@ -1,0 +1,228 @@
+// Shared device helpers for the cryojax_b200 kernels: geometry of one
+// launch, cryoJAX's trilinear sampling rule, the CTF / envelope /
+// translation epilogue, and host-side error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/cryojax_b200.h"
+#include "cjx_fft.cuh"
+
+namespace cjx {
+
+constexpr int kWarps = 8;  // warps per CTA in the column / row passes
+
+// Geometry of one (volume side, image shape) group.
+struct SliceGeom {
+  int n;            // volume side N
+  int py, px;       // padded image shape
+  int nxh;          // N/2 + 1 (half-plane columns of the slice)
+  int pxh;          // Px/2 + 1
+  int ld1, ld2;     // row pitch (complex elements) of workspace T1, T2
+  int pad_left_y;   // left pad when Py > N (cryojax/ndimage/_edges.py:175-185)
+  int pad_left_x;
+  uint32_t flags;
+  float2 fill;      // out-of-bounds fill value
+  FftPlan plan_n, plan_py, plan_px;
+};
+
+// ---------------------------------------------------------------------------
+// Index helpers
+// ---------------------------------------------------------------------------
+
+// Signed frequency index of entry i of an fftfreq-ordered axis of length n
+// (numpy.fft.fftfreq(n) * n).
+__device__ __forceinline__ int fft_index(int i, int n) { return (i < n - n / 2) ? i : i - n; }
+
+// Resize window along one axis (irfftn -> fftshift -> centre crop or pad ->
+// ifftshift -> rfftn, cryojax/simulator/_volume_integrator/
+// fourier_voxel_extract.py:133-138 with cryojax/ndimage/_edges.py:15-62,
+// 110-185): destination sample m of the unshifted length-n_dst signal comes
+// from sample win_src(m) of the unshifted length-n_src signal, or is zero
+// padding when win_src returns -1.
+__device__ __forceinline__ int win_src(int m, int n_src, int n_dst, int pad_left) {
+  const int mm = (m + n_dst / 2) % n_dst;  // position in the centred destination
+  int s;
+  if (n_dst <= n_src) {
+    s = mm + (n_src / 2 - n_dst / 2);
+  } else {
+    s = mm - pad_left;
+    if (s < 0 || s >= n_src) return -1;
+  }
+  return (s - n_src / 2 + n_src) % n_src;
+}
+
+// ---------------------------------------------------------------------------
+// Trilinear sampling with cryoJAX's rule
+// (cryojax/ndimage/_map_coordinates.py:85-123, 168-175): lower = floor(c),
+// w_hi = c - lower, w_lo = 1 - w_hi; each of the 8 corners is read with
+// `.at[idx].get(mode="fill")`: a negative index wraps once to idx + N, any
+// index still outside [0, N) yields the fill value.
+//
+// The coordinate is passed as an offset from the grid centre N/2 (the
+// logical coordinate is offset + N/2, cryojax/simulator/_volume_integrator/
+// fourier_voxel_extract.py:528): floor and weights are taken on the offset,
+// so the interpolation weights keep full single precision near the origin
+// where the spectrum is largest.
+// ---------------------------------------------------------------------------
+struct AxisNodes {
+  int i0, i1;      // wrapped corner indices (clamped when invalid)
+  bool v0, v1;     // corner inside [0, N)
+  float w0, w1;    // lower / upper weights
+};
+
+__device__ __forceinline__ AxisNodes axis_nodes(float off, int n, bool wrap_negative) {
+  AxisNodes a;
+  const float f = floorf(off);
+  a.w1 = off - f;
+  a.w0 = 1.0f - a.w1;
+  int i0 = (int)f + n / 2;
+  int i1 = i0 + 1;
+  if (wrap_negative) {
+    if (i0 < 0) i0 += n;
+    if (i1 < 0) i1 += n;
+  }
+  a.v0 = (unsigned)i0 < (unsigned)n;
+  a.v1 = (unsigned)i1 < (unsigned)n;
+  a.i0 = a.v0 ? i0 : 0;
+  a.i1 = a.v1 ? i1 : 0;
+  return a;
+}
+
+__device__ __forceinline__ float2 sample_trilinear(const float2* __restrict__ grid, int n, float ox, float oy,
+                                                   float oz, bool wrap_negative, float2 fill) {
+  const AxisNodes ax = axis_nodes(ox, n, wrap_negative);
+  const AxisNodes ay = axis_nodes(oy, n, wrap_negative);
+  const AxisNodes az = axis_nodes(oz, n, wrap_negative);
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz) {
+    const int iz = dz ? az.i1 : az.i0;
+    const bool vz = dz ? az.v1 : az.v0;
+    const float wz = dz ? az.w1 : az.w0;
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy) {
+      const int iy = dy ? ay.i1 : ay.i0;
+      const bool vy = dy ? ay.v1 : ay.v0;
+      const float wzy = wz * (dy ? ay.w1 : ay.w0);
+      const size_t row = ((size_t)iz * n + iy) * n;
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const int ix = dx ? ax.i1 : ax.i0;
+        const bool ok = vz && vy && (dx ? ax.v1 : ax.v0);
+        const float w = wzy * (dx ? ax.w1 : ax.w0);
+        const float2 g = ok ? __ldg(&grid[row + ix]) : fill;
+        acc.x = fmaf(w, g.x, acc.x);
+        acc.y = fmaf(w, g.y, acc.y);
+      }
+    }
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Epilogue: scale, CTF, envelope, translation
+// ---------------------------------------------------------------------------
+struct ImageConsts {
+  double inv_px;        // 1 / pixel_size
+  double defocus;
+  double half_astig;    // 0.5 * astigmatism
+  double c_def;         // -0.5 * wavelength                (cycles per A^2 per A)
+  double c_sph;         // 0.25 * Cs * wavelength^3
+  double phase_cycles;  // phase_total / (2 pi)
+  double tx, ty;
+  float cos2a, sin2a;   // cos / sin of 2 * astigmatism_angle
+  float scale;
+  float env_amp, env_quarter_b;
+};
+
+__device__ __forceinline__ ImageConsts load_image_consts(const cjx_image_params* __restrict__ p, float extra_scale) {
+  ImageConsts c;
+  c.inv_px = 1.0 / p->pixel_size;
+  c.defocus = p->defocus;
+  c.half_astig = 0.5 * p->astigmatism;
+  const double wl = p->wavelength;
+  c.c_def = -0.5 * wl;
+  c.c_sph = 0.25 * p->spherical_aberration * wl * wl * wl;
+  c.phase_cycles = p->phase_total * 0.15915494309189533577;  // 1 / (2 pi)
+  c.tx = p->shift_x;
+  c.ty = p->shift_y;
+  double s2, c2;
+  sincos(2.0 * p->astigmatism_angle, &s2, &c2);
+  c.cos2a = (float)c2;
+  c.sin2a = (float)s2;
+  c.scale = (float)(p->scale * (double)extra_scale);
+  c.env_amp = (float)p->envelope_amplitude;
+  c.env_quarter_b = (float)(0.25 * p->envelope_b_factor);
+  return c;
+}
+
+// Value at rfft-grid entry (i, j) of a (py, px) image.
+//   qx = rfftfreq(px)[j] / pixel_size, qy = fftfreq(py)[i] / pixel_size
+//   (cryojax/simulator/_image_config.py:194-201);
+//   CTF = sin(chi - phase_total), chi = 2 pi (-1/2 df(theta) lambda k^2
+//   + 1/4 Cs lambda^3 k^4), df(theta) = df + astig/2 cos(2 (theta - alpha)),
+//   theta = atan2(qx, qy)  (cryojax/simulator/_transfer_theory/
+//   common_functions.py:9-40, transfer_function.py:27-82, 130-169).
+//   cos(2 theta) = (qy^2 - qx^2) / k^2 and sin(2 theta) = 2 qx qy / k^2, so
+//   no per-pixel atan2 is needed; at k = 0 theta = atan2(0, 0) = 0.
+//   chi is accumulated in cycles in double and reduced to [-1/2, 1/2]
+//   before the single-precision sinpi, so large defocus keeps full accuracy.
+//   Translation: zero the even-size Nyquist self-conjugates, then multiply
+//   by exp(-2 pi i (qx tx + qy ty))  (cryojax/simulator/_pose.py:68-114).
+__device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
+                                                 const ImageConsts& c) {
+  v.x *= c.scale;
+  v.y *= c.scale;
+  if (flags & (CJX_APPLY_CTF | CJX_APPLY_ENVELOPE | CJX_APPLY_TRANSLATION)) {
+    const double qy = (double)fft_index(i, py) / (double)py * c.inv_px;
+    const double qx = (double)j / (double)px * c.inv_px;
+    const double k2 = qx * qx + qy * qy;
+    if (flags & CJX_APPLY_CTF) {
+      float c2t = 1.0f, s2t = 0.0f;
+      if (k2 > 0.0) {
+        const double inv = 1.0 / k2;
+        c2t = (float)((qy * qy - qx * qx) * inv);
+        s2t = (float)(2.0 * qx * qy * inv);
+      }
+      const double df = c.defocus + c.half_astig * (double)(c2t * c.cos2a + s2t * c.sin2a);
+      const double arg = (c.c_def * df + c.c_sph * k2) * k2 - c.phase_cycles;
+      const float r = (float)(arg - rint(arg));
+      const float ctf = sinpif(2.0f * r);
+      v.x *= ctf;
+      v.y *= ctf;
+    }
+    if (flags & CJX_APPLY_ENVELOPE) {
+      const float e = c.env_amp * expf(-c.env_quarter_b * (float)k2);
+      v.x *= e;
+      v.y *= e;
+    }
+    if (flags & CJX_APPLY_TRANSLATION) {
+      const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
+      const bool self_conj = (ey && i == py / 2 && j == 0) || (ex && i == 0 && j == px / 2) ||
+                             (ey && ex && i == py / 2 && j == px / 2);
+      if (self_conj) {
+        v = make_float2(0.f, 0.f);
+      } else {
+        const double ph = qx * c.tx + qy * c.ty;
+        const float r = (float)(ph - rint(ph));
+        float s, co;
+        sincospif(2.0f * r, &s, &co);
+        v = make_float2(fmaf(v.x, co, v.y * s), fmaf(v.y, co, -v.x * s));
+      }
+    }
+  }
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side error plumbing
+// ---------------------------------------------------------------------------
+void set_last_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int check_cuda(cudaError_t e, const char* what);
+
+}  // namespace cjx

@@ -1,0 +1,221 @@
+// Warp-level shared-memory FFTs for the resize stage of the Fourier-slice path.
+//
+// One warp transforms one length-n complex sequence held in shared memory,
+// out of place between two buffers (Stockham autosort, natural order in and
+// out).  Radices 8, 4, 2, 3, 5 have hand-written butterflies, radix 7 uses
+// the twiddle table; a length with any other prime factor falls back to a
+// direct O(n^2) DFT.  Twiddles exp(-2 pi i m / n) are computed per launch in
+// double precision and stored as float2 in shared memory.
+//
+// Sign convention: DIR = -1 is the forward transform (numpy.fft.fft),
+// DIR = +1 the unnormalised inverse (n * numpy.fft.ifft).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace cjx {
+
+constexpr int kMaxStages = 16;
+
+struct FftPlan {
+  int n;
+  int nstages;  // 0 => direct DFT
+  int radix[kMaxStages];
+};
+
+__host__ inline FftPlan make_fft_plan(int n) {
+  FftPlan p{};
+  p.n = n;
+  int m = n, s = 0;
+  const int radices[] = {8, 4, 2, 3, 5, 7};
+  for (int r : radices) {
+    while (m % r == 0 && s < kMaxStages) {
+      p.radix[s++] = r;
+      m /= r;
+    }
+  }
+  p.nstages = (m == 1) ? s : 0;
+  return p;
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by DIR * i
+template <int DIR>
+__device__ __forceinline__ float2 cmul_i(float2 a) {
+  return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+// twiddle exp(DIR * 2 pi i m / n) from the forward table
+template <int DIR>
+__device__ __forceinline__ float2 twiddle(const float2* tw, int m) {
+  float2 w = tw[m];
+  return DIR > 0 ? cconj(w) : w;
+}
+
+// Fill tw[m] = exp(-2 pi i m / n), m in [0, n), cooperatively by the block.
+__device__ inline void build_twiddles(float2* tw, int n) {
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)n, &s, &c);
+    tw[m] = make_float2((float)c, (float)s);
+  }
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft2(float2* v) {
+  float2 a = v[0];
+  v[0] = cadd(a, v[1]);
+  v[1] = csub(a, v[1]);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+  float2 s02 = cadd(a0, a2), d02 = csub(a0, a2);
+  float2 s13 = cadd(a1, a3), d13 = csub(a1, a3);
+  float2 t = cmul_i<DIR>(d13);
+  a0 = cadd(s02, s13);
+  a2 = csub(s02, s13);
+  a1 = cadd(d02, t);
+  a3 = csub(d02, t);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft3(float2* v) {
+  const float c = 0.86602540378443864676f;  // sqrt(3)/2
+  float2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+  float2 x0 = cadd(v[0], s);
+  float2 m = make_float2(fmaf(-0.5f, s.x, v[0].x), fmaf(-0.5f, s.y, v[0].y));
+  float2 t = cscale(cmul_i<DIR>(d), c);
+  v[0] = x0;
+  v[1] = cadd(m, t);
+  v[2] = csub(m, t);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft5(float2* v) {
+  const float c1 = 0.30901699437494742410f;   // cos(2 pi / 5)
+  const float c2 = -0.80901699437494742410f;  // cos(4 pi / 5)
+  const float s1 = 0.95105651629515357212f;   // sin(2 pi / 5)
+  const float s2 = 0.58778525229247312917f;   // sin(4 pi / 5)
+  float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+  float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+  float2 a0 = v[0];
+  float2 m1 = make_float2(a0.x + c1 * t1.x + c2 * t2.x, a0.y + c1 * t1.y + c2 * t2.y);
+  float2 m2 = make_float2(a0.x + c2 * t1.x + c1 * t2.x, a0.y + c2 * t1.y + c1 * t2.y);
+  float2 n1 = cmul_i<DIR>(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+  float2 n2 = cmul_i<DIR>(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+  v[0] = cadd(a0, cadd(t1, t2));
+  v[1] = cadd(m1, n1);
+  v[4] = csub(m1, n1);
+  v[2] = cadd(m2, n2);
+  v[3] = csub(m2, n2);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft8(float2* v) {
+  const float r = 0.70710678118654752440f;
+  float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<DIR>(e0, e1, e2, e3);
+  dft4<DIR>(o0, o1, o2, o3);
+  // o_k *= exp(DIR 2 pi i k / 8)
+  o1 = make_float2((o1.x - DIR * o1.y) * r, (o1.y + DIR * o1.x) * r);
+  o2 = cmul_i<DIR>(o2);
+  o3 = make_float2((-o3.x - DIR * o3.y) * r, (-o3.y + DIR * o3.x) * r);
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[7] = csub(e3, o3);
+}
+
+// Generic radix-R DFT with twiddles exp(DIR 2 pi i r q / R) = tw[(r q n / R) mod n].
+template <int R, int DIR>
+__device__ __forceinline__ void dft_generic(float2* v, const float2* tw, int n) {
+  float2 out[R];
+  const int step = n / R;
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    float2 acc = v[0];
+#pragma unroll
+    for (int r = 1; r < R; ++r) acc = cadd(acc, cmul(v[r], twiddle<DIR>(tw, ((r * q) % R) * step)));
+    out[q] = acc;
+  }
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = out[q];
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, float2* __restrict__ out,
+                                               int n, int Ns, const float2* tw, int lane) {
+  const int nb = n / R;
+  const int tstep = n / (Ns * R);
+  for (int j = lane; j < nb; j += 32) {
+    const int k = j % Ns;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = in[j + q * nb];
+    if (Ns > 1) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle<DIR>(tw, (q * k * tstep) % n));
+    }
+    if constexpr (R == 2) dft2<DIR>(v);
+    else if constexpr (R == 3) dft3<DIR>(v);
+    else if constexpr (R == 4) dft4<DIR>(v[0], v[1], v[2], v[3]);
+    else if constexpr (R == 5) dft5<DIR>(v);
+    else if constexpr (R == 8) dft8<DIR>(v);
+    else dft_generic<R, DIR>(v, tw, n);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int q = 0; q < R; ++q) out[base + q * Ns] = v[q];
+  }
+}
+
+// Transform buffer `a` (length plan.n) with scratch `b`; returns the buffer
+// holding the result (a or b).  Executed by one full warp; ends with __syncwarp.
+template <int DIR>
+__device__ float2* warp_fft(float2* a, float2* b, const FftPlan& plan, const float2* tw, int lane) {
+  const int n = plan.n;
+  if (plan.nstages == 0) {
+    for (int k = lane; k < n; k += 32) {
+      float2 acc = make_float2(0.f, 0.f);
+      int m = 0;
+      for (int j = 0; j < n; ++j) {
+        acc = cadd(acc, cmul(a[j], twiddle<DIR>(tw, m)));
+        m += k;
+        if (m >= n) m -= n;
+      }
+      b[k] = acc;
+    }
+    __syncwarp();
+    return b;
+  }
+  int Ns = 1;
+  for (int s = 0; s < plan.nstages; ++s) {
+    const int R = plan.radix[s];
+    switch (R) {
+      case 8: stockham_stage<8, DIR>(a, b, n, Ns, tw, lane); break;
+      case 4: stockham_stage<4, DIR>(a, b, n, Ns, tw, lane); break;
+      case 2: stockham_stage<2, DIR>(a, b, n, Ns, tw, lane); break;
+      case 3: stockham_stage<3, DIR>(a, b, n, Ns, tw, lane); break;
+      case 5: stockham_stage<5, DIR>(a, b, n, Ns, tw, lane); break;
+      default: stockham_stage<7, DIR>(a, b, n, Ns, tw, lane); break;
+    }
+    __syncwarp();
+    float2* t = a;
+    a = b;
+    b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+}  // namespace cjx

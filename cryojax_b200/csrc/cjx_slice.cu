@@ -1,0 +1,337 @@
+// Forward Fourier-slice + CTF kernels (sm_100a).
+//
+// Resize path ((Py, Px) != (N, N)), three passes per chunk of images, with
+// the two intermediates kept in a workspace sized so a chunk stays L2
+// resident:
+//   A  gather + column inverse FFT: one warp per slice column kx.  The warp
+//      samples the N points of that column of the rotated central plane,
+//      makes columns kx = 0 and kx = N/2 Hermitian in ky (the irfftn of the
+//      reference ignores the non-Hermitian part there), runs an N-point
+//      inverse FFT and keeps the Py rows of the real-space crop/pad window.
+//   B  rows: two rows packed as A + iB, Hermitian-extended, N-point inverse
+//      FFT (= irfft of both rows), crop/pad window to Px, Px-point forward
+//      FFT, split into the two rfft half rows.
+//   C  columns: Py-point forward FFT of each half-plane column, then scale,
+//      CTF, envelope and translation, written to the output.
+// No-resize path ((Py, Px) == (N, N)): one fused kernel samples each output
+// pixel and applies the epilogue directly.
+#include <algorithm>
+#include <mutex>
+
+#include "cjx_common.cuh"
+
+namespace cjx {
+
+// ---------------------------------------------------------------------------
+// Pass A
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarps * 32)
+    k_gather_colifft(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
+                     float2* __restrict__ t1, SliceGeom g, int64_t img0) {
+  extern __shared__ float2 smem[];
+  const int n = g.n, h = n / 2;
+  const int stride = 2 * n + 2;  // per-warp buffers (+2 to stagger banks)
+  float2* tw = smem;
+  float2* bufs = smem + n;
+  build_twiddles(tw, n);
+
+  const int64_t img = img0 + blockIdx.y;
+  const double* R = params[img].rot;
+  const float r00 = (float)R[0], r01 = (float)R[1];
+  const float r10 = (float)R[3], r11 = (float)R[4];
+  const float r20 = (float)R[6], r21 = (float)R[7];
+  const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j0 = blockIdx.x * kWarps;
+  const int j = j0 + warp;
+  float2* a = bufs + warp * stride;
+  float2* b = a + n;
+  if (j < g.nxh) {
+    const float ux = (float)fft_index(j, n);
+    const float bx = r00 * ux, by = r10 * ux, bz = r20 * ux;
+    for (int i = lane; i < n; i += 32) {
+      const float vy = (float)fft_index(i, n);
+      a[i] = sample_trilinear(grid, n, fmaf(r01, vy, bx), fmaf(r11, vy, by), fmaf(r21, vy, bz), wrap, g.fill);
+    }
+    __syncwarp();
+    if (j == 0 || ((n % 2 == 0) && j == h)) {
+      // S'[v] = (S[v] + conj(S[-v])) / 2  (covers the mode="real" fix at v = 0, N/2)
+      for (int i = lane; i <= n / 2; i += 32) {
+        const int i2 = (i == 0) ? 0 : n - i;
+        const float2 x = a[i], y = a[i2];
+        const float2 s = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        a[i] = s;
+        a[i2] = cconj(s);
+      }
+      __syncwarp();
+    }
+    warp_fft<+1>(a, b, g.plan_n, tw, lane);
+  }
+  __syncthreads();
+
+  // The FFT result sits in buffer a after an even number of Stockham stages,
+  // in b after an odd number (or after the direct DFT).
+  const int res_off = (g.plan_n.nstages == 0 || (g.plan_n.nstages & 1)) ? n : 0;
+  const int ncols = min(kWarps, g.nxh - j0);
+  float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
+  for (int e = threadIdx.x; e < g.py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      const int src = win_src(m, n, g.py, g.pad_left_y);
+      dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? bufs[jj * stride + res_off + src] : make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass B
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarps * 32)
+    k_rows_c2r_r2c(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g) {
+  extern __shared__ float2 smem[];
+  const int n = g.n, px = g.px;
+  const int L = max(n, px);
+  float2* twn = smem;
+  float2* twp = twn + n;
+  float2* bufs = twp + px;
+  build_twiddles(twn, n);
+  build_twiddles(twp, px);
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  if (ra >= g.py) return;
+  const bool has_b = (ra + 1) < g.py;
+  float2* a = bufs + warp * (2 * L + 2);
+  float2* b = a + L;
+  const float2* rowA = t1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
+  const float2* rowB = rowA + g.ld1;
+
+  // Z = A + iB on the Hermitian extension; DC and (even N) Nyquist bins use
+  // the real part only, as an irfft does.
+  const int h = n / 2;
+  for (int k = lane; k <= h; k += 32) {
+    float2 A = rowA[k];
+    float2 B = has_b ? rowB[k] : make_float2(0.f, 0.f);
+    if (k == 0 || ((n % 2 == 0) && k == h)) {
+      a[k] = make_float2(A.x, B.x);
+    } else {
+      a[k] = make_float2(A.x - B.y, A.y + B.x);
+      a[n - k] = make_float2(A.x + B.y, B.x - A.y);
+    }
+  }
+  __syncwarp();
+  float2* z = warp_fft<+1>(a, b, g.plan_n, twn, lane);  // z = a_row + i b_row (real rows)
+  float2* w = (z == a) ? b : a;
+  for (int m = lane; m < px; m += 32) {
+    const int src = win_src(m, n, px, g.pad_left_x);
+    w[m] = (src >= 0) ? z[src] : make_float2(0.f, 0.f);
+  }
+  __syncwarp();
+  float2* W = warp_fft<-1>(w, z, g.plan_px, twp, lane);
+  float2* outA = t2 + ((size_t)blockIdx.y * g.py + ra) * g.ld2;
+  for (int k = lane; k < g.pxh; k += 32) {
+    const float2 Wk = W[k];
+    const float2 Wm = W[(px - k) % px];
+    outA[k] = make_float2(0.5f * (Wk.x + Wm.x), 0.5f * (Wk.y - Wm.y));
+    if (has_b) outA[g.ld2 + k] = make_float2(0.5f * (Wk.y + Wm.y), -0.5f * (Wk.x - Wm.x));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass C
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colfft_epilogue(const float2* __restrict__ t2, const cjx_image_params* __restrict__ params,
+                      float2* __restrict__ out, SliceGeom g, int64_t img0, float norm) {
+  extern __shared__ float2 smem[];
+  const int py = g.py;
+  const int stride = 2 * py + 2;
+  float2* tw = smem;
+  float2* bufs = smem + py;
+  build_twiddles(tw, py);
+
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.pxh - j0);
+  const float2* src = t2 + (size_t)blockIdx.y * py * g.ld2 + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + m] = src[(size_t)m * g.ld2 + jj];
+  }
+  const int64_t img = img0 + blockIdx.y;
+  const ImageConsts c = load_image_consts(params + img, norm);
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) {
+    float2* a = bufs + warp * stride;
+    float2* X = warp_fft<-1>(a, a + py, g.plan_py, tw, lane);
+    const int j = j0 + warp;
+    for (int i = lane; i < py; i += 32) X[i] = apply_epilogue(X[i], i, j, py, g.px, g.flags, c);
+  }
+  __syncthreads();
+  const int res_off = (g.plan_py.nstages == 0 || (g.plan_py.nstages & 1)) ? py : 0;
+  float2* dst = out + (size_t)img * py * g.pxh + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) dst[(size_t)m * g.pxh + jj] = bufs[jj * stride + res_off + m];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// No-resize path: fused slice + epilogue, one thread per output pixel.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_slice_direct(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
+                   float2* __restrict__ out, SliceGeom g) {
+  const int n = g.n, h = n / 2;
+  const int64_t img = blockIdx.y;
+  const double* R = params[img].rot;
+  const float r00 = (float)R[0], r01 = (float)R[1];
+  const float r10 = (float)R[3], r11 = (float)R[4];
+  const float r20 = (float)R[6], r21 = (float)R[7];
+  const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
+  const ImageConsts c = load_image_consts(params + img, 1.0f);
+  const int total = n * g.nxh;
+  float2* dst = out + (size_t)img * total;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int i = e / g.nxh, j = e - i * g.nxh;
+    const float ux = (float)fft_index(j, n), vy = (float)fft_index(i, n);
+    float2 v = sample_trilinear(grid, n, fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux),
+                                fmaf(r21, vy, r20 * ux), wrap, g.fill);
+    // convert_fftn_to_rfftn(mode="real")  (cryojax/ndimage/_fourier_utils.py:6-57)
+    if ((n % 2 == 0) && ((i == h && j == 0) || (i == 0 && j == h) || (i == h && j == h))) v.y = 0.f;
+    dst[e] = apply_epilogue(v, i, j, n, n, g.flags, c);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+static size_t smem_a(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.n + kWarps * (2 * g.n + 2)); }
+static size_t smem_b(const SliceGeom& g) {
+  const int L = std::max(g.n, g.px);
+  return sizeof(float2) * (size_t)(g.n + g.px + kWarps * (2 * L + 2));
+}
+static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py + kWarps * (2 * g.py + 2)); }
+
+static int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
+  if (!d) return fail(CJX_ERR_INVALID_ARGUMENT, "desc is NULL");
+  if (d->n < 2 || d->py < 1 || d->px < 2)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "need n >= 2, py >= 1, px >= 2");
+  if (d->n > CJX_MAX_SIDE || d->py > CJX_MAX_SIDE || d->px > CJX_MAX_SIDE)
+    return fail(CJX_ERR_UNSUPPORTED, "volume side and image sides are limited to CJX_MAX_SIDE");
+  const uint32_t known = CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE;
+  if (d->flags & ~known) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown flag bits");
+  g->n = d->n;
+  g->py = d->py;
+  g->px = d->px;
+  g->nxh = d->n / 2 + 1;
+  g->pxh = d->px / 2 + 1;
+  g->ld1 = round_up(g->nxh, 8);
+  g->ld2 = round_up(g->pxh, 8);
+  auto left_pad = [](int pad_dim, int image_dim) {
+    const int pad = pad_dim - image_dim;
+    if (pad_dim % 2 == 0 && image_dim % 2 == 1) return pad / 2 + 1;
+    return pad / 2;
+  };
+  g->pad_left_y = d->py > d->n ? left_pad(d->py, d->n) : 0;
+  g->pad_left_x = d->px > d->n ? left_pad(d->px, d->n) : 0;
+  g->flags = d->flags;
+  g->fill = make_float2(d->fill_re, d->fill_im);
+  g->plan_n = make_fft_plan(d->n);
+  g->plan_py = make_fft_plan(d->py);
+  g->plan_px = make_fft_plan(d->px);
+  return CJX_OK;
+}
+
+bool needs_resize(const SliceGeom& g) { return !(g.py == g.n && g.px == g.n); }
+
+size_t workspace_per_image(const SliceGeom& g) {
+  return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2);
+}
+
+// Default chunk: about 64 MB of intermediates, so a chunk stays in L2.
+int64_t default_chunk(const SliceGeom& g, int64_t n_images) {
+  const size_t per = workspace_per_image(g);
+  int64_t c = (int64_t)((64u << 20) / std::max<size_t>(per, 1));
+  c = std::max<int64_t>(c, 1);
+  c = std::min<int64_t>(c, 65535);
+  return std::min<int64_t>(c, std::max<int64_t>(n_images, 1));
+}
+
+static int ensure_smem_attrs() {
+  static std::once_flag flags[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
+  int err = CJX_OK;
+  std::call_once(flags[dev & 63], [&] {
+    const int max_bytes = 227 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_gather_colifft, cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_rows_c2r_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_colfft_epilogue, cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
+    if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
+  });
+  return err;
+}
+
+int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, int64_t n_images,
+                   float2* out, void* workspace, int64_t chunk, cudaStream_t stream) {
+  if (n_images == 0) return CJX_OK;
+  if (!needs_resize(g)) {
+    const int total = g.n * g.nxh;
+    const int blocks = std::min((total + 255) / 256, 1024);
+    for (int64_t i0 = 0; i0 < n_images; i0 += 65535) {
+      const int cnt = (int)std::min<int64_t>(65535, n_images - i0);
+      k_slice_direct<<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params + i0, out + (size_t)i0 * total, g);
+    }
+    return check_cuda(cudaGetLastError(), "k_slice_direct launch");
+  }
+  if (int e = ensure_smem_attrs()) return e;
+  const size_t sa = smem_a(g), sb = smem_b(g), sc = smem_c(g);
+  if (sa > 227 * 1024 || sb > 227 * 1024 || sc > 227 * 1024)
+    return fail(CJX_ERR_UNSUPPORTED, "shared-memory footprint exceeds 227 KB for these sizes");
+  float2* t1 = static_cast<float2*>(workspace);
+  float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
+  const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
+  for (int64_t i0 = 0; i0 < n_images; i0 += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_images - i0);
+    k_gather_colifft<<<dim3((g.nxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sa, stream>>>(grid, params, t1, g,
+                                                                                             i0);
+    k_rows_c2r_r2c<<<dim3((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, sb, stream>>>(t1, t2, g);
+    k_colfft_epilogue<<<dim3((g.pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sc, stream>>>(t2, params, out, g,
+                                                                                             i0, norm);
+  }
+  return check_cuda(cudaGetLastError(), "forward launch");
+}
+
+// ---------------------------------------------------------------------------
+// Read-bandwidth probe
+// ---------------------------------------------------------------------------
+__global__ void k_read_probe(const float4* __restrict__ buf, size_t n16, int passes, float* sink) {
+  float acc = 0.f;
+  for (int p = 0; p < passes; ++p) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x) {
+      const float4 v = __ldcg(&buf[i]);
+      acc += (v.x + v.y) + (v.z + v.w);
+    }
+  }
+  if (acc == 1.2345e-30f) sink[0] = acc;  // keeps the loads live
+}
+
+int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_read_probe<<<sms * 4, 512, 0, stream>>>(static_cast<const float4*>(buf), bytes / 16, passes,
+                                            static_cast<float*>(sink));
+  return check_cuda(cudaGetLastError(), "k_read_probe launch");
+}
+
+}  // namespace cjx

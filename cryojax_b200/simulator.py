@@ -1,0 +1,600 @@
+"""Host-side mirror of cryoJAX's simulator API for the Fourier-slice path.
+
+Same class names, argument names and meanings as ``cryojax.simulator``
+(the reference is JAX/Equinox; this mirror holds NumPy parameters on the
+host and torch CUDA tensors on the device).  Every field of a pose, CTF or
+image config may carry a leading batch axis: a batched model simulates all
+its images in ONE launch of ``cjx_slice_ctf_forward`` — the counterpart of
+wrapping ``simulate`` in ``eqx.filter_vmap`` over (pose, transfer theory)
+with the volume broadcast.
+
+Covered (reference file:line):
+  BasicImageConfig            cryojax/simulator/_image_config.py:280-338
+  EulerAnglePose, QuaternionPose, AxisAnglePose
+                              cryojax/simulator/_pose.py:203-403
+  AstigmaticCTF               cryojax/simulator/_transfer_theory/transfer_function.py:84-169
+  ContrastTransferTheory      cryojax/simulator/_transfer_theory/transfer_theory.py:21-119
+  FourierGaussian (envelope)  cryojax/ndimage/operators/_fourier_operator.py:183-234
+  FourierVoxelGridVolume      cryojax/simulator/_volume/representations/voxel_volume.py:40-119
+  FourierSliceExtraction      cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-146
+  WeakPhaseScatteringTheory   cryojax/simulator/_scattering_theory/weak_phase_scattering_theory.py:13-80
+  LinearImageModel, ProjectionImageModel
+                              cryojax/simulator/_image_model/base_image_model.py:216-432
+  ContrastImageModel          cryojax/simulator/_image_model/physical_image_model.py:30-137
+  make_image_model            cryojax/simulator/_api_utils.py:36-223
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Any
+
+import numpy as np
+
+from . import _native as nat
+from . import constants as C
+from . import rotations as rot
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+
+def _arr(x):
+    return np.asarray(x, dtype=np.float64)
+
+
+def _batch_size(*xs) -> int | None:
+    """Size of the common leading batch axis (None if all are unbatched)."""
+    n = None
+    for x in xs:
+        if x is None:
+            continue
+        a = np.asarray(x)
+        if a.ndim == 0:
+            continue
+        if n is None:
+            n = a.shape[0]
+        elif a.shape[0] != n and a.shape[0] != 1:
+            raise ValueError(f"inconsistent batch sizes {n} and {a.shape[0]}")
+    return n
+
+
+def _per_image(x, n):
+    a = _arr(x)
+    if a.ndim == 0:
+        return np.full(n, float(a))
+    return np.broadcast_to(a.reshape(a.shape[0]), (n,)).astype(np.float64)
+
+
+def _require_positive(name, x):
+    if np.any(_arr(x) <= 0):
+        raise ValueError(f"`{name}` must be positive")
+
+
+# ---------------------------------------------------------------------------
+# Image configuration
+# ---------------------------------------------------------------------------
+
+
+class BasicImageConfig:
+    """Image shape, pixel size, voltage and padding options.
+
+    cryojax/simulator/_image_config.py:280-338 (``pad_options`` keys
+    ``shape`` and ``mode``; only ``mode="constant"`` is implemented on the
+    device).
+    """
+
+    def __init__(self, shape, pixel_size, voltage_in_kilovolts, *, pad_options: dict | None = None):
+        pad_options = dict(pad_options or {})
+        self.shape = tuple(int(s) for s in shape)
+        _require_positive("pixel_size", pixel_size)
+        _require_positive("voltage_in_kilovolts", voltage_in_kilovolts)
+        self.pixel_size = _arr(pixel_size)
+        self.voltage_in_kilovolts = _arr(voltage_in_kilovolts)
+        self.pad_options = {
+            "shape": tuple(int(s) for s in pad_options.get("shape", self.shape)),
+            "mode": pad_options.get("mode", "constant"),
+        }
+        if self.padded_shape[0] < self.shape[0] or self.padded_shape[1] < self.shape[1]:
+            raise AttributeError("`padded_shape` is less than `shape` in one or more dimensions.")
+
+    @property
+    def padded_shape(self):
+        return self.pad_options["shape"]
+
+    @property
+    def pad_mode(self):
+        return self.pad_options["mode"]
+
+    @property
+    def wavelength_in_angstroms(self):
+        return C.wavelength_from_kilovolts(self.voltage_in_kilovolts)
+
+    @property
+    def interaction_constant(self):
+        return C.interaction_constant_from_kilovolts(self.voltage_in_kilovolts)
+
+    @property
+    def n_pixels(self):
+        return math.prod(self.shape)
+
+    @property
+    def padded_n_pixels(self):
+        return math.prod(self.padded_shape)
+
+
+# ---------------------------------------------------------------------------
+# Poses
+# ---------------------------------------------------------------------------
+
+
+class AbstractPose:
+    offset_in_angstroms: np.ndarray
+
+    def rotation_matrices(self) -> np.ndarray:
+        """(..., 3, 3) float64 matrices R with rotated k = R k."""
+        return rot.quat_to_matrix(self.quaternion())
+
+    def quaternion(self) -> np.ndarray:  # pragma: no cover - abstract
+        raise NotImplementedError
+
+    @property
+    def offset_z_in_angstroms(self):
+        o = self.offset_in_angstroms
+        return None if o.shape[-1] == 2 else o[..., 2]
+
+    @property
+    def batch_size(self):
+        q = self.quaternion()
+        return None if q.ndim == 1 else q.shape[0]
+
+
+def _stack_offsets(x, y, z):
+    arrs = [_arr(x), _arr(y)] + ([] if z is None else [_arr(z)])
+    arrs = np.broadcast_arrays(*arrs)
+    return np.stack(arrs, axis=-1)
+
+
+class EulerAnglePose(AbstractPose):
+    """zyz extrinsic Euler angles in degrees.  cryojax/simulator/_pose.py:203-280."""
+
+    def __init__(self, offset_x_in_angstroms=0.0, offset_y_in_angstroms=0.0, phi_angle=0.0,
+                 theta_angle=0.0, psi_angle=0.0, *, offset_z_in_angstroms=None):
+        self.offset_in_angstroms = _stack_offsets(offset_x_in_angstroms, offset_y_in_angstroms, offset_z_in_angstroms)
+        self.phi_angle = _arr(phi_angle)
+        self.theta_angle = _arr(theta_angle)
+        self.psi_angle = _arr(psi_angle)
+
+    def quaternion(self):
+        return rot.euler_zyz_to_quat(self.phi_angle, self.theta_angle, self.psi_angle)
+
+
+class QuaternionPose(AbstractPose):
+    """Unit quaternion q / |q|.  cryojax/simulator/_pose.py:283-335."""
+
+    def __init__(self, offset_x_in_angstroms=0.0, offset_y_in_angstroms=0.0, wxyz=(1.0, 0.0, 0.0, 0.0), *,
+                 offset_z_in_angstroms=None):
+        self.offset_in_angstroms = _stack_offsets(offset_x_in_angstroms, offset_y_in_angstroms, offset_z_in_angstroms)
+        wxyz = _arr(wxyz)
+        if wxyz.shape[-1] != 4:
+            raise ValueError("Expected `wxyz` to be a sequence of floats with length 4")
+        self.wxyz = wxyz
+
+    def quaternion(self):
+        return rot.quat_normalize(self.wxyz)
+
+
+class AxisAnglePose(AbstractPose):
+    """Euler vector in degrees through the exponential map.  cryojax/simulator/_pose.py:338-403."""
+
+    def __init__(self, offset_x_in_angstroms=0.0, offset_y_in_angstroms=0.0, euler_vector=(0.0, 0.0, 0.0), *,
+                 offset_z_in_angstroms=None):
+        self.offset_in_angstroms = _stack_offsets(offset_x_in_angstroms, offset_y_in_angstroms, offset_z_in_angstroms)
+        ev = _arr(euler_vector)
+        if ev.shape[-1] != 3:
+            raise ValueError("Expected `euler_vector` to be a sequence of floats with length 3")
+        self.euler_vector = ev
+
+    def quaternion(self):
+        return rot.so3_exp(np.deg2rad(self.euler_vector))
+
+
+# ---------------------------------------------------------------------------
+# CTF, envelope, transfer theory
+# ---------------------------------------------------------------------------
+
+
+class AstigmaticCTF:
+    """cryojax/simulator/_transfer_theory/transfer_function.py:84-169."""
+
+    def __init__(self, defocus_in_angstroms=10000.0, astigmatism_in_angstroms=0.0, astigmatism_angle=0.0,
+                 spherical_aberration_in_mm=2.7):
+        if np.any(_arr(spherical_aberration_in_mm) < 0):
+            raise ValueError("`spherical_aberration_in_mm` must be non-negative")
+        self.defocus_in_angstroms = _arr(defocus_in_angstroms)
+        self.astigmatism_in_angstroms = _arr(astigmatism_in_angstroms)
+        self.astigmatism_angle = _arr(astigmatism_angle)
+        self.spherical_aberration_in_mm = _arr(spherical_aberration_in_mm)
+
+
+class FourierGaussian:
+    """amplitude * exp(-b_factor k^2 / 4).  cryojax/ndimage/operators/_fourier_operator.py:183-234."""
+
+    def __init__(self, amplitude=1.0, b_factor=1.0):
+        _require_positive("b_factor", b_factor)
+        self.amplitude = _arr(amplitude)
+        self.b_factor = _arr(b_factor)
+
+
+class ContrastTransferTheory:
+    """cryojax/simulator/_transfer_theory/transfer_theory.py:21-119 (projection branch)."""
+
+    def __init__(self, ctf: AstigmaticCTF, envelope: FourierGaussian | None = None, amplitude_contrast_ratio=0.1,
+                 phase_shift=0.0):
+        ac = _arr(amplitude_contrast_ratio)
+        if np.any(ac < 0) or np.any(ac > 1):
+            raise ValueError("`amplitude_contrast_ratio` must be in [0, 1]")
+        if envelope is not None and not isinstance(envelope, FourierGaussian):
+            raise NotImplementedError("only FourierGaussian envelopes run on the device")
+        self.ctf = ctf
+        self.envelope = envelope
+        self.amplitude_contrast_ratio = ac
+        self.phase_shift = _arr(phase_shift)
+
+
+# ---------------------------------------------------------------------------
+# Volume
+# ---------------------------------------------------------------------------
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class FourierVoxelGridVolume:
+    """Centred full 3-D FFT grid of a padded real volume (complex64, CUDA).
+
+    cryojax/simulator/_volume/representations/voxel_volume.py:40-119.  The
+    kernels read the grid as stored (C-order [z][y][x], zero frequency at
+    index N//2); ``frequency_slice_in_pixels`` is implicit (the rotated plane
+    is generated in the kernel from the pose).
+    """
+
+    def __init__(self, fourier_voxel_grid, rotation=None):
+        torch = _torch()
+        g = fourier_voxel_grid
+        if not isinstance(g, torch.Tensor):
+            g = torch.as_tensor(np.asarray(g))
+        if g.dim() != 3 or len(set(g.shape)) != 1:
+            raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
+        self.fourier_voxel_grid = g
+        self.rotation = rotation  # AbstractPose attached by rotate_to_pose
+
+    @property
+    def shape(self):
+        return tuple(self.fourier_voxel_grid.shape)
+
+    @classmethod
+    def from_real_voxel_grid(cls, real_voxel_grid, *, pad_scale: float = 1.0, pad_mode: str = "constant",
+                             device: str = "cuda", fft_dtype=None):
+        """pad -> ifftshift -> fftn -> fftshift, as the reference (voxel_volume.py:69-119).
+
+        The FFT runs in float64 on ``device`` and the grid is stored as
+        complex64 (one-time volume preparation, not part of the image path).
+        """
+        torch = _torch()
+        if pad_scale < 1.0:
+            raise ValueError("`pad_scale` must be greater than 1.0")
+        if pad_mode != "constant":
+            raise NotImplementedError("only constant padding is implemented")
+        real = real_voxel_grid
+        if not isinstance(real, torch.Tensor):
+            real = torch.as_tensor(np.asarray(real, np.float64))
+        real = real.to(device=device, dtype=fft_dtype or torch.float64)
+        shape = tuple(int(s * pad_scale) for s in real.shape)
+        pads = []
+        for s, d in zip(reversed(shape), reversed(real.shape)):
+            pad = s - d
+            if s % 2 == 1 and d % 2 == 0:
+                lr = (pad // 2, pad // 2 + 1)
+            elif s % 2 == 0 and d % 2 == 1:
+                lr = (pad // 2 + 1, pad // 2)
+            else:
+                lr = (pad // 2, pad // 2)
+            pads.extend(lr)
+        padded = torch.nn.functional.pad(real, pads, mode="constant", value=0.0)
+        ft = torch.fft.fftn(torch.fft.ifftshift(padded))
+        grid = torch.fft.fftshift(ft).to(torch.complex64).contiguous()
+        return cls(grid)
+
+    def rotate_to_pose(self, pose: AbstractPose, inverse: bool = False):
+        """Attach the pose (the frequency slice is rotated inside the kernel)."""
+        if inverse:
+            pose = QuaternionPose(*np.moveaxis(pose.offset_in_angstroms[..., :2], -1, 0),
+                                  wxyz=rot.quat_inverse(pose.quaternion()))
+        return FourierVoxelGridVolume(self.fourier_voxel_grid, rotation=pose)
+
+    def get_representation(self, rng_key=None):
+        return self
+
+
+# ---------------------------------------------------------------------------
+# Parameter packing
+# ---------------------------------------------------------------------------
+
+
+def pack_image_params(pose: AbstractPose, image_config: BasicImageConfig,
+                      transfer_theory: ContrastTransferTheory | None = None, scale=1.0, n: int | None = None):
+    """Build the float64 [n, 32] cjx_image_params records for a batch."""
+    q = pose.quaternion()
+    ctf = transfer_theory.ctf if transfer_theory is not None else None
+    cands = [q if q.ndim > 1 else None, pose.offset_in_angstroms if pose.offset_in_angstroms.ndim > 1 else None,
+             image_config.pixel_size, image_config.voltage_in_kilovolts, scale]
+    if transfer_theory is not None:
+        cands += [ctf.defocus_in_angstroms, ctf.astigmatism_in_angstroms, ctf.astigmatism_angle,
+                  ctf.spherical_aberration_in_mm, transfer_theory.amplitude_contrast_ratio,
+                  transfer_theory.phase_shift]
+        if transfer_theory.envelope is not None:
+            cands += [transfer_theory.envelope.amplitude, transfer_theory.envelope.b_factor]
+    if n is None:
+        n = _batch_size(*cands) or 1
+    p = nat.empty_params(n)
+    R = rot.quat_to_matrix(q)
+    p[:, 0:9] = np.broadcast_to(R.reshape(-1, 9) if R.ndim == 3 else R.reshape(1, 9), (n, 9))
+    off = pose.offset_in_angstroms
+    off = off.reshape(-1, off.shape[-1]) if off.ndim > 1 else off[None]
+    off = np.broadcast_to(off, (n, off.shape[-1]))
+    p[:, nat.P_SHIFT_X] = off[:, 0]
+    p[:, nat.P_SHIFT_Y] = off[:, 1]
+    px = _per_image(image_config.pixel_size, n)
+    kv = _per_image(image_config.voltage_in_kilovolts, n)
+    p[:, nat.P_PIXEL_SIZE] = px
+    p[:, nat.P_WAVELENGTH] = C.wavelength_from_kilovolts(kv)
+    p[:, nat.P_SCALE] = _per_image(scale, n)
+    if transfer_theory is not None:
+        df = _per_image(ctf.defocus_in_angstroms, n)
+        if off.shape[-1] == 3:
+            df = df + off[:, 2]
+        p[:, nat.P_DEFOCUS] = df
+        p[:, nat.P_ASTIG] = _per_image(ctf.astigmatism_in_angstroms, n)
+        p[:, nat.P_ASTIG_ANGLE] = np.deg2rad(_per_image(ctf.astigmatism_angle, n))
+        p[:, nat.P_CS] = _per_image(ctf.spherical_aberration_in_mm, n) * 1e7
+        ac = _per_image(transfer_theory.amplitude_contrast_ratio, n)
+        p[:, nat.P_PHASE_TOTAL] = np.deg2rad(_per_image(transfer_theory.phase_shift, n)) + np.arctan(
+            ac / np.sqrt(1.0 - ac**2))
+        if transfer_theory.envelope is not None:
+            p[:, nat.P_ENV_AMP] = _per_image(transfer_theory.envelope.amplitude, n)
+            p[:, nat.P_ENV_B] = _per_image(transfer_theory.envelope.b_factor, n)
+    return p
+
+
+# ---------------------------------------------------------------------------
+# Integrator
+# ---------------------------------------------------------------------------
+
+
+class FourierSliceExtraction:
+    """Fourier-slice projection of a FourierVoxelGridVolume on the B200.
+
+    cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-146
+    (trilinear grid path; ``correction_mask`` and spline volumes are not
+    implemented).  ``out_of_bounds_mode="fill"`` with ``fill_value`` follows
+    the reference; ``"zero_fill_negative"`` fills negative indices too
+    (not the reference's rule, see CJX_ZERO_FILL_NEGATIVE).
+    """
+
+    is_projection_approximation = True
+
+    def __init__(self, *, outputs_integral: bool = True, correction_mask=None, out_of_bounds_mode: str = "fill",
+                 fill_value: complex = 0.0 + 0.0j):
+        if correction_mask is not None:
+            raise NotImplementedError("correction_mask is not implemented on the device")
+        if out_of_bounds_mode not in ("fill", "zero_fill_negative"):
+            raise NotImplementedError(f"out_of_bounds_mode={out_of_bounds_mode!r}")
+        self.outputs_integral = outputs_integral
+        self.correction_mask = None
+        self.out_of_bounds_mode = out_of_bounds_mode
+        self.fill_value = complex(fill_value)
+
+    def _base_flags(self):
+        return nat.CJX_ZERO_FILL_NEGATIVE if self.out_of_bounds_mode == "zero_fill_negative" else 0
+
+    def run(self, volume: FourierVoxelGridVolume, image_config: BasicImageConfig, params: np.ndarray,
+            flags: int, *, params_device=None, out=None, workspace=None, stream=None, images_per_chunk=0):
+        """Launch the batched kernel; returns a complex64 [n, Py, Px//2+1] CUDA tensor."""
+        torch = _torch()
+        grid = volume.fourier_voxel_grid
+        n_vol = grid.shape[0]
+        if image_config.pad_mode != "constant":
+            raise NotImplementedError("only constant padding is implemented on the device")
+        py, px = image_config.padded_shape
+        desc = nat.make_desc(n_vol, py, px, flags | self._base_flags(), self.fill_value, images_per_chunk)
+        n = params.shape[0]
+        if params_device is None:
+            params_device = torch.as_tensor(params, dtype=torch.float64, device=grid.device)
+        if out is None:
+            out = torch.empty((n, py, px // 2 + 1), dtype=torch.complex64, device=grid.device)
+        ws_bytes = nat.workspace_size(desc, n)
+        if ws_bytes and (workspace is None or workspace.numel() * workspace.element_size() < ws_bytes):
+            workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=grid.device)
+        nat.slice_ctf_forward(desc, grid, params_device, out, workspace if ws_bytes else None, stream)
+        return out
+
+    def integrate(self, volume_representation: FourierVoxelGridVolume, image_config: BasicImageConfig,
+                  outputs_real_space: bool = False):
+        """cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:78-146."""
+        pose = volume_representation.rotation or QuaternionPose()
+        scale = image_config.pixel_size if self.outputs_integral else 1.0
+        params = pack_image_params(pose, image_config, None, scale=scale)
+        out = self.run(volume_representation, image_config, params, 0)
+        if pose.batch_size is None and _batch_size(image_config.pixel_size) is None:
+            out = out[0]
+        if outputs_real_space:
+            from . import _postprocess
+
+            return _postprocess.irfftn(out, image_config.padded_shape)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Scattering theory and image models
+# ---------------------------------------------------------------------------
+
+
+class WeakPhaseScatteringTheory:
+    """cryojax/simulator/_scattering_theory/weak_phase_scattering_theory.py:13-80."""
+
+    def __init__(self, volume_integrator: FourierSliceExtraction, transfer_theory: ContrastTransferTheory,
+                 solvent=None):
+        if solvent is not None:
+            raise NotImplementedError("solvent models are not implemented on the device")
+        self.volume_integrator = volume_integrator
+        self.transfer_theory = transfer_theory
+        self.solvent = None
+
+
+class AbstractImageModel:
+    normalizes_signal: bool = False
+
+    # subclasses set: volume_parametrization, pose, image_config, volume_integrator,
+    # transfer_theory (or None), applies_translation, translate_mode, _quantity
+    def _scale(self):
+        cfg = self.image_config
+        s = cfg.pixel_size if self.volume_integrator.outputs_integral else np.float64(1.0)
+        if self._quantity:
+            s = s * cfg.interaction_constant
+        return s
+
+    def _flags(self):
+        f = 0
+        if self.transfer_theory is not None:
+            f |= nat.CJX_APPLY_CTF
+            if self.transfer_theory.envelope is not None:
+                f |= nat.CJX_APPLY_ENVELOPE
+        if self.applies_translation:
+            if self.translate_mode != "fft":
+                raise ValueError("translate_mode='atom' needs an atom volume, not a FourierVoxelGridVolume")
+            f |= nat.CJX_APPLY_TRANSLATION
+        return f
+
+    def image_params(self) -> np.ndarray:
+        return pack_image_params(self.pose, self.image_config, self.transfer_theory, scale=self._scale())
+
+    @property
+    def batch_size(self):
+        return _batch_size(*[None if p is None else p for p in self._batched_fields()])
+
+    def _batched_fields(self):
+        tt = self.transfer_theory
+        fields = [self.pose.quaternion() if self.pose.quaternion().ndim > 1 else None,
+                  self.pose.offset_in_angstroms if self.pose.offset_in_angstroms.ndim > 1 else None,
+                  self.image_config.pixel_size, self.image_config.voltage_in_kilovolts]
+        if tt is not None:
+            fields += [tt.ctf.defocus_in_angstroms, tt.ctf.astigmatism_in_angstroms, tt.ctf.astigmatism_angle,
+                       tt.ctf.spherical_aberration_in_mm, tt.amplitude_contrast_ratio, tt.phase_shift]
+        return fields
+
+    def get_pose(self):
+        return self.pose
+
+    def get_image_config(self):
+        return self.image_config
+
+    def compute_fourier_image(self, rng_key=None, *, out=None, workspace=None, stream=None, params_device=None):
+        """One launch for the whole batch: rotate -> integrate -> CTF -> translate.
+
+        cryojax/simulator/_image_model/base_image_model.py:297-328.
+        """
+        params = self.image_params()
+        img = self.volume_integrator.run(self.volume_parametrization.get_representation(), self.image_config,
+                                         params, self._flags(), out=out, workspace=workspace, stream=stream,
+                                         params_device=params_device)
+        return img if self.batch_size is not None else img[0]
+
+    def simulate(self, rng_key=None, *, removes_padding: bool = True, outputs_real_space: bool = True, mask=None,
+                 filter=None):
+        """cryojax/simulator/_image_model/base_image_model.py:68-105."""
+        if mask is not None or filter is not None:
+            raise NotImplementedError("masks and filters are not implemented on the device")
+        fourier_image = self.compute_fourier_image(rng_key)
+        from . import _postprocess
+
+        cfg = self.image_config
+        if removes_padding:
+            return _postprocess.postprocess(fourier_image, cfg.shape, cfg.padded_shape,
+                                            outputs_real_space=outputs_real_space,
+                                            normalizes_signal=self.normalizes_signal)
+        return _postprocess.irfftn(fourier_image, cfg.padded_shape) if outputs_real_space else fourier_image
+
+
+class LinearImageModel(AbstractImageModel):
+    """cryojax/simulator/_image_model/base_image_model.py:216-328."""
+
+    def __init__(self, volume_parametrization, pose, image_config, volume_integrator, transfer_theory, *,
+                 applies_translation=True, normalizes_signal=False, signal_region=None, translate_mode="fft"):
+        if signal_region is not None:
+            raise NotImplementedError("signal_region is not implemented on the device")
+        self.volume_parametrization = volume_parametrization
+        self.pose = pose
+        self.image_config = image_config
+        self.volume_integrator = volume_integrator
+        self.transfer_theory = transfer_theory
+        self.applies_translation = applies_translation
+        self.normalizes_signal = normalizes_signal
+        self.translate_mode = translate_mode
+        self._quantity = False
+
+
+class ProjectionImageModel(LinearImageModel):
+    """cryojax/simulator/_image_model/base_image_model.py:331-432 (no transfer theory)."""
+
+    def __init__(self, volume_parametrization, pose, image_config, volume_integrator, *, applies_translation=True,
+                 normalizes_signal=False, signal_region=None, translate_mode="fft"):
+        super().__init__(volume_parametrization, pose, image_config, volume_integrator, None,
+                         applies_translation=applies_translation, normalizes_signal=normalizes_signal,
+                         signal_region=signal_region, translate_mode=translate_mode)
+
+
+class ContrastImageModel(AbstractImageModel):
+    """cryojax/simulator/_image_model/physical_image_model.py:30-137 with WeakPhaseScatteringTheory."""
+
+    def __init__(self, volume_parametrization, pose, image_config, scattering_theory: WeakPhaseScatteringTheory, *,
+                 applies_translation=True, normalizes_signal=False, signal_region=None, translate_mode="fft"):
+        if signal_region is not None:
+            raise NotImplementedError("signal_region is not implemented on the device")
+        self.volume_parametrization = volume_parametrization
+        self.pose = pose
+        self.image_config = image_config
+        self.scattering_theory = scattering_theory
+        self.volume_integrator = scattering_theory.volume_integrator
+        self.transfer_theory = scattering_theory.transfer_theory
+        self.applies_translation = applies_translation
+        self.normalizes_signal = normalizes_signal
+        self.translate_mode = translate_mode
+        self._quantity = True
+
+
+def make_image_model(volume_parametrization, image_config, pose, transfer_theory=None, volume_integrator=None,
+                     detector=None, *, applies_translation=True, normalizes_signal=False, signal_region=None,
+                     simulates_quantity=False, quantity_mode="contrast", translate_mode="fft"):
+    """cryojax/simulator/_api_utils.py:36-223 (FourierVoxelGridVolume routes)."""
+    if not isinstance(volume_parametrization, FourierVoxelGridVolume):
+        raise ValueError(
+            "Could not select default integrator for volume of type "
+            f"{type(volume_parametrization).__name__}: only FourierVoxelGridVolume runs on the device")
+    if volume_integrator is None:
+        volume_integrator = FourierSliceExtraction(outputs_integral=simulates_quantity)
+    kw = dict(applies_translation=applies_translation, normalizes_signal=normalizes_signal,
+              signal_region=signal_region, translate_mode=translate_mode)
+    if transfer_theory is None:
+        return ProjectionImageModel(volume_parametrization, pose, image_config, volume_integrator, **kw)
+    if simulates_quantity:
+        if quantity_mode != "contrast":
+            raise NotImplementedError(f"quantity_mode={quantity_mode!r} is not implemented on the device")
+        theory = WeakPhaseScatteringTheory(volume_integrator, transfer_theory)
+        return ContrastImageModel(volume_parametrization, pose, image_config, theory, **kw)
+    return LinearImageModel(volume_parametrization, pose, image_config, volume_integrator, transfer_theory, **kw)

@@ -1,0 +1,148 @@
+/*
+ * cryojax_b200 — C-ABI of the B200 (sm_100a) Fourier-slice + CTF image path.
+ *
+ * Plain C: pointers, sizes and POD structs only.  Every device pointer is a
+ * CUDA global-memory address on the current device; `stream` is a
+ * cudaStream_t passed as void*.  All work is stream-ordered: no entry point
+ * synchronises the device or allocates device memory unless it says so.
+ * Every entry point returns CJX_OK (0) or a nonzero CJX_ERR_* code;
+ * cjx_get_last_error() returns the calling thread's last message.
+ *
+ * Data conventions follow cryoJAX exactly:
+ *   - volume grid: the full, centred (fftshifted) 3-D FFT of the padded real
+ *     volume, complex64, C-order [z][y][x], side N
+ *     (FourierVoxelGridVolume.fourier_voxel_grid,
+ *      cryojax/simulator/_volume/representations/voxel_volume.py:40-119);
+ *   - image output: rfft half-plane, complex64, C-order [Py][Px/2+1], zero
+ *     frequency in the corner (cryojax/ndimage/_fft.py:80-99 conventions).
+ */
+#ifndef CRYOJAX_B200_H
+#define CRYOJAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CJX_API __attribute__((visibility("default")))
+#else
+#define CJX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CJX_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define CJX_OK 0
+#define CJX_ERR_INVALID_ARGUMENT 1 /* bad shape, null pointer, bad flag  */
+#define CJX_ERR_UNSUPPORTED 2      /* size beyond the compiled limits     */
+#define CJX_ERR_CUDA 3             /* a CUDA runtime call failed          */
+#define CJX_ERR_WORKSPACE 4        /* workspace too small                  */
+
+/* ---- limits ------------------------------------------------------------ */
+#define CJX_MAX_SIDE 1024 /* max volume side N and max image side Py, Px */
+
+/* ---- flags for cjx_slice_desc.flags ----------------------------------- */
+/* multiply by the AstigmaticCTF of ContrastTransferTheory
+ * (cryojax/simulator/_transfer_theory/transfer_theory.py:53-119)          */
+#define CJX_APPLY_CTF (1u << 0)
+/* zero the even-size Nyquist self-conjugates, then multiply by
+ * exp(-2 pi i q.t) (cryojax/simulator/_pose.py:68-114)                    */
+#define CJX_APPLY_TRANSLATION (1u << 1)
+/* multiply by envelope_amplitude * exp(-b/4 k^2) (FourierGaussian,
+ * cryojax/ndimage/operators/_fourier_operator.py:183-234)                 */
+#define CJX_APPLY_ENVELOPE (1u << 2)
+/* out-of-bounds corners with a negative index read the fill value instead
+ * of wrapping to index + N.  NOT the reference's behaviour (JAX's
+ * `.at[].get(mode="fill")` wraps negative indices once); offered for
+ * comparison only.                                                        */
+#define CJX_ZERO_FILL_NEGATIVE (1u << 3)
+
+/* ---- per-image parameters (one record per image, device memory) ------
+ * 32 doubles (256 bytes).  Built on the host from a pose, a CTF and an
+ * image config.                                                            */
+typedef struct cjx_image_params {
+  double rot[9];              /* row-major R; sample point = R (kx, ky, 0)
+                                 (QuaternionPose.rotation applied with
+                                 SO3.apply, cryojax/simulator/_pose.py:29-66) */
+  double shift_x, shift_y;    /* in-plane offset, Angstrom                  */
+  double defocus;             /* mean defocus + out-of-plane offset, A      */
+  double astigmatism;         /* Angstrom                                   */
+  double astigmatism_angle;   /* radians                                    */
+  double spherical_aberration;/* Angstrom (mm * 1e7)                        */
+  double wavelength;          /* Angstrom                                   */
+  double phase_total;         /* radians: deg2rad(phase_shift)
+                                 + atan(ac / sqrt(1 - ac^2))                 */
+  double pixel_size;          /* Angstrom                                   */
+  double scale;               /* prefactor: pixel_size if outputs_integral,
+                                 times the interaction constant for the
+                                 contrast model, else 1                      */
+  double envelope_amplitude;  /* used with CJX_APPLY_ENVELOPE               */
+  double envelope_b_factor;   /* Angstrom^2                                 */
+  double reserved[11];
+} cjx_image_params;
+
+/* ---- geometry of one launch ------------------------------------------- */
+typedef struct cjx_slice_desc {
+  int32_t n;                 /* volume side N (grid is N^3)                 */
+  int32_t py, px;            /* image padded shape (Py, Px)                 */
+  uint32_t flags;            /* CJX_* flags above                           */
+  float fill_re, fill_im;    /* FourierSliceExtraction.fill_value           */
+  int32_t images_per_chunk;  /* resize path: images per workspace chunk;
+                                0 = library default                         */
+  int32_t reserved;
+} cjx_slice_desc;
+
+/* Library ABI version (CJX_ABI_VERSION). */
+CJX_API int cjx_get_version(void);
+
+/* Last error message of the calling thread ("" if none). */
+CJX_API const char* cjx_get_last_error(void);
+
+/* Workspace needed by cjx_slice_ctf_forward for `n_images` images.
+ * Zero when (Py, Px) == (N, N) (no resize stage).  The workspace is
+ * scratch: its contents on entry are ignored.                              */
+CJX_API int cjx_slice_ctf_workspace_size(const cjx_slice_desc* desc, int64_t n_images,
+                                 size_t* bytes);
+
+/* Batched Fourier-slice extraction (+ CTF, envelope, translation).
+ *
+ * For image b: rotate the central slice by params[b].rot, sample `grid`
+ * trilinearly with cryoJAX's out-of-bounds rule, keep the rfft half-plane,
+ * resize to (Py, Px) when (Py, Px) != (N, N) (irfftn -> centre crop or pad
+ * -> rfftn), multiply by params[b].scale, then apply the flagged CTF,
+ * envelope and translation.  Writes out[b][Py][Px/2+1] (complex64).
+ *
+ * Replaces, for a FourierVoxelGridVolume under eqx.filter_vmap:
+ *   flags = CTF|TRANSLATION : LinearImageModel.compute_fourier_image
+ *        (cryojax/simulator/_image_model/base_image_model.py:297-328)
+ *   flags = 0               : volume.rotate_to_pose(pose) then
+ *        FourierSliceExtraction.integrate(..., outputs_real_space=False)
+ *        (cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:78-146)
+ *   flags = TRANSLATION     : ProjectionImageModel.compute_fourier_image
+ *        (cryojax/simulator/_image_model/base_image_model.py:412-432)
+ *
+ * grid:    device, complex64 [N][N][N]
+ * params:  device, n_images records
+ * out:     device, complex64 [n_images][Py][Px/2+1]
+ * workspace: device scratch of at least cjx_slice_ctf_workspace_size bytes
+ *          (may be NULL when that size is 0)                              */
+CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
+                          const cjx_image_params* params, int64_t n_images,
+                          void* out, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
+/* Measurement helper: streams `bytes` of `buf` `passes` times through the
+ * SMs (read-only, 16-byte vector loads, result folded into `sink`).  With a
+ * buffer smaller than L2 this measures L2 read bandwidth; larger, HBM.
+ * No counterpart in the reference (roofline denominator).                  */
+CJX_API int cjx_probe_read_bandwidth(const void* buf, size_t bytes, int passes,
+                             void* sink, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRYOJAX_B200_H */

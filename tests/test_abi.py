@@ -1,0 +1,67 @@
+"""The C-ABI library loads and exports every symbol include/cryojax_b200.h declares.
+
+No compute calls here (no GPU needed): argument validation paths only.
+"""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from cryojax_b200 import _native as nat
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "cryojax_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"CJX_API\s+[\w\s\*]+?\b(cjx_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "cjx_slice_ctf_forward" in syms and "cjx_get_version" in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = nat.load_library()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert set(declared_symbols()) == set(nat.exported_symbols())
+
+
+def test_version():
+    assert nat.load_library().cjx_get_version() == 1
+
+
+def test_struct_sizes_match_header():
+    assert ctypes.sizeof(nat.SliceDesc) == 32
+    assert nat.PARAMS_DOUBLES * 8 == 256
+
+
+def test_workspace_size_and_validation():
+    d = nat.make_desc(64, 32, 32, nat.CJX_APPLY_CTF | nat.CJX_APPLY_TRANSLATION)
+    ws = nat.workspace_size(d, 10)
+    # per image: Py * round8(N/2+1) + Py * round8(Px/2+1) complex64
+    assert ws == 10 * 8 * (32 * 40 + 32 * 24)
+    assert nat.workspace_size(nat.make_desc(64, 64, 64, 0), 10) == 0  # no resize stage
+    with pytest.raises(nat.CryojaxB200Error) as e:
+        nat.workspace_size(nat.make_desc(1, 32, 32, 0), 1)
+    assert e.value.code == nat.CJX_ERR_INVALID_ARGUMENT
+    with pytest.raises(nat.CryojaxB200Error) as e:
+        nat.workspace_size(nat.make_desc(2048, 32, 32, 0), 1)
+    assert e.value.code == nat.CJX_ERR_UNSUPPORTED
+    with pytest.raises(nat.CryojaxB200Error) as e:
+        nat.workspace_size(nat.make_desc(64, 32, 32, 1 << 20), 1)
+    assert "flag" in str(e.value)
+
+
+def test_forward_rejects_null_pointers_without_touching_the_gpu():
+    lib = nat.load_library()
+    d = nat.make_desc(64, 32, 32, 0)
+    rc = lib.cjx_slice_ctf_forward(ctypes.byref(d), None, None, 4, None, None, 0, None)
+    assert rc == nat.CJX_ERR_INVALID_ARGUMENT
+    assert b"non-NULL" in lib.cjx_get_last_error()
+    # zero images is a no-op
+    assert lib.cjx_slice_ctf_forward(ctypes.byref(d), None, None, 0, None, None, 0, None) == nat.CJX_OK

@@ -1,0 +1,144 @@
+"""GPU parity: cjx_slice_ctf_forward (through the C-ABI) against the float64 oracle.
+
+Tolerance: relative L2 error per image <= 1e-5 (helpers.IMAGE_REL_L2_TOL).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cryojax_oracle as O
+from tests.helpers import IMAGE_REL_L2_TOL, make_volume, random_specs, rel_l2_per_image, specs_to_model_args
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_volume(grid):
+    import torch
+
+    from cryojax_b200 import simulator as S
+
+    return S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+
+
+def _run_model(grid, specs, *, transfer=True, translate=True, quantity=False, integrator_kw=None, chunk=0):
+    from cryojax_b200 import simulator as S
+
+    pose, tt, cfg = specs_to_model_args(specs)
+    vol = _device_volume(grid)
+    integ = S.FourierSliceExtraction(outputs_integral=quantity, **(integrator_kw or {}))
+    model = S.make_image_model(vol, cfg, pose, tt if transfer else None, volume_integrator=integ,
+                               applies_translation=translate, simulates_quantity=quantity)
+    params = model.image_params()
+    out = integ.run(vol, cfg, params, model._flags(), images_per_chunk=chunk)
+    return out.cpu().numpy()
+
+
+def _oracle(grid, fs, specs, **kw):
+    return np.stack([O.compute_fourier_image(grid, fs, s, **kw) for s in specs])
+
+
+CASES = [
+    # (box, pad_scale, shape, padded_shape)  -- N = int(box * pad_scale)
+    (32, 2.0, (32, 32), None),     # crop 64 -> 32 (the configs' resize)
+    (32, 2.0, (64, 64), None),     # no resize: fused direct kernel
+    (32, 2.0, (40, 24), None),     # non-square crop
+    (32, 2.0, (70, 66), None),     # pad 64 -> 70 x 66
+    (32, 2.0, (80, 48), None),     # pad y, crop x
+    (31, 2.0, (31, 31), None),     # N = 62 (even), odd image
+    (25, 1.0, (25, 25), None),     # odd N = 25, no resize
+    (32, 1.3, (41, 41), None),     # prime N = 41: direct-DFT fallback, no resize
+    (32, 1.3, (30, 30), (44, 42)), # prime N with pad and padded_shape != shape
+    (48, 2.0, (48, 48), None),     # N = 96 = 2^5 * 3
+    (40, 2.0, (40, 40), None),     # N = 80 = 2^4 * 5, image 40 = 2^3 * 5
+]
+
+
+@pytest.mark.parametrize("box,pad_scale,shape,padded", CASES)
+def test_linear_image_model_matches_oracle(cuda_device, box, pad_scale, shape, padded):
+    vol, grid, fs = make_volume(box, 60, seed=box, pad_scale=pad_scale)
+    specs = random_specs(6, seed=7 * box, shape=shape, padded_shape=padded)
+    got = _run_model(grid, specs)
+    ref = _oracle(grid, fs, specs)
+    errs = rel_l2_per_image(got, ref)
+    assert max(errs) <= IMAGE_REL_L2_TOL, errs
+
+
+@pytest.mark.parametrize("shape", [(32, 32), (64, 64)])
+def test_integrate_only_matches_oracle(cuda_device, shape):
+    """FourierSliceExtraction.integrate (no CTF, no translation), outputs_integral=True."""
+    from cryojax_b200 import simulator as S
+
+    vol, grid, fs = make_volume(32, 80, seed=3)
+    specs = random_specs(4, seed=11, shape=shape)
+    pose, _, cfg = specs_to_model_args(specs)
+    dvol = _device_volume(grid).rotate_to_pose(pose)
+    got = S.FourierSliceExtraction(outputs_integral=True).integrate(dvol, cfg).cpu().numpy()
+    ref = np.stack([
+        O.fourier_slice_integrate(grid, O.rotate_frequency_slice(fs, O.quat_normalize(s.wxyz)), s.padded_shape,
+                                  s.pixel_size, outputs_integral=True)
+        for s in specs])
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+@pytest.mark.parametrize("shape", [(32, 32), (64, 64)])
+def test_envelope_offset_z_and_contrast_model(cuda_device, shape):
+    vol, grid, fs = make_volume(32, 60, seed=5)
+    specs = random_specs(5, seed=13, shape=shape, offset_z=True, envelope=True)
+    got = _run_model(grid, specs, quantity=True)
+    ref = _oracle(grid, fs, specs, outputs_integral=True, simulates_quantity=True)
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+@pytest.mark.parametrize("shape", [(32, 32), (64, 64)])
+def test_projection_model_and_fill_value(cuda_device, shape):
+    vol, grid, fs = make_volume(32, 60, seed=9)
+    specs = random_specs(4, seed=17, shape=shape)
+    fill = 0.25 - 0.5j
+    got = _run_model(grid, specs, transfer=False, integrator_kw=dict(fill_value=fill))
+    ref = _oracle(grid, fs, specs, apply_ctf=False, cval=fill)
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+def test_out_of_bounds_rules(cuda_device):
+    """Default: negative corner indices wrap (the reference's rule); optional pure zero fill."""
+    # sharp Gaussians put spectrum into the plane corners that leave the cube
+    vol, grid, fs = make_volume(32, 60, seed=21, sigma_range=(0.4, 0.7))
+    specs = random_specs(4, seed=23, shape=(32, 32))
+    ref_wrap = _oracle(grid, fs, specs)
+    ref_zero = _oracle(grid, fs, specs, wrap_negative=False)
+    assert max(rel_l2_per_image(ref_wrap, ref_zero)) > 1e-3  # the two rules really differ here
+    got_zero = _run_model(grid, specs, integrator_kw=dict(out_of_bounds_mode="zero_fill_negative"))
+    assert max(rel_l2_per_image(got_zero, ref_zero)) <= IMAGE_REL_L2_TOL
+    got_wrap = _run_model(grid, specs)
+    assert max(rel_l2_per_image(got_wrap, ref_wrap)) <= IMAGE_REL_L2_TOL
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 0])
+def test_chunking_is_invisible(cuda_device, chunk):
+    vol, grid, fs = make_volume(32, 60, seed=31)
+    specs = random_specs(7, seed=37, shape=(32, 32))
+    got = _run_model(grid, specs, chunk=chunk)
+    ref = _oracle(grid, fs, specs)
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+def test_simulate_real_space_matches_oracle(cuda_device):
+    from cryojax_b200 import simulator as S
+
+    vol, grid, fs = make_volume(32, 60, seed=41)
+    specs = random_specs(3, seed=43, shape=(28, 28), padded_shape=(32, 32))
+    pose, tt, cfg = specs_to_model_args(specs)
+    model = S.make_image_model(_device_volume(grid), cfg, pose, tt)
+    got = model.simulate().cpu().numpy()
+    ref = np.stack([O.simulate(grid, fs, s) for s in specs])
+    assert got.shape == (3, 28, 28)
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+def test_from_real_voxel_grid_matches_oracle(cuda_device):
+    from cryojax_b200 import simulator as S
+
+    vol, grid, fs = make_volume(20, 30, seed=51, pad_scale=1.3)
+    dvol = S.FourierVoxelGridVolume.from_real_voxel_grid(vol, pad_scale=1.3)
+    assert dvol.shape == grid.shape
+    assert O.relative_l2(dvol.fourier_voxel_grid.cpu().numpy(), grid) < 1e-6

@@ -1,0 +1,113 @@
+"""Pins of the float64 oracle against the reference's own known answers.
+
+The reference stores no golden arrays for this path; its hot-path tests
+check mathematical known answers, restated here on the oracle:
+  - Euler zyz matrices vs the closed form (tests/test_agree_with_cistem.py:88-116)
+  - identity-pose Fourier slice == FFT of the direct projection (the
+    Fourier-slice theorem behind tests/test_volume_integrators.py:188-251)
+  - even/odd image shapes agree after cropping (tests/test_image_model.py:84-105)
+  - pose parametrisations agree (tests/test_pose.py:11-86)
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cryojax_oracle as O
+
+
+@pytest.mark.parametrize(
+    "phi, theta, psi",
+    [(10.0, 90.0, 170.0), (10.0, 80.0, -20.0), (-1.2, 90.5, 67.0), (-50.0, 62.0, -21.0)],
+)
+def test_euler_matrix_closed_form(phi, theta, psi):
+    p, t, s = np.deg2rad([phi, theta, psi])
+    cp, sp, ct, st, cs, ss = np.cos(p), np.sin(p), np.cos(t), np.sin(t), np.cos(s), np.sin(s)
+    m = np.array(
+        [
+            [cp * ct * cs - sp * ss, sp * ct * cs + cp * ss, -st * cs],
+            [-cp * ct * ss - sp * cs, -sp * ct * ss + cp * cs, st * ss],
+            [st * cp, st * sp, ct],
+        ]
+    )
+    q = O.euler_pose_quaternion(-phi, -theta, -psi)
+    np.testing.assert_allclose(O.quat_as_matrix(q), m, atol=1e-12)
+
+
+@pytest.mark.parametrize("box,pad_scale", [(32, 1.0), (31, 1.0), (16, 2.0), (15, 2.0)])
+def test_fourier_slice_theorem_identity_pose(box, pad_scale):
+    vol = O.gaussian_sum_volume(box, 40, seed=box, sigma_range=(1.0, 2.5))
+    grid, fs = O.fourier_voxel_grid_from_real_voxel_grid(vol, pad_scale=pad_scale)
+    n = grid.shape[0]
+    sl = O.extract_slice(grid, O.rotate_frequency_slice(fs, np.array([1.0, 0.0, 0.0, 0.0])))
+    proj = O.pad_to_shape(vol, (n, n, n)).sum(axis=0)
+    ref = O.rfftn(proj)
+    np.testing.assert_allclose(sl, ref, atol=1e-12 * np.abs(ref).max())
+
+
+def test_slice_theorem_with_integral_and_resize():
+    """integrate() at identity pose with a crop equals rfftn(crop(projection)) * pixel_size."""
+    vol = O.gaussian_sum_volume(24, 40, seed=4, sigma_range=(1.0, 2.0))
+    grid, fs = O.fourier_voxel_grid_from_real_voxel_grid(vol, pad_scale=2.0)
+    n = grid.shape[0]
+    out = O.fourier_slice_integrate(grid, fs, (24, 24), 2.0, outputs_integral=True)
+    proj = O.pad_to_shape(vol, (n, n, n)).sum(axis=0)
+    ref = O.rfftn(O.crop_to_shape(proj, (24, 24))) * 2.0
+    np.testing.assert_allclose(out, ref, atol=1e-11 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("extra_y, extra_x", [(1, 1), (1, 0), (0, 1)])
+def test_even_vs_odd_image_shape(extra_y, extra_x):
+    # a compact volume in the box centre (the reference uses a small-molecule
+    # potential); tolerance: 5e-4 of the image maximum (the reference's
+    # atol=1e-4 on its fixture's image scale)
+    vol = O.gaussian_sum_volume(32, 60, seed=1, sigma_range=(2.0, 3.0), centre_region=(10, 22))
+    grid, fs = O.fourier_voxel_grid_from_real_voxel_grid(vol, pad_scale=1.3)
+    n = grid.shape[0]
+    control = (n, n)
+    test = (n + extra_y, n + extra_x)
+    sc = O.ImageSpec(shape=control, pixel_size=4.4)
+    st = O.ImageSpec(shape=test, pixel_size=4.4)
+    a = O.simulate(grid, fs, st)
+    b = O.simulate(grid, fs, sc)
+    np.testing.assert_allclose(O.crop_to_shape(a, control), b, atol=5e-4 * np.abs(b).max())
+
+
+def test_pose_parametrisations_agree():
+    wxyz = O.quat_normalize(np.array([1.0, 2.0, 3.0, 0.5]))
+    r = O.quat_as_matrix(wxyz)
+    # quaternion -> zyz Euler (cryojax/rotations/_utils.py:5-54 convention) -> back
+    e = np.array([0.0, 0.0, 0.0])
+    # solve the Euler angles from the matrix of an extrinsic zyz rotation R = Rz(psi) Ry(theta) Rz(phi)
+    theta = np.arccos(np.clip(r[2, 2], -1, 1))
+    phi = np.arctan2(r[2, 1], -r[2, 0])
+    psi = np.arctan2(r[1, 2], r[0, 2])
+    e = np.rad2deg([phi, theta, psi])
+    np.testing.assert_allclose(O.quat_as_matrix(O.euler_pose_quaternion(*e)), r, atol=1e-12)
+    # axis-angle: log map of the quaternion
+    ang = 2 * np.arctan2(np.linalg.norm(wxyz[1:]), wxyz[0])
+    ev = np.rad2deg(ang * wxyz[1:] / np.linalg.norm(wxyz[1:]))
+    np.testing.assert_allclose(O.quat_as_matrix(O.axis_angle_pose_quaternion(ev)), r, atol=1e-12)
+
+
+def test_quaternion_apply_equals_matrix():
+    rng = np.random.default_rng(0)
+    q = O.quat_normalize(rng.standard_normal(4))
+    v = rng.standard_normal((5, 7, 3))
+    np.testing.assert_allclose(O.quat_apply(q, v), v @ O.quat_as_matrix(q).T, atol=1e-14)
+
+
+def test_ctf_known_values():
+    """CTF at k = 0 is -sin(phase_total); wavelength at 300 kV is 0.019687 A."""
+    np.testing.assert_allclose(O.wavelength_from_kilovolts(300.0), 0.019687, atol=1e-6)
+    freqs = O.padded_frequency_grid_in_angstroms((8, 8), 1.0)
+    ctf = O.astigmatic_ctf(freqs, 300.0, amplitude_contrast_ratio=0.1, phase_shift=0.0)
+    np.testing.assert_allclose(ctf[0, 0], -np.sin(np.arctan(0.1 / np.sqrt(0.99))), atol=1e-15)
+
+
+def test_map_coordinates_out_of_bounds_rule():
+    """Negative indices wrap once (JAX default); indices >= n read the fill value."""
+    g = np.arange(4.0)
+    assert O.map_coordinates_linear(g, (np.array([-1.0]),))[0] == pytest.approx(3.0)
+    assert O.map_coordinates_linear(g, (np.array([3.5]),), cval=10.0)[0] == pytest.approx(0.5 * 3 + 0.5 * 10)
+    assert O.map_coordinates_linear(g, (np.array([-0.5]),), wrap_negative=False)[0] == pytest.approx(0.0)
+    assert O.map_coordinates_linear(g, (np.array([-0.5]),))[0] == pytest.approx(0.5 * 3 + 0.5 * 0)
