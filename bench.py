@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Benchmark: batched Fourier-slice + CTF image simulation on B200.
+
+Workload (default): a 256^3 Gaussian-sum volume (6000 Gaussians, sigma 1-3
+voxels, seeded) prepared as a FourierVoxelGridVolume with pad factor 2
+(N = 512, complex64, 1.07 GB), and 16384 images of 320 x 320 at 2 A / 300 kV,
+each with its own uniform SO(3) pose, +-20 A offsets and AstigmaticCTF
+(defocus U(5000, 25000) A, astigmatism U(0, 500) A, angle U(0, 180) deg).
+One step = simulate the whole batch (rfft half-plane output, complex64
+[16384, 320, 161]) through one cjx_slice_ctf_forward call.  Inputs (volume,
+per-image parameters) are resident in HBM; the volume (1.07 GB) and the
+output (6.75 GB) both exceed L2, so no flush is needed between steps.
+
+Under torchrun each rank simulates its own 16384 images from its own
+replica of the volume (images shard with no collective: weak scaling).
+
+``--impl reference`` times the reference path's CPU restatement (the
+float64 NumPy oracle; JAX is not installed, so the reference itself cannot
+run) on all host cores, on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "slice+CTF images/s at 320^2 (256^3 volume, pad 2)"
+UNIT = "images/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--images", type=int, default=16384)
+    ap.add_argument("--box", type=int, default=256)
+    ap.add_argument("--gaussians", type=int, default=6000)
+    ap.add_argument("--image", type=int, default=320)
+    ap.add_argument("--pad-scale", type=float, default=2.0)
+    ap.add_argument("--chunk", type=int, default=0, help="images per workspace chunk (0 = library default)")
+    ap.add_argument("--cpu-sample", type=int, default=6, help="images in the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--seed", type=int, default=2024)
+    return ap.parse_args()
+
+
+def config_dict(args, world):
+    n = int(args.box * args.pad_scale)
+    return {
+        "workload": f"{args.images} images {args.image}x{args.image} from a {args.box}^3 volume "
+                    f"(N={n} padded grid), per-image pose+CTF, rfft output",
+        "volume_box": args.box, "padded_volume_side": n, "gaussians": args.gaussians,
+        "image_shape": [args.image, args.image], "images_per_gpu": args.images,
+        "global_batch": args.images * world, "pixel_size_A": 2.0, "voltage_kV": 300.0,
+        "l2_flush": "not needed: volume (1.07 GB) and output (6.75 GB per step) exceed the 126 MB L2",
+        "parallelism": f"replicas x{world} (images sharded, no collective)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu_index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the float64 oracle on host cores
+# ---------------------------------------------------------------------------
+def _cpu_worker(args_tuple):
+    path, specs = args_tuple
+    import numpy as np
+
+    from oracle import cryojax_oracle as O
+
+    grid = np.load(path, mmap_mode="r")
+    fs = O.make_frequency_slice((grid.shape[0], grid.shape[0]), outputs_rfftfreqs=False)
+    t0 = time.perf_counter()
+    for s in specs:
+        O.compute_fourier_image(grid, fs, s)
+    return len(specs), time.perf_counter() - t0
+
+
+def cpu_oracle_throughput(grid_c128, batch, n_images, image, pixel_size, voltage, workers):
+    """images/s of the float64 oracle over `n_images` images.
+
+    workers == 1: in this process.  workers > 1: a spawn pool whose workers
+    map the grid read-only from a temporary .npy file (shared page cache).
+    Throughput = images / the slowest worker's busy time.
+    """
+    from oracle import cryojax_oracle as O
+
+    specs = []
+    for b in range(n_images):
+        specs.append(O.ImageSpec(shape=(image, image), pixel_size=pixel_size, voltage_in_kilovolts=voltage,
+                                 wxyz=batch.wxyz[b], offset_in_angstroms=batch.offsets[b],
+                                 defocus_in_angstroms=batch.defocus[b], astigmatism_in_angstroms=batch.astigmatism[b],
+                                 astigmatism_angle=batch.astigmatism_angle[b]))
+    t0 = time.perf_counter()
+    if workers == 1:
+        fs = O.make_frequency_slice((grid_c128.shape[0], grid_c128.shape[0]), outputs_rfftfreqs=False)
+        t1 = time.perf_counter()
+        for s in specs:
+            O.compute_fourier_image(grid_c128, fs, s)
+        busy = time.perf_counter() - t1
+        return len(specs) / busy, len(specs), time.perf_counter() - t0
+    import multiprocessing as mp
+
+    import numpy as np
+
+    fd, path = tempfile.mkstemp(suffix=".npy")
+    os.close(fd)
+    try:
+        np.save(path, grid_c128)
+        per = [p for p in (specs[i::workers] for i in range(workers)) if p]
+        with mp.get_context("spawn").Pool(len(per)) as pool:
+            res = pool.map(_cpu_worker, [(path, p) for p in per])
+    finally:
+        os.unlink(path)
+    done = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return done / busy, done, time.perf_counter() - t0
+
+
+def run_reference(args):
+    """Reference arm: the oracle port on all host cores, same config/metric."""
+    import numpy as np
+
+    from cryojax_b200 import synthetic
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    vol = synthetic.gaussian_sum_volume(args.box, args.gaussians, args.seed, sigma_range=(1.0, 3.0))
+    n = int(args.box * args.pad_scale)
+    from oracle import cryojax_oracle as O
+
+    grid, _ = O.fourier_voxel_grid_from_real_voxel_grid(vol, pad_scale=args.pad_scale)
+    batch = synthetic.image_batch(args.images, args.seed + 1)
+    workers = max(1, len(os.sched_getaffinity(0)))
+    sample = max(workers, args.cpu_sample)
+    vals = []
+    t_all = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        v, done, _ = cpu_oracle_throughput(grid, batch, sample, args.image, 2.0, 300.0, workers)
+        vals.append(v)
+    wall = time.perf_counter() - t_all
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * args.images / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args, 1),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                         "sample": f"{sample} images per step of the same workload (N={n}, {args.image}^2), float64 NumPy "
+                                   f"oracle of the reference path, {workers} spawn workers; JAX is not installed so "
+                                   f"the reference itself cannot run"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def algorithmic_bytes_per_image(kernel, n, py, px):
+    """Bytes one image moves through a kernel at the algorithmic level.
+
+    k_gather_colifft: 8 corner loads of 8 B per slice sample over the
+      N x (N/2+1) half-plane, plus the Py x (N/2+1) complex window written.
+    k_rows_c2r_r2c:  read Py x (N/2+1), write Py x (Px/2+1) complex.
+    k_colfft_epilogue: read Py x (Px/2+1), write Py x (Px/2+1) complex.
+    k_slice_direct:  8 corner loads + one store per output pixel.
+    """
+    nxh, pxh = n // 2 + 1, px // 2 + 1
+    if kernel == "k_gather_colifft":
+        return 64 * n * nxh + 8 * py * nxh
+    if kernel == "k_rows_c2r_r2c":
+        return 8 * py * nxh + 8 * py * pxh
+    if kernel == "k_colfft_epilogue":
+        return 16 * py * pxh
+    if kernel == "k_slice_direct":
+        return 72 * n * nxh
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per image of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        d = json.load(open(path))
+        return d.get(kernel, {}).get("dram_bytes_per_image")
+    except Exception:
+        return None
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+    from cryojax_b200 import synthetic
+    from cryojax_b200.pipeline import HostStreamingSimulator
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nat.load_library()
+
+    # ---- inputs (seeded; one volume replica per rank, own images per rank)
+    vol_np = synthetic.gaussian_sum_volume(args.box, args.gaussians, args.seed, sigma_range=(1.0, 3.0))
+    volume = S.FourierVoxelGridVolume.from_real_voxel_grid(vol_np, pad_scale=args.pad_scale, device=str(dev))
+    n = volume.shape[0]
+    batch = synthetic.image_batch(args.images, args.seed + 1 + 1000 * rank)
+    pose = S.QuaternionPose(batch.offsets[:, 0], batch.offsets[:, 1], wxyz=batch.wxyz)
+    tt = S.ContrastTransferTheory(S.AstigmaticCTF(batch.defocus, batch.astigmatism, batch.astigmatism_angle))
+    cfg = S.BasicImageConfig((args.image, args.image), 2.0, 300.0)
+    model = S.make_image_model(volume, cfg, pose, tt)
+    params_h = model.image_params()
+    params_d = torch.as_tensor(params_h, device=dev)
+    flags = model._flags()
+    integ = model.volume_integrator
+    py, px = cfg.padded_shape
+    out = torch.empty((args.images, py, px // 2 + 1), dtype=torch.complex64, device=dev)
+    desc = nat.make_desc(n, py, px, flags, integ.fill_value, args.chunk)
+    ws_bytes = nat.workspace_size(desc, args.images)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        integ.run(volume, cfg, None, flags, params_device=params_d, out=out, workspace=ws, stream=stream,
+                  images_per_chunk=args.chunk)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- device-timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    t_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    value = args.images * world * args.steps / (t_ms / 1000.0)
+
+    # ---- per-kernel timing (one extra profiled step, not part of `value`)
+    nat.profile_enable(True)
+    step()
+    torch.cuda.synchronize()
+    prof = nat.profile_read()
+    nat.profile_enable(False)
+    launches_per_step = sum(c for c, _ in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    top_name, (top_count, top_ms) = top
+    images_per_launch = args.images / top_count
+    alg = algorithmic_bytes_per_image(top_name, n, py, px)
+    achieved = alg * images_per_launch / (top_ms / top_count / 1000.0) / 1e9
+    hbm_peak, peak_kind = measured_peaks()
+    trf = ncu_traffic(top_name)
+
+    # ---- L2 read bandwidth probe (roofline denominator for the gather)
+    l2 = None
+    try:
+        buf = torch.empty(48 << 20, dtype=torch.uint8, device=dev)
+        sink = torch.zeros(4, dtype=torch.float32, device=dev)
+        nat.probe_read_bandwidth(buf, 2, sink)
+        torch.cuda.synchronize()
+        nat.profile_enable(True)
+        nat.probe_read_bandwidth(buf, 50, sink)
+        torch.cuda.synchronize()
+        pr = nat.profile_read()
+        nat.profile_enable(False)
+        l2_gbs = buf.numel() * 50 / (pr["k_read_probe"][1] / 1000.0) / 1e9
+        gather = prof.get("k_gather_colifft") or prof.get("k_slice_direct")
+        gname = "k_gather_colifft" if "k_gather_colifft" in prof else "k_slice_direct"
+        g_alg = algorithmic_bytes_per_image(gname, n, py, px) * args.images / (gather[1] / 1000.0) / 1e9
+        l2 = {"kernel": gname, "achieved": g_alg, "peak": l2_gbs, "unit": "GB/s", "frac": g_alg / l2_gbs,
+              "peak_source": "k_read_probe, 48 MB buffer x 50 passes (measured in this run)"}
+        del buf
+    except Exception as e:  # measurement helper only
+        l2 = {"error": str(e)}
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        sim = HostStreamingSimulator(volume, cfg, integ, flags, sub_batch=2048, images_per_chunk=args.chunk)
+        ph = sim.pinned_params(params_h)
+        oh = sim.pinned_output(args.images)
+        for _ in range(2):
+            sim.run(ph, oh)
+        torch.cuda.synchronize()
+        barrier()
+        e_steps = max(2, min(args.steps, 5))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            sim.run(ph, oh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        et = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": args.images * world * e_steps / (float(et.item()) / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int(ph.numel() * ph.element_size()),
+               "d2h_bytes_per_step": int(oh.numel() * oh.element_size()),
+               "path": "HostStreamingSimulator: pinned host params -> H2D -> cjx_slice_ctf_forward -> D2H "
+                       "into pinned host images, 2 streams, 2048-image sub-batches"}
+        del oh, ph, sim
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            grid_host = volume.fourier_voxel_grid.cpu().numpy().astype(np.complex128)
+            v, done, wall = cpu_oracle_throughput(grid_host, batch, args.cpu_sample, args.image, 2.0, 300.0, 1)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"{done} images of this workload through the float64 NumPy oracle of the reference "
+                             f"path, 1 process ({wall:.1f} s)"}
+            del grid_host
+        except Exception as e:
+            cpu = {"error": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian-sum volume and poses)",
+            "config": config_dict(args, world),
+            "roofline": {"bound": "hbm", "kernel": top_name, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": (trf * images_per_launch if trf else None),
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg * images_per_launch,
+                         "avg_launch_ms": top_ms / top_count, "launches_per_step": top_count},
+            "l2": l2,
+            "kernels_per_step": {k: {"launches": c, "ms": ms} for k, (c, ms) in prof.items()},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -92,6 +92,17 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "cjx_profile_enable": (ctypes.c_int, [ctypes.c_int]),
+    "cjx_profile_read": (
+        ctypes.c_int,
+        [
+            ctypes.c_char_p,
+            ctypes.POINTER(ctypes.c_int64),
+            ctypes.POINTER(ctypes.c_double),
+            ctypes.c_int,
+            ctypes.POINTER(ctypes.c_int),
+        ],
+    ),
 }
 
 _lib = None
@@ -200,6 +211,24 @@ def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:
             _stream_ptr(stream),
         )
     )
+
+
+def profile_enable(on: bool) -> None:
+    _check(load_library().cjx_profile_enable(1 if on else 0))
+
+
+def profile_read(max_kernels: int = 32) -> dict:
+    """{kernel name: (launches, total ms)} recorded since the last read."""
+    names = ctypes.create_string_buffer(32 * max_kernels)
+    counts = (ctypes.c_int64 * max_kernels)()
+    ms = (ctypes.c_double * max_kernels)()
+    n = ctypes.c_int(0)
+    _check(load_library().cjx_profile_read(names, counts, ms, max_kernels, ctypes.byref(n)))
+    out = {}
+    for i in range(n.value):
+        name = names.raw[32 * i: 32 * (i + 1)].split(b"\0", 1)[0].decode()
+        out[name] = (int(counts[i]), float(ms[i]))
+    return out
 
 
 def empty_params(n_images: int) -> np.ndarray:

@@ -19,6 +19,7 @@
 #include <mutex>
 
 #include "cjx_common.cuh"
+#include "cjx_profile.cuh"
 
 namespace cjx {
 
@@ -289,7 +290,9 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     const int blocks = std::min((total + 255) / 256, 1024);
     for (int64_t i0 = 0; i0 < n_images; i0 += 65535) {
       const int cnt = (int)std::min<int64_t>(65535, n_images - i0);
+      prof_begin(stream);
       k_slice_direct<<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params + i0, out + (size_t)i0 * total, g);
+      prof_end("k_slice_direct", stream);
     }
     return check_cuda(cudaGetLastError(), "k_slice_direct launch");
   }
@@ -302,11 +305,17 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   for (int64_t i0 = 0; i0 < n_images; i0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - i0);
+    prof_begin(stream);
     k_gather_colifft<<<dim3((g.nxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sa, stream>>>(grid, params, t1, g,
                                                                                              i0);
+    prof_end("k_gather_colifft", stream);
+    prof_begin(stream);
     k_rows_c2r_r2c<<<dim3((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, sb, stream>>>(t1, t2, g);
+    prof_end("k_rows_c2r_r2c", stream);
+    prof_begin(stream);
     k_colfft_epilogue<<<dim3((g.pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sc, stream>>>(t2, params, out, g,
                                                                                              i0, norm);
+    prof_end("k_colfft_epilogue", stream);
   }
   return check_cuda(cudaGetLastError(), "forward launch");
 }
@@ -329,8 +338,10 @@ int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cud
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  prof_begin(stream);
   k_read_probe<<<sms * 4, 512, 0, stream>>>(static_cast<const float4*>(buf), bytes / 16, passes,
                                             static_cast<float*>(sink));
+  prof_end("k_read_probe", stream);
   return check_cuda(cudaGetLastError(), "k_read_probe launch");
 }
 

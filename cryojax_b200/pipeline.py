@@ -1,0 +1,73 @@
+"""Host-resident batches: simulate images whose parameters and outputs live in
+pinned host memory, overlapping host->device copies, the slice + CTF
+launches and device->host copies on two CUDA streams.
+
+This is the end-to-end form of a batched ``simulate`` call when the caller
+holds its poses and CTF parameters on the host and wants the image stack
+back on the host.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native as nat
+
+
+class HostStreamingSimulator:
+    """Two-stream pipeline over sub-batches of ``sub_batch`` images."""
+
+    def __init__(self, volume, image_config, integrator, flags, *, sub_batch=2048, images_per_chunk=0):
+        import torch
+
+        self.torch = torch
+        self.volume = volume
+        self.cfg = image_config
+        self.integrator = integrator
+        self.flags = flags
+        self.sub_batch = int(sub_batch)
+        self.chunk = images_per_chunk
+        dev = volume.fourier_voxel_grid.device
+        py, px = image_config.padded_shape
+        self.out_shape = (py, px // 2 + 1)
+        self.streams = [torch.cuda.Stream(device=dev) for _ in range(2)]
+        self.params_d = [torch.empty((self.sub_batch, nat.PARAMS_DOUBLES), dtype=torch.float64, device=dev)
+                         for _ in range(2)]
+        self.out_d = [torch.empty((self.sub_batch,) + self.out_shape, dtype=torch.complex64, device=dev)
+                      for _ in range(2)]
+        desc = nat.make_desc(volume.shape[0], py, px, flags, integrator.fill_value, images_per_chunk)
+        ws = nat.workspace_size(desc, self.sub_batch)
+        self.ws = [torch.empty(max(ws, 1), dtype=torch.uint8, device=dev) for _ in range(2)]
+
+    @staticmethod
+    def pinned_params(params: np.ndarray):
+        import torch
+
+        t = torch.empty(params.shape, dtype=torch.float64, pin_memory=True)
+        t.copy_(torch.from_numpy(np.ascontiguousarray(params)))
+        return t
+
+    def pinned_output(self, n):
+        return self.torch.empty((n,) + self.out_shape, dtype=self.torch.complex64, pin_memory=True)
+
+    def run(self, params_host, out_host):
+        """params_host: pinned float64 [n, 32]; out_host: pinned complex64 [n, Py, Px//2+1]."""
+        torch = self.torch
+        n = params_host.shape[0]
+        cur = torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(cur)
+        for i, s0 in enumerate(range(0, n, self.sub_batch)):
+            k = i % 2
+            cnt = min(self.sub_batch, n - s0)
+            st = self.streams[k]
+            with torch.cuda.stream(st):
+                pd = self.params_d[k][:cnt]
+                od = self.out_d[k][:cnt]
+                pd.copy_(params_host[s0:s0 + cnt], non_blocking=True)
+                self.integrator.run(self.volume, self.cfg, None, self.flags, params_device=pd, out=od,
+                                    workspace=self.ws[k], stream=st, images_per_chunk=self.chunk, n=cnt)
+                out_host[s0:s0 + cnt].copy_(od, non_blocking=True)
+        for s in self.streams:
+            cur.wait_stream(s)
+        return out_host

@@ -403,9 +403,15 @@ class FourierSliceExtraction:
     def _base_flags(self):
         return nat.CJX_ZERO_FILL_NEGATIVE if self.out_of_bounds_mode == "zero_fill_negative" else 0
 
-    def run(self, volume: FourierVoxelGridVolume, image_config: BasicImageConfig, params: np.ndarray,
-            flags: int, *, params_device=None, out=None, workspace=None, stream=None, images_per_chunk=0):
-        """Launch the batched kernel; returns a complex64 [n, Py, Px//2+1] CUDA tensor."""
+    def run(self, volume: FourierVoxelGridVolume, image_config: BasicImageConfig, params: np.ndarray | None,
+            flags: int, *, params_device=None, out=None, workspace=None, stream=None, images_per_chunk=0,
+            n=None):
+        """Launch the batched kernel; returns a complex64 [n, Py, Px//2+1] CUDA tensor.
+
+        ``params`` (host float64 [n, 32]) is copied to the device unless
+        ``params_device`` is given.  ``out`` and ``workspace`` are allocated
+        when not supplied.
+        """
         torch = _torch()
         grid = volume.fourier_voxel_grid
         n_vol = grid.shape[0]
@@ -413,7 +419,8 @@ class FourierSliceExtraction:
             raise NotImplementedError("only constant padding is implemented on the device")
         py, px = image_config.padded_shape
         desc = nat.make_desc(n_vol, py, px, flags | self._base_flags(), self.fill_value, images_per_chunk)
-        n = params.shape[0]
+        if n is None:
+            n = params_device.shape[0] if params_device is not None else params.shape[0]
         if params_device is None:
             params_device = torch.as_tensor(params, dtype=torch.float64, device=grid.device)
         if out is None:

@@ -141,6 +141,16 @@ CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
 CJX_API int cjx_probe_read_bandwidth(const void* buf, size_t bytes, int passes,
                              void* sink, void* stream);
 
+/* Measurement helpers (no counterpart in the reference).  While enabled on
+ * the calling thread, each kernel launch the library makes is bracketed by
+ * a pair of CUDA events on its stream.  cjx_profile_read waits for those
+ * events, then writes up to max_kernels entries: kernel name (32 chars,
+ * NUL-padded, into names[32*i]), launch count and summed milliseconds; it
+ * clears the record.                                                       */
+CJX_API int cjx_profile_enable(int on);
+CJX_API int cjx_profile_read(char* names, int64_t* counts, double* total_ms,
+                             int max_kernels, int* n_kernels);
+
 #ifdef __cplusplus
 }
 #endif
