@@ -88,6 +88,17 @@ _SIGNATURES = {
             ctypes.c_void_p,
         ],
     ),
+    "cjx_slice_ctf_forward_noalloc": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(SliceDesc),
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_int64,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+        ],
+    ),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -196,6 +207,29 @@ def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream
             _cuda_ptr(out, "out"),
             ws_ptr,
             ws_bytes,
+            _stream_ptr(stream),
+        )
+    )
+
+
+NOALLOC_SCRATCH_BYTES = 32 << 20  # CJX_NOALLOC_SCRATCH_BYTES
+
+
+def slice_ctf_forward_noalloc(desc: SliceDesc, grid, params, out, stream=None) -> None:
+    """Launch cjx_slice_ctf_forward_noalloc (scratch inside the library, no allocation)."""
+    import torch
+
+    if params.dtype != torch.float64 or params.shape[-1] != PARAMS_DOUBLES:
+        raise ValueError("params must be float64 [n_images, 32]")
+    if grid.dtype != torch.complex64 or out.dtype != torch.complex64:
+        raise ValueError("grid and out must be complex64")
+    _check(
+        load_library().cjx_slice_ctf_forward_noalloc(
+            ctypes.byref(desc),
+            _cuda_ptr(grid, "grid"),
+            _cuda_ptr(params, "params"),
+            int(params.shape[0]),
+            _cuda_ptr(out, "out"),
             _stream_ptr(stream),
         )
     )

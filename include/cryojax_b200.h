@@ -134,6 +134,26 @@ CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
                           void* out, void* workspace, size_t workspace_bytes,
                           void* stream);
 
+/* Allocation-free variant of cjx_slice_ctf_forward.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory, because the
+ * runtime hosting them owns every allocation (for example an XLA custom call
+ * without a scratch allocator) or forbids allocation once it is running: the
+ * caller passes only inputs and outputs, and the resize stage's scratch is a
+ * fixed array of CJX_NOALLOC_SCRATCH_BYTES inside the library, held by every
+ * GPU that loads the library until the process exits.  Results equal
+ * cjx_slice_ctf_forward's.
+ *  - The first call on each device looks up that array's device address;
+ *    make that first call before any stream capture.
+ *  - All calls on a device share the array: calls that overlap on the GPU
+ *    (other streams, other host threads) race; serialise them.
+ *  - Returns CJX_ERR_UNSUPPORTED if one image, or desc->images_per_chunk
+ *    images, need more scratch than CJX_NOALLOC_SCRATCH_BYTES.
+ *  - Calls no cudaMalloc / cudaFree or any allocating library routine.      */
+#define CJX_NOALLOC_SCRATCH_BYTES (32u << 20)
+CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void* grid,
+                                          const cjx_image_params* params, int64_t n_images,
+                                          void* out, void* stream);
+
 /* Measurement helper: streams `bytes` of `buf` `passes` times through the
  * SMs (read-only, 16-byte vector loads, result folded into `sink`).  With a
  * buffer smaller than L2 this measures L2 read bandwidth; larger, HBM.
