@@ -50,6 +50,9 @@ def parse_args():
     ap.add_argument("--image", type=int, default=320)
     ap.add_argument("--pad-scale", type=float, default=2.0)
     ap.add_argument("--chunk", type=int, default=0, help="images per workspace chunk (0 = library default)")
+    ap.add_argument("--ilp", type=int, default=0, help="gather ILP (1, 2, 4; 0 = library default)")
+    ap.add_argument("--order", choices=["orientation", "none"], default="orientation",
+                    help="image processing order (orientation-sorted for L2 reuse, or as given)")
     ap.add_argument("--cpu-sample", type=int, default=6, help="images in the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -67,6 +70,7 @@ def config_dict(args, world):
         "global_batch": args.images * world, "pixel_size_A": 2.0, "voltage_kV": 300.0,
         "l2_flush": "not needed: volume (1.07 GB) and output (6.75 GB per step) exceed the 126 MB L2",
         "parallelism": f"replicas x{world} (images sharded, no collective)",
+        "processing_order": args.order,
     }
 
 
@@ -226,6 +230,8 @@ def algorithmic_bytes_per_image(kernel, n, py, px):
 
     k_gather_colifft: 8 corner loads of 8 B per slice sample over the
       N x (N/2+1) half-plane, plus the Py x (N/2+1) complex window written.
+    k_gather_slice:  8 corner loads + one 8 B store per slice sample.
+    k_colifft_window: read the N x (N/2+1) slice, write the Py x (N/2+1) window.
     k_rows_c2r_r2c:  read Py x (N/2+1), write Py x (Px/2+1) complex.
     k_colfft_epilogue: read Py x (Px/2+1), write Py x (Px/2+1) complex.
     k_slice_direct:  8 corner loads + one store per output pixel.
@@ -233,6 +239,10 @@ def algorithmic_bytes_per_image(kernel, n, py, px):
     nxh, pxh = n // 2 + 1, px // 2 + 1
     if kernel == "k_gather_colifft":
         return 64 * n * nxh + 8 * py * nxh
+    if kernel == "k_gather_slice":
+        return 72 * n * nxh
+    if kernel == "k_colifft_window":
+        return 8 * n * nxh + 8 * py * nxh
     if kernel == "k_rows_c2r_r2c":
         return 8 * py * nxh + 8 * py * pxh
     if kernel == "k_colfft_epilogue":
@@ -298,6 +308,11 @@ def main():
     model = S.make_image_model(volume, cfg, pose, tt)
     params_h = model.image_params()
     params_d = torch.as_tensor(params_h, device=dev)
+    if args.ilp:
+        nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, args.ilp)
+    order_d = None
+    if args.order == "orientation":
+        order_d = torch.as_tensor(S.orientation_order(pose.rotation_matrices()), device=dev)
     flags = model._flags()
     integ = model.volume_integrator
     py, px = cfg.padded_shape
@@ -309,7 +324,7 @@ def main():
 
     def step():
         integ.run(volume, cfg, None, flags, params_device=params_d, out=out, workspace=ws, stream=stream,
-                  images_per_chunk=args.chunk)
+                  images_per_chunk=args.chunk, order=order_d)
 
     def barrier():
         if world > 1:
@@ -367,8 +382,8 @@ def main():
         pr = nat.profile_read()
         nat.profile_enable(False)
         l2_gbs = buf.numel() * 50 / (pr["k_read_probe"][1] / 1000.0) / 1e9
-        gather = prof.get("k_gather_colifft") or prof.get("k_slice_direct")
-        gname = "k_gather_colifft" if "k_gather_colifft" in prof else "k_slice_direct"
+        gname = next(k for k in ("k_gather_slice", "k_gather_colifft", "k_slice_direct") if k in prof)
+        gather = prof[gname]
         g_alg = algorithmic_bytes_per_image(gname, n, py, px) * args.images / (gather[1] / 1000.0) / 1e9
         l2 = {"kernel": gname, "achieved": g_alg, "peak": l2_gbs, "unit": "GB/s", "frac": g_alg / l2_gbs,
               "peak_source": "k_read_probe, 48 MB buffer x 50 passes (measured in this run)"}

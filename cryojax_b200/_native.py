@@ -28,6 +28,9 @@ CJX_APPLY_ENVELOPE = 1 << 2
 CJX_ZERO_FILL_NEGATIVE = 1 << 3
 
 CJX_MAX_SIDE = 1024
+CJX_TUNE_GATHER_ILP = 1
+CJX_TUNE_CHUNK_BYTES = 2
+CJX_TUNE_GATHER_MODE = 3
 PARAMS_DOUBLES = 32  # sizeof(cjx_image_params) / 8
 
 # field offsets (in doubles) of cjx_image_params
@@ -81,6 +84,7 @@ _SIGNATURES = {
             ctypes.POINTER(SliceDesc),
             ctypes.c_void_p,
             ctypes.c_void_p,
+            ctypes.c_void_p,
             ctypes.c_int64,
             ctypes.c_void_p,
             ctypes.c_void_p,
@@ -94,11 +98,14 @@ _SIGNATURES = {
             ctypes.POINTER(SliceDesc),
             ctypes.c_void_p,
             ctypes.c_void_p,
+            ctypes.c_void_p,
             ctypes.c_int64,
             ctypes.c_void_p,
             ctypes.c_void_p,
         ],
     ),
+    "cjx_tuning_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64]),
+    "cjx_tuning_get": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -182,7 +189,17 @@ def _stream_ptr(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
-def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream=None) -> None:
+def _order_ptr(order, n_images):
+    import torch
+
+    if order is None:
+        return ctypes.c_void_p(0)
+    if order.dtype != torch.int32 or order.numel() != n_images:
+        raise ValueError("order must be an int32 permutation of length n_images")
+    return _cuda_ptr(order, "order")
+
+
+def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream=None, order=None) -> None:
     """Launch cjx_slice_ctf_forward on torch CUDA tensors (stream-ordered)."""
     import torch
 
@@ -203,6 +220,7 @@ def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream
             ctypes.byref(desc),
             _cuda_ptr(grid, "grid"),
             _cuda_ptr(params, "params"),
+            _order_ptr(order, n_images),
             int(n_images),
             _cuda_ptr(out, "out"),
             ws_ptr,
@@ -215,7 +233,7 @@ def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CJX_NOALLOC_SCRATCH_BYTES
 
 
-def slice_ctf_forward_noalloc(desc: SliceDesc, grid, params, out, stream=None) -> None:
+def slice_ctf_forward_noalloc(desc: SliceDesc, grid, params, out, stream=None, order=None) -> None:
     """Launch cjx_slice_ctf_forward_noalloc (scratch inside the library, no allocation)."""
     import torch
 
@@ -228,6 +246,7 @@ def slice_ctf_forward_noalloc(desc: SliceDesc, grid, params, out, stream=None) -
             ctypes.byref(desc),
             _cuda_ptr(grid, "grid"),
             _cuda_ptr(params, "params"),
+            _order_ptr(order, params.shape[0]),
             int(params.shape[0]),
             _cuda_ptr(out, "out"),
             _stream_ptr(stream),
@@ -245,6 +264,16 @@ def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:
             _stream_ptr(stream),
         )
     )
+
+
+def tuning_set(key: int, value: int) -> None:
+    _check(load_library().cjx_tuning_set(int(key), int(value)))
+
+
+def tuning_get(key: int) -> int:
+    v = ctypes.c_int64(0)
+    _check(load_library().cjx_tuning_get(int(key), ctypes.byref(v)))
+    return int(v.value)
 
 
 def profile_enable(on: bool) -> None:

@@ -11,8 +11,10 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g);
 bool needs_resize(const SliceGeom& g);
 size_t workspace_per_image(const SliceGeom& g);
 int64_t default_chunk(const SliceGeom& g, int64_t n_images);
-int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, int64_t n_images,
-                   float2* out, void* workspace, int64_t chunk, cudaStream_t stream);
+int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream);
+int64_t tuning_get(int key);
+int tuning_set(int key, int64_t value);
 int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
 
 static thread_local std::string g_last_error;
@@ -54,7 +56,8 @@ int cjx_slice_ctf_workspace_size(const cjx_slice_desc* desc, int64_t n_images, s
 }
 
 int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cjx_image_params* params,
-                          int64_t n_images, void* out, void* workspace, size_t workspace_bytes, void* stream) {
+                          const int32_t* order, int64_t n_images, void* out, void* workspace, size_t workspace_bytes,
+                          void* stream) {
   SliceGeom g;
   if (int e = make_geom(desc, &g)) return e;
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
@@ -67,8 +70,18 @@ int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cj
     if (!workspace || workspace_bytes < need)
       return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_workspace_size()");
   }
-  return launch_forward(g, static_cast<const float2*>(grid), params, n_images, static_cast<float2*>(out),
+  return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images, static_cast<float2*>(out),
                         workspace, chunk, static_cast<cudaStream_t>(stream));
+}
+
+int cjx_tuning_set(int key, int64_t value) { return tuning_set(key, value); }
+
+int cjx_tuning_get(int key, int64_t* value) {
+  if (!value) return fail(CJX_ERR_INVALID_ARGUMENT, "value is NULL");
+  const int64_t v = tuning_get(key);
+  if (v < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown tuning key");
+  *value = v;
+  return CJX_OK;
 }
 
 int cjx_probe_read_bandwidth(const void* buf, size_t bytes, int passes, void* sink, void* stream) {

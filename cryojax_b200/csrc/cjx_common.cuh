@@ -22,6 +22,7 @@ struct SliceGeom {
   int nxh;          // N/2 + 1 (half-plane columns of the slice)
   int pxh;          // Px/2 + 1
   int ld1, ld2;     // row pitch (complex elements) of workspace T1, T2
+  int ldh;          // column pitch of the slice buffer H ([kx][ky], split gather)
   int pad_left_y;   // left pad when Py > N (cryojax/ndimage/_edges.py:175-185)
   int pad_left_x;
   uint32_t flags;
@@ -121,6 +122,42 @@ __device__ __forceinline__ float2 sample_trilinear(const float2* __restrict__ gr
     }
   }
   return acc;
+}
+
+// S samples at once: every corner load of all S samples is issued before
+// any is consumed, so one lane keeps 8*S independent loads in flight.
+template <int S>
+__device__ __forceinline__ void sample_trilinear_batch(const float2* __restrict__ grid, int n, const float* ox,
+                                                       const float* oy, const float* oz, const bool* active,
+                                                       bool wrap_negative, float2 fill, float2* out) {
+  float2 v[S][8];
+  float w[S][6];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const AxisNodes ax = axis_nodes(ox[s], n, wrap_negative);
+    const AxisNodes ay = axis_nodes(oy[s], n, wrap_negative);
+    const AxisNodes az = axis_nodes(oz[s], n, wrap_negative);
+    w[s][0] = ax.w0; w[s][1] = ax.w1; w[s][2] = ay.w0; w[s][3] = ay.w1; w[s][4] = az.w0; w[s][5] = az.w1;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+      const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
+      const bool ok = active[s] && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
+      v[s][c] = ok ? __ldg(&grid[((size_t)iz * n + iy) * n + ix]) : fill;
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+      const float wt = (w[s][4 + dz] * w[s][2 + dy]) * w[s][dx];
+      acc.x = fmaf(wt, v[s][c].x, acc.x);
+      acc.y = fmaf(wt, v[s][c].y, acc.y);
+    }
+    out[s] = acc;
+  }
 }
 
 // ---------------------------------------------------------------------------

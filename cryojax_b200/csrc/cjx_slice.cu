@@ -16,6 +16,7 @@
 // No-resize path ((Py, Px) == (N, N)): one fused kernel samples each output
 // pixel and applies the epilogue directly.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "cjx_common.cuh"
@@ -26,9 +27,10 @@ namespace cjx {
 // ---------------------------------------------------------------------------
 // Pass A
 // ---------------------------------------------------------------------------
+template <int S>
 __global__ void __launch_bounds__(kWarps * 32)
     k_gather_colifft(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
-                     float2* __restrict__ t1, SliceGeom g, int64_t img0) {
+                     const int32_t* __restrict__ order, float2* __restrict__ t1, SliceGeom g, int64_t k0) {
   extern __shared__ float2 smem[];
   const int n = g.n, h = n / 2;
   const int stride = 2 * n + 2;  // per-warp buffers (+2 to stagger banks)
@@ -36,7 +38,8 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2* bufs = smem + n;
   build_twiddles(tw, n);
 
-  const int64_t img = img0 + blockIdx.y;
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
   const double* R = params[img].rot;
   const float r00 = (float)R[0], r01 = (float)R[1];
   const float r10 = (float)R[3], r11 = (float)R[4];
@@ -52,9 +55,23 @@ __global__ void __launch_bounds__(kWarps * 32)
   if (j < g.nxh) {
     const float ux = (float)fft_index(j, n);
     const float bx = r00 * ux, by = r10 * ux, bz = r20 * ux;
-    for (int i = lane; i < n; i += 32) {
-      const float vy = (float)fft_index(i, n);
-      a[i] = sample_trilinear(grid, n, fmaf(r01, vy, bx), fmaf(r11, vy, by), fmaf(r21, vy, bz), wrap, g.fill);
+    for (int i0 = lane; i0 < n; i0 += 32 * S) {
+      float ox[S], oy[S], oz[S];
+      bool act[S];
+      float2 val[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        const int i = i0 + 32 * s;
+        act[s] = i < n;
+        const float vy = (float)fft_index(act[s] ? i : 0, n);
+        ox[s] = fmaf(r01, vy, bx);
+        oy[s] = fmaf(r11, vy, by);
+        oz[s] = fmaf(r21, vy, bz);
+      }
+      sample_trilinear_batch<S>(grid, n, ox, oy, oz, act, wrap, g.fill, val);
+#pragma unroll
+      for (int s = 0; s < S; ++s)
+        if (act[s]) a[i0 + 32 * s] = val[s];
     }
     __syncwarp();
     if (j == 0 || ((n % 2 == 0) && j == h)) {
@@ -62,9 +79,9 @@ __global__ void __launch_bounds__(kWarps * 32)
       for (int i = lane; i <= n / 2; i += 32) {
         const int i2 = (i == 0) ? 0 : n - i;
         const float2 x = a[i], y = a[i2];
-        const float2 s = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
-        a[i] = s;
-        a[i2] = cconj(s);
+        const float2 sv = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        a[i] = sv;
+        a[i2] = cconj(sv);
       }
       __syncwarp();
     }
@@ -74,6 +91,93 @@ __global__ void __launch_bounds__(kWarps * 32)
 
   // The FFT result sits in buffer a after an even number of Stockham stages,
   // in b after an odd number (or after the direct DFT).
+  const int res_off = (g.plan_n.nstages == 0 || (g.plan_n.nstages & 1)) ? n : 0;
+  const int ncols = min(kWarps, g.nxh - j0);
+  float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
+  for (int e = threadIdx.x; e < g.py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      const int src = win_src(m, n, g.py, g.pad_left_y);
+      dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? bufs[jj * stride + res_off + src] : make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass A, split form: a shared-memory-free gather kernel (the L1 cache keeps
+// its full capacity for the corner loads of neighbouring samples) writing the
+// half-plane slice H[kx][ky] to an L2-resident buffer, then a column kernel
+// that runs the Hermitian fix, inverse FFT and window on H.
+// ---------------------------------------------------------------------------
+template <int S>
+__global__ void __launch_bounds__(256)
+    k_gather_slice(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
+                   const int32_t* __restrict__ order, float2* __restrict__ hbuf, SliceGeom g, int64_t k0) {
+  const int n = g.n;
+  const int64_t k = k0 + blockIdx.z;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  const double* R = params[img].rot;
+  const float r00 = (float)R[0], r01 = (float)R[1];
+  const float r10 = (float)R[3], r11 = (float)R[4];
+  const float r20 = (float)R[6], r21 = (float)R[7];
+  const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
+  // CTA patch: 16 columns x 16*S rows; a warp covers 2 columns x 16 rows per step
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * 16 + warp * 2 + (lane >> 4);
+  if (u >= g.nxh) return;
+  const int vbase = blockIdx.y * (16 * S) + (lane & 15);
+  const float ux = (float)fft_index(u, n);
+  const float bx = r00 * ux, by = r10 * ux, bz = r20 * ux;
+  float ox[S], oy[S], oz[S];
+  bool act[S];
+  float2 val[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int v = vbase + 16 * s;
+    act[s] = v < n;
+    const float vy = (float)fft_index(act[s] ? v : 0, n);
+    ox[s] = fmaf(r01, vy, bx);
+    oy[s] = fmaf(r11, vy, by);
+    oz[s] = fmaf(r21, vy, bz);
+  }
+  sample_trilinear_batch<S>(grid, n, ox, oy, oz, act, wrap, g.fill, val);
+  float2* col = hbuf + ((size_t)blockIdx.z * g.nxh + u) * g.ldh;
+#pragma unroll
+  for (int s = 0; s < S; ++s)
+    if (act[s]) col[vbase + 16 * s] = val[s];
+}
+
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colifft_window(const float2* __restrict__ hbuf, float2* __restrict__ t1, SliceGeom g) {
+  extern __shared__ float2 smem[];
+  const int n = g.n, h = n / 2;
+  const int stride = 2 * n + 2;
+  float2* tw = smem;
+  float2* bufs = smem + n;
+  build_twiddles(tw, n);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j0 = blockIdx.x * kWarps;
+  const int j = j0 + warp;
+  float2* a = bufs + warp * stride;
+  float2* b = a + n;
+  if (j < g.nxh) {
+    const float2* col = hbuf + ((size_t)blockIdx.y * g.nxh + j) * g.ldh;
+    for (int i = lane; i < n; i += 32) a[i] = col[i];
+    __syncwarp();
+    if (j == 0 || ((n % 2 == 0) && j == h)) {
+      for (int i = lane; i <= n / 2; i += 32) {
+        const int i2 = (i == 0) ? 0 : n - i;
+        const float2 x = a[i], y = a[i2];
+        const float2 sv = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        a[i] = sv;
+        a[i2] = cconj(sv);
+      }
+      __syncwarp();
+    }
+    warp_fft<+1>(a, b, g.plan_n, tw, lane);
+  }
+  __syncthreads();
   const int res_off = (g.plan_n.nstages == 0 || (g.plan_n.nstages & 1)) ? n : 0;
   const int ncols = min(kWarps, g.nxh - j0);
   float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
@@ -146,7 +250,8 @@ __global__ void __launch_bounds__(kWarps * 32)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kWarps * 32)
     k_colfft_epilogue(const float2* __restrict__ t2, const cjx_image_params* __restrict__ params,
-                      float2* __restrict__ out, SliceGeom g, int64_t img0, float norm) {
+                      const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0,
+                      float norm) {
   extern __shared__ float2 smem[];
   const int py = g.py;
   const int stride = 2 * py + 2;
@@ -161,7 +266,8 @@ __global__ void __launch_bounds__(kWarps * 32)
     const int m = e / kWarps, jj = e % kWarps;
     if (jj < ncols) bufs[jj * stride + m] = src[(size_t)m * g.ld2 + jj];
   }
-  const int64_t img = img0 + blockIdx.y;
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
   const ImageConsts c = load_image_consts(params + img, norm);
   __syncthreads();
 
@@ -186,9 +292,10 @@ __global__ void __launch_bounds__(kWarps * 32)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     k_slice_direct(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
-                   float2* __restrict__ out, SliceGeom g) {
+                   const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0) {
   const int n = g.n, h = n / 2;
-  const int64_t img = blockIdx.y;
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
   const double* R = params[img].rot;
   const float r00 = (float)R[0], r01 = (float)R[1];
   const float r10 = (float)R[3], r11 = (float)R[4];
@@ -218,6 +325,11 @@ static size_t smem_b(const SliceGeom& g) {
 }
 static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py + kWarps * (2 * g.py + 2)); }
 
+// Process-wide tuning knobs (cjx_tuning_set / cjx_tuning_get).
+static std::atomic<int64_t> g_gather_ilp{2};
+static std::atomic<int64_t> g_chunk_bytes{256ll << 20};
+static std::atomic<int64_t> g_gather_mode{1};
+
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
@@ -235,6 +347,7 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
   g->pxh = d->px / 2 + 1;
   g->ld1 = round_up(g->nxh, 8);
   g->ld2 = round_up(g->pxh, 8);
+  g->ldh = round_up(g->n, 8);
   auto left_pad = [](int pad_dim, int image_dim) {
     const int pad = pad_dim - image_dim;
     if (pad_dim % 2 == 0 && image_dim % 2 == 1) return pad / 2 + 1;
@@ -252,17 +365,51 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
 
 bool needs_resize(const SliceGeom& g) { return !(g.py == g.n && g.px == g.n); }
 
+// Per image: T1 [Py][ld1], T2 [Py][ld2] and the split gather's H [N/2+1][ldh].
 size_t workspace_per_image(const SliceGeom& g) {
-  return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2);
+  return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2 + (size_t)g.nxh * g.ldh);
 }
 
 // Default chunk: about 64 MB of intermediates, so a chunk stays in L2.
 int64_t default_chunk(const SliceGeom& g, int64_t n_images) {
   const size_t per = workspace_per_image(g);
-  int64_t c = (int64_t)((64u << 20) / std::max<size_t>(per, 1));
+  int64_t c = (int64_t)((size_t)g_chunk_bytes.load() / std::max<size_t>(per, 1));
   c = std::max<int64_t>(c, 1);
   c = std::min<int64_t>(c, 65535);
   return std::min<int64_t>(c, std::max<int64_t>(n_images, 1));
+}
+
+// Process-wide tuning knobs (cjx_tuning_set / cjx_tuning_get), declared above.
+
+int64_t tuning_get(int key) {
+  if (key == CJX_TUNE_GATHER_ILP) return g_gather_ilp.load();
+  if (key == CJX_TUNE_CHUNK_BYTES) return g_chunk_bytes.load();
+  if (key == CJX_TUNE_GATHER_MODE) return g_gather_mode.load();
+  return -1;
+}
+
+int tuning_set(int key, int64_t value) {
+  if (key == CJX_TUNE_GATHER_ILP) {
+    if (value != 1 && value != 2 && value != 4) return fail(CJX_ERR_INVALID_ARGUMENT, "gather ILP must be 1, 2 or 4");
+    g_gather_ilp = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_CHUNK_BYTES) {
+    if (value < (1 << 20)) return fail(CJX_ERR_INVALID_ARGUMENT, "chunk bytes must be >= 1 MiB");
+    g_chunk_bytes = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_GATHER_MODE) {
+    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0 or 1");
+    g_gather_mode = value;
+    return CJX_OK;
+  }
+  return fail(CJX_ERR_INVALID_ARGUMENT, "unknown tuning key");
+}
+
+template <typename K>
+static cudaError_t allow_smem(K kernel) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
 static int ensure_smem_attrs() {
@@ -271,27 +418,27 @@ static int ensure_smem_attrs() {
   if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
   int err = CJX_OK;
   std::call_once(flags[dev & 63], [&] {
-    const int max_bytes = 227 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_gather_colifft, cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_rows_c2r_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_colfft_epilogue, cudaFuncAttributeMaxDynamicSharedMemorySize, max_bytes);
+    cudaError_t e = allow_smem(k_gather_colifft<1>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<2>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<4>);
+    if (e == cudaSuccess) e = allow_smem(k_colifft_window);
+    if (e == cudaSuccess) e = allow_smem(k_rows_c2r_r2c);
+    if (e == cudaSuccess) e = allow_smem(k_colfft_epilogue);
     if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
   });
   return err;
 }
 
-int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, int64_t n_images,
-                   float2* out, void* workspace, int64_t chunk, cudaStream_t stream) {
+int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream) {
   if (n_images == 0) return CJX_OK;
   if (!needs_resize(g)) {
     const int total = g.n * g.nxh;
     const int blocks = std::min((total + 255) / 256, 1024);
-    for (int64_t i0 = 0; i0 < n_images; i0 += 65535) {
-      const int cnt = (int)std::min<int64_t>(65535, n_images - i0);
+    for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
+      const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
       prof_begin(stream);
-      k_slice_direct<<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params + i0, out + (size_t)i0 * total, g);
+      k_slice_direct<<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
       prof_end("k_slice_direct", stream);
     }
     return check_cuda(cudaGetLastError(), "k_slice_direct launch");
@@ -302,19 +449,42 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     return fail(CJX_ERR_UNSUPPORTED, "shared-memory footprint exceeds 227 KB for these sizes");
   float2* t1 = static_cast<float2*>(workspace);
   float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
+  float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
-  for (int64_t i0 = 0; i0 < n_images; i0 += chunk) {
-    const int cnt = (int)std::min<int64_t>(chunk, n_images - i0);
-    prof_begin(stream);
-    k_gather_colifft<<<dim3((g.nxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sa, stream>>>(grid, params, t1, g,
-                                                                                             i0);
-    prof_end("k_gather_colifft", stream);
+  const int64_t ilp = g_gather_ilp.load();
+  const bool split = g_gather_mode.load() == 1;
+  for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
+    if (split) {
+      const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
+      prof_begin(stream);
+      if (ilp == 4)
+        k_gather_slice<4><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+      else if (ilp == 2)
+        k_gather_slice<2><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+      else
+        k_gather_slice<1><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+      prof_end("k_gather_slice", stream);
+      prof_begin(stream);
+      k_colifft_window<<<dim3((g.nxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sa, stream>>>(hb, t1, g);
+      prof_end("k_colifft_window", stream);
+    } else {
+      const dim3 ga((g.nxh + kWarps - 1) / kWarps, cnt);
+      prof_begin(stream);
+      if (ilp == 4)
+        k_gather_colifft<4><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
+      else if (ilp == 2)
+        k_gather_colifft<2><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
+      else
+        k_gather_colifft<1><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
+      prof_end("k_gather_colifft", stream);
+    }
     prof_begin(stream);
     k_rows_c2r_r2c<<<dim3((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, sb, stream>>>(t1, t2, g);
     prof_end("k_rows_c2r_r2c", stream);
     prof_begin(stream);
-    k_colfft_epilogue<<<dim3((g.pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sc, stream>>>(t2, params, out, g,
-                                                                                             i0, norm);
+    k_colfft_epilogue<<<dim3((g.pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sc, stream>>>(t2, params, order, out,
+                                                                                             g, k0, norm);
     prof_end("k_colfft_epilogue", stream);
   }
   return check_cuda(cudaGetLastError(), "forward launch");

@@ -17,7 +17,8 @@ from . import _native as nat
 class HostStreamingSimulator:
     """Two-stream pipeline over sub-batches of ``sub_batch`` images."""
 
-    def __init__(self, volume, image_config, integrator, flags, *, sub_batch=2048, images_per_chunk=0):
+    def __init__(self, volume, image_config, integrator, flags, *, sub_batch=2048, images_per_chunk=0,
+                 sort_orientations=True):
         import torch
 
         self.torch = torch
@@ -27,6 +28,8 @@ class HostStreamingSimulator:
         self.flags = flags
         self.sub_batch = int(sub_batch)
         self.chunk = images_per_chunk
+        self.sort = sort_orientations
+        self.order_d = [None, None]
         dev = volume.fourier_voxel_grid.device
         py, px = image_config.padded_shape
         self.out_shape = (py, px // 2 + 1)
@@ -51,9 +54,21 @@ class HostStreamingSimulator:
         return self.torch.empty((n,) + self.out_shape, dtype=self.torch.complex64, pin_memory=True)
 
     def run(self, params_host, out_host):
-        """params_host: pinned float64 [n, 32]; out_host: pinned complex64 [n, Py, Px//2+1]."""
+        """params_host: pinned float64 [n, 32]; out_host: pinned complex64 [n, Py, Px//2+1].
+
+        With ``sort_orientations`` each sub-batch is processed in
+        orientation order (outputs still land in their own slots).
+        """
         torch = self.torch
         n = params_host.shape[0]
+        orders = []
+        if self.sort:
+            from .simulator import orientation_order
+
+            rots = params_host[:, 0:9].numpy().reshape(-1, 3, 3)
+            for s0 in range(0, n, self.sub_batch):
+                o = orientation_order(rots[s0:s0 + self.sub_batch])
+                orders.append(torch.from_numpy(o).pin_memory())
         cur = torch.cuda.current_stream()
         for s in self.streams:
             s.wait_stream(cur)
@@ -65,8 +80,15 @@ class HostStreamingSimulator:
                 pd = self.params_d[k][:cnt]
                 od = self.out_d[k][:cnt]
                 pd.copy_(params_host[s0:s0 + cnt], non_blocking=True)
+                od_order = None
+                if self.sort:
+                    if self.order_d[k] is None:
+                        self.order_d[k] = torch.empty(self.sub_batch, dtype=torch.int32, device=pd.device)
+                    od_order = self.order_d[k][:cnt]
+                    od_order.copy_(orders[i], non_blocking=True)
                 self.integrator.run(self.volume, self.cfg, None, self.flags, params_device=pd, out=od,
-                                    workspace=self.ws[k], stream=st, images_per_chunk=self.chunk, n=cnt)
+                                    workspace=self.ws[k], stream=st, images_per_chunk=self.chunk, n=cnt,
+                                    order=od_order)
                 out_host[s0:s0 + cnt].copy_(od, non_blocking=True)
         for s in self.streams:
             cur.wait_stream(s)

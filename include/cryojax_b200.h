@@ -126,13 +126,18 @@ CJX_API int cjx_slice_ctf_workspace_size(const cjx_slice_desc* desc, int64_t n_i
  *
  * grid:    device, complex64 [N][N][N]
  * params:  device, n_images records
+ * order:   device int32 [n_images], a permutation giving the processing
+ *          order (image order[k] is processed k-th; its output still lands
+ *          in out[order[k]]), or NULL for 0, 1, 2, ...  Processing images
+ *          with similar plane orientations together lets their gathers share
+ *          L2 (see cryojax_b200.simulator.orientation_order).
  * out:     device, complex64 [n_images][Py][Px/2+1]
  * workspace: device scratch of at least cjx_slice_ctf_workspace_size bytes
  *          (may be NULL when that size is 0)                              */
 CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
-                          const cjx_image_params* params, int64_t n_images,
-                          void* out, void* workspace, size_t workspace_bytes,
-                          void* stream);
+                                  const cjx_image_params* params, const int32_t* order,
+                                  int64_t n_images, void* out, void* workspace,
+                                  size_t workspace_bytes, void* stream);
 
 /* Allocation-free variant of cjx_slice_ctf_forward.  No counterpart in the
  * reference.  For callers that cannot allocate device memory, because the
@@ -151,8 +156,20 @@ CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
  *  - Calls no cudaMalloc / cudaFree or any allocating library routine.      */
 #define CJX_NOALLOC_SCRATCH_BYTES (32u << 20)
 CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void* grid,
-                                          const cjx_image_params* params, int64_t n_images,
-                                          void* out, void* stream);
+                                          const cjx_image_params* params, const int32_t* order,
+                                          int64_t n_images, void* out, void* stream);
+
+/* Process-wide tuning knobs (no counterpart in the reference; set by the
+ * autotuner).  CJX_TUNE_GATHER_ILP: samples whose corner loads one lane
+ * issues together in the gather (1, 2 or 4).  CJX_TUNE_CHUNK_BYTES: target
+ * workspace bytes per chunk when desc->images_per_chunk is 0.
+ * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
+ * column-FFT kernel, 0 = one fused gather + column-FFT kernel.              */
+#define CJX_TUNE_GATHER_ILP 1
+#define CJX_TUNE_CHUNK_BYTES 2
+#define CJX_TUNE_GATHER_MODE 3
+CJX_API int cjx_tuning_set(int key, int64_t value);
+CJX_API int cjx_tuning_get(int key, int64_t* value);
 
 /* Measurement helper: streams `bytes` of `buf` `passes` times through the
  * SMs (read-only, 16-byte vector loads, result folded into `sink`).  With a

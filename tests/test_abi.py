@@ -43,8 +43,8 @@ def test_struct_sizes_match_header():
 def test_workspace_size_and_validation():
     d = nat.make_desc(64, 32, 32, nat.CJX_APPLY_CTF | nat.CJX_APPLY_TRANSLATION)
     ws = nat.workspace_size(d, 10)
-    # per image: Py * round8(N/2+1) + Py * round8(Px/2+1) complex64
-    assert ws == 10 * 8 * (32 * 40 + 32 * 24)
+    # per image: Py * round8(N/2+1) + Py * round8(Px/2+1) + (N/2+1) * round8(N) complex64
+    assert ws == 10 * 8 * (32 * 40 + 32 * 24 + 33 * 64)
     assert nat.workspace_size(nat.make_desc(64, 64, 64, 0), 10) == 0  # no resize stage
     with pytest.raises(nat.CryojaxB200Error) as e:
         nat.workspace_size(nat.make_desc(1, 32, 32, 0), 1)
@@ -60,8 +60,20 @@ def test_workspace_size_and_validation():
 def test_forward_rejects_null_pointers_without_touching_the_gpu():
     lib = nat.load_library()
     d = nat.make_desc(64, 32, 32, 0)
-    rc = lib.cjx_slice_ctf_forward(ctypes.byref(d), None, None, 4, None, None, 0, None)
+    rc = lib.cjx_slice_ctf_forward(ctypes.byref(d), None, None, None, 4, None, None, 0, None)
     assert rc == nat.CJX_ERR_INVALID_ARGUMENT
     assert b"non-NULL" in lib.cjx_get_last_error()
     # zero images is a no-op
-    assert lib.cjx_slice_ctf_forward(ctypes.byref(d), None, None, 0, None, None, 0, None) == nat.CJX_OK
+    assert lib.cjx_slice_ctf_forward(ctypes.byref(d), None, None, None, 0, None, None, 0, None) == nat.CJX_OK
+
+
+def test_tuning_knobs():
+    assert nat.tuning_get(nat.CJX_TUNE_GATHER_ILP) in (1, 2, 4)
+    old = nat.tuning_get(nat.CJX_TUNE_GATHER_ILP)
+    nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, 4)
+    assert nat.tuning_get(nat.CJX_TUNE_GATHER_ILP) == 4
+    nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, old)
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, 3)
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(99, 1)

@@ -122,6 +122,33 @@ def test_chunking_is_invisible(cuda_device, chunk):
     assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("ilp", [1, 2, 4])
+def test_processing_order_and_gather_ilp_are_invisible(cuda_device, ilp, mode):
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+
+    vol, grid, fs = make_volume(32, 60, seed=33)
+    specs = random_specs(9, seed=39, shape=(32, 32))
+    pose, tt, cfg = specs_to_model_args(specs)
+    dvol = _device_volume(grid)
+    model = S.make_image_model(dvol, cfg, pose, tt)
+    order = S.orientation_order(pose.rotation_matrices())
+    old = nat.tuning_get(nat.CJX_TUNE_GATHER_ILP), nat.tuning_get(nat.CJX_TUNE_GATHER_MODE)
+    try:
+        nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, ilp)
+        nat.tuning_set(nat.CJX_TUNE_GATHER_MODE, mode)
+        got = model.volume_integrator.run(dvol, cfg, model.image_params(), model._flags(), order=order,
+                                          images_per_chunk=4).cpu().numpy()
+    finally:
+        nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, old[0])
+        nat.tuning_set(nat.CJX_TUNE_GATHER_MODE, old[1])
+    ref = _oracle(grid, fs, specs)
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
 def test_simulate_real_space_matches_oracle(cuda_device):
     from cryojax_b200 import simulator as S
 
