@@ -31,6 +31,7 @@ CJX_MAX_SIDE = 1024
 CJX_TUNE_GATHER_ILP = 1
 CJX_TUNE_CHUNK_BYTES = 2
 CJX_TUNE_GATHER_MODE = 3
+CJX_TUNE_FFT_MODE = 4
 PARAMS_DOUBLES = 32  # sizeof(cjx_image_params) / 8
 
 # field offsets (in doubles) of cjx_image_params
@@ -103,6 +104,10 @@ _SIGNATURES = {
             ctypes.c_void_p,
             ctypes.c_void_p,
         ],
+    ),
+    "cjx_fft_c2c": (
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     ),
     "cjx_tuning_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64]),
     "cjx_tuning_get": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
@@ -264,6 +269,21 @@ def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:
             _stream_ptr(stream),
         )
     )
+
+
+def fft_c2c(x, direction: int, out=None, stream=None):
+    """Row-wise complex64 FFT of a CUDA tensor [..., n] with the library's warp FFTs."""
+    import torch
+
+    if x.dtype != torch.complex64:
+        raise ValueError("x must be complex64")
+    x = x.contiguous()
+    if out is None:
+        out = torch.empty_like(x)
+    n = x.shape[-1]
+    _check(load_library().cjx_fft_c2c(int(n), int(direction), _cuda_ptr(x, "x"), _cuda_ptr(out, "out"),
+                                      int(x.numel() // n), _stream_ptr(stream)))
+    return out
 
 
 def tuning_set(key: int, value: int) -> None:

@@ -13,6 +13,8 @@
 
 #include <cuda_runtime.h>
 
+#include <utility>
+
 namespace cjx {
 
 constexpr int kMaxStages = 16;
@@ -216,6 +218,226 @@ __device__ float2* warp_fft(float2* a, float2* b, const FftPlan& plan, const flo
     Ns *= R;
   }
   return a;
+}
+
+
+// ===========================================================================
+// Register FFT for n = 32 R (R in {1, 2, 3, 4, 5, 6, 8, 10, 12, 16}).
+//
+// Four-step split n = 32 n1 + n2, k = k1 + R k2 (n2, k2 across the 32 lanes;
+// n1, k1 in registers):
+//   X[k1 + R k2] = sum_n2 W_32^(n2 k2) W_n^(n2 k1) sum_n1 x[32 n1 + n2] W_R^(n1 k1)
+// 1. lane l holds x[32 n1 + brev5(l)] for n1 = 0..R-1 (the caller loads them);
+// 2. R-point DFT over n1 in registers (compile-time twiddles);
+// 3. multiply by W_n^(brev5(l) k1) from a [R][32] table (conflict-free);
+// 4. 32-point radix-2 decimation-in-time across lanes with warp shuffles;
+//    bit-reversed lane order in, natural order out.
+// Afterwards lane l holds X[k1 + R l] for k1 = 0..R-1.
+// Shared-memory buffers that receive these outputs use the padded layout
+// pad16(e) = e + e / 16, which keeps the stride-R stores near conflict-free.
+// ===========================================================================
+
+__host__ __device__ constexpr int pad16(int e) { return e + (e >> 4); }
+
+__device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+
+// Compile-time cos / sin of 2 pi m / R via Taylor series after reduction to
+// |x| <= pi/4 (enough terms for double precision); used only for the small
+// constant twiddles of the in-register DFTs.
+namespace ct {
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double taylor_sin(double x) {
+  double term = x, sum = x;
+  for (int k = 1; k < 14; ++k) {
+    term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+    sum += term;
+  }
+  return sum;
+}
+constexpr double taylor_cos(double x) {
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 14; ++k) {
+    term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+    sum += term;
+  }
+  return sum;
+}
+// angle = 2 pi m / R reduced by octant symmetry
+constexpr double cos2pi(int m, int R) {
+  m = ((m % R) + R) % R;
+  const double x = 2.0 * kPi * m / R;  // [0, 2 pi)
+  if (x <= kPi / 4) return taylor_cos(x);
+  if (x <= 3 * kPi / 4) return -taylor_sin(x - kPi / 2);
+  if (x <= 5 * kPi / 4) return -taylor_cos(x - kPi);
+  if (x <= 7 * kPi / 4) return taylor_sin(x - 3 * kPi / 2);
+  return taylor_cos(x - 2 * kPi);
+}
+constexpr double sin2pi(int m, int R) { return cos2pi(m * 4 - R, 4 * R); }
+}  // namespace ct
+
+// exp(DIR 2 pi i m / R) as a compile-time constant
+template <int DIR, int M, int R>
+__device__ __forceinline__ float2 ctw() {
+  constexpr float c = (float)ct::cos2pi(M, R);
+  constexpr float s = (float)ct::sin2pi(M, R);
+  return make_float2(c, DIR > 0 ? s : -s);
+}
+
+template <int DIR, int M, int R>
+__device__ __forceinline__ float2 ctw_mul(float2 v) {
+  if constexpr ((M % R) == 0) {
+    return v;
+  } else {
+    return cmul(v, ctw<DIR, M, R>());
+  }
+}
+
+template <int R, int DIR>
+struct RegDft;
+
+template <int DIR>
+struct RegDft<1, DIR> {
+  __device__ __forceinline__ static void run(float2*) {}
+};
+template <int DIR>
+struct RegDft<2, DIR> {
+  __device__ __forceinline__ static void run(float2* v) { dft2<DIR>(v); }
+};
+template <int DIR>
+struct RegDft<3, DIR> {
+  __device__ __forceinline__ static void run(float2* v) { dft3<DIR>(v); }
+};
+template <int DIR>
+struct RegDft<4, DIR> {
+  __device__ __forceinline__ static void run(float2* v) { dft4<DIR>(v[0], v[1], v[2], v[3]); }
+};
+template <int DIR>
+struct RegDft<5, DIR> {
+  __device__ __forceinline__ static void run(float2* v) { dft5<DIR>(v); }
+};
+template <int DIR>
+struct RegDft<8, DIR> {
+  __device__ __forceinline__ static void run(float2* v) { dft8<DIR>(v); }
+};
+
+// R = A * B: X[kA + A kB] = sum_b W_B^(b kB) W_R^(b kA) sum_a v[B a + b] W_A^(a kA)
+template <int A, int B, int DIR>
+struct RegDftAB {
+  template <int b, int kA>
+  __device__ __forceinline__ static void twiddle_one(float2 (&u)[B][A]) {
+    u[b][kA] = ctw_mul<DIR, b * kA, A * B>(u[b][kA]);
+  }
+  template <int b, int... kA>
+  __device__ __forceinline__ static void twiddle_row(float2 (&u)[B][A], std::integer_sequence<int, kA...>) {
+    (twiddle_one<b, kA>(u), ...);
+  }
+  template <int... b>
+  __device__ __forceinline__ static void twiddle_all(float2 (&u)[B][A], std::integer_sequence<int, b...>) {
+    (twiddle_row<b>(u, std::make_integer_sequence<int, A>{}), ...);
+  }
+  __device__ __forceinline__ static void run(float2* v) {
+    float2 u[B][A];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+#pragma unroll
+      for (int a = 0; a < A; ++a) u[b][a] = v[B * a + b];
+      RegDft<A, DIR>::run(u[b]);
+    }
+    twiddle_all(u, std::make_integer_sequence<int, B>{});
+#pragma unroll
+    for (int kA = 0; kA < A; ++kA) {
+      float2 w[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) w[b] = u[b][kA];
+      RegDft<B, DIR>::run(w);
+#pragma unroll
+      for (int kB = 0; kB < B; ++kB) v[kA + A * kB] = w[kB];
+    }
+  }
+};
+
+template <int DIR>
+struct RegDft<6, DIR> : RegDftAB<2, 3, DIR> {};
+template <int DIR>
+struct RegDft<10, DIR> : RegDftAB<2, 5, DIR> {};
+template <int DIR>
+struct RegDft<12, DIR> : RegDftAB<4, 3, DIR> {};
+template <int DIR>
+struct RegDft<16, DIR> : RegDftAB<4, 4, DIR> {};
+
+// Per-lane twiddles of the 5 cross-lane DIT stages (forward sign):
+// stage s (span h = 2^s) uses exp(-2 pi i (l mod h) / (2h)) =
+// W32[(l mod h) * 16 / h].  Only upper lanes (bit h set) use them.
+struct LaneTwiddles {
+  float2 w[5];
+};
+
+// w32[m] = exp(-2 pi i m / 32), m in [0, 32) (block-cooperative).
+__device__ inline void build_w32(float2* w32) {
+  if (threadIdx.x < 32) {
+    double s, c;
+    sincospi(-(double)threadIdx.x / 16.0, &s, &c);
+    w32[threadIdx.x] = make_float2((float)c, (float)s);
+  }
+}
+
+__device__ __forceinline__ LaneTwiddles make_lane_twiddles(const float2* w32, int lane) {
+  LaneTwiddles t;
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 1 << s;
+    t.w[s] = (lane & h) ? w32[(lane & (h - 1)) * (16 >> s)] : make_float2(1.f, 0.f);
+  }
+  return t;
+}
+
+// Fill tab[k1 * 32 + l] = exp(-2 pi i brev5(l) k1 / n), k1 in [0, R) (block-cooperative).
+__device__ inline void build_reg_twiddles(float2* tab, int n) {
+  const int R = n / 32;
+  for (int e = threadIdx.x; e < R * 32; e += blockDim.x) {
+    const int k1 = e >> 5, l = e & 31;
+    double s, c;
+    sincospi(-2.0 * (double)(brev5(l) * k1) / (double)n, &s, &c);
+    tab[e] = make_float2((float)c, (float)s);
+  }
+}
+
+// Steps 2-4 on the lane's R values (step 1 input already loaded).
+// Cross-lane DIT butterfly: the upper lane pre-multiplies its value by the
+// stage twiddle (lower lanes hold w = 1), the pair exchanges values, then
+// lower = own + partner and upper = partner - own.
+template <int R, int DIR>
+__device__ __forceinline__ void warp_fft_reg(float2 (&x)[R], const float2* __restrict__ tab, const LaneTwiddles& lt,
+                                             int lane) {
+  RegDft<R, DIR>::run(x);
+#pragma unroll
+  for (int k1 = 1; k1 < R; ++k1) x[k1] = cmul(x[k1], twiddle<DIR>(tab, k1 * 32 + lane));
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int h = 1 << s;
+    const float sg = (lane & h) ? -1.f : 1.f;
+    const float2 w = DIR > 0 ? cconj(lt.w[s]) : lt.w[s];
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) {
+      float2 v = (s == 0) ? x[k1] : cmul(x[k1], w);
+      float2 p;
+      p.x = __shfl_xor_sync(0xffffffffu, v.x, h);
+      p.y = __shfl_xor_sync(0xffffffffu, v.y, h);
+      x[k1] = make_float2(fmaf(sg, v.x, p.x), fmaf(sg, v.y, p.y));
+    }
+  }
+}
+
+// Sizes the register FFT handles: n = 32 R with R in the list above.
+__host__ __device__ inline int reg_fft_radix(int n) {
+  if (n % 32 != 0) return 0;
+  const int R = n / 32;
+  switch (R) {
+    case 1: case 2: case 3: case 4: case 5: case 6: case 8: case 10: case 12: case 16:
+      return R;
+    default:
+      return 0;
+  }
 }
 
 }  // namespace cjx

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256)
     oy[s] = fmaf(r11, vy, by);
     oz[s] = fmaf(r21, vy, bz);
   }
-  sample_trilinear_batch<S>(grid, n, ox, oy, oz, act, wrap, g.fill, val);
+  sample_trilinear_batch_fast<S>(grid, n, ox, oy, oz, act, wrap, g.fill, val);
   float2* col = hbuf + ((size_t)blockIdx.z * g.nxh + u) * g.ldh;
 #pragma unroll
   for (int s = 0; s < S; ++s)
@@ -288,6 +288,199 @@ __global__ void __launch_bounds__(kWarps * 32)
 }
 
 // ---------------------------------------------------------------------------
+// Register-FFT forms of the three resize passes (n = 32 R sizes).  Same data
+// flow as the shared-memory Stockham kernels above; the transforms run in
+// registers with warp shuffles (cjx_fft.cuh) and shared memory only holds
+// twiddle tables and the transposes (padded layout pad16).
+// ---------------------------------------------------------------------------
+
+// Pass A (split): column inverse FFT + window of the gathered slice H.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colifft_window_reg(const float2* __restrict__ hbuf, float2* __restrict__ t1, SliceGeom g) {
+  constexpr int n = 32 * R;
+  constexpr int stride = pad16(n) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  int* winy = reinterpret_cast<int*>(bufs + kWarps * stride);
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  for (int m = threadIdx.x; m < g.py; m += blockDim.x) winy[m] = win_src(m, n, g.py, g.pad_left_y);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j0 = blockIdx.x * kWarps;
+  const int j = j0 + warp;
+  float2* buf = bufs + warp * stride;
+  if (j < g.nxh) {
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const float2* col = hbuf + ((size_t)blockIdx.y * g.nxh + j) * g.ldh;
+    const int bl = brev5(lane);
+    float2 x[R];
+    const bool sym = (j == 0) || (j == n / 2);
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) {
+      const int idx = 32 * n1 + bl;
+      float2 v = col[idx];
+      if (sym) {  // (S[v] + conj(S[-v])) / 2, as the irfftn of the reference sees it
+        const float2 m = col[idx == 0 ? 0 : n - idx];
+        v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
+      }
+      x[n1] = v;
+    }
+    warp_fft_reg<R, +1>(x, tab, lt, lane);
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+  }
+  __syncthreads();
+  const int ncols = min(kWarps, g.nxh - j0);
+  float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
+  for (int e = threadIdx.x; e < g.py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      const int src = winy[m];
+      dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? bufs[jj * stride + pad16(src)] : make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// Pass B: two rows per warp.  N-point inverse FFT of A + iB (register form,
+// R = RN), Px window, Px-point forward FFT (register form, RP), split.
+template <int RN, int RP>
+__device__ __forceinline__ void rows_pair_reg(const float2* __restrict__ rowA, const float2* __restrict__ rowB,
+                                              bool has_b, float2* __restrict__ outA, int ld2, float2* buf,
+                                              const float2* tabN, const float2* tabP, const LaneTwiddles& lt,
+                                              int lane, const int* winx) {
+  constexpr int n = 32 * RN, px = 32 * RP, h = n / 2;
+  const int bl = brev5(lane);
+  float2 z[RN];
+#pragma unroll
+  for (int n1 = 0; n1 < RN; ++n1) {
+    const int idx = 32 * n1 + bl;
+    if (idx == 0 || idx == h) {
+      const float2 A = rowA[idx];
+      const float2 B = has_b ? rowB[idx] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x, B.x);
+    } else if (idx < h) {
+      const float2 A = rowA[idx];
+      const float2 B = has_b ? rowB[idx] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x - B.y, A.y + B.x);
+    } else {
+      const float2 A = rowA[n - idx];
+      const float2 B = has_b ? rowB[n - idx] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x + B.y, B.x - A.y);
+    }
+  }
+  warp_fft_reg<RN, +1>(z, tabN, lt, lane);  // z = a + i b (the two real rows)
+#pragma unroll
+  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+  __syncwarp();
+  float2 w[RP];
+#pragma unroll
+  for (int n1 = 0; n1 < RP; ++n1) {
+    const int src = winx[32 * n1 + bl];
+    w[n1] = (src >= 0) ? buf[pad16(src)] : make_float2(0.f, 0.f);
+  }
+  __syncwarp();
+  warp_fft_reg<RP, -1>(w, tabP, lt, lane);
+#pragma unroll
+  for (int k1 = 0; k1 < RP; ++k1) buf[pad16(k1 + RP * lane)] = w[k1];
+  __syncwarp();
+  for (int k = lane; k <= px / 2; k += 32) {
+    const float2 Wk = buf[pad16(k)];
+    const float2 Wm = buf[pad16((px - k) % px)];
+    outA[k] = make_float2(0.5f * (Wk.x + Wm.x), 0.5f * (Wk.y - Wm.y));
+    if (has_b) outA[ld2 + k] = make_float2(0.5f * (Wk.y + Wm.y), -0.5f * (Wk.x - Wm.x));
+  }
+}
+
+template <int RN>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
+  constexpr int n = 32 * RN;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int px = g.px;
+  const int stride = pad16(max(n, px)) + 1;
+  float2* tabN = smem;
+  float2* tabP = tabN + n;
+  float2* bufs = tabP + px;
+  int* winx = reinterpret_cast<int*>(bufs + kWarps * stride);
+  build_reg_twiddles(tabN, n);
+  build_reg_twiddles(tabP, px);
+  build_w32(w32);
+  for (int m = threadIdx.x; m < px; m += blockDim.x) winx[m] = win_src(m, n, px, g.pad_left_x);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  if (ra >= g.py) return;
+  const bool has_b = (ra + 1) < g.py;
+  const float2* rowA = t1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
+  float2* outA = t2 + ((size_t)blockIdx.y * g.py + ra) * g.ld2;
+  float2* buf = bufs + warp * stride;
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  switch (rp) {
+#define CJX_ROWS_CASE(RPV) \
+  case RPV: rows_pair_reg<RN, RPV>(rowA, rowA + g.ld1, has_b, outA, g.ld2, buf, tabN, tabP, lt, lane, winx); break;
+    CJX_ROWS_CASE(1) CJX_ROWS_CASE(2) CJX_ROWS_CASE(3) CJX_ROWS_CASE(4) CJX_ROWS_CASE(5)
+    CJX_ROWS_CASE(6) CJX_ROWS_CASE(8) CJX_ROWS_CASE(10) CJX_ROWS_CASE(12) CJX_ROWS_CASE(16)
+#undef CJX_ROWS_CASE
+    default: break;
+  }
+}
+
+// Pass C: column forward FFT of T2 + epilogue.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colfft_epilogue_reg(const float2* __restrict__ t2, const cjx_image_params* __restrict__ params,
+                          const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0,
+                          float norm) {
+  constexpr int py = 32 * R;
+  constexpr int stride = pad16(py) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  float2* tab = smem;
+  float2* bufs = smem + py;
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.pxh - j0);
+  const float2* src = t2 + (size_t)blockIdx.y * py * g.ld2 + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld2 + jj];
+  }
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  const ImageConsts c = load_image_consts(params + img, norm);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) {
+    float2* buf = bufs + warp * stride;
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const int bl = brev5(lane);
+    float2 x[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(x, tab, lt, lane);
+    const int j = j0 + warp;
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) {
+      const int i = k1 + R * lane;
+      buf[pad16(i)] = apply_epilogue(x[k1], i, j, py, g.px, g.flags, c);
+    }
+  }
+  __syncthreads();
+  float2* dst = out + (size_t)img * py * g.pxh + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) dst[(size_t)m * g.pxh + jj] = bufs[jj * stride + pad16(m)];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // No-resize path: fused slice + epilogue, one thread per output pixel.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
@@ -329,6 +522,7 @@ static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py
 static std::atomic<int64_t> g_gather_ilp{2};
 static std::atomic<int64_t> g_chunk_bytes{256ll << 20};
 static std::atomic<int64_t> g_gather_mode{1};
+static std::atomic<int64_t> g_fft_mode{1};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -385,6 +579,7 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_GATHER_ILP) return g_gather_ilp.load();
   if (key == CJX_TUNE_CHUNK_BYTES) return g_chunk_bytes.load();
   if (key == CJX_TUNE_GATHER_MODE) return g_gather_mode.load();
+  if (key == CJX_TUNE_FFT_MODE) return g_fft_mode.load();
   return -1;
 }
 
@@ -402,6 +597,11 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_GATHER_MODE) {
     if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0 or 1");
     g_gather_mode = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_FFT_MODE) {
+    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "FFT mode must be 0 or 1");
+    g_fft_mode = value;
     return CJX_OK;
   }
   return fail(CJX_ERR_INVALID_ARGUMENT, "unknown tuning key");
@@ -453,6 +653,12 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   const int64_t ilp = g_gather_ilp.load();
   const bool split = g_gather_mode.load() == 1;
+  const int rn = reg_fft_radix(g.n), rpy = reg_fft_radix(g.py), rpx = reg_fft_radix(g.px);
+  const bool fast = g_fft_mode.load() == 1;
+  const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
+  const size_t sb_reg =
+      sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
+  const size_t sc_reg = sizeof(float2) * (size_t)(g.py + kWarps * (pad16(g.py) + 1));
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (split) {
@@ -466,7 +672,18 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
         k_gather_slice<1><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
       prof_end("k_gather_slice", stream);
       prof_begin(stream);
-      k_colifft_window<<<dim3((g.nxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sa, stream>>>(hb, t1, g);
+      const dim3 gc((g.nxh + kWarps - 1) / kWarps, cnt);
+      if (fast && rn) {
+        switch (rn) {
+#define CJX_A_CASE(R) \
+  case R: k_colifft_window_reg<R><<<gc, kWarps * 32, sa_reg, stream>>>(hb, t1, g); break;
+          CJX_A_CASE(1) CJX_A_CASE(2) CJX_A_CASE(3) CJX_A_CASE(4) CJX_A_CASE(5)
+          CJX_A_CASE(6) CJX_A_CASE(8) CJX_A_CASE(10) CJX_A_CASE(12) CJX_A_CASE(16)
+#undef CJX_A_CASE
+        }
+      } else {
+        k_colifft_window<<<gc, kWarps * 32, sa, stream>>>(hb, t1, g);
+      }
       prof_end("k_colifft_window", stream);
     } else {
       const dim3 ga((g.nxh + kWarps - 1) / kWarps, cnt);
@@ -480,11 +697,33 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
       prof_end("k_gather_colifft", stream);
     }
     prof_begin(stream);
-    k_rows_c2r_r2c<<<dim3((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, sb, stream>>>(t1, t2, g);
+    const dim3 gb((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt);
+    if (fast && rn && rpx) {
+      switch (rn) {
+#define CJX_B_CASE(R) \
+  case R: k_rows_reg<R><<<gb, kWarps * 32, sb_reg, stream>>>(t1, t2, g, rpx); break;
+        CJX_B_CASE(1) CJX_B_CASE(2) CJX_B_CASE(3) CJX_B_CASE(4) CJX_B_CASE(5)
+        CJX_B_CASE(6) CJX_B_CASE(8) CJX_B_CASE(10) CJX_B_CASE(12) CJX_B_CASE(16)
+#undef CJX_B_CASE
+      }
+    } else {
+      k_rows_c2r_r2c<<<gb, kWarps * 32, sb, stream>>>(t1, t2, g);
+    }
     prof_end("k_rows_c2r_r2c", stream);
     prof_begin(stream);
-    k_colfft_epilogue<<<dim3((g.pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, sc, stream>>>(t2, params, order, out,
-                                                                                             g, k0, norm);
+    const dim3 gcc((g.pxh + kWarps - 1) / kWarps, cnt);
+    if (fast && rpy) {
+      switch (rpy) {
+#define CJX_C_CASE(R) \
+  case R:             \
+    k_colfft_epilogue_reg<R><<<gcc, kWarps * 32, sc_reg, stream>>>(t2, params, order, out, g, k0, norm); break;
+        CJX_C_CASE(1) CJX_C_CASE(2) CJX_C_CASE(3) CJX_C_CASE(4) CJX_C_CASE(5)
+        CJX_C_CASE(6) CJX_C_CASE(8) CJX_C_CASE(10) CJX_C_CASE(12) CJX_C_CASE(16)
+#undef CJX_C_CASE
+      }
+    } else {
+      k_colfft_epilogue<<<gcc, kWarps * 32, sc, stream>>>(t2, params, order, out, g, k0, norm);
+    }
     prof_end("k_colfft_epilogue", stream);
   }
   return check_cuda(cudaGetLastError(), "forward launch");

@@ -159,15 +159,26 @@ CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void
                                           const cjx_image_params* params, const int32_t* order,
                                           int64_t n_images, void* out, void* stream);
 
+/* Batched complex-to-complex FFTs of `count` contiguous rows of n complex64
+ * values (direction -1: forward, numpy.fft.fft; +1: unnormalised inverse,
+ * n * numpy.fft.ifft), with the same warp FFTs the resize stage uses.  No
+ * counterpart in the reference (which calls jnp.fft); a utility and test
+ * hook.  in and out must not alias.                                        */
+CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t count,
+                        void* stream);
+
 /* Process-wide tuning knobs (no counterpart in the reference; set by the
  * autotuner).  CJX_TUNE_GATHER_ILP: samples whose corner loads one lane
  * issues together in the gather (1, 2 or 4).  CJX_TUNE_CHUNK_BYTES: target
  * workspace bytes per chunk when desc->images_per_chunk is 0.
  * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
- * column-FFT kernel, 0 = one fused gather + column-FFT kernel.              */
+ * column-FFT kernel, 0 = one fused gather + column-FFT kernel.
+ * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
+ * (R in 1-6, 8, 10, 12, 16), 0 = shared-memory Stockham FFTs everywhere.    */
 #define CJX_TUNE_GATHER_ILP 1
 #define CJX_TUNE_CHUNK_BYTES 2
 #define CJX_TUNE_GATHER_MODE 3
+#define CJX_TUNE_FFT_MODE 4
 CJX_API int cjx_tuning_set(int key, int64_t value);
 CJX_API int cjx_tuning_get(int key, int64_t* value);
 
