@@ -26,6 +26,7 @@ CJX_APPLY_CTF = 1 << 0
 CJX_APPLY_TRANSLATION = 1 << 1
 CJX_APPLY_ENVELOPE = 1 << 2
 CJX_ZERO_FILL_NEGATIVE = 1 << 3
+CJX_GRID_BRICKED = 1 << 4
 
 CJX_MAX_SIDE = 1024
 CJX_TUNE_GATHER_ILP = 1
@@ -105,6 +106,8 @@ _SIGNATURES = {
             ctypes.c_void_p,
         ],
     ),
+    "cjx_bricked_volume_size": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "cjx_brick_volume": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cjx_fft_c2c": (
         ctypes.c_int,
         [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
@@ -269,6 +272,25 @@ def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:
             _stream_ptr(stream),
         )
     )
+
+
+def bricked_volume_size(n: int) -> int:
+    out = ctypes.c_size_t(0)
+    _check(load_library().cjx_bricked_volume_size(int(n), ctypes.byref(out)))
+    return int(out.value)
+
+
+def brick_volume(grid, stream=None):
+    """Bricked copy (complex64, 1-D) of a complex64 [N, N, N] CUDA grid."""
+    import torch
+
+    n = grid.shape[0]
+    if grid.dtype != torch.complex64 or tuple(grid.shape) != (n, n, n):
+        raise ValueError("grid must be complex64 [N, N, N]")
+    out = torch.empty(bricked_volume_size(n) // 8, dtype=torch.complex64, device=grid.device)
+    _check(load_library().cjx_brick_volume(int(n), _cuda_ptr(grid, "grid"), _cuda_ptr(out, "bricked"),
+                                           _stream_ptr(stream)))
+    return out
 
 
 def fft_c2c(x, direction: int, out=None, stream=None):

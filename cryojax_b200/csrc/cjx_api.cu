@@ -16,6 +16,8 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
 int64_t tuning_get(int key);
 int tuning_set(int key, int64_t value);
 int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
+size_t bricked_elements(int n);
+int launch_brick_volume(int n, const float2* grid, float2* bricked, cudaStream_t stream);
 
 static thread_local std::string g_last_error;
 
@@ -72,6 +74,21 @@ int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cj
   }
   return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images, static_cast<float2*>(out),
                         workspace, chunk, static_cast<cudaStream_t>(stream));
+}
+
+int cjx_bricked_volume_size(int n, size_t* bytes) {
+  if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  if (n < 2 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE]");
+  *bytes = bricked_elements(n) * sizeof(float2);
+  return CJX_OK;
+}
+
+int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream) {
+  if (n < 2 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE]");
+  if (!grid || !bricked) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and bricked must be non-NULL");
+  if (grid == bricked) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and bricked must not alias");
+  return launch_brick_volume(n, static_cast<const float2*>(grid), static_cast<float2*>(bricked),
+                             static_cast<cudaStream_t>(stream));
 }
 
 int cjx_tuning_set(int key, int64_t value) { return tuning_set(key, value); }

@@ -160,18 +160,48 @@ __device__ __forceinline__ void sample_trilinear_batch(const float2* __restrict_
   }
 }
 
+// ---------------------------------------------------------------------------
+// Volume layouts.  The address of voxel (z, y, x) is ax(x) + ay(y) + az(z)
+// in complex elements.
+//  - LinearLayout: the reference's C-order [z][y][x] array.
+//  - BrickLayout: 8x8x8 blocks in C order; inside a block the 512 voxels are
+//    in Morton order (bit pattern z2 y2 x2 z1 y1 x1 z0 y0 x0), so every
+//    2x2x2 brick is 64 contiguous bytes and every 4x4x4 brick 512 bytes.
+//    A randomly oriented slice plane then touches compact clusters of
+//    voxels per DRAM burst and per cache line instead of x-runs.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int spread3(int v) { return (v & 1) | ((v & 2) << 2) | ((v & 4) << 4); }
+
+__host__ __device__ __forceinline__ int brick_blocks(int n) { return (n + 7) / 8; }
+
+struct LinearLayout {
+  int n, nn;
+  __host__ __device__ explicit LinearLayout(int n_) : n(n_), nn(n_ * n_) {}
+  __device__ __forceinline__ int ax(int i) const { return i; }
+  __device__ __forceinline__ int ay(int i) const { return i * n; }
+  __device__ __forceinline__ int az(int i) const { return i * nn; }
+};
+
+struct BrickLayout {
+  int sy, sz;  // block strides (elements) along y and z
+  __host__ __device__ explicit BrickLayout(int n) : sy(brick_blocks(n) * 512), sz(brick_blocks(n) * brick_blocks(n) * 512) {}
+  __device__ __forceinline__ int ax(int i) const { return ((i >> 3) << 9) + spread3(i & 7); }
+  __device__ __forceinline__ int ay(int i) const { return (i >> 3) * sy + (spread3(i & 7) << 1); }
+  __device__ __forceinline__ int az(int i) const { return (i >> 3) * sz + (spread3(i & 7) << 2); }
+};
+
 // Same result as sample_trilinear_batch with a fast path: when all 8 corners
 // of a sample are inside [0, N)^3 (every sample away from the cube faces)
 // they are read at base + {0, 1, N, N+1, N^2, ...} with 32-bit offsets and no
 // per-corner checks; samples near the faces take the general rule.
-template <int S>
-__device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __restrict__ grid, int n, const float* ox,
-                                                            const float* oy, const float* oz, const bool* active,
-                                                            bool wrap_negative, float2 fill, float2* out) {
+template <int S, typename Layout>
+__device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __restrict__ grid, int n, const Layout& L,
+                                                            const float* ox, const float* oy, const float* oz,
+                                                            const bool* active, bool wrap_negative, float2 fill,
+                                                            float2* out) {
   float2 v[S][8];
   float w[S][6];
   const int h = n / 2;
-  const int nn = n * n;
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const float fx = floorf(ox[s]), fy = floorf(oy[s]), fz = floorf(oz[s]);
@@ -182,16 +212,19 @@ __device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __rest
     const bool interior = (unsigned)ix0 < (unsigned)(n - 1) && (unsigned)iy0 < (unsigned)(n - 1) &&
                           (unsigned)iz0 < (unsigned)(n - 1);
     if (interior) {
-      const float2* p = grid + ((iz0 * n + iy0) * n + ix0);
       if (active[s]) {
-        v[s][0] = __ldg(p);
-        v[s][1] = __ldg(p + 1);
-        v[s][2] = __ldg(p + n);
-        v[s][3] = __ldg(p + n + 1);
-        v[s][4] = __ldg(p + nn);
-        v[s][5] = __ldg(p + nn + 1);
-        v[s][6] = __ldg(p + nn + n);
-        v[s][7] = __ldg(p + nn + n + 1);
+        const int x0 = L.ax(ix0), x1 = L.ax(ix0 + 1);
+        const int y0 = L.ay(iy0), y1 = L.ay(iy0 + 1);
+        const int z0 = L.az(iz0), z1 = L.az(iz0 + 1);
+        const int zy00 = z0 + y0, zy01 = z0 + y1, zy10 = z1 + y0, zy11 = z1 + y1;
+        v[s][0] = __ldg(grid + zy00 + x0);
+        v[s][1] = __ldg(grid + zy00 + x1);
+        v[s][2] = __ldg(grid + zy01 + x0);
+        v[s][3] = __ldg(grid + zy01 + x1);
+        v[s][4] = __ldg(grid + zy10 + x0);
+        v[s][5] = __ldg(grid + zy10 + x1);
+        v[s][6] = __ldg(grid + zy11 + x0);
+        v[s][7] = __ldg(grid + zy11 + x1);
       } else {
 #pragma unroll
         for (int c = 0; c < 8; ++c) v[s][c] = make_float2(0.f, 0.f);
@@ -205,7 +238,7 @@ __device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __rest
         const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
         const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
         const bool ok = active[s] && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
-        v[s][c] = ok ? __ldg(&grid[(iz * n + iy) * n + ix]) : fill;
+        v[s][c] = ok ? __ldg(&grid[L.az(iz) + L.ay(iy) + L.ax(ix)]) : fill;
       }
     }
   }
@@ -228,6 +261,8 @@ __device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __rest
 // ---------------------------------------------------------------------------
 struct ImageConsts {
   double inv_px;        // 1 / pixel_size
+  double qy_step;       // 1 / (py * pixel_size): qy = fftfreq index * qy_step
+  double qx_step;       // 1 / (px * pixel_size)
   double defocus;
   double half_astig;    // 0.5 * astigmatism
   double c_def;         // -0.5 * wavelength                (cycles per A^2 per A)
@@ -239,9 +274,12 @@ struct ImageConsts {
   float env_amp, env_quarter_b;
 };
 
-__device__ __forceinline__ ImageConsts load_image_consts(const cjx_image_params* __restrict__ p, float extra_scale) {
+__device__ __forceinline__ ImageConsts load_image_consts(const cjx_image_params* __restrict__ p, float extra_scale,
+                                                         int py, int px) {
   ImageConsts c;
   c.inv_px = 1.0 / p->pixel_size;
+  c.qy_step = c.inv_px / (double)py;
+  c.qx_step = c.inv_px / (double)px;
   c.defocus = p->defocus;
   c.half_astig = 0.5 * p->astigmatism;
   const double wl = p->wavelength;
@@ -278,15 +316,18 @@ __device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py,
   v.x *= c.scale;
   v.y *= c.scale;
   if (flags & (CJX_APPLY_CTF | CJX_APPLY_ENVELOPE | CJX_APPLY_TRANSLATION)) {
-    const double qy = (double)fft_index(i, py) / (double)py * c.inv_px;
-    const double qx = (double)j / (double)px * c.inv_px;
+    const double qy = (double)fft_index(i, py) * c.qy_step;
+    const double qx = (double)j * c.qx_step;
     const double k2 = qx * qx + qy * qy;
     if (flags & CJX_APPLY_CTF) {
+      // angle terms only scale the astigmatism (|astig| / 2 <~ 1e3 A), so
+      // single precision is ample for them
       float c2t = 1.0f, s2t = 0.0f;
       if (k2 > 0.0) {
-        const double inv = 1.0 / k2;
-        c2t = (float)((qy * qy - qx * qx) * inv);
-        s2t = (float)(2.0 * qx * qy * inv);
+        const float qxf = (float)qx, qyf = (float)qy;
+        const float inv = 1.0f / (float)k2;
+        c2t = (qyf * qyf - qxf * qxf) * inv;
+        s2t = 2.0f * qxf * qyf * inv;
       }
       const double df = c.defocus + c.half_astig * (double)(c2t * c.cos2a + s2t * c.sin2a);
       const double arg = (c.c_def * df + c.c_sph * k2) * k2 - c.phase_cycles;

@@ -27,10 +27,11 @@ namespace cjx {
 // ---------------------------------------------------------------------------
 // Pass A
 // ---------------------------------------------------------------------------
-template <int S>
+template <int S, typename Layout>
 __global__ void __launch_bounds__(kWarps * 32)
     k_gather_colifft(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
                      const int32_t* __restrict__ order, float2* __restrict__ t1, SliceGeom g, int64_t k0) {
+  const Layout L(g.n);
   extern __shared__ float2 smem[];
   const int n = g.n, h = n / 2;
   const int stride = 2 * n + 2;  // per-warp buffers (+2 to stagger banks)
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(kWarps * 32)
         oy[s] = fmaf(r11, vy, by);
         oz[s] = fmaf(r21, vy, bz);
       }
-      sample_trilinear_batch<S>(grid, n, ox, oy, oz, act, wrap, g.fill, val);
+      sample_trilinear_batch_fast<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
 #pragma unroll
       for (int s = 0; s < S; ++s)
         if (act[s]) a[i0 + 32 * s] = val[s];
@@ -109,10 +110,11 @@ __global__ void __launch_bounds__(kWarps * 32)
 // half-plane slice H[kx][ky] to an L2-resident buffer, then a column kernel
 // that runs the Hermitian fix, inverse FFT and window on H.
 // ---------------------------------------------------------------------------
-template <int S>
+template <int S, typename Layout>
 __global__ void __launch_bounds__(256)
     k_gather_slice(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
                    const int32_t* __restrict__ order, float2* __restrict__ hbuf, SliceGeom g, int64_t k0) {
+  const Layout L(g.n);
   const int n = g.n;
   const int64_t k = k0 + blockIdx.z;
   const int64_t img = order ? (int64_t)order[k] : k;
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(256)
     oy[s] = fmaf(r11, vy, by);
     oz[s] = fmaf(r21, vy, bz);
   }
-  sample_trilinear_batch_fast<S>(grid, n, ox, oy, oz, act, wrap, g.fill, val);
+  sample_trilinear_batch_fast<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
   float2* col = hbuf + ((size_t)blockIdx.z * g.nxh + u) * g.ldh;
 #pragma unroll
   for (int s = 0; s < S; ++s)
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   const int64_t k = k0 + blockIdx.y;
   const int64_t img = order ? (int64_t)order[k] : k;
-  const ImageConsts c = load_image_consts(params + img, norm);
+  const ImageConsts c = load_image_consts(params + img, norm, g.py, g.px);
   __syncthreads();
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   const int64_t k = k0 + blockIdx.y;
   const int64_t img = order ? (int64_t)order[k] : k;
-  const ImageConsts c = load_image_consts(params + img, norm);
+  const ImageConsts c = load_image_consts(params + img, norm, g.py, g.px);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < ncols) {
@@ -483,9 +485,11 @@ __global__ void __launch_bounds__(kWarps * 32)
 // ---------------------------------------------------------------------------
 // No-resize path: fused slice + epilogue, one thread per output pixel.
 // ---------------------------------------------------------------------------
+template <typename Layout>
 __global__ void __launch_bounds__(256)
     k_slice_direct(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
                    const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0) {
+  const Layout L(g.n);
   const int n = g.n, h = n / 2;
   const int64_t k = k0 + blockIdx.y;
   const int64_t img = order ? (int64_t)order[k] : k;
@@ -494,14 +498,16 @@ __global__ void __launch_bounds__(256)
   const float r10 = (float)R[3], r11 = (float)R[4];
   const float r20 = (float)R[6], r21 = (float)R[7];
   const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
-  const ImageConsts c = load_image_consts(params + img, 1.0f);
+  const ImageConsts c = load_image_consts(params + img, 1.0f, n, n);
   const int total = n * g.nxh;
   float2* dst = out + (size_t)img * total;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const int i = e / g.nxh, j = e - i * g.nxh;
     const float ux = (float)fft_index(j, n), vy = (float)fft_index(i, n);
-    float2 v = sample_trilinear(grid, n, fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux),
-                                fmaf(r21, vy, r20 * ux), wrap, g.fill);
+    const float ox = fmaf(r01, vy, r00 * ux), oy = fmaf(r11, vy, r10 * ux), oz = fmaf(r21, vy, r20 * ux);
+    const bool act = true;
+    float2 v;
+    sample_trilinear_batch_fast<1>(grid, n, L, &ox, &oy, &oz, &act, wrap, g.fill, &v);
     // convert_fftn_to_rfftn(mode="real")  (cryojax/ndimage/_fourier_utils.py:6-57)
     if ((n % 2 == 0) && ((i == h && j == 0) || (i == 0 && j == h) || (i == h && j == h))) v.y = 0.f;
     dst[e] = apply_epilogue(v, i, j, n, n, g.flags, c);
@@ -520,7 +526,7 @@ static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py
 
 // Process-wide tuning knobs (cjx_tuning_set / cjx_tuning_get).
 static std::atomic<int64_t> g_gather_ilp{2};
-static std::atomic<int64_t> g_chunk_bytes{256ll << 20};
+static std::atomic<int64_t> g_chunk_bytes{512ll << 20};
 static std::atomic<int64_t> g_gather_mode{1};
 static std::atomic<int64_t> g_fft_mode{1};
 
@@ -532,7 +538,8 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
     return fail(CJX_ERR_INVALID_ARGUMENT, "need n >= 2, py >= 1, px >= 2");
   if (d->n > CJX_MAX_SIDE || d->py > CJX_MAX_SIDE || d->px > CJX_MAX_SIDE)
     return fail(CJX_ERR_UNSUPPORTED, "volume side and image sides are limited to CJX_MAX_SIDE");
-  const uint32_t known = CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE;
+  const uint32_t known =
+      CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE | CJX_GRID_BRICKED;
   if (d->flags & ~known) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown flag bits");
   g->n = d->n;
   g->py = d->py;
@@ -618,9 +625,12 @@ static int ensure_smem_attrs() {
   if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
   int err = CJX_OK;
   std::call_once(flags[dev & 63], [&] {
-    cudaError_t e = allow_smem(k_gather_colifft<1>);
-    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<2>);
-    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<4>);
+    cudaError_t e = allow_smem(k_gather_colifft<1, LinearLayout>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<2, LinearLayout>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<4, LinearLayout>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<1, BrickLayout>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<2, BrickLayout>);
+    if (e == cudaSuccess) e = allow_smem(k_gather_colifft<4, BrickLayout>);
     if (e == cudaSuccess) e = allow_smem(k_colifft_window);
     if (e == cudaSuccess) e = allow_smem(k_rows_c2r_r2c);
     if (e == cudaSuccess) e = allow_smem(k_colfft_epilogue);
@@ -638,7 +648,10 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
       const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
       prof_begin(stream);
-      k_slice_direct<<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      if (g.flags & CJX_GRID_BRICKED)
+        k_slice_direct<BrickLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      else
+        k_slice_direct<LinearLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
       prof_end("k_slice_direct", stream);
     }
     return check_cuda(cudaGetLastError(), "k_slice_direct launch");
@@ -664,12 +677,20 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     if (split) {
       const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
-      if (ilp == 4)
-        k_gather_slice<4><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
-      else if (ilp == 2)
-        k_gather_slice<2><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
-      else
-        k_gather_slice<1><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+      const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
+#define CJX_GS(S)                                                                         \
+  if (bricked)                                                                            \
+    k_gather_slice<S, BrickLayout><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0); \
+  else                                                                                    \
+    k_gather_slice<S, LinearLayout><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+      if (ilp == 4) {
+        CJX_GS(4)
+      } else if (ilp == 2) {
+        CJX_GS(2)
+      } else {
+        CJX_GS(1)
+      }
+#undef CJX_GS
       prof_end("k_gather_slice", stream);
       prof_begin(stream);
       const dim3 gc((g.nxh + kWarps - 1) / kWarps, cnt);
@@ -688,12 +709,20 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     } else {
       const dim3 ga((g.nxh + kWarps - 1) / kWarps, cnt);
       prof_begin(stream);
-      if (ilp == 4)
-        k_gather_colifft<4><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
-      else if (ilp == 2)
-        k_gather_colifft<2><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
-      else
-        k_gather_colifft<1><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
+      const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
+#define CJX_GC(S)                                                                                     \
+  if (bricked)                                                                                        \
+    k_gather_colifft<S, BrickLayout><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0); \
+  else                                                                                                \
+    k_gather_colifft<S, LinearLayout><<<ga, kWarps * 32, sa, stream>>>(grid, params, order, t1, g, k0);
+      if (ilp == 4) {
+        CJX_GC(4)
+      } else if (ilp == 2) {
+        CJX_GC(2)
+      } else {
+        CJX_GC(1)
+      }
+#undef CJX_GC
       prof_end("k_gather_colifft", stream);
     }
     prof_begin(stream);
@@ -727,6 +756,39 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     prof_end("k_colfft_epilogue", stream);
   }
   return check_cuda(cudaGetLastError(), "forward launch");
+}
+
+// ---------------------------------------------------------------------------
+// Volume re-layout: C-order [z][y][x] -> BrickLayout (one-time preparation).
+// One thread per bricked element; elements beyond N on any axis are zero.
+// ---------------------------------------------------------------------------
+__global__ void k_brick_volume(const float2* __restrict__ grid, float2* __restrict__ bricked, int n, int nb) {
+  const int64_t total = (int64_t)nb * nb * nb * 512;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(e & 511);
+    const int64_t blk = e >> 9;
+    const int bx = (int)(blk % nb), by = (int)((blk / nb) % nb), bz = (int)(blk / ((int64_t)nb * nb));
+    // de-interleave the Morton index (x bits 0,3,6; y bits 1,4,7; z bits 2,5,8)
+    const int x = bx * 8 + ((w & 1) | ((w >> 2) & 2) | ((w >> 4) & 4));
+    const int y = by * 8 + (((w >> 1) & 1) | ((w >> 3) & 2) | ((w >> 5) & 4));
+    const int z = bz * 8 + (((w >> 2) & 1) | ((w >> 4) & 2) | ((w >> 6) & 4));
+    bricked[e] = (x < n && y < n && z < n) ? grid[((int64_t)z * n + y) * n + x] : make_float2(0.f, 0.f);
+  }
+}
+
+size_t bricked_elements(int n) {
+  const size_t nb = (size_t)brick_blocks(n);
+  return nb * nb * nb * 512;
+}
+
+int launch_brick_volume(int n, const float2* grid, float2* bricked, cudaStream_t stream) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  prof_begin(stream);
+  k_brick_volume<<<sms * 8, 256, 0, stream>>>(grid, bricked, n, brick_blocks(n));
+  prof_end("k_brick_volume", stream);
+  return check_cuda(cudaGetLastError(), "k_brick_volume launch");
 }
 
 // ---------------------------------------------------------------------------

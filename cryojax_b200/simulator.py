@@ -264,7 +264,7 @@ class FourierVoxelGridVolume:
     is generated in the kernel from the pose).
     """
 
-    def __init__(self, fourier_voxel_grid, rotation=None):
+    def __init__(self, fourier_voxel_grid, rotation=None, *, bricked=None):
         torch = _torch()
         g = fourier_voxel_grid
         if not isinstance(g, torch.Tensor):
@@ -273,6 +273,13 @@ class FourierVoxelGridVolume:
             raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
         self.fourier_voxel_grid = g
         self.rotation = rotation  # AbstractPose attached by rotate_to_pose
+        self._bricked = bricked   # device re-layout for the gather (built on first use)
+
+    def bricked_grid(self):
+        """The grid in the library's bricked layout (cached; same values)."""
+        if self._bricked is None:
+            self._bricked = nat.brick_volume(self.fourier_voxel_grid.contiguous())
+        return self._bricked
 
     @property
     def shape(self):
@@ -316,7 +323,9 @@ class FourierVoxelGridVolume:
         if inverse:
             pose = QuaternionPose(*np.moveaxis(pose.offset_in_angstroms[..., :2], -1, 0),
                                   wxyz=rot.quat_inverse(pose.quaternion()))
-        return FourierVoxelGridVolume(self.fourier_voxel_grid, rotation=pose)
+        if self._bricked is None and self.fourier_voxel_grid.is_cuda:
+            self.bricked_grid()
+        return FourierVoxelGridVolume(self.fourier_voxel_grid, rotation=pose, bricked=self._bricked)
 
     def get_representation(self, rng_key=None):
         return self
@@ -436,7 +445,7 @@ class FourierSliceExtraction:
     is_projection_approximation = True
 
     def __init__(self, *, outputs_integral: bool = True, correction_mask=None, out_of_bounds_mode: str = "fill",
-                 fill_value: complex = 0.0 + 0.0j):
+                 fill_value: complex = 0.0 + 0.0j, use_bricked_layout: bool = True):
         if correction_mask is not None:
             raise NotImplementedError("correction_mask is not implemented on the device")
         if out_of_bounds_mode not in ("fill", "zero_fill_negative"):
@@ -445,6 +454,7 @@ class FourierSliceExtraction:
         self.correction_mask = None
         self.out_of_bounds_mode = out_of_bounds_mode
         self.fill_value = complex(fill_value)
+        self.use_bricked_layout = use_bricked_layout
 
     def _base_flags(self):
         return nat.CJX_ZERO_FILL_NEGATIVE if self.out_of_bounds_mode == "zero_fill_negative" else 0
@@ -461,6 +471,9 @@ class FourierSliceExtraction:
         torch = _torch()
         grid = volume.fourier_voxel_grid
         n_vol = grid.shape[0]
+        if self.use_bricked_layout and grid.is_cuda:
+            grid = volume.bricked_grid()
+            flags = flags | nat.CJX_GRID_BRICKED
         if image_config.pad_mode != "constant":
             raise NotImplementedError("only constant padding is implemented on the device")
         py, px = image_config.padded_shape

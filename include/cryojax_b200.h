@@ -59,6 +59,9 @@ extern "C" {
  * `.at[].get(mode="fill")` wraps negative indices once); offered for
  * comparison only.                                                        */
 #define CJX_ZERO_FILL_NEGATIVE (1u << 3)
+/* `grid` is in the bricked layout written by cjx_brick_volume instead of
+ * the reference's C-order array.                                          */
+#define CJX_GRID_BRICKED (1u << 4)
 
 /* ---- per-image parameters (one record per image, device memory) ------
  * 32 doubles (256 bytes).  Built on the host from a pose, a CTF and an
@@ -158,6 +161,17 @@ CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
 CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void* grid,
                                           const cjx_image_params* params, const int32_t* order,
                                           int64_t n_images, void* out, void* stream);
+
+/* Bricked volume layout (no counterpart in the reference; a device-side
+ * re-layout of FourierVoxelGridVolume.fourier_voxel_grid).  8x8x8 blocks in
+ * C order; inside a block the voxels are in Morton order, so every 2x2x2
+ * brick is 64 contiguous bytes.  A slice plane at any orientation then reads
+ * compact voxel clusters per DRAM burst.  Sides are padded to a multiple of
+ * 8 with zeros (never read: indices >= N are out of bounds).
+ * cjx_bricked_volume_size: bytes of the bricked copy of an N^3 grid.
+ * cjx_brick_volume: write it (stream-ordered; grid and bricked distinct).  */
+CJX_API int cjx_bricked_volume_size(int n, size_t* bytes);
+CJX_API int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream);
 
 /* Batched complex-to-complex FFTs of `count` contiguous rows of n complex64
  * values (direction -1: forward, numpy.fft.fft; +1: unnormalised inverse,

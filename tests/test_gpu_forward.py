@@ -149,6 +149,43 @@ def test_processing_order_and_gather_ilp_are_invisible(cuda_device, ilp, mode):
     assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
 
 
+@pytest.mark.parametrize("box,pad_scale,shape", [(32, 2.0, (32, 32)), (31, 2.0, (31, 31)), (32, 1.3, (30, 30)),
+                                                  (32, 2.0, (64, 64)), (25, 1.0, (25, 25))])
+def test_linear_and_bricked_layouts_match_oracle(cuda_device, box, pad_scale, shape):
+    from cryojax_b200 import simulator as S
+
+    vol, grid, fs = make_volume(box, 60, seed=box + 3, pad_scale=pad_scale)
+    specs = random_specs(4, seed=box + 5, shape=shape)
+    ref = _oracle(grid, fs, specs)
+    for bricked in (False, True):
+        got = _run_model(grid, specs, integrator_kw=dict(use_bricked_layout=bricked))
+        assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL, bricked
+
+
+def test_brick_volume_layout(cuda_device):
+    """cjx_brick_volume places voxel (z, y, x) at its Morton-in-block address."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    n = 21
+    g = (np.arange(n**3, dtype=np.float32) + 1j * np.arange(n**3, dtype=np.float32)[::-1]).reshape(n, n, n)
+    b = nat.brick_volume(torch.as_tensor(g.astype(np.complex64)).cuda()).cpu().numpy()
+    nb = (n + 7) // 8
+    assert b.size == nb**3 * 512
+
+    def spread(v):
+        return (v & 1) | ((v & 2) << 2) | ((v & 4) << 4)
+
+    rng = np.random.default_rng(0)
+    for z, y, x in rng.integers(0, n, size=(200, 3)):
+        addr = ((z // 8) * nb + (y // 8)) * nb * 512 + (x // 8) * 512 + spread(x % 8) + (spread(y % 8) << 1) + (
+            spread(z % 8) << 2)
+        assert b[addr] == g[z, y, x]
+    # every voxel of g is nonzero; the padding of the last blocks is zero
+    assert np.count_nonzero(b) == n**3
+
+
 def test_simulate_real_space_matches_oracle(cuda_device):
     from cryojax_b200 import simulator as S
 
