@@ -33,6 +33,7 @@ CJX_TUNE_GATHER_ILP = 1
 CJX_TUNE_CHUNK_BYTES = 2
 CJX_TUNE_GATHER_MODE = 3
 CJX_TUNE_FFT_MODE = 4
+CJX_TUNE_GATHER_TILE = 5
 PARAMS_DOUBLES = 32  # sizeof(cjx_image_params) / 8
 
 # field offsets (in doubles) of cjx_image_params

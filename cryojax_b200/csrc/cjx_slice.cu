@@ -110,7 +110,23 @@ __global__ void __launch_bounds__(kWarps * 32)
 // half-plane slice H[kx][ky] to an L2-resident buffer, then a column kernel
 // that runs the Hermitian fix, inverse FFT and window on H.
 // ---------------------------------------------------------------------------
-template <int S, typename Layout>
+// Lane -> sample mapping inside a CTA's 16 x 16 patch of the plane (MAP):
+//   0: each warp 2 columns x 16 rows, 1: 4 x 8, 2: 8 x 4.
+template <int MAP>
+__device__ __forceinline__ void gather_lane_offsets(int warp, int lane, int& du, int& dv) {
+  if constexpr (MAP == 0) {
+    du = 2 * warp + (lane >> 4);
+    dv = lane & 15;
+  } else if constexpr (MAP == 1) {
+    du = 4 * (warp & 3) + (lane & 3);
+    dv = 8 * (warp >> 2) + (lane >> 2);
+  } else {
+    du = 8 * (warp & 1) + (lane & 7);
+    dv = 4 * (warp >> 1) + (lane >> 3);
+  }
+}
+
+template <int S, typename Layout, int MAP>
 __global__ void __launch_bounds__(256)
     k_gather_slice(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
                    const int32_t* __restrict__ order, float2* __restrict__ hbuf, SliceGeom g, int64_t k0) {
@@ -123,11 +139,13 @@ __global__ void __launch_bounds__(256)
   const float r10 = (float)R[3], r11 = (float)R[4];
   const float r20 = (float)R[6], r21 = (float)R[7];
   const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
-  // CTA patch: 16 columns x 16*S rows; a warp covers 2 columns x 16 rows per step
+  // CTA patch: 16 columns x 16*S rows, S sample rows 16 apart per thread
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * 16 + warp * 2 + (lane >> 4);
+  int du, dv;
+  gather_lane_offsets<MAP>(warp, lane, du, dv);
+  const int u = blockIdx.x * 16 + du;
   if (u >= g.nxh) return;
-  const int vbase = blockIdx.y * (16 * S) + (lane & 15);
+  const int vbase = blockIdx.y * (16 * S) + dv;
   const float ux = (float)fft_index(u, n);
   const float bx = r00 * ux, by = r10 * ux, bz = r20 * ux;
   float ox[S], oy[S], oz[S];
@@ -529,6 +547,7 @@ static std::atomic<int64_t> g_gather_ilp{2};
 static std::atomic<int64_t> g_chunk_bytes{512ll << 20};
 static std::atomic<int64_t> g_gather_mode{1};
 static std::atomic<int64_t> g_fft_mode{1};
+static std::atomic<int64_t> g_gather_tile{1};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -587,6 +606,7 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_CHUNK_BYTES) return g_chunk_bytes.load();
   if (key == CJX_TUNE_GATHER_MODE) return g_gather_mode.load();
   if (key == CJX_TUNE_FFT_MODE) return g_fft_mode.load();
+  if (key == CJX_TUNE_GATHER_TILE) return g_gather_tile.load();
   return -1;
 }
 
@@ -609,6 +629,11 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_FFT_MODE) {
     if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "FFT mode must be 0 or 1");
     g_fft_mode = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_GATHER_TILE) {
+    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather tile must be 0, 1 or 2");
+    g_gather_tile = value;
     return CJX_OK;
   }
   return fail(CJX_ERR_INVALID_ARGUMENT, "unknown tuning key");
@@ -678,11 +703,20 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
       const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
       const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
-#define CJX_GS(S)                                                                         \
-  if (bricked)                                                                            \
-    k_gather_slice<S, BrickLayout><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0); \
-  else                                                                                    \
-    k_gather_slice<S, LinearLayout><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+      const int64_t map = g_gather_tile.load();
+#define CJX_GSM(S, M)                                                                               \
+  if (bricked)                                                                                      \
+    k_gather_slice<S, BrickLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);  \
+  else                                                                                              \
+    k_gather_slice<S, LinearLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
+#define CJX_GS(S)       \
+  if (map == 1) {       \
+    CJX_GSM(S, 1)       \
+  } else if (map == 2) { \
+    CJX_GSM(S, 2)       \
+  } else {              \
+    CJX_GSM(S, 0)       \
+  }
       if (ilp == 4) {
         CJX_GS(4)
       } else if (ilp == 2) {
@@ -691,6 +725,7 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
         CJX_GS(1)
       }
 #undef CJX_GS
+#undef CJX_GSM
       prof_end("k_gather_slice", stream);
       prof_begin(stream);
       const dim3 gc((g.nxh + kWarps - 1) / kWarps, cnt);
