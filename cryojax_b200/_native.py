@@ -65,6 +65,21 @@ class SliceDesc(ctypes.Structure):
     ]
 
 
+class SliceGroup(ctypes.Structure):
+    _fields_ = [
+        ("desc", SliceDesc),
+        ("grid", ctypes.c_void_p),
+        ("params", ctypes.c_void_p),
+        ("order", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("n_images", ctypes.c_int64),
+        ("tuning_valid", ctypes.c_int32),
+        ("gather_ilp", ctypes.c_int32),
+        ("gather_tile", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class CryojaxB200Error(RuntimeError):
     """Raised when a C-ABI entry point returns a nonzero status."""
 
@@ -94,6 +109,14 @@ _SIGNATURES = {
             ctypes.c_size_t,
             ctypes.c_void_p,
         ],
+    ),
+    "cjx_slice_ctf_multi_workspace_size": (
+        ctypes.c_int,
+        [ctypes.POINTER(SliceGroup), ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)],
+    ),
+    "cjx_slice_ctf_forward_multi": (
+        ctypes.c_int,
+        [ctypes.POINTER(SliceGroup), ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
     "cjx_slice_ctf_forward_noalloc": (
         ctypes.c_int,
@@ -237,6 +260,40 @@ def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream
             _stream_ptr(stream),
         )
     )
+
+
+def make_groups(groups):
+    """ctypes array of SliceGroup from dicts with desc, grid, params, order, out, tuning."""
+    arr = (SliceGroup * len(groups))()
+    for i, g in enumerate(groups):
+        arr[i].desc = g["desc"]
+        arr[i].grid = g["grid"].data_ptr() if g.get("grid") is not None else 0
+        arr[i].params = g["params"].data_ptr() if g.get("params") is not None else 0
+        arr[i].order = g["order"].data_ptr() if g.get("order") is not None else 0
+        arr[i].out = g["out"].data_ptr() if g.get("out") is not None else 0
+        arr[i].n_images = int(g["n_images"])
+        tun = g.get("tuning")
+        if tun:
+            arr[i].tuning_valid = 1
+            arr[i].gather_ilp = int(tun["ilp"])
+            arr[i].gather_tile = int(tun["tile"])
+    return arr
+
+
+def multi_workspace_size(groups_arr) -> int:
+    out = ctypes.c_size_t(0)
+    _check(load_library().cjx_slice_ctf_multi_workspace_size(groups_arr, len(groups_arr), ctypes.byref(out)))
+    return int(out.value)
+
+
+def slice_ctf_forward_multi(groups_arr, workspace=None, stream=None) -> None:
+    ws_ptr = ctypes.c_void_p(0)
+    ws_bytes = 0
+    if workspace is not None:
+        ws_ptr = _cuda_ptr(workspace, "workspace")
+        ws_bytes = workspace.numel() * workspace.element_size()
+    _check(load_library().cjx_slice_ctf_forward_multi(groups_arr, len(groups_arr), ws_ptr, ws_bytes,
+                                                      _stream_ptr(stream)))
 
 
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CJX_NOALLOC_SCRATCH_BYTES

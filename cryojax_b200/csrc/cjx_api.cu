@@ -1,6 +1,7 @@
 // extern "C" entry points of libcryojax_b200 (declared in include/cryojax_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 
 #include "cjx_common.cuh"
@@ -12,7 +13,8 @@ bool needs_resize(const SliceGeom& g);
 size_t workspace_per_image(const SliceGeom& g);
 int64_t default_chunk(const SliceGeom& g, int64_t n_images);
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream);
+                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
+                   const Tuning& tn);
 int64_t tuning_get(int key);
 int tuning_set(int key, int64_t value);
 int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
@@ -73,7 +75,71 @@ int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cj
       return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_workspace_size()");
   }
   return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images, static_cast<float2*>(out),
-                        workspace, chunk, static_cast<cudaStream_t>(stream));
+                        workspace, chunk, static_cast<cudaStream_t>(stream), current_tuning());
+}
+
+static int group_plan(const cjx_slice_group& gr, SliceGeom* g, int64_t* chunk, size_t* need) {
+  if (int e = make_geom(&gr.desc, g)) return e;
+  if (gr.n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "group n_images < 0");
+  *chunk = needs_resize(*g) ? chunk_for(*g, &gr.desc, gr.n_images) : 0;
+  *need = needs_resize(*g) ? (size_t)*chunk * workspace_per_image(*g) : 0;
+  return CJX_OK;
+}
+
+int cjx_slice_ctf_multi_workspace_size(const cjx_slice_group* groups, int n_groups, size_t* bytes) {
+  if (!bytes || (!groups && n_groups > 0) || n_groups < 0)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "need groups, n_groups >= 0 and bytes");
+  size_t mx = 0;
+  for (int i = 0; i < n_groups; ++i) {
+    SliceGeom g;
+    int64_t chunk;
+    size_t need;
+    if (int e = group_plan(groups[i], &g, &chunk, &need)) return e;
+    mx = std::max(mx, need);
+  }
+  *bytes = mx;
+  return CJX_OK;
+}
+
+int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  if ((!groups && n_groups > 0) || n_groups < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "need groups, n_groups >= 0");
+  // validate every group before launching anything
+  for (int i = 0; i < n_groups; ++i) {
+    const cjx_slice_group& gr = groups[i];
+    SliceGeom g;
+    int64_t chunk;
+    size_t need;
+    if (int e = group_plan(gr, &g, &chunk, &need)) return e;
+    if (gr.n_images > 0 && (!gr.grid || !gr.params || !gr.out))
+      return fail(CJX_ERR_INVALID_ARGUMENT, "group grid, params and out must be non-NULL");
+    if (need && (!workspace || workspace_bytes < need))
+      return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_multi_workspace_size()");
+    if (gr.tuning_valid) {
+      if (gr.gather_ilp != 1 && gr.gather_ilp != 2 && gr.gather_ilp != 4)
+        return fail(CJX_ERR_INVALID_ARGUMENT, "group gather_ilp must be 1, 2 or 4");
+      if (gr.gather_tile < 0 || gr.gather_tile > 2)
+        return fail(CJX_ERR_INVALID_ARGUMENT, "group gather_tile must be 0, 1 or 2");
+    }
+  }
+  const Tuning base = current_tuning();
+  for (int i = 0; i < n_groups; ++i) {
+    const cjx_slice_group& gr = groups[i];
+    if (gr.n_images == 0) continue;
+    SliceGeom g;
+    int64_t chunk;
+    size_t need;
+    group_plan(gr, &g, &chunk, &need);
+    Tuning tn = base;
+    if (gr.tuning_valid) {
+      tn.ilp = gr.gather_ilp;
+      tn.tile = gr.gather_tile;
+    }
+    if (int e = launch_forward(g, static_cast<const float2*>(gr.grid), gr.params, gr.order, gr.n_images,
+                               static_cast<float2*>(gr.out), workspace, chunk, static_cast<cudaStream_t>(stream), tn))
+      return e;
+  }
+  return CJX_OK;
 }
 
 int cjx_bricked_volume_size(int n, size_t* bytes) {

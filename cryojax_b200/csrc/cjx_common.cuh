@@ -360,6 +360,17 @@ __device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py,
 }
 
 // ---------------------------------------------------------------------------
+// Per-call kernel choices (process defaults come from cjx_tuning_set)
+// ---------------------------------------------------------------------------
+struct Tuning {
+  int ilp;          // samples per gather lane issued together (1, 2, 4)
+  int tile;         // gather lane tile (0, 1, 2)
+  int gather_mode;  // 1 = separate gather kernel, 0 = fused gather + column FFT
+  int fft_mode;     // 1 = register FFTs where possible
+};
+Tuning current_tuning();
+
+// ---------------------------------------------------------------------------
 // Host-side error plumbing
 // ---------------------------------------------------------------------------
 void set_last_error(const std::string& msg);

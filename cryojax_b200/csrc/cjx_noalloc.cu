@@ -27,7 +27,8 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g);
 bool needs_resize(const SliceGeom& g);
 size_t workspace_per_image(const SliceGeom& g);
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream);
+                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
+                   const Tuning& tn);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CJX_NOALLOC_SCRATCH_BYTES];
 
@@ -66,7 +67,7 @@ extern "C" int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const v
   if (!grid || !params || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params and out must be non-NULL");
   if (!needs_resize(g))  // the fused no-resize kernel uses no scratch
     return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images,
-                          static_cast<float2*>(out), nullptr, 0, static_cast<cudaStream_t>(stream));
+                          static_cast<float2*>(out), nullptr, 0, static_cast<cudaStream_t>(stream), current_tuning());
   const size_t per = workspace_per_image(g);
   if (per > CJX_NOALLOC_SCRATCH_BYTES)
     return fail(CJX_ERR_UNSUPPORTED, "one image needs more scratch than CJX_NOALLOC_SCRATCH_BYTES");
@@ -80,5 +81,5 @@ extern "C" int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const v
   void* scratch = nullptr;
   if (int e = noalloc_scratch(&scratch)) return e;
   return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images, static_cast<float2*>(out),
-                        scratch, chunk, static_cast<cudaStream_t>(stream));
+                        scratch, chunk, static_cast<cudaStream_t>(stream), current_tuning());
 }

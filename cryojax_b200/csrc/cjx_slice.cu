@@ -664,8 +664,14 @@ static int ensure_smem_attrs() {
   return err;
 }
 
+Tuning current_tuning() {
+  return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
+                (int)g_fft_mode.load()};
+}
+
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream) {
+                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
+                   const Tuning& tn) {
   if (n_images == 0) return CJX_OK;
   if (!needs_resize(g)) {
     const int total = g.n * g.nxh;
@@ -689,10 +695,10 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
   float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
-  const int64_t ilp = g_gather_ilp.load();
-  const bool split = g_gather_mode.load() == 1;
+  const int64_t ilp = tn.ilp;
+  const bool split = tn.gather_mode == 1;
   const int rn = reg_fft_radix(g.n), rpy = reg_fft_radix(g.py), rpx = reg_fft_radix(g.px);
-  const bool fast = g_fft_mode.load() == 1;
+  const bool fast = tn.fft_mode == 1;
   const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
   const size_t sb_reg =
       sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
@@ -703,7 +709,7 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
       const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
       const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
-      const int64_t map = g_gather_tile.load();
+      const int64_t map = tn.tile;
 #define CJX_GSM(S, M)                                                                               \
   if (bricked)                                                                                      \
     k_gather_slice<S, BrickLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);  \

@@ -142,6 +142,32 @@ CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
                                   int64_t n_images, void* out, void* workspace,
                                   size_t workspace_bytes, void* stream);
 
+/* ---- several volumes / image shapes in one call ----------------------- */
+typedef struct cjx_slice_group {
+  cjx_slice_desc desc;             /* geometry and flags of this group        */
+  const void* grid;                /* device, this group's volume             */
+  const cjx_image_params* params;  /* device, n_images records                */
+  const int32_t* order;            /* device processing order or NULL         */
+  void* out;                       /* device complex64 [n_images][Py][Px/2+1] */
+  int64_t n_images;
+  int32_t tuning_valid;            /* 0: process defaults (cjx_tuning_set)     */
+  int32_t gather_ilp;              /* 1, 2 or 4 when tuning_valid              */
+  int32_t gather_tile;             /* 0, 1 or 2 when tuning_valid              */
+  int32_t reserved;
+} cjx_slice_group;
+
+/* Workspace for cjx_slice_ctf_forward_multi: the largest group's need (the
+ * groups run one after another on the stream and share it).                */
+CJX_API int cjx_slice_ctf_multi_workspace_size(const cjx_slice_group* groups, int n_groups,
+                                               size_t* bytes);
+/* cjx_slice_ctf_forward for each group in turn on one stream, with per-group
+ * kernel choices (from the autotuner).  All groups are validated before any
+ * launch.  Replaces eqx.filter_vmap(simulate) over batches whose volumes and
+ * image shapes differ, which the reference runs as separate traces.  The
+ * whole call can be captured into one CUDA graph.                          */
+CJX_API int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
 /* Allocation-free variant of cjx_slice_ctf_forward.  No counterpart in the
  * reference.  For callers that cannot allocate device memory, because the
  * runtime hosting them owns every allocation (for example an XLA custom call
