@@ -110,6 +110,26 @@ _SIGNATURES = {
             ctypes.c_void_p,
         ],
     ),
+    "cjx_slice_ctf_loss_workspace_size": (
+        ctypes.c_int,
+        [ctypes.POINTER(SliceDesc), ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)],
+    ),
+    "cjx_slice_ctf_loss_grad": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(SliceDesc),
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_int64,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_size_t,
+            ctypes.c_void_p,
+        ],
+    ),
     "cjx_slice_ctf_multi_workspace_size": (
         ctypes.c_int,
         [ctypes.POINTER(SliceGroup), ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)],
@@ -260,6 +280,36 @@ def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream
             _stream_ptr(stream),
         )
     )
+
+
+GRAD_DOUBLES = 16  # sizeof(cjx_image_grads) / 8
+G_LOSS, G_TX, G_TY, G_DF, G_ROT = 0, 1, 2, 3, 4
+
+
+def loss_workspace_size(desc: SliceDesc, n_images: int) -> int:
+    out = ctypes.c_size_t(0)
+    _check(load_library().cjx_slice_ctf_loss_workspace_size(ctypes.byref(desc), int(n_images), ctypes.byref(out)))
+    return int(out.value)
+
+
+def slice_ctf_loss_grad(desc: SliceDesc, grid, params, observed, image_grads, grid_grad=None, workspace=None,
+                        stream=None, order=None) -> None:
+    """cjx_slice_ctf_loss_grad on torch CUDA tensors."""
+    import torch
+
+    n = params.shape[0]
+    if image_grads.dtype != torch.float64 or tuple(image_grads.shape) != (n, GRAD_DOUBLES):
+        raise ValueError("image_grads must be float64 [n_images, 16]")
+    if observed.dtype != torch.complex64:
+        raise ValueError("observed must be complex64")
+    gg = ctypes.c_void_p(0) if grid_grad is None else _cuda_ptr(grid_grad, "grid_grad")
+    ws_ptr = _cuda_ptr(workspace, "workspace") if workspace is not None else ctypes.c_void_p(0)
+    ws_bytes = workspace.numel() * workspace.element_size() if workspace is not None else 0
+    _check(
+        load_library().cjx_slice_ctf_loss_grad(
+            ctypes.byref(desc), _cuda_ptr(grid, "grid"), _cuda_ptr(params, "params"), _order_ptr(order, n), int(n),
+            _cuda_ptr(observed, "observed"), _cuda_ptr(image_grads, "image_grads"), gg, ws_ptr, ws_bytes,
+            _stream_ptr(stream)))
 
 
 def make_groups(groups):

@@ -1,0 +1,544 @@
+// Squared-residual loss and its adjoint (reverse mode) for the resize path.
+//
+// Loss per image: L = sum over real-space pixels of (x - obs)^2, where x is
+// the simulated image (irfftn of the Fourier image F, as simulate() returns
+// it with padded_shape == shape) and obs the observed image.  With O =
+// rfftn(obs) and F_h = F with its kx = 0 and kx = Px/2 columns made
+// Hermitian (what irfftn actually reads), Parseval gives
+//   L = 1/(Py Px) sum_half w_j |F_h - O|^2,   w_j = 1 (j = 0, Px/2), else 2.
+// The adjoint runs the forward passes in reverse with their transposes:
+//   k_colfft_loss_adj   column FFT (forward), epilogue, loss, E = dL/dF,
+//                       d/d(shift, defocus), g_X = conj(multiplier) E, then
+//                       the column inverse FFT (adjoint of the forward FFT);
+//   k_rows_adj          per row: adjoint of r2c_Px, of the Px window, of the
+//                       unnormalised c2r_N;
+//   k_colfft_adj        per column: adjoint of the Py window, forward FFT
+//                       (adjoint of the unnormalised inverse), Hermitian fix
+//                       of kx = 0, N/2 (self-adjoint);
+//   k_scatter_slice     trilinear scatter-add of the slice gradient into the
+//                       grid gradient (float2 atomics) and d/dR from the
+//                       derivative of the interpolation weights.
+// The gradient of a real loss w.r.t. a complex value z is reported as
+// dL/dRe z + i dL/dIm z (jax.grad returns its complex conjugate).
+#include <algorithm>
+#include <mutex>
+
+#include "cjx_common.cuh"
+#include "cjx_profile.cuh"
+
+namespace cjx {
+
+// Per-image gradient record (16 doubles), matches cjx_image_grads.
+constexpr int kGradLoss = 0, kGradTx = 1, kGradTy = 2, kGradDf = 3, kGradRot = 4;
+
+// Multiplier of pass C's epilogue and its defocus derivative at (i, j):
+// F = mult * X, dF/d(defocus) = dmult * X (X = unnormalised column FFT).
+struct EpiTerms {
+  float2 mult, dmult;
+  double qx, qy;
+};
+
+__device__ __forceinline__ EpiTerms epilogue_terms(int i, int j, int py, int px, uint32_t flags,
+                                                   const ImageConsts& c, double wavelength) {
+  EpiTerms t;
+  t.qy = (double)fft_index(i, py) * c.qy_step;
+  t.qx = (double)j * c.qx_step;
+  const double k2 = t.qx * t.qx + t.qy * t.qy;
+  float m = c.scale, dm = 0.f;
+  if (flags & CJX_APPLY_CTF) {
+    float c2t = 1.0f, s2t = 0.0f;
+    if (k2 > 0.0) {
+      const float qxf = (float)t.qx, qyf = (float)t.qy;
+      const float inv = 1.0f / (float)k2;
+      c2t = (qyf * qyf - qxf * qxf) * inv;
+      s2t = 2.0f * qxf * qyf * inv;
+    }
+    const double df = c.defocus + c.half_astig * (double)(c2t * c.cos2a + s2t * c.sin2a);
+    const double arg = (c.c_def * df + c.c_sph * k2) * k2 - c.phase_cycles;
+    const float r = (float)(arg - rint(arg));
+    float sn, cs;
+    sincospif(2.0f * r, &sn, &cs);
+    dm = c.scale * cs * (float)(-3.14159265358979323846 * wavelength * k2);  // d chi / d df = -pi lambda k^2
+    m = c.scale * sn;
+  }
+  if (flags & CJX_APPLY_ENVELOPE) {
+    const float e = c.env_amp * expf(-c.env_quarter_b * (float)k2);
+    m *= e;
+    dm *= e;
+  }
+  t.mult = make_float2(m, 0.f);
+  t.dmult = make_float2(dm, 0.f);
+  if (flags & CJX_APPLY_TRANSLATION) {
+    const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
+    const bool self_conj = (ey && i == py / 2 && j == 0) || (ex && i == 0 && j == px / 2) ||
+                           (ey && ex && i == py / 2 && j == px / 2);
+    if (self_conj) {
+      t.mult = make_float2(0.f, 0.f);
+      t.dmult = make_float2(0.f, 0.f);
+    } else {
+      const double ph = t.qx * c.tx + t.qy * c.ty;
+      const float r = (float)(ph - rint(ph));
+      float s, co;
+      sincospif(2.0f * r, &s, &co);
+      const float2 p = make_float2(co, -s);
+      t.mult = make_float2(m * p.x, m * p.y);
+      t.dmult = make_float2(dm * p.x, dm * p.y);
+    }
+  }
+  return t;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Loss + column kernel (adjoint of pass C).  t2 holds T2 on entry and the
+// gradient g_T2 on exit (each CTA reads and writes only its own columns).
+// ---------------------------------------------------------------------------
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colfft_loss_adj(float2* __restrict__ t2, const float2* __restrict__ obs, const cjx_image_params* __restrict__ params,
+                      const int32_t* __restrict__ order, double* __restrict__ grads, SliceGeom g, int64_t k0,
+                      float norm) {
+  constexpr int py = 32 * R;
+  constexpr int stride = pad16(py) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  __shared__ float red[kWarps][4];
+  float2* tab = smem;
+  float2* bufs = smem + py;                  // T2 columns, then F, then g_X
+  float2* obuf = bufs + kWarps * stride;     // observed columns
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.pxh - j0);
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  float2* col0 = t2 + (size_t)blockIdx.y * py * g.ld2 + j0;
+  const float2* ocol0 = obs + (size_t)img * py * g.pxh + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      bufs[jj * stride + pad16(m)] = col0[(size_t)m * g.ld2 + jj];
+      obuf[jj * stride + pad16(m)] = ocol0[(size_t)m * g.pxh + jj];
+    }
+  }
+  const ImageConsts c = load_image_consts(params + img, norm, g.py, g.px);
+  const double wl = params[img].wavelength;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float sl = 0.f, stx = 0.f, sty = 0.f, sdf = 0.f;
+  if (warp < ncols) {
+    float2* buf = bufs + warp * stride;
+    const float2* ob = obuf + warp * stride;
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const int bl = brev5(lane);
+    const int j = j0 + warp;
+    float2 x[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(x, tab, lt, lane);  // x[k1] = X[k1 + R lane]
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) {
+      const int i = k1 + R * lane;
+      const EpiTerms et = epilogue_terms(i, j, py, g.px, g.flags, c, wl);
+      buf[pad16(i)] = cmul(et.mult, x[k1]);
+    }
+    __syncwarp();
+    const bool self_col = (j == 0) || ((g.px % 2 == 0) && j == g.px / 2);
+    const float wj = self_col ? 1.f : 2.f;
+    const float inv_pp = 1.0f / ((float)py * (float)g.px);
+    float2 gx[R];
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) {
+      const int i = k1 + R * lane;
+      const EpiTerms et = epilogue_terms(i, j, py, g.px, g.flags, c, wl);
+      const float2 f = buf[pad16(i)];
+      float2 fh = f;
+      if (self_col) {
+        const float2 fm = buf[pad16(i == 0 ? 0 : py - i)];
+        fh = make_float2(0.5f * (f.x + fm.x), 0.5f * (f.y - fm.y));
+      }
+      const float2 o = ob[pad16(i)];
+      const float2 d = make_float2(fh.x - o.x, fh.y - o.y);
+      sl += wj * inv_pp * (d.x * d.x + d.y * d.y);
+      const float2 E = make_float2(2.f * wj * inv_pp * d.x, 2.f * wj * inv_pp * d.y);
+      // z = conj(E) F ; dL/dt = 2 pi q Im(z)
+      const float zim = E.x * f.y - E.y * f.x;
+      stx += 6.283185307179586f * (float)et.qx * zim;
+      sty += 6.283185307179586f * (float)et.qy * zim;
+      // dL/ddf = Re(conj(E) dmult X)
+      const float2 dfx = cmul(et.dmult, x[k1]);
+      sdf += E.x * dfx.x + E.y * dfx.y;
+      // g_X = conj(mult) E
+      gx[k1] = cmul(cconj(et.mult), E);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = gx[k1];
+    __syncwarp();
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
+    __syncwarp();
+    warp_fft_reg<R, +1>(x, tab, lt, lane);  // adjoint of the forward column FFT
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+  }
+  sl = warp_sum(sl);
+  stx = warp_sum(stx);
+  sty = warp_sum(sty);
+  sdf = warp_sum(sdf);
+  if (lane == 0) {
+    red[warp][0] = sl;
+    red[warp][1] = stx;
+    red[warp][2] = sty;
+    red[warp][3] = sdf;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (int w = 0; w < kWarps; ++w) acc += (double)red[w][threadIdx.x];
+    atomicAdd(&grads[img * 16 + threadIdx.x], acc);
+  }
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) col0[(size_t)m * g.ld2 + jj] = bufs[jj * stride + pad16(m)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row adjoint (transpose of pass B).  g_T2 rows -> g_T1 rows.
+// ---------------------------------------------------------------------------
+template <int RN, int RP>
+__device__ __forceinline__ void rows_pair_adj(const float2* __restrict__ gA, const float2* __restrict__ gB, bool has_b,
+                                              float2* __restrict__ outA, int ld1, float2* buf, const float2* tabN,
+                                              const float2* tabP, const LaneTwiddles& lt, int lane, const int* invx) {
+  constexpr int n = 32 * RN, px = 32 * RP, hp = px / 2, h = n / 2;
+  const int bl = brev5(lane);
+  // adjoint of r2c_Px: Z = half spectrum with interior bins halved, DC / Nyquist real
+  float2 z[RP];
+#pragma unroll
+  for (int n1 = 0; n1 < RP; ++n1) {
+    const int k = 32 * n1 + bl;
+    if (k == 0 || k == hp) {
+      const float2 A = gA[k];
+      const float2 B = has_b ? gB[k] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x, B.x);
+    } else if (k < hp) {
+      const float2 A = gA[k];
+      const float2 B = has_b ? gB[k] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(0.5f * (A.x - B.y), 0.5f * (A.y + B.x));
+    } else {
+      const float2 A = gA[px - k];
+      const float2 B = has_b ? gB[px - k] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(0.5f * (A.x + B.y), 0.5f * (B.x - A.y));
+    }
+  }
+  warp_fft_reg<RP, +1>(z, tabP, lt, lane);  // real rows a + i b (length Px)
+#pragma unroll
+  for (int k1 = 0; k1 < RP; ++k1) buf[pad16(k1 + RP * lane)] = z[k1];
+  __syncwarp();
+  // adjoint of the Px window: place sample m at src(m), zeros elsewhere
+  float2 y[RN];
+#pragma unroll
+  for (int n1 = 0; n1 < RN; ++n1) {
+    const int m = invx[32 * n1 + bl];
+    y[n1] = (m >= 0) ? buf[pad16(m)] : make_float2(0.f, 0.f);
+  }
+  __syncwarp();
+  warp_fft_reg<RN, -1>(y, tabN, lt, lane);  // adjoint of the unnormalised inverse
+#pragma unroll
+  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = y[k1];
+  __syncwarp();
+  // split A + iB and apply the c2r weights (interior x2, DC / Nyquist real)
+  for (int kk = lane; kk <= h; kk += 32) {
+    const float2 Wk = buf[pad16(kk)];
+    const float2 Wm = buf[pad16((n - kk) % n)];
+    float2 a = make_float2(0.5f * (Wk.x + Wm.x), 0.5f * (Wk.y - Wm.y));
+    float2 b = make_float2(0.5f * (Wk.y + Wm.y), -0.5f * (Wk.x - Wm.x));
+    if (kk == 0 || kk == h) {
+      a.y = 0.f;
+      b.y = 0.f;
+    } else {
+      a = make_float2(2.f * a.x, 2.f * a.y);
+      b = make_float2(2.f * b.x, 2.f * b.y);
+    }
+    outA[kk] = a;
+    if (has_b) outA[ld1 + kk] = b;
+  }
+}
+
+template <int RN>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_rows_adj(const float2* __restrict__ gt2, float2* __restrict__ gt1, SliceGeom g, int rp) {
+  constexpr int n = 32 * RN;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int px = g.px;
+  const int stride = pad16(max(n, px)) + 1;
+  float2* tabN = smem;
+  float2* tabP = tabN + n;
+  float2* bufs = tabP + px;
+  int* invx = reinterpret_cast<int*>(bufs + kWarps * stride);
+  build_reg_twiddles(tabN, n);
+  build_reg_twiddles(tabP, px);
+  build_w32(w32);
+  for (int q = threadIdx.x; q < n; q += blockDim.x) invx[q] = -1;
+  __syncthreads();
+  for (int m = threadIdx.x; m < px; m += blockDim.x) {
+    const int s = win_src(m, n, px, g.pad_left_x);
+    if (s >= 0) invx[s] = m;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  if (ra >= g.py) return;
+  const bool has_b = (ra + 1) < g.py;
+  const float2* gA = gt2 + ((size_t)blockIdx.y * g.py + ra) * g.ld2;
+  float2* outA = gt1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
+  float2* buf = bufs + warp * stride;
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  switch (rp) {
+#define CJX_RA_CASE(RPV) \
+  case RPV: rows_pair_adj<RN, RPV>(gA, gA + g.ld2, has_b, outA, g.ld1, buf, tabN, tabP, lt, lane, invx); break;
+    CJX_RA_CASE(1) CJX_RA_CASE(2) CJX_RA_CASE(3) CJX_RA_CASE(4) CJX_RA_CASE(5)
+    CJX_RA_CASE(6) CJX_RA_CASE(8) CJX_RA_CASE(10) CJX_RA_CASE(12) CJX_RA_CASE(16)
+#undef CJX_RA_CASE
+    default: break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column adjoint (transpose of pass A's FFT + window).  g_T1 -> g_H.
+// ---------------------------------------------------------------------------
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colfft_adj(const float2* __restrict__ gt1, float2* __restrict__ gh, SliceGeom g) {
+  constexpr int n = 32 * R;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int stride = pad16(max(n, g.py)) + 1;
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  int* invy = reinterpret_cast<int*>(bufs + kWarps * stride);
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  for (int q = threadIdx.x; q < n; q += blockDim.x) invy[q] = -1;
+  __syncthreads();
+  for (int m = threadIdx.x; m < g.py; m += blockDim.x) {
+    const int s = win_src(m, n, g.py, g.pad_left_y);
+    if (s >= 0) invy[s] = m;
+  }
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.nxh - j0);
+  const float2* src = gt1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
+  for (int e = threadIdx.x; e < g.py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld1 + jj];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = j0 + warp;
+  if (j < g.nxh) {
+    float2* buf = bufs + warp * stride;
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const int bl = brev5(lane);
+    float2 y[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) {
+      const int m = invy[32 * n1 + bl];
+      y[n1] = (m >= 0) ? buf[pad16(m)] : make_float2(0.f, 0.f);
+    }
+    __syncwarp();
+    warp_fft_reg<R, -1>(y, tab, lt, lane);
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = y[k1];
+    __syncwarp();
+    float2* col = gh + ((size_t)blockIdx.y * g.nxh + j) * g.ldh;
+    const bool sym = (j == 0) || (j == n / 2);
+    for (int i = lane; i < n; i += 32) {
+      float2 v = buf[pad16(i)];
+      if (sym) {
+        const float2 m = buf[pad16(i == 0 ? 0 : n - i)];
+        v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
+      }
+      col[i] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Trilinear scatter-add of the slice gradient and d/dR.
+// ---------------------------------------------------------------------------
+template <typename Layout>
+__global__ void __launch_bounds__(256)
+    k_scatter_slice(const float2* __restrict__ grid, const float2* __restrict__ gh,
+                    const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
+                    float2* __restrict__ grad_grid, double* __restrict__ grads, SliceGeom g, int64_t k0) {
+  const Layout L(g.n);
+  __shared__ float red[8][6];
+  const int n = g.n, h = n / 2;
+  const int64_t k = k0 + blockIdx.z;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  const double* Rm = params[img].rot;
+  const float r00 = (float)Rm[0], r01 = (float)Rm[1];
+  const float r10 = (float)Rm[3], r11 = (float)Rm[4];
+  const float r20 = (float)Rm[6], r21 = (float)Rm[7];
+  const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int du, dv;
+  gather_lane_offsets<1>(warp, lane, du, dv);
+  const int u = blockIdx.x * 16 + du;
+  const int v = blockIdx.y * 16 + dv;
+  float gr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (u < g.nxh && v < n) {
+    const float2 gs = gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v];
+    const float ux = (float)fft_index(u, n), vy = (float)fft_index(v, n);
+    const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    const AxisNodes ax = axis_nodes(o[0], n, wrap);
+    const AxisNodes ay = axis_nodes(o[1], n, wrap);
+    const AxisNodes az = axis_nodes(o[2], n, wrap);
+    float dH[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // dH/do_axis (complex)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+      const bool ok = (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
+      const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
+      const float wx = dx ? ax.w1 : ax.w0, wy = dy ? ay.w1 : ay.w0, wz = dz ? az.w1 : az.w0;
+      const float2 val = ok ? __ldg(&grid[L.az(iz) + L.ay(iy) + L.ax(ix)]) : g.fill;
+      const float sx = dx ? 1.f : -1.f, sy = dy ? 1.f : -1.f, sz = dz ? 1.f : -1.f;
+      const float gwx = sx * wy * wz, gwy = sy * wx * wz, gwz = sz * wx * wy;
+      dH[0][0] += gwx * val.x; dH[0][1] += gwx * val.y;
+      dH[1][0] += gwy * val.x; dH[1][1] += gwy * val.y;
+      dH[2][0] += gwz * val.x; dH[2][1] += gwz * val.y;
+      if (ok && grad_grid) {
+        const float w = (wz * wy) * wx;
+        atomicAdd(&grad_grid[((size_t)iz * n + iy) * n + ix], make_float2(w * gs.x, w * gs.y));
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float dLdo = gs.x * dH[a][0] + gs.y * dH[a][1];
+      gr[2 * a] = dLdo * ux;
+      gr[2 * a + 1] = dLdo * vy;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) gr[q] = warp_sum(gr[q]);
+  if (lane == 0)
+    for (int q = 0; q < 6; ++q) red[warp][q] = gr[q];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double acc = 0.0;
+    for (int w = 0; w < 8; ++w) acc += (double)red[w][threadIdx.x];
+    atomicAdd(&grads[img * 16 + kGradRot + threadIdx.x], acc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launcher
+// ---------------------------------------------------------------------------
+int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                         int64_t k0, int cnt, float2* t1, float2* t2, float2* hb, cudaStream_t stream,
+                         const Tuning& tn);
+
+template <typename K>
+static cudaError_t allow_smem_adj(K kernel) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+static int ensure_adjoint_smem_attrs() {
+  static std::once_flag flags[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
+  int err = CJX_OK;
+  std::call_once(flags[dev & 63], [&] {
+    cudaError_t e = cudaSuccess;
+#define CJX_ADJ_ATTR(R)                                                    \
+  if (e == cudaSuccess) e = allow_smem_adj(k_colfft_loss_adj<R>);          \
+  if (e == cudaSuccess) e = allow_smem_adj(k_rows_adj<R>);                 \
+  if (e == cudaSuccess) e = allow_smem_adj(k_colfft_adj<R>);
+    CJX_ADJ_ATTR(1) CJX_ADJ_ATTR(2) CJX_ADJ_ATTR(3) CJX_ADJ_ATTR(4) CJX_ADJ_ATTR(5)
+    CJX_ADJ_ATTR(6) CJX_ADJ_ATTR(8) CJX_ADJ_ATTR(10) CJX_ADJ_ATTR(12) CJX_ADJ_ATTR(16)
+#undef CJX_ADJ_ATTR
+    if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
+  });
+  return err;
+}
+
+__global__ void k_zero_doubles(double* p, int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = 0.0;
+}
+
+int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                     int64_t n_images, const float2* obs, double* grads, float2* grad_grid, void* workspace,
+                     int64_t chunk, cudaStream_t stream, const Tuning& tn) {
+  const int rn = reg_fft_radix(g.n), rpy = reg_fft_radix(g.py), rpx = reg_fft_radix(g.px);
+  if (!rn || !rpy || !rpx)
+    return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs N, Py, Px = 32 R with R in {1-6, 8, 10, 12, 16}");
+  prof_begin(stream);
+  k_zero_doubles<<<64, 256, 0, stream>>>(grads, n_images * 16);
+  prof_end("k_zero_doubles", stream);
+  float2* t1 = static_cast<float2*>(workspace);
+  float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
+  float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
+  const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
+  const size_t s_loss = sizeof(float2) * (size_t)(g.py + 2 * kWarps * (pad16(g.py) + 1));
+  const size_t s_rows = sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) +
+                        sizeof(int) * (size_t)g.n;
+  const size_t s_cols = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(std::max(g.n, g.py)) + 1)) +
+                        sizeof(int) * (size_t)g.n;
+  if (s_loss > 227 * 1024 || s_rows > 227 * 1024 || s_cols > 227 * 1024)
+    return fail(CJX_ERR_UNSUPPORTED, "loss gradient shared-memory footprint above 227 KB for these sizes");
+  if (int e = ensure_adjoint_smem_attrs()) return e;
+  const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
+  for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
+    if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
+    prof_begin(stream);
+    const dim3 gl((g.pxh + kWarps - 1) / kWarps, cnt);
+    switch (rpy) {
+#define CJX_L_CASE(R) \
+  case R: k_colfft_loss_adj<R><<<gl, kWarps * 32, s_loss, stream>>>(t2, obs, params, order, grads, g, k0, norm); break;
+      CJX_L_CASE(1) CJX_L_CASE(2) CJX_L_CASE(3) CJX_L_CASE(4) CJX_L_CASE(5)
+      CJX_L_CASE(6) CJX_L_CASE(8) CJX_L_CASE(10) CJX_L_CASE(12) CJX_L_CASE(16)
+#undef CJX_L_CASE
+    }
+    prof_end("k_colfft_loss_adj", stream);
+    prof_begin(stream);
+    const dim3 gr((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt);
+    switch (rn) {
+#define CJX_RB_CASE(R) \
+  case R: k_rows_adj<R><<<gr, kWarps * 32, s_rows, stream>>>(t2, t1, g, rpx); break;
+      CJX_RB_CASE(1) CJX_RB_CASE(2) CJX_RB_CASE(3) CJX_RB_CASE(4) CJX_RB_CASE(5)
+      CJX_RB_CASE(6) CJX_RB_CASE(8) CJX_RB_CASE(10) CJX_RB_CASE(12) CJX_RB_CASE(16)
+#undef CJX_RB_CASE
+    }
+    prof_end("k_rows_adj", stream);
+    prof_begin(stream);
+    const dim3 gc((g.nxh + kWarps - 1) / kWarps, cnt);
+    switch (rn) {
+#define CJX_CA_CASE(R) \
+  case R: k_colfft_adj<R><<<gc, kWarps * 32, s_cols, stream>>>(t1, hb, g); break;
+      CJX_CA_CASE(1) CJX_CA_CASE(2) CJX_CA_CASE(3) CJX_CA_CASE(4) CJX_CA_CASE(5)
+      CJX_CA_CASE(6) CJX_CA_CASE(8) CJX_CA_CASE(10) CJX_CA_CASE(12) CJX_CA_CASE(16)
+#undef CJX_CA_CASE
+    }
+    prof_end("k_colfft_adj", stream);
+    prof_begin(stream);
+    const dim3 gs((g.nxh + 15) / 16, (g.n + 15) / 16, cnt);
+    if (bricked)
+      k_scatter_slice<BrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    else
+      k_scatter_slice<LinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    prof_end("k_scatter_slice", stream);
+  }
+  return check_cuda(cudaGetLastError(), "loss gradient launch");
+}
+
+}  // namespace cjx

@@ -16,6 +16,9 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
                    int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
                    const Tuning& tn);
 int64_t tuning_get(int key);
+int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                     int64_t n_images, const float2* obs, double* grads, float2* grad_grid, void* workspace,
+                     int64_t chunk, cudaStream_t stream, const Tuning& tn);
 int tuning_set(int key, int64_t value);
 int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
 size_t bricked_elements(int n);
@@ -155,6 +158,34 @@ int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream) {
   if (grid == bricked) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and bricked must not alias");
   return launch_brick_volume(n, static_cast<const float2*>(grid), static_cast<float2*>(bricked),
                              static_cast<cudaStream_t>(stream));
+}
+
+int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_images, size_t* bytes) {
+  if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
+  SliceGeom g;
+  if (int e = make_geom(desc, &g)) return e;
+  if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
+  *bytes = (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g);
+  return CJX_OK;
+}
+
+int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const cjx_image_params* params,
+                            const int32_t* order, int64_t n_images, const void* observed, double* image_grads,
+                            void* grid_grad, void* workspace, size_t workspace_bytes, void* stream) {
+  SliceGeom g;
+  if (int e = make_geom(desc, &g)) return e;
+  if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
+  if (n_images == 0) return CJX_OK;
+  if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
+  if (!grid || !params || !observed || !image_grads)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");
+  const int64_t chunk = chunk_for(g, desc, n_images);
+  if (!workspace || workspace_bytes < (size_t)chunk * workspace_per_image(g))
+    return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_loss_workspace_size()");
+  return launch_loss_grad(g, static_cast<const float2*>(grid), params, order, n_images,
+                          static_cast<const float2*>(observed), image_grads, static_cast<float2*>(grid_grad),
+                          workspace, chunk, static_cast<cudaStream_t>(stream), current_tuning());
 }
 
 int cjx_tuning_set(int key, int64_t value) { return tuning_set(key, value); }

@@ -256,6 +256,22 @@ __device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __rest
   }
 }
 
+// Lane -> sample mapping inside a CTA's 16 x 16 patch of the plane (MAP):
+//   0: each warp 2 columns x 16 rows, 1: 4 x 8, 2: 8 x 4.
+template <int MAP>
+__device__ __forceinline__ void gather_lane_offsets(int warp, int lane, int& du, int& dv) {
+  if constexpr (MAP == 0) {
+    du = 2 * warp + (lane >> 4);
+    dv = lane & 15;
+  } else if constexpr (MAP == 1) {
+    du = 4 * (warp & 3) + (lane & 3);
+    dv = 8 * (warp >> 2) + (lane >> 2);
+  } else {
+    du = 8 * (warp & 1) + (lane & 7);
+    dv = 4 * (warp >> 1) + (lane >> 3);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Epilogue: scale, CTF, envelope, translation
 // ---------------------------------------------------------------------------

@@ -110,22 +110,6 @@ __global__ void __launch_bounds__(kWarps * 32)
 // half-plane slice H[kx][ky] to an L2-resident buffer, then a column kernel
 // that runs the Hermitian fix, inverse FFT and window on H.
 // ---------------------------------------------------------------------------
-// Lane -> sample mapping inside a CTA's 16 x 16 patch of the plane (MAP):
-//   0: each warp 2 columns x 16 rows, 1: 4 x 8, 2: 8 x 4.
-template <int MAP>
-__device__ __forceinline__ void gather_lane_offsets(int warp, int lane, int& du, int& dv) {
-  if constexpr (MAP == 0) {
-    du = 2 * warp + (lane >> 4);
-    dv = lane & 15;
-  } else if constexpr (MAP == 1) {
-    du = 4 * (warp & 3) + (lane & 3);
-    dv = 8 * (warp >> 2) + (lane >> 2);
-  } else {
-    du = 8 * (warp & 1) + (lane & 7);
-    dv = 4 * (warp >> 1) + (lane >> 3);
-  }
-}
-
 template <int S, typename Layout, int MAP>
 __global__ void __launch_bounds__(256)
     k_gather_slice(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
@@ -664,47 +648,20 @@ static int ensure_smem_attrs() {
   return err;
 }
 
-Tuning current_tuning() {
-  return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
-                (int)g_fft_mode.load()};
-}
-
-int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
-                   const Tuning& tn) {
-  if (n_images == 0) return CJX_OK;
-  if (!needs_resize(g)) {
-    const int total = g.n * g.nxh;
-    const int blocks = std::min((total + 255) / 256, 1024);
-    for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
-      const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
-      prof_begin(stream);
-      if (g.flags & CJX_GRID_BRICKED)
-        k_slice_direct<BrickLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
-      else
-        k_slice_direct<LinearLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
-      prof_end("k_slice_direct", stream);
-    }
-    return check_cuda(cudaGetLastError(), "k_slice_direct launch");
-  }
+// Passes up to T2 (gather, column inverse FFT + window, rows) for one chunk of
+// `cnt` images starting at processing index k0.
+int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                         int64_t k0, int cnt, float2* t1, float2* t2, float2* hb, cudaStream_t stream,
+                         const Tuning& tn) {
   if (int e = ensure_smem_attrs()) return e;
-  const size_t sa = smem_a(g), sb = smem_b(g), sc = smem_c(g);
-  if (sa > 227 * 1024 || sb > 227 * 1024 || sc > 227 * 1024)
-    return fail(CJX_ERR_UNSUPPORTED, "shared-memory footprint exceeds 227 KB for these sizes");
-  float2* t1 = static_cast<float2*>(workspace);
-  float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
-  float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
-  const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   const int64_t ilp = tn.ilp;
   const bool split = tn.gather_mode == 1;
-  const int rn = reg_fft_radix(g.n), rpy = reg_fft_radix(g.py), rpx = reg_fft_radix(g.px);
+  const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
   const bool fast = tn.fft_mode == 1;
+  const size_t sa = smem_a(g), sb = smem_b(g);
   const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
   const size_t sb_reg =
       sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
-  const size_t sc_reg = sizeof(float2) * (size_t)(g.py + kWarps * (pad16(g.py) + 1));
-  for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
-    const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (split) {
       const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
@@ -780,6 +737,46 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
       k_rows_c2r_r2c<<<gb, kWarps * 32, sb, stream>>>(t1, t2, g);
     }
     prof_end("k_rows_c2r_r2c", stream);
+  return check_cuda(cudaGetLastError(), "forward launch");
+}
+
+Tuning current_tuning() {
+  return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
+                (int)g_fft_mode.load()};
+}
+
+int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                   int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
+                   const Tuning& tn) {
+  if (n_images == 0) return CJX_OK;
+  if (!needs_resize(g)) {
+    const int total = g.n * g.nxh;
+    const int blocks = std::min((total + 255) / 256, 1024);
+    for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
+      const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
+      prof_begin(stream);
+      if (g.flags & CJX_GRID_BRICKED)
+        k_slice_direct<BrickLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      else
+        k_slice_direct<LinearLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      prof_end("k_slice_direct", stream);
+    }
+    return check_cuda(cudaGetLastError(), "k_slice_direct launch");
+  }
+  if (int e = ensure_smem_attrs()) return e;
+  const size_t sa = smem_a(g), sb = smem_b(g), sc = smem_c(g);
+  if (sa > 227 * 1024 || sb > 227 * 1024 || sc > 227 * 1024)
+    return fail(CJX_ERR_UNSUPPORTED, "shared-memory footprint exceeds 227 KB for these sizes");
+  float2* t1 = static_cast<float2*>(workspace);
+  float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
+  float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
+  const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
+  const int rpy = reg_fft_radix(g.py);
+  const bool fast = tn.fft_mode == 1;
+  const size_t sc_reg = sizeof(float2) * (size_t)(g.py + kWarps * (pad16(g.py) + 1));
+  for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
+    if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
     prof_begin(stream);
     const dim3 gcc((g.pxh + kWarps - 1) / kWarps, cnt);
     if (fast && rpy) {

@@ -142,6 +142,42 @@ CJX_API int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid,
                                   int64_t n_images, void* out, void* workspace,
                                   size_t workspace_bytes, void* stream);
 
+/* ---- squared-residual loss and gradients (reverse mode) -------------- */
+/* Per-image result record (16 doubles, device memory).                    */
+typedef struct cjx_image_grads {
+  double loss;        /* sum over pixels of (x - obs)^2                      */
+  double d_shift_x;   /* dL / d shift_x   (Angstrom^-1)                      */
+  double d_shift_y;
+  double d_defocus;   /* dL / d defocus (the mean defocus incl. offset_z)    */
+  double d_rot[6];    /* dL / dR[i][j] for j = 0, 1 (the columns that span
+                         the slice plane), row-major [3][2]; chain to the
+                         pose parameters on the host                         */
+  double reserved[6];
+} cjx_image_grads;
+
+/* Workspace for cjx_slice_ctf_loss_grad (same per-image need as the
+ * forward's resize path).                                                  */
+CJX_API int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_images,
+                                              size_t* bytes);
+/* Loss L_b = sum_pixels (simulate_b() - obs_b)^2 in real space (the
+ * squared residual of the reference's README gradient example, with
+ * padded_shape == shape) and its gradients, for every image b:
+ *  - image_grads[b]: loss, dL/d(shift_x, shift_y, defocus) and dL/dR;
+ *  - grid_grad (optional, complex64 N^3 in the reference's [z][y][x]
+ *    layout): ACCUMULATES sum_b dL_b/dG by trilinear scatter-add (float2
+ *    atomics), reported as dL/dRe + i dL/dIm (jax.grad returns the complex
+ *    conjugate).  The caller zeroes it.
+ * observed: device complex64 [n_images][Py][Px/2+1], rfftn of the observed
+ * real-space images in cryoJAX's convention (ifftshift, then rfft2).
+ * Resize path only, with N, Py, Px of the form 32 R (R in 1-6, 8, 10, 12, 16).
+ * Replaces jax.grad / eqx.filter_grad through LinearImageModel.simulate
+ * (cryojax/simulator/_image_model/base_image_model.py:68-105, 297-328).      */
+CJX_API int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid,
+                                    const cjx_image_params* params, const int32_t* order,
+                                    int64_t n_images, const void* observed,
+                                    double* image_grads, void* grid_grad, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+
 /* ---- several volumes / image shapes in one call ----------------------- */
 typedef struct cjx_slice_group {
   cjx_slice_desc desc;             /* geometry and flags of this group        */

@@ -1,0 +1,172 @@
+"""GPU: squared-residual loss and gradients against float64 central differences of the oracle.
+
+Each observed image is the oracle's simulation at a seeded true pose plus
+white noise.  The loss is evaluated at a perturbed pose (<= 3 deg, +-2 A,
++-300 A defocus).  Central differences use step 1e-6 on the pose (so
+almost no sample crosses a voxel-cell boundary, where trilinear
+interpolation has a kink) and 1e-4 on offsets, defocus and grid values.
+Tolerances: loss rel 1e-5; each gradient vector (per image) rel L2 1e-4;
+grid-gradient entries within 1e-4 of the largest checked entry.
+"""
+
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import cryojax_oracle as O
+from tests.helpers import make_volume
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-4
+
+
+def _loss(grid, fs, specs, obs):
+    return sum(float(np.sum((O.simulate(grid, fs, s) - o) ** 2)) for s, o in zip(specs, obs))
+
+
+def _setup(box=32, shape=(32, 32), n=3, seed=0, euler=False):
+    rng = np.random.default_rng(seed)
+    vol, grid, fs = make_volume(box, 60, seed=seed)
+    true_q, off = O.uniform_poses(n, seed + 1, 8.0)
+    specs, obs = [], []
+    for b in range(n):
+        s_true = O.ImageSpec(shape=shape, pixel_size=2.0, wxyz=true_q[b], offset_in_angstroms=off[b],
+                             defocus_in_angstroms=rng.uniform(8000, 15000), astigmatism_in_angstroms=150.0,
+                             astigmatism_angle=30.0)
+        img = O.simulate(grid, fs, s_true)
+        noise = rng.standard_normal(img.shape) * np.sqrt(img.var() / 0.1)
+        obs.append(img + noise)
+        # perturbed evaluation pose: <= 3 degrees, +-2 A, +-300 A
+        axis = rng.standard_normal(3)
+        axis /= np.linalg.norm(axis)
+        dq = O.so3_exp(np.deg2rad(rng.uniform(0.5, 3.0)) * axis)
+        s = copy.deepcopy(s_true)
+        s.wxyz = O.quat_compose(dq, true_q[b])
+        s.offset_in_angstroms = off[b] + rng.uniform(-2, 2, 2)
+        s.defocus_in_angstroms = s_true.defocus_in_angstroms + rng.uniform(-300, 300)
+        specs.append(s)
+    return grid, fs, specs, np.stack(obs)
+
+
+def _model(grid, specs, euler=False):
+    import torch
+
+    from cryojax_b200 import simulator as S
+    from tests.helpers import specs_to_model_args
+
+    pose, tt, cfg = specs_to_model_args(specs)
+    if euler:
+        angles = []
+        for s in specs:  # zyz Euler angles of each quaternion (extrinsic, degrees)
+            r = O.quat_as_matrix(O.quat_normalize(s.wxyz))
+            theta = np.arccos(np.clip(r[2, 2], -1, 1))
+            phi = np.arctan2(r[2, 1], -r[2, 0])
+            psi = np.arctan2(r[1, 2], r[0, 2])
+            angles.append(np.rad2deg([phi, theta, psi]))
+        a = np.array(angles)
+        off = np.stack([s.offset_in_angstroms for s in specs])
+        pose = S.EulerAnglePose(off[:, 0], off[:, 1], a[:, 0], a[:, 1], a[:, 2])
+    vol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+    return S.make_image_model(vol, cfg, pose, tt), pose
+
+
+def _fd(f, h):
+    return (f(h) - f(-h)) / (2 * h)
+
+
+@pytest.mark.parametrize("box,shape", [(32, (32, 32)), (48, (64, 64))])
+def test_loss_and_parameter_gradients(cuda_device, box, shape):
+    from cryojax_b200.gradients import squared_residual_and_grad
+
+    grid, fs, specs, obs = _setup(box=box, shape=shape, seed=box)
+    model, _ = _model(grid, specs)
+    res = squared_residual_and_grad(model, obs, grid_grad=False)
+    for b, s in enumerate(specs):
+        ref_loss = _loss(grid, fs, [s], obs[b:b + 1])
+        assert abs(res["loss"][b] - ref_loss) <= 1e-5 * ref_loss
+
+        def with_(fn, h):
+            s2 = copy.deepcopy(s)
+            fn(s2, h)
+            return _loss(grid, fs, [s2], obs[b:b + 1])
+
+        g_fd = []
+        for c in range(4):
+            def fq(s2, h, c=c):
+                s2.wxyz = s.wxyz + h * np.eye(4)[c]
+            g_fd.append(_fd(lambda h: with_(fq, h), 1e-6))
+        g_fd += [_fd(lambda h: with_(lambda s2, h: setattr(s2, "offset_in_angstroms",
+                                                           s.offset_in_angstroms + [h, 0]), h), 1e-4),
+                 _fd(lambda h: with_(lambda s2, h: setattr(s2, "offset_in_angstroms",
+                                                           s.offset_in_angstroms + [0, h]), h), 1e-4),
+                 _fd(lambda h: with_(lambda s2, h: setattr(s2, "defocus_in_angstroms",
+                                                           s.defocus_in_angstroms + h), h), 1e-4)]
+        g_fd = np.array(g_fd)
+        g_gpu = np.concatenate([res["d_wxyz"][b], res["d_offset"][b], [res["d_defocus"][b]]])
+        # per-group relative error (quaternion, offsets, defocus have different scales)
+        for sl in (slice(0, 4), slice(4, 6), slice(6, 7)):
+            err = np.linalg.norm(g_gpu[sl] - g_fd[sl]) / max(np.linalg.norm(g_fd[sl]), 1e-30)
+            assert err <= GRAD_TOL, (b, sl, g_gpu[sl], g_fd[sl], err)
+
+
+def test_euler_pose_chain(cuda_device):
+    from cryojax_b200.gradients import squared_residual_and_grad
+
+    grid, fs, specs, obs = _setup(seed=5, n=2)
+    model, pose = _model(grid, specs, euler=True)
+    res = squared_residual_and_grad(model, obs, grid_grad=False)
+    for b, s in enumerate(specs):
+        ang = np.array([pose.phi_angle[b], pose.theta_angle[b], pose.psi_angle[b]])
+
+        def loss_at(a):
+            s2 = copy.deepcopy(s)
+            s2.wxyz = O.euler_pose_quaternion(*a)
+            return _loss(grid, fs, [s2], obs[b:b + 1])
+
+        g_fd = np.array([_fd(lambda h, c=c: loss_at(ang + h * np.eye(3)[c]), 1e-5) for c in range(3)])
+        err = np.linalg.norm(res["d_euler_angles"][b] - g_fd) / np.linalg.norm(g_fd)
+        assert err <= GRAD_TOL, (res["d_euler_angles"][b], g_fd)
+
+
+def test_grid_gradient_scatter(cuda_device):
+    from cryojax_b200.gradients import squared_residual_and_grad
+
+    grid, fs, specs, obs = _setup(seed=9, n=2)
+    model, _ = _model(grid, specs)
+    res = squared_residual_and_grad(model, obs, grid_grad=True)
+    gg = res["d_grid"].cpu().numpy()
+    n = grid.shape[0]
+    # check entries with the largest gradient magnitude plus a few random ones
+    flat = np.argsort(np.abs(gg).ravel())[::-1][:6]
+    rng = np.random.default_rng(0)
+    nz = np.flatnonzero(np.abs(gg).ravel() > 0)
+    idxs = list(flat) + list(rng.choice(nz, 4, replace=False))
+    scale = np.abs(gg).max()
+    for flat_i in idxs:
+        z, y, x = np.unravel_index(flat_i, gg.shape)
+
+        def loss_at(h, part):
+            g2 = grid.copy()
+            g2[z, y, x] += h * (1.0 if part == 0 else 1.0j)
+            return _loss(g2, fs, specs, obs)
+
+        fd = _fd(lambda h: loss_at(h, 0), 1e-4) + 1j * _fd(lambda h: loss_at(h, 1), 1e-4)
+        assert abs(gg[z, y, x] - fd) <= GRAD_TOL * scale, ((z, y, x), gg[z, y, x], fd, scale)
+    assert gg.shape == (n, n, n)
+
+
+def test_bricked_and_linear_layouts_give_same_gradients(cuda_device):
+    from cryojax_b200.gradients import squared_residual_and_grad
+
+    grid, fs, specs, obs = _setup(seed=13, n=2)
+    out = []
+    for bricked in (True, False):
+        model, _ = _model(grid, specs)
+        model.volume_integrator.use_bricked_layout = bricked
+        out.append(squared_residual_and_grad(model, obs, grid_grad=True))
+    for key in ("loss", "d_wxyz", "d_offset", "d_defocus"):
+        np.testing.assert_allclose(out[0][key], out[1][key], rtol=1e-5, atol=1e-8 * np.abs(out[1][key]).max())
+    a, b = out[0]["d_grid"].cpu().numpy(), out[1]["d_grid"].cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max()
