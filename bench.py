@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-batched", action="store_true", help="skip the mixed-size batch measurement")
+    ap.add_argument("--no-grad", action="store_true", help="skip the loss-gradient measurement")
     return ap.parse_args()
 
 
@@ -339,6 +340,81 @@ def measure_batched_uneven(dev, steps, warmup, seed):
             "autotuned": tun}
 
 
+def measure_gradient(dev, steps, warmup, seed):
+    """Squared residual + gradients w.r.t. pose, offsets, defocus and the grid.
+
+    A 192^3 Gaussian-sum volume (2000 Gaussians, pad 2 -> N = 384) and 1024
+    observed 192 x 192 images simulated at seeded true poses plus white noise
+    at SNR 0.1 (the noise model's recipe); loss and gradients evaluated at
+    poses perturbed by <= 3 deg, +-2 A offsets and +-300 A defocus.  One step =
+    one cjx_slice_ctf_loss_grad call over the 1024 images (forward, adjoint
+    passes, grid scatter-add).
+    """
+    import numpy as np
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import rotations as rot
+    from cryojax_b200 import simulator as S
+    from cryojax_b200 import synthetic
+    from cryojax_b200.gradients import observed_to_fourier, squared_residual_and_grad
+    from cryojax_b200.noise import GaussianWhiteNoiseModel, noise_variance_for_snr
+
+    n_img = 1024
+    vol_np = synthetic.gaussian_sum_volume(192, 2000, seed + 30, sigma_range=(1.0, 3.0))
+    vol = S.FourierVoxelGridVolume.from_real_voxel_grid(vol_np, pad_scale=2.0, device=str(dev))
+    rng = np.random.default_rng(seed + 31)
+    b = synthetic.image_batch(n_img, seed + 32, max_offset=10.0, defocus_range=(8000.0, 20000.0))
+    cfg = S.BasicImageConfig((192, 192), 2.0, 300.0)
+    true_model = S.make_image_model(vol, cfg, S.QuaternionPose(b.offsets[:, 0], b.offsets[:, 1], wxyz=b.wxyz),
+                                    S.ContrastTransferTheory(S.AstigmaticCTF(b.defocus, b.astigmatism,
+                                                                             b.astigmatism_angle)))
+    signal = true_model.simulate()
+    var = noise_variance_for_snr(signal, 0.1)
+    gen = torch.Generator(device=dev).manual_seed(seed + 33)
+    obs = signal + GaussianWhiteNoiseModel(true_model, variance=var).compute_noise(gen)
+    axis = rng.standard_normal((n_img, 3))
+    axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+    dq = rot.so3_exp(np.deg2rad(rng.uniform(0, 3.0, n_img))[:, None] * axis)
+    q = rot.quat_compose(dq, b.wxyz)
+    off = b.offsets + rng.uniform(-2, 2, (n_img, 2))
+    df = b.defocus + rng.uniform(-300, 300, n_img)
+    model = S.make_image_model(vol, cfg, S.QuaternionPose(off[:, 0], off[:, 1], wxyz=q),
+                               S.ContrastTransferTheory(S.AstigmaticCTF(df, b.astigmatism, b.astigmatism_angle)))
+    obs_f = observed_to_fourier(obs)
+    # full public call once (host chain to quaternion gradients included)
+    res = squared_residual_and_grad(model, obs_f, observed_is_fourier=True, grid_grad=True)
+    # device-timed loop of the library call
+    integ = model.volume_integrator
+    flags = model._flags() | nat.CJX_GRID_BRICKED
+    desc = nat.make_desc(vol.shape[0], 192, 192, flags)
+    pd = torch.as_tensor(model.image_params(), device=dev)
+    order = torch.as_tensor(S.orientation_order(model.image_params()[:, 0:9].reshape(-1, 3, 3)), device=dev)
+    grads = torch.empty((n_img, nat.GRAD_DOUBLES), dtype=torch.float64, device=dev)
+    gg = torch.zeros(vol.shape, dtype=torch.complex64, device=dev)
+    ws = torch.empty(nat.loss_workspace_size(desc, n_img), dtype=torch.uint8, device=dev)
+    grid_b = vol.bricked_grid()
+    for _ in range(warmup):
+        nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
+    torch.cuda.synchronize()
+    nat.profile_enable(True)
+    nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
+    torch.cuda.synchronize()
+    prof = nat.profile_read()
+    nat.profile_enable(False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"metric": "loss + gradient images/s (192^3 volume, 192^2 images, pose/offset/defocus/grid)",
+            "value": n_img / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms, "images_per_step": n_img,
+            "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()},
+            "mean_loss": float(np.mean(res["loss"])), "grid_grad_norm": float(gg.abs().pow(2).sum().sqrt())}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -518,6 +594,15 @@ def main():
         except Exception as e:
             batched = {"error": repr(e)}
 
+    # ---- loss + gradient (differentiation configuration)
+    gradient = None
+    if not args.no_grad:
+        try:
+            torch.cuda.empty_cache()
+            gradient = measure_gradient(dev, max(3, min(args.steps, 10)), 2, args.seed)
+        except Exception as e:
+            gradient = {"error": repr(e)}
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -550,6 +635,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "batched_uneven": batched,
+            "gradient": gradient,
         }
         print(json.dumps(line))
     if world > 1:
