@@ -80,6 +80,16 @@ class SliceGroup(ctypes.Structure):
     ]
 
 
+class SearchDesc(ctypes.Structure):
+    _fields_ = [
+        ("slice", SliceDesc),
+        ("n_images", ctypes.c_int64),
+        ("n_orientations", ctypes.c_int64),
+        ("candidates_per_image", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class CryojaxB200Error(RuntimeError):
     """Raised when a C-ABI entry point returns a nonzero status."""
 
@@ -129,6 +139,11 @@ _SIGNATURES = {
             ctypes.c_size_t,
             ctypes.c_void_p,
         ],
+    ),
+    "cjx_search_workspace_size": (ctypes.c_int, [ctypes.POINTER(SearchDesc), ctypes.POINTER(ctypes.c_size_t)]),
+    "cjx_search": (
+        ctypes.c_int,
+        [ctypes.POINTER(SearchDesc)] + [ctypes.c_void_p] * 9 + [ctypes.c_size_t, ctypes.c_void_p],
     ),
     "cjx_slice_ctf_multi_workspace_size": (
         ctypes.c_int,
@@ -310,6 +325,25 @@ def slice_ctf_loss_grad(desc: SliceDesc, grid, params, observed, image_grads, gr
             ctypes.byref(desc), _cuda_ptr(grid, "grid"), _cuda_ptr(params, "params"), _order_ptr(order, n), int(n),
             _cuda_ptr(observed, "observed"), _cuda_ptr(image_grads, "image_grads"), gg, ws_ptr, ws_bytes,
             _stream_ptr(stream)))
+
+
+def search_workspace_size(sdesc: SearchDesc) -> int:
+    out = ctypes.c_size_t(0)
+    _check(load_library().cjx_search_workspace_size(ctypes.byref(sdesc), ctypes.byref(out)))
+    return int(out.value)
+
+
+def search(sdesc: SearchDesc, grid, image_params, rotations, observed, best_score, best_orientation, workspace,
+           candidates=None, scores=None, stream=None) -> None:
+    """cjx_search on torch CUDA tensors."""
+    def ptr(t, what):
+        return ctypes.c_void_p(0) if t is None else _cuda_ptr(t, what)
+
+    _check(load_library().cjx_search(
+        ctypes.byref(sdesc), ptr(grid, "grid"), ptr(image_params, "image_params"), ptr(rotations, "rotations"),
+        ptr(candidates, "candidates"), ptr(observed, "observed"), ptr(scores, "scores"),
+        ptr(best_score, "best_score"), ptr(best_orientation, "best_orientation"), ptr(workspace, "workspace"),
+        workspace.numel() * workspace.element_size(), _stream_ptr(stream)))
 
 
 def make_groups(groups):

@@ -16,6 +16,12 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
                    int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
                    const Tuning& tn);
 int64_t tuning_get(int key);
+size_t search_candidate_bytes(const SliceGeom& g, size_t per_image_fwd);
+size_t search_workspace_bytes(const SliceGeom& g, size_t per_fwd, int64_t chunk, int64_t n_images);
+int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float2* grid,
+                  const cjx_image_params* image_params, const double* rot, const int32_t* candidates,
+                  int64_t n_images, int K, const float2* obs, float* scores, float* best_score, int32_t* best_orient,
+                  void* workspace, cudaStream_t stream, const Tuning& tn);
 int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                      int64_t n_images, const float2* obs, double* grads, float2* grad_grid, void* workspace,
                      int64_t chunk, cudaStream_t stream, const Tuning& tn);
@@ -186,6 +192,49 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   return launch_loss_grad(g, static_cast<const float2*>(grid), params, order, n_images,
                           static_cast<const float2*>(observed), image_grads, static_cast<float2*>(grid_grad),
                           workspace, chunk, static_cast<cudaStream_t>(stream), current_tuning());
+}
+
+static int search_plan(const cjx_search_desc* d, SliceGeom* g, int* K, int64_t* chunk, size_t* bytes) {
+  if (!d) return fail(CJX_ERR_INVALID_ARGUMENT, "desc is NULL");
+  if (int e = make_geom(&d->slice, g)) return e;
+  if (!needs_resize(*g)) return fail(CJX_ERR_UNSUPPORTED, "search needs the resize path ((Py, Px) != (N, N))");
+  if (d->n_images < 0 || d->n_orientations < 1 || d->candidates_per_image < 0)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "need n_images >= 0, n_orientations >= 1, candidates_per_image >= 0");
+  if (d->n_orientations > 2147483647LL) return fail(CJX_ERR_UNSUPPORTED, "too many orientations");
+  *K = d->candidates_per_image ? d->candidates_per_image : (int)d->n_orientations;
+  const size_t per = search_candidate_bytes(*g, workspace_per_image(*g));
+  int64_t c = (int64_t)((size_t)tuning_get(CJX_TUNE_CHUNK_BYTES) / per);
+  const int64_t total = std::max<int64_t>(1, d->n_images * (int64_t)*K);
+  c = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(c, 65535), total));
+  if (d->slice.images_per_chunk > 0) c = std::min<int64_t>(d->slice.images_per_chunk, total);
+  *chunk = c;
+  *bytes = search_workspace_bytes(*g, workspace_per_image(*g), c, std::max<int64_t>(d->n_images, 1));
+  return CJX_OK;
+}
+
+int cjx_search_workspace_size(const cjx_search_desc* desc, size_t* bytes) {
+  if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  SliceGeom g;
+  int K;
+  int64_t chunk;
+  return search_plan(desc, &g, &K, &chunk, bytes);
+}
+
+int cjx_search(const cjx_search_desc* desc, const void* grid, const cjx_image_params* image_params,
+               const double* rotations, const int32_t* candidates, const void* observed, float* scores,
+               float* best_score, int32_t* best_orientation, void* workspace, size_t workspace_bytes, void* stream) {
+  SliceGeom g;
+  int K;
+  int64_t chunk;
+  size_t need;
+  if (int e = search_plan(desc, &g, &K, &chunk, &need)) return e;
+  if (desc->n_images == 0) return CJX_OK;
+  if (!grid || !image_params || !rotations || !observed)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "grid, image_params, rotations and observed must be non-NULL");
+  if (!workspace || workspace_bytes < need) return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_search_workspace_size()");
+  return launch_search(g, workspace_per_image(g), chunk, static_cast<const float2*>(grid), image_params, rotations,
+                       candidates, desc->n_images, K, static_cast<const float2*>(observed), scores, best_score,
+                       best_orientation, workspace, static_cast<cudaStream_t>(stream), current_tuning());
 }
 
 int cjx_tuning_set(int key, int64_t value) { return tuning_set(key, value); }

@@ -178,6 +178,32 @@ CJX_API int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid
                                     double* image_grads, void* grid_grad, void* workspace,
                                     size_t workspace_bytes, void* stream);
 
+/* ---- orientation search ---------------------------------------------- */
+typedef struct cjx_search_desc {
+  cjx_slice_desc slice;          /* volume side, image shape, flags          */
+  int64_t n_images;              /* observed images                          */
+  int64_t n_orientations;        /* rows of the rotation table               */
+  int32_t candidates_per_image;  /* K; 0 = every orientation (exhaustive)    */
+  int32_t reserved;
+} cjx_search_desc;
+
+CJX_API int cjx_search_workspace_size(const cjx_search_desc* desc, size_t* bytes);
+/* For every observed image b and each of its candidate orientations t
+ * (candidates[b*K + k], or every t when candidates is NULL): simulate with
+ * rotation rotations[t] (row-major 3x3 doubles) and image_params[b]'s CTF,
+ * scale and shift (its rot field is ignored), score by normalised
+ * cross-correlation against observed[b] (complex64 [Py][Px/2+1], rfftn of
+ * the observed image), and keep the best.  Outputs: best_score[b],
+ * best_orientation[b] (ties -> lowest index) and, when scores is non-NULL,
+ * scores[b*K + k].  Replaces run_grid_search with MinimumSearchMethod over
+ * an orientation grid whose fn simulates and scores
+ * (cryojax/jax_util/_grid_search/search_loop.py:24-158).                    */
+CJX_API int cjx_search(const cjx_search_desc* desc, const void* grid,
+                       const cjx_image_params* image_params, const double* rotations,
+                       const int32_t* candidates, const void* observed, float* scores,
+                       float* best_score, int32_t* best_orientation, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
 /* ---- several volumes / image shapes in one call ----------------------- */
 typedef struct cjx_slice_group {
   cjx_slice_desc desc;             /* geometry and flags of this group        */
