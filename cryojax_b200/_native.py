@@ -173,6 +173,13 @@ _SIGNATURES = {
     ),
     "cjx_tuning_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64]),
     "cjx_tuning_get": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
+    "cjx_gemm": (
+        ctypes.c_int,
+        [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+         ctypes.c_void_p],
+    ),
+    "cjx_device_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_void_p]),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -402,6 +409,33 @@ def slice_ctf_forward_noalloc(desc: SliceDesc, grid, params, out, stream=None, o
             _stream_ptr(stream),
         )
     )
+
+
+CJX_GEMM_OUT_BF16 = 1
+CJX_GEMM_BIAS = 2
+CJX_GEMM_RELU = 4
+CJX_GEMM_ACCUMULATE = 8
+CJX_GEMM_F16 = 16
+
+
+def gemm(a, b, c, *, bias=None, flags=0, split_k=1, m=None, n=None, k=None, stream=None) -> None:
+    """cjx_gemm: c[:m, :n] (op)= a[:m, :k] @ b[:n, :k].T on torch CUDA tensors (row-major 2-D)."""
+    m = a.shape[0] if m is None else m
+    n = b.shape[0] if n is None else n
+    k = a.shape[1] if k is None else k
+    if bias is not None:
+        flags |= CJX_GEMM_BIAS
+    _check(load_library().cjx_gemm(
+        int(m), int(n), int(k), _cuda_ptr(a, "a"), int(a.stride(0)), _cuda_ptr(b, "b"), int(b.stride(0)),
+        _cuda_ptr(c, "c"), int(c.stride(0)), ctypes.c_void_p(0) if bias is None else _cuda_ptr(bias, "bias"),
+        int(flags), int(split_k), _stream_ptr(stream)))
+
+
+def device_status(reset: bool = True, stream=None) -> int:
+    """First error code a device-side wait recorded (0 = none); synchronises the stream."""
+    v = ctypes.c_int(0)
+    _check(load_library().cjx_device_status(ctypes.byref(v), 1 if reset else 0, _stream_ptr(stream)))
+    return int(v.value)
 
 
 def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:

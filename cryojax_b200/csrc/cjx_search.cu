@@ -145,10 +145,10 @@ __global__ void __launch_bounds__(kWarps * 32)
     red[warp][1] = den;
   }
   __syncthreads();
-  if (threadIdx.x < 2) {
+  if (threadIdx.x < 2) {  // per-block partials: the finalize pass sums them in a fixed order
     float t = 0.f;
     for (int w = 0; w < kWarps; ++w) t += red[w][threadIdx.x];
-    atomicAdd(&sums[2 * k + threadIdx.x], t);
+    sums[((size_t)k * gridDim.x + blockIdx.x) * 2 + threadIdx.x] = t;
   }
 }
 
@@ -160,14 +160,19 @@ __device__ __forceinline__ unsigned long long score_key(float s, int32_t orient)
   return ((unsigned long long)u << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned int)orient);
 }
 
-__global__ void k_finalize_scores(const float* __restrict__ sums, const int32_t* __restrict__ cimg,
+__global__ void k_finalize_scores(const float* __restrict__ sums, int nparts, const int32_t* __restrict__ cimg,
                                   const int32_t* __restrict__ corient, const float* __restrict__ oo,
                                   float* __restrict__ scores, unsigned long long* __restrict__ best, int64_t c0,
                                   int cnt) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= cnt) return;
   const int32_t img = cimg[k];
-  const float num = sums[2 * k], den = sums[2 * k + 1], o2 = oo[img];
+  float num = 0.f, den = 0.f;
+  for (int p = 0; p < nparts; ++p) {
+    num += sums[((size_t)k * nparts + p) * 2];
+    den += sums[((size_t)k * nparts + p) * 2 + 1];
+  }
+  const float o2 = oo[img];
   const float s = (den > 0.f && o2 > 0.f) ? num * rsqrtf(den * o2) : 0.f;
   if (scores) scores[c0 + k] = s;
   atomicMax(&best[img], score_key(s, corient[k]));
@@ -205,8 +210,10 @@ static cudaError_t search_smem_attrs() {
 // Workspace: per candidate the forward intermediates + a params record,
 // image / orientation ids and two sums; per image the power of O and the
 // packed best key.
+static int score_parts(const SliceGeom& g) { return (g.pxh + kWarps - 1) / kWarps; }
+
 size_t search_candidate_bytes(const SliceGeom& g, size_t per_image_fwd) {
-  return per_image_fwd + sizeof(cjx_image_params) + 2 * sizeof(int32_t) + 2 * sizeof(float);
+  return per_image_fwd + sizeof(cjx_image_params) + 2 * sizeof(int32_t) + 2 * sizeof(float) * score_parts(g);
 }
 
 int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float2* grid,
@@ -230,7 +237,8 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
   int32_t* corient = reinterpret_cast<int32_t*>(p);
   p += align((size_t)chunk * sizeof(int32_t));
   float* sums = reinterpret_cast<float*>(p);
-  p += align((size_t)chunk * 2 * sizeof(float));
+  const int nparts = score_parts(g);
+  p += align((size_t)chunk * nparts * 2 * sizeof(float));
   float* oo = reinterpret_cast<float*>(p);
   p += align((size_t)n_images * sizeof(float));
   unsigned long long* best = reinterpret_cast<unsigned long long*>(p);
@@ -249,9 +257,8 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
         image_params, rot, candidates, c0, cnt, K, cparams, cimg, corient);
     prof_end("k_build_candidates", stream);
     if (int e = launch_forward_to_t2(g, grid, cparams, nullptr, 0, cnt, t1, t2, hb, stream, tn)) return e;
-    cudaMemsetAsync(sums, 0, (size_t)cnt * 2 * sizeof(float), stream);
     prof_begin(stream);
-    const dim3 gs((g.pxh + kWarps - 1) / kWarps, cnt);
+    const dim3 gs(nparts, cnt);
     switch (rpy) {
 #define CJX_S_CASE(R) \
   case R: k_colfft_score_reg<R><<<gs, kWarps * 32, s_score, stream>>>(t2, cparams, cimg, obs, sums, g, norm); break;
@@ -261,7 +268,7 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
     }
     prof_end("k_colfft_score", stream);
     prof_begin(stream);
-    k_finalize_scores<<<(cnt + 255) / 256, 256, 0, stream>>>(sums, cimg, corient, oo, scores, best, c0, cnt);
+    k_finalize_scores<<<(cnt + 255) / 256, 256, 0, stream>>>(sums, nparts, cimg, corient, oo, scores, best, c0, cnt);
     prof_end("k_finalize_scores", stream);
   }
   k_unpack_best<<<64, 256, 0, stream>>>(best, best_score, best_orient, n_images);
@@ -271,7 +278,7 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
 size_t search_workspace_bytes(const SliceGeom& g, size_t per_fwd, int64_t chunk, int64_t n_images) {
   auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
   return align((size_t)chunk * per_fwd) + align((size_t)chunk * sizeof(cjx_image_params)) +
-         2 * align((size_t)chunk * sizeof(int32_t)) + align((size_t)chunk * 2 * sizeof(float)) +
+         2 * align((size_t)chunk * sizeof(int32_t)) + align((size_t)chunk * score_parts(g) * 2 * sizeof(float)) +
          align((size_t)n_images * sizeof(float)) + align((size_t)n_images * sizeof(unsigned long long));
 }
 

@@ -1,0 +1,128 @@
+"""Orientation search on the device: simulate every candidate pose with the
+image's own CTF and keep the best normalised cross-correlation.
+
+In the reference a pose search is ``run_grid_search(fn, MinimumSearchMethod,
+grid, args)``: fn simulates the image at one grid point and returns a cost,
+and the method keeps an elementwise running argmin with the earliest index
+winning ties (cryojax/jax_util/_grid_search/search_loop.py:24-158,
+search_method.py:149-310).  Here fn is fixed to "simulate with this image's
+CTF and shifts, score by NCC against the observed image" and the whole
+(image x orientation) sweep is one C-ABI call (cjx_search): candidate
+simulation through the same gather / resize kernels as the forward, and a
+scoring pass that replaces the final column FFT's store by the two NCC sums.
+
+The score is Pearson's r between the simulated and observed real-space
+images -- the mean of normalize_image(sim) * normalize_image(obs)
+(cryojax/ndimage/_normalize.py:11-28) -- computed in Fourier space by
+Parseval with the DC term left out.  It needs padded_shape == shape, so that
+the real-space image is the whole padded image.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as nat
+from .gradients import observed_to_fourier
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+@dataclass
+class SearchResult:
+    best_orientation: np.ndarray   # (n,) int64, index into the rotation table
+    best_score: np.ndarray         # (n,) float32, NCC of the best orientation
+    scores: object = None          # (n, K) float32 CUDA tensor when requested
+    candidates: object = None      # (n, K) int32 CUDA tensor of the orientations scored
+
+
+class PoseSearch:
+    """Exhaustive or candidate-list orientation search over a fixed rotation table.
+
+    ``rotations``: (T, 3, 3) rotation matrices (the grid's orientations, e.g.
+    ``healpix.OrientationGrid(8, 48).rotation_matrices()``), uploaded once.
+    ``image_model``: a batched LinearImageModel / ContrastImageModel over the
+    observed images; its CTF, scale and in-plane offsets are used per image,
+    its pose rotation is replaced by every candidate's.
+    """
+
+    def __init__(self, rotations, *, device="cuda"):
+        torch = _torch()
+        r = np.ascontiguousarray(np.asarray(rotations, np.float64).reshape(-1, 9))
+        self.n_orientations = r.shape[0]
+        self.rotations = torch.as_tensor(r, device=device)
+        self._ws = None
+
+    def _desc(self, image_model, n, k):
+        cfg = image_model.image_config
+        if tuple(cfg.padded_shape) != tuple(cfg.shape):
+            raise NotImplementedError("the NCC search needs padded_shape == shape")
+        integ = image_model.volume_integrator
+        vol = image_model.volume_parametrization.get_representation()
+        flags = image_model._flags() | integ._base_flags()
+        grid = vol.fourier_voxel_grid
+        if integ.use_bricked_layout:
+            grid = vol.bricked_grid()
+            flags |= nat.CJX_GRID_BRICKED
+        py, px = cfg.padded_shape
+        sdesc = nat.SearchDesc()
+        sdesc.slice = nat.make_desc(vol.shape[0], py, px, flags, integ.fill_value)
+        sdesc.n_images = n
+        sdesc.n_orientations = self.n_orientations
+        sdesc.candidates_per_image = k
+        return sdesc, grid
+
+    def run(self, image_model, observed, *, candidates=None, return_scores=False, observed_is_fourier=False,
+            image_params_device=None, stream=None) -> SearchResult:
+        """Best orientation per observed image.
+
+        observed: real-space images (n, P, P) in cryoJAX's centred convention,
+        or their rfftn (complex64 (n, P, P//2+1) on the device) when
+        ``observed_is_fourier``.  candidates: optional (n, K) orientation
+        indices to score per image (each in [0, T)); default every
+        orientation.
+        """
+        torch = _torch()
+        dev = self.rotations.device
+        params = image_model.image_params() if image_params_device is None else None
+        n = image_params_device.shape[0] if image_params_device is not None else params.shape[0]
+        obs_f = observed if observed_is_fourier else observed_to_fourier(observed)
+        py, px = image_model.image_config.padded_shape
+        if tuple(obs_f.shape) != (n, py, px // 2 + 1):
+            raise ValueError(f"observed has shape {tuple(obs_f.shape)}, expected {(n, py, px // 2 + 1)} "
+                             "in Fourier space")
+        cand = None
+        k = 0
+        if candidates is not None:
+            cand = candidates if isinstance(candidates, torch.Tensor) else torch.as_tensor(
+                np.asarray(candidates, np.int32))
+            cand = cand.to(device=dev, dtype=torch.int32).reshape(n, -1).contiguous()
+            k = cand.shape[1]
+            if k == 0:
+                raise ValueError("candidates must list at least one orientation per image")
+            lo, hi = int(cand.min()), int(cand.max())
+            if lo < 0 or hi >= self.n_orientations:
+                raise ValueError(f"candidate orientation indices must lie in [0, {self.n_orientations})")
+        sdesc, grid = self._desc(image_model, n, k)
+        pd = image_params_device if image_params_device is not None else torch.as_tensor(params, device=dev)
+        ws_bytes = nat.search_workspace_size(sdesc)
+        if self._ws is None or self._ws.numel() < ws_bytes:
+            self._ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+        kk = k if k else self.n_orientations
+        scores = torch.empty((n, kk), dtype=torch.float32, device=dev) if return_scores else None
+        best_score = torch.empty(n, dtype=torch.float32, device=dev)
+        best_orient = torch.empty(n, dtype=torch.int32, device=dev)
+        nat.search(sdesc, grid, pd, self.rotations, obs_f, best_score, best_orient, self._ws,
+                   candidates=cand, scores=scores, stream=stream)
+        return SearchResult(best_orient.cpu().numpy().astype(np.int64), best_score.cpu().numpy(), scores, cand)
+
+
+def search_orientations(image_model, observed, rotations, **kw) -> SearchResult:
+    """One-shot exhaustive / candidate search (see PoseSearch.run)."""
+    return PoseSearch(rotations).run(image_model, observed, **kw)

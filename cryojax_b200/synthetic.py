@@ -52,3 +52,22 @@ def image_batch(n, seed, *, max_offset=20.0, defocus_range=(5000.0, 25000.0), as
     off = rng.uniform(-max_offset, max_offset, size=(n, 2))
     return ImageBatch(q, off, rng.uniform(*defocus_range, n), rng.uniform(*astig_range, n),
                       rng.uniform(*angle_range, n))
+
+
+def noisy_images(image_model, snr, generator=None):
+    """Real-space images of a batched image model plus white Gaussian noise.
+
+    SNR is signal variance / noise variance per image, in real space (the
+    pose-search configurations' definition); white noise of variance s^2 in
+    real space is the reference's GaussianWhiteNoiseModel draw
+    (cryojax/simulator/_noise_model/gaussian_noise_model.py:167-205) up to
+    its [0, 0] Fourier term.  Returns (noisy, clean) float32 CUDA tensors.
+    """
+    import torch
+
+    clean = image_model.simulate(outputs_real_space=True).float()
+    if clean.dim() == 2:
+        clean = clean[None]
+    var = clean.var(dim=(-2, -1), unbiased=False, keepdim=True) / float(snr)
+    noise = torch.randn(clean.shape, generator=generator, device=clean.device, dtype=torch.float32)
+    return clean + noise * torch.sqrt(var), clean

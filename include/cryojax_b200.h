@@ -304,6 +304,27 @@ CJX_API int cjx_profile_enable(int on);
 CJX_API int cjx_profile_read(char* names, int64_t* counts, double* total_ms,
                              int max_kernels, int* n_kernels);
 
+/* ---- tensor-core GEMM (pose-proposal network) -------------------------- */
+#define CJX_GEMM_OUT_BF16 1   /* store C as BF16 (default FP32)              */
+#define CJX_GEMM_BIAS 2       /* C[:, n] += bias[n] (FP32)                    */
+#define CJX_GEMM_RELU 4       /* C = max(C, 0) after the bias                 */
+#define CJX_GEMM_ACCUMULATE 8 /* C += A B^T with FP32 atomics (split_k > 1)   */
+#define CJX_GEMM_F16 16       /* A and B are FP16 (default BF16)              */
+/* C[M][ldc] = A B^T for A [M][lda], B [N][ldb] (16-bit, K-major; base
+ * 16-byte aligned, lda and ldb multiples of 8 elements), FP32 accumulation
+ * on the tensor cores (tcgen05.mma, accumulator in tensor memory, operands
+ * staged by TMA).  split_k > 1 splits the K loop over CTAs and needs
+ * CJX_GEMM_ACCUMULATE.  The network's layers are implicit GEMMs over
+ * these.  No counterpart in the reference (its pose search has no network).
+ * Kernels that give up on a wait (2 s limit) record a code readable with
+ * cjx_device_status.                                                       */
+CJX_API int cjx_gemm(int64_t M, int64_t N, int64_t K, const void* A, int64_t lda,
+                     const void* B, int64_t ldb, void* C, int64_t ldc,
+                     const float* bias, int flags, int split_k, void* stream);
+/* First error code recorded by a device-side wait that gave up (0 = none);
+ * synchronises `stream`; reset != 0 clears it.                             */
+CJX_API int cjx_device_status(int* status, int reset, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -681,6 +681,45 @@ def normalize_image(image):
     return (image - image.mean()) / image.std()
 
 
+def normalized_cross_correlation(simulated, observed):
+    """Mean over pixels of normalize_image(sim) * normalize_image(obs) (Pearson r).
+
+    The score of the pose-search benchmark: the zero-mean, unit-std real-space
+    dot product (cryojax/ndimage/_normalize.py:11-28), divided by the pixel
+    count so that it lies in [-1, 1].
+    """
+    return float(np.mean(normalize_image(simulated) * normalize_image(observed)))
+
+
+def grid_search_orientations(grid, frequency_slice, specs, observed, quaternions):
+    """Exhaustive orientation search: best (max NCC) grid index per image.
+
+    For each image b, simulate spec b at every orientation of the grid (its
+    own CTF, offsets and scale; the spec's wxyz is replaced) and keep the
+    running best with the first index winning ties -- the elementwise
+    running argmin of MinimumSearchMethod.batch_update applied to -NCC
+    (cryojax/jax_util/_grid_search/search_method.py:237-265,
+    search_loop.py:24-158).  Returns (best_index (n,), scores (n, T)).
+    """
+    import copy
+
+    n, t = len(specs), len(quaternions)
+    scores = np.empty((n, t))
+    for b, spec in enumerate(specs):
+        for k, q in enumerate(quaternions):
+            s = copy.copy(spec)
+            s.wxyz = np.asarray(q, np.float64)
+            scores[b, k] = normalized_cross_correlation(simulate(grid, frequency_slice, s), observed[b])
+    best = np.empty(n, np.int64)
+    for b in range(n):
+        cur, idx = np.inf, 0
+        for k in range(t):  # strict "<" keeps the earliest index on ties
+            if -scores[b, k] < cur:
+                cur, idx = -scores[b, k], k
+        best[b] = idx
+    return best, scores
+
+
 # ---------------------------------------------------------------------------
 # Synthetic inputs (seeded): Gaussian-sum volumes, poses, CTF draws
 # ---------------------------------------------------------------------------

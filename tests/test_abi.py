@@ -77,3 +77,23 @@ def test_tuning_knobs():
         nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, 3)
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(99, 1)
+
+
+def _search_desc(n, py, px, n_img, n_orient, k):
+    s = nat.SearchDesc()
+    s.slice = nat.make_desc(n, py, px, nat.CJX_APPLY_CTF)
+    s.n_images, s.n_orientations, s.candidates_per_image = n_img, n_orient, k
+    return s
+
+
+def test_search_workspace_plan():
+    assert ctypes.sizeof(nat.SearchDesc) == 32 + 24
+    small = nat.search_workspace_size(_search_desc(64, 32, 32, 2, 96, 5))
+    big = nat.search_workspace_size(_search_desc(64, 32, 32, 2, 96, 0))
+    assert 0 < small < big  # exhaustive: 96 candidates per image, candidate lists: 5
+    with pytest.raises(nat.CryojaxB200Error) as e:  # the score needs the resize stage
+        nat.search_workspace_size(_search_desc(64, 64, 64, 2, 96, 0))
+    assert e.value.code == nat.CJX_ERR_UNSUPPORTED
+    with pytest.raises(nat.CryojaxB200Error) as e:
+        nat.search_workspace_size(_search_desc(64, 32, 32, 2, 0, 0))
+    assert e.value.code == nat.CJX_ERR_INVALID_ARGUMENT

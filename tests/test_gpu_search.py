@@ -1,0 +1,123 @@
+"""GPU: orientation search (cjx_search through the C-ABI) against the oracle's grid search.
+
+The oracle simulates every (image, orientation) pair in float64 and scores
+it with normalize_image semantics (Pearson r); its running argmin of -NCC
+keeps the earliest index on ties.  Tolerances: every device score within
+NCC_ABS_TOL of the oracle's; the device's best orientation equals the
+oracle's wherever the oracle's top two scores differ by more than
+2 * NCC_ABS_TOL, and otherwise scores within NCC_ABS_TOL of the maximum.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import cryojax_oracle as O
+from tests.helpers import make_volume, specs_to_model_args
+
+pytestmark = pytest.mark.gpu
+
+NCC_ABS_TOL = 5e-5
+
+
+def _specs(n, seed, shape, quats):
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(n):
+        out.append(O.ImageSpec(shape=shape, pixel_size=2.0, wxyz=quats[b],
+                               offset_in_angstroms=rng.uniform(-4, 4, 2),
+                               defocus_in_angstroms=rng.uniform(8000, 20000),
+                               astigmatism_in_angstroms=rng.uniform(0, 300), astigmatism_angle=rng.uniform(0, 180)))
+    return out
+
+
+def _observed(grid, fs, specs, seed, snr):
+    rng = np.random.default_rng(seed)
+    obs = []
+    for s in specs:
+        img = O.simulate(grid, fs, s)
+        if snr is not None:
+            img = img + rng.standard_normal(img.shape) * np.sqrt(img.var() / snr)
+        obs.append(img)
+    return np.stack(obs)
+
+
+def _model(grid, specs):
+    import torch
+
+    from cryojax_b200 import simulator as S
+
+    pose, tt, cfg = specs_to_model_args(specs)
+    vol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+    return S.make_image_model(vol, cfg, pose, tt)
+
+
+def _check_best(best, ref_scores):
+    for b in range(ref_scores.shape[0]):
+        s = np.sort(ref_scores[b])[::-1]
+        if s[0] - s[1] > 2 * NCC_ABS_TOL:
+            assert best[b] == int(np.argmax(ref_scores[b])), b
+        else:
+            assert ref_scores[b, best[b]] >= s[0] - NCC_ABS_TOL, b
+
+
+@pytest.mark.parametrize("box,shape,snr", [(32, (32, 32), None), (32, (32, 32), 0.5), (48, (64, 64), 0.2)])
+def test_exhaustive_scores_match_oracle(cuda_device, box, shape, snr):
+    from cryojax_b200.healpix import OrientationGrid
+    from cryojax_b200.search import PoseSearch
+
+    og = OrientationGrid(nside=1, n_inplane=8)  # 96 orientations
+    quats = og.quaternions()
+    _, grid, fs = make_volume(box, 40, seed=box + 1)
+    rng = np.random.default_rng(box)
+    true_idx = rng.choice(og.size, 3, replace=False)
+    specs = _specs(3, box + 2, shape, quats[true_idx])
+    obs = _observed(grid, fs, specs, box + 3, snr)
+    ref_best, ref_scores = O.grid_search_orientations(grid, fs, specs, obs, quats)
+
+    res = PoseSearch(og.rotation_matrices()).run(_model(grid, specs), obs, return_scores=True)
+    got = res.scores.cpu().numpy()
+    assert got.shape == ref_scores.shape
+    err = np.abs(got - ref_scores).max()
+    assert err <= NCC_ABS_TOL, err
+    _check_best(res.best_orientation, ref_scores)
+    np.testing.assert_allclose(res.best_score, got[np.arange(3), res.best_orientation], rtol=0, atol=0)
+    if snr is None:  # noiseless images drawn at grid orientations: the search recovers them
+        np.testing.assert_array_equal(res.best_orientation, true_idx)
+        assert np.all(res.best_score > 0.999)
+
+
+def test_candidate_lists_score_the_same_as_exhaustive(cuda_device):
+    from cryojax_b200.healpix import OrientationGrid
+    from cryojax_b200.search import PoseSearch
+
+    og = OrientationGrid(nside=1, n_inplane=8)
+    quats = og.quaternions()
+    _, grid, fs = make_volume(32, 40, seed=7)
+    specs = _specs(4, 8, (32, 32), quats[[5, 17, 40, 90]])
+    obs = _observed(grid, fs, specs, 9, 1.0)
+    search = PoseSearch(og.rotation_matrices())
+    model = _model(grid, specs)
+    full = search.run(model, obs, return_scores=True)
+    rng = np.random.default_rng(3)
+    cand = np.stack([rng.choice(og.size, 11, replace=False) for _ in range(4)]).astype(np.int32)
+    cand[:, 0] = cand[:, 3]  # a repeated candidate must not change the result
+    part = search.run(model, obs, candidates=cand, return_scores=True)
+    fs_ = full.scores.cpu().numpy()
+    np.testing.assert_array_equal(part.scores.cpu().numpy(), fs_[np.arange(4)[:, None], cand])
+    for b in range(4):
+        sc = fs_[b, cand[b]]
+        top = sc.max()
+        assert part.best_score[b] == top
+        assert part.best_orientation[b] == cand[b][sc == top].min()
+
+
+def test_search_rejects_bad_candidates(cuda_device):
+    from cryojax_b200.healpix import OrientationGrid
+    from cryojax_b200.search import PoseSearch
+
+    og = OrientationGrid(nside=1, n_inplane=4)
+    _, grid, fs = make_volume(32, 10, seed=1)
+    specs = _specs(2, 2, (32, 32), og.quaternions()[[0, 1]])
+    obs = _observed(grid, fs, specs, 3, None)
+    with pytest.raises(ValueError):
+        PoseSearch(og.rotation_matrices()).run(_model(grid, specs), obs, candidates=np.full((2, 3), og.size))
