@@ -180,6 +180,49 @@ _SIGNATURES = {
          ctypes.c_void_p],
     ),
     "cjx_device_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_void_p]),
+    "cjx_cnn_noisy_normalize": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+         ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "cjx_cnn_im2col": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_void_p],
+    ),
+    "cjx_cnn_col2im": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "cjx_transpose_to_bf16": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "cjx_relu_mask": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                     ctypes.c_void_p]),
+    "cjx_colsum": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_void_p],
+    ),
+    "cjx_softmax_xent": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+         ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "cjx_adamw": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+         ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "cjx_topk_candidates": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -420,6 +463,9 @@ CJX_GEMM_F16 = 16
 
 def gemm(a, b, c, *, bias=None, flags=0, split_k=1, m=None, n=None, k=None, stream=None) -> None:
     """cjx_gemm: c[:m, :n] (op)= a[:m, :k] @ b[:n, :k].T on torch CUDA tensors (row-major 2-D)."""
+    for t, what in ((a, "a"), (b, "b"), (c, "c")):
+        if t.dim() != 2:
+            raise ValueError(f"gemm operand {what} must be a 2-D tensor (row pitch = stride(0))")
     m = a.shape[0] if m is None else m
     n = b.shape[0] if n is None else n
     k = a.shape[1] if k is None else k
@@ -429,6 +475,86 @@ def gemm(a, b, c, *, bias=None, flags=0, split_k=1, m=None, n=None, k=None, stre
         int(m), int(n), int(k), _cuda_ptr(a, "a"), int(a.stride(0)), _cuda_ptr(b, "b"), int(b.stride(0)),
         _cuda_ptr(c, "c"), int(c.stride(0)), ctypes.c_void_p(0) if bias is None else _cuda_ptr(bias, "bias"),
         int(flags), int(split_k), _stream_ptr(stream)))
+
+
+class ParamSegment(ctypes.Structure):
+    _fields_ = [
+        ("offset", ctypes.c_int64),
+        ("count", ctypes.c_int64),
+        ("cols", ctypes.c_int64),
+        ("ldk", ctypes.c_int64),
+        ("w_bf16", ctypes.c_void_p),
+        ("wt_bf16", ctypes.c_void_p),
+        ("weight_decay", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+def _opt_ptr(t, what):
+    return ctypes.c_void_p(0) if t is None else _cuda_ptr(t, what)
+
+
+def cnn_noisy_normalize(images, out, *, index=None, snr=0.0, seed=0, n=None, stream=None) -> None:
+    n = out.shape[0] if n is None else n
+    h, w = images.shape[-2], images.shape[-1]
+    _check(load_library().cjx_cnn_noisy_normalize(
+        _cuda_ptr(images, "images"), _opt_ptr(index, "index"), int(n), int(h), int(w), float(snr),
+        ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), _cuda_ptr(out, "out"), _stream_ptr(stream)))
+
+
+def cnn_im2col(x, B, H, W, C, col, ldk, stream=None) -> None:
+    _check(load_library().cjx_cnn_im2col(_cuda_ptr(x, "x"), int(B), int(H), int(W), int(C), _cuda_ptr(col, "col"),
+                                         int(ldk), _stream_ptr(stream)))
+
+
+def cnn_col2im(dcol, ldk, act, B, H, W, C, dx, stream=None) -> None:
+    _check(load_library().cjx_cnn_col2im(_cuda_ptr(dcol, "dcol"), int(ldk), _opt_ptr(act, "act"), int(B), int(H),
+                                         int(W), int(C), _cuda_ptr(dx, "dx"), _stream_ptr(stream)))
+
+
+def transpose_to_bf16(inp, rows, cols, ld_in, out, ld_out, stream=None) -> None:
+    import torch
+
+    _check(load_library().cjx_transpose_to_bf16(
+        _cuda_ptr(inp, "in"), 1 if inp.dtype == torch.bfloat16 else 0, int(rows), int(cols), int(ld_in),
+        _cuda_ptr(out, "out"), int(ld_out), _stream_ptr(stream)))
+
+
+def relu_mask(grad, act, n, out, stream=None) -> None:
+    _check(load_library().cjx_relu_mask(_cuda_ptr(grad, "grad"), _opt_ptr(act, "act"), int(n), _cuda_ptr(out, "out"),
+                                        _stream_ptr(stream)))
+
+
+def colsum(x, rows, cols, ld, out, stream=None) -> None:
+    import torch
+
+    _check(load_library().cjx_colsum(_cuda_ptr(x, "x"), 1 if x.dtype == torch.bfloat16 else 0, int(rows), int(cols),
+                                     int(ld), _cuda_ptr(out, "out"), _stream_ptr(stream)))
+
+
+def softmax_xent(logits, labels, *, neighbours=None, smoothing=0.0, grad_scale=1.0, loss=None, dlogits=None,
+                 B=None, stream=None) -> None:
+    B = logits.shape[0] if B is None else B
+    n_nb = 0 if neighbours is None else neighbours.shape[1]
+    _check(load_library().cjx_softmax_xent(
+        _cuda_ptr(logits, "logits"), int(B), int(logits.shape[1]), _cuda_ptr(labels, "labels"),
+        _opt_ptr(neighbours, "neighbours"), int(n_nb), float(smoothing), float(grad_scale), _opt_ptr(loss, "loss"),
+        _opt_ptr(dlogits, "dlogits"), _stream_ptr(stream)))
+
+
+def adamw(params, grads, m, v, segments, *, lr, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0, step,
+          stream=None) -> None:
+    _check(load_library().cjx_adamw(
+        _cuda_ptr(params, "params"), _cuda_ptr(grads, "grads"), _cuda_ptr(m, "m"), _cuda_ptr(v, "v"),
+        int(params.numel()), ctypes.cast(segments, ctypes.c_void_p), len(segments), float(lr), float(beta1),
+        float(beta2), float(eps), float(weight_decay), int(step), _stream_ptr(stream)))
+
+
+def topk_candidates(logits, k, n_inplane, *, dirs=None, candidates=None, B=None, stream=None) -> None:
+    B = logits.shape[0] if B is None else B
+    _check(load_library().cjx_topk_candidates(
+        _cuda_ptr(logits, "logits"), int(B), int(logits.shape[1]), int(k), int(n_inplane), _opt_ptr(dirs, "dirs"),
+        _opt_ptr(candidates, "candidates"), _stream_ptr(stream)))
 
 
 def device_status(reset: bool = True, stream=None) -> int:

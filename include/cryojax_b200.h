@@ -325,6 +325,65 @@ CJX_API int cjx_gemm(int64_t M, int64_t N, int64_t K, const void* A, int64_t lda
  * synchronises `stream`; reset != 0 clears it.                             */
 CJX_API int cjx_device_status(int* status, int reset, void* stream);
 
+/* ---- pose-proposal network kernels (no counterpart in the reference) --- */
+/* Activations are NHWC BF16; a 3x3 stride-2 pad-1 convolution is
+ * im2col -> cjx_gemm (bias + ReLU fused) and its backward is cjx_gemm ->
+ * cjx_cnn_col2im.  Sizes are in elements.                                  */
+
+/* out[b] (BF16 [h][w]) = (x - mean) / std of x = images[index ? index[b] : b]
+ * + sigma_b * N(0, 1), sigma_b^2 = var(images[.]) / snr; snr <= 0 adds no
+ * noise.  The normal draws are a counter-based function of (seed, source
+ * image, pixel).                                                           */
+CJX_API int cjx_cnn_noisy_normalize(const float* images, const int64_t* index, int64_t n,
+                                    int h, int w, float snr, uint64_t seed, void* out,
+                                    void* stream);
+/* col[p][k] (BF16, row pitch ldk >= 9C, ldk % 8 == 0) of x [B][H][W][C]:
+ * p = (b H/2 + oy) W/2 + ox, k = (3 ky + kx) C + c, zeros in [9C, ldk).    */
+CJX_API int cjx_cnn_im2col(const void* x, int64_t B, int H, int W, int C, void* col,
+                           int64_t ldk, void* stream);
+/* dx (BF16 [B][H][W][C]) = col2im(dcol) (FP32 [p][ldk]), multiplied by
+ * (act > 0) when act (BF16, same shape as dx) is non-NULL.                 */
+CJX_API int cjx_cnn_col2im(const float* dcol, int64_t ldk, const void* act, int64_t B, int H,
+                           int W, int C, void* dx, void* stream);
+/* out[c][r] (BF16, pitch ld_out) = in[r][c] (FP32 or BF16, pitch ld_in).   */
+CJX_API int cjx_transpose_to_bf16(const void* in, int in_is_bf16, int64_t rows, int64_t cols,
+                                  int64_t ld_in, void* out, int64_t ld_out, void* stream);
+/* out[i] (BF16) = grad[i] * (act == NULL || act[i] > 0).                   */
+CJX_API int cjx_relu_mask(const float* grad, const void* act, int64_t n, void* out,
+                          void* stream);
+/* out[c] += sum_r x[r][c] (FP32 atomics; the caller zeroes out).          */
+CJX_API int cjx_colsum(const void* x, int x_is_bf16, int64_t rows, int64_t cols, int64_t ld,
+                       float* out, void* stream);
+/* Softmax cross entropy per row of logits [B][C] against the target
+ * (1 - smoothing) at labels[r] plus smoothing spread evenly over the
+ * n_neighbours entries neighbours[labels[r]][.] (over all C classes when
+ * neighbours is NULL).  loss[r] (optional) and dlogits (BF16 [B][C],
+ * optional) = (softmax - target) * grad_scale.                             */
+CJX_API int cjx_softmax_xent(const float* logits, int64_t B, int C, const int32_t* labels,
+                             const int32_t* neighbours, int n_neighbours, float smoothing,
+                             float grad_scale, float* loss, void* dlogits, void* stream);
+typedef struct cjx_param_segment {
+  int64_t offset;       /* first element in the flat parameter vector       */
+  int64_t count;        /* elements                                         */
+  int64_t cols;         /* > 0: a weight stored [count/cols][cols] (K x out) */
+  int64_t ldk;          /* row pitch of w_bf16 (>= count / cols)            */
+  void* w_bf16;         /* optional BF16 copy [cols][ldk] (out x K)         */
+  void* wt_bf16;        /* optional BF16 copy [count/cols][cols]            */
+  int32_t weight_decay; /* 1: apply decoupled weight decay                  */
+  int32_t reserved;
+} cjx_param_segment;
+/* AdamW step `step` (>= 1) over the flat FP32 vector params (n elements)
+ * with gradients grads and moments m, v; refreshes the weight segments'
+ * BF16 copies.  Segments are sorted by offset, the first at 0, <= 24.     */
+CJX_API int cjx_adamw(float* params, const float* grads, float* m, float* v, int64_t n,
+                      const cjx_param_segment* segments, int n_segments, float lr, float beta1,
+                      float beta2, float eps, float weight_decay, int64_t step, void* stream);
+/* Per row of logits [B][C] (C <= 1024): the k largest (ties -> lower
+ * index) into dirs[B][k] (optional) and candidates[B][k * n_inplane] =
+ * dirs * n_inplane + a for a in [0, n_inplane) (optional).                 */
+CJX_API int cjx_topk_candidates(const float* logits, int64_t B, int C, int k, int n_inplane,
+                                int32_t* dirs, int32_t* candidates, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
