@@ -126,3 +126,68 @@ class PoseSearch:
 def search_orientations(image_model, observed, rotations, **kw) -> SearchResult:
     """One-shot exhaustive / candidate search (see PoseSearch.run)."""
     return PoseSearch(rotations).run(image_model, observed, **kw)
+
+
+@dataclass
+class LearnedSearchResult:
+    best_orientation: np.ndarray   # (n,) int64
+    best_score: np.ndarray         # (n,) float32
+    fallback: np.ndarray           # (n,) bool: the exhaustive grid search decided this image
+    proposed_directions: object    # (n, k) int32 CUDA tensor, the network's top-k directions
+
+
+class LearnedPoseSearch:
+    """Network-proposed candidates rescored by the grid search's scorer, exhaustive fallback.
+
+    For each observed image the pose-proposal network ranks the grid's
+    HEALPix directions; the top ``top_k`` directions x every in-plane angle
+    are simulated and scored exactly as in the exhaustive search
+    (PoseSearch with a candidate list), and images whose best score falls
+    below ``threshold`` are searched exhaustively.  The exhaustive grid
+    search therefore stays both the fallback and the judge of the result.
+    """
+
+    def __init__(self, net, grid, *, top_k=16, threshold=float("-inf"), search: PoseSearch | None = None):
+        if net.n_classes != grid.n_dir:
+            raise ValueError("the network's classes must be the grid's directions")
+        self.net = net
+        self.grid = grid
+        self.top_k = top_k
+        self.threshold = threshold
+        self.search = search if search is not None else PoseSearch(grid.rotation_matrices())
+
+    def run(self, image_model, observed, *, batch=None, fallback=True) -> LearnedSearchResult:
+        """observed: real-space float32 CUDA images (n, P, P)."""
+        torch = _torch()
+        obs = observed if isinstance(observed, torch.Tensor) else torch.as_tensor(np.asarray(observed, np.float32))
+        obs = obs.to(device=self.search.rotations.device, dtype=torch.float32).contiguous()
+        obs_f = observed_to_fourier(obs)
+        pd = torch.as_tensor(image_model.image_params(), device=obs.device)
+        dirs, cand = self.net.propose(obs, k=self.top_k, n_inplane=self.grid.n_inplane, batch=batch)
+        res = self.search.run(image_model, obs_f, candidates=cand, observed_is_fourier=True, image_params_device=pd)
+        best, score = res.best_orientation.copy(), res.best_score.copy()
+        low = score < self.threshold
+        if fallback and low.any():
+            idx = torch.as_tensor(np.flatnonzero(low), device=obs.device)
+            ex = self.search.run(image_model, obs_f.index_select(0, idx).contiguous(), observed_is_fourier=True,
+                                 image_params_device=pd.index_select(0, idx).contiguous())
+            best[low] = ex.best_orientation
+            score[low] = ex.best_score
+        return LearnedSearchResult(best, score, low if fallback else np.zeros_like(low), dirs)
+
+    def calibrate_threshold(self, image_model, observed, exhaustive_best, *, target_agreement=0.995):
+        """Lowest threshold at which the calibration images agree with the exhaustive optimum.
+
+        Runs the learned search without fallback on calibration images whose
+        exhaustive optimum is known; images that disagree need the fallback,
+        so the threshold is set just above the best score of the disagreeing
+        images, allowing (1 - target_agreement) of the set to disagree above
+        it.  Sets and returns ``self.threshold``.
+        """
+        res = self.run(image_model, observed, fallback=False)
+        wrong = res.best_orientation != np.asarray(exhaustive_best)
+        allowed = int(np.floor((1.0 - target_agreement) * len(wrong)))
+        s = np.sort(res.best_score[wrong])[::-1]
+        self.threshold = float(np.nextafter(np.float32(s[allowed]), np.float32(np.inf))) if len(s) > allowed else \
+            float("-inf")
+        return self.threshold
