@@ -223,6 +223,22 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
          ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "cjx_pack_templates": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p],
+    ),
+    "cjx_pack_observed": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "cjx_ncc_argmax": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    ),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -555,6 +571,28 @@ def topk_candidates(logits, k, n_inplane, *, dirs=None, candidates=None, B=None,
     _check(load_library().cjx_topk_candidates(
         _cuda_ptr(logits, "logits"), int(B), int(logits.shape[1]), int(k), int(n_inplane), _opt_ptr(dirs, "dirs"),
         _opt_ptr(candidates, "candidates"), _stream_ptr(stream)))
+
+
+def pack_templates(images, py, px, s16, p16, n=None, stream=None) -> None:
+    n = images.shape[0] if n is None else n
+    _check(load_library().cjx_pack_templates(_cuda_ptr(images, "images"), int(n), int(py), int(px),
+                                             _cuda_ptr(s16, "s16"), _cuda_ptr(p16, "p16"), _stream_ptr(stream)))
+
+
+def pack_observed(observed, params, py, px, flags, y16, z16, oo, yinv, zinv, stream=None) -> None:
+    _check(load_library().cjx_pack_observed(
+        _cuda_ptr(observed, "observed"), _cuda_ptr(params, "params"), int(observed.shape[0]), int(py), int(px),
+        int(flags), _cuda_ptr(y16, "y16"), _cuda_ptr(z16, "z16"), _cuda_ptr(oo, "oo"), _cuda_ptr(yinv, "yinv"),
+        _cuda_ptr(zinv, "zinv"), _stream_ptr(stream)))
+
+
+def ncc_argmax(num, den, n, T, oo, yinv, zinv, best_score, best_orientation, *, t0=0, scores=None,
+               accumulate_best=False, stream=None) -> None:
+    _check(load_library().cjx_ncc_argmax(
+        _cuda_ptr(num, "num"), _cuda_ptr(den, "den"), int(num.stride(0)), int(n), int(T), _cuda_ptr(oo, "oo"),
+        _cuda_ptr(yinv, "yinv"), _cuda_ptr(zinv, "zinv"), int(t0), _opt_ptr(scores, "scores"),
+        int(scores.stride(0)) if scores is not None else 0, _cuda_ptr(best_score, "best_score"),
+        _cuda_ptr(best_orientation, "best_orientation"), 1 if accumulate_best else 0, _stream_ptr(stream)))
 
 
 def device_status(reset: bool = True, stream=None) -> int:

@@ -1,0 +1,202 @@
+// Template-sharing exhaustive search: the NCC of every (image, orientation)
+// pair from two tensor-core GEMMs instead of one simulation per pair.
+//
+// The simulated image of orientation t for image b is F = m_b * S_t, with
+// S_t the CTF-free central slice (resized, Hermitian-fixed columns) and m_b
+// the image's multiplier (scale, CTF, envelope, translation phase, Nyquist
+// zeroing; real and even in ky on the self-conjugate columns, so it
+// commutes with their Hermitian fix).  With Parseval weights w (0 at DC, 1
+// on the self-conjugate columns kx = 0 and kx = Px/2, 2 elsewhere):
+//   num(b, t) = sum w Re(conj(O_b) m_b S_t) = sum Y_b . S_t,  Y_b = w conj(m_b) O_b
+//   den(b, t) = sum w |m_b|^2 |S_t|^2      = sum Z_b |S_t|^2, Z_b = w |m_b|^2
+//   NCC = num / sqrt(den * sum w |O_b|^2)
+// so num is a GEMM over K = 2 Py (Px/2+1) interleaved (re, im) values and
+// den one over K = Py (Px/2+1).  Rows are stored in FP16 after a per-row
+// scale to unit RMS (the scales cancel in the NCC except for the image's).
+// No counterpart in the reference: its grid search simulates every pair.
+#include <cuda_fp16.h>
+
+#include "cjx_common.cuh"
+
+namespace cjx {
+
+__device__ __forceinline__ float block_sum_f(float v, float* red) {
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  float t = 0.f;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  return t;
+}
+
+__device__ __forceinline__ bool self_conj_col(int j, int px) { return j == 0 || ((px % 2 == 0) && j == px / 2); }
+
+// Hermitian fix of the self-conjugate columns: (S(i) + conj S(-i)) / 2.
+__device__ __forceinline__ float2 sym_value(const float2* img, int i, int j, int py, int px, int pxh) {
+  float2 v = img[(size_t)i * pxh + j];
+  if (self_conj_col(j, px)) {
+    const float2 m = img[(size_t)((py - i) % py) * pxh + j];
+    v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
+  }
+  return v;
+}
+
+// Per template (block): S16 row = s (re, im) of the Hermitian-fixed slice,
+// P16 row = s^2 |S|^2, with s = sqrt(Py pxh / sum |S|^2).
+__global__ void k_pack_templates(const float2* __restrict__ img, int py, int px, __half* __restrict__ s16,
+                                 __half* __restrict__ p16) {
+  __shared__ float red[32];
+  const int pxh = px / 2 + 1;
+  const int kp = py * pxh;
+  const float2* a = img + (size_t)blockIdx.x * kp;
+  float acc = 0.f;
+  for (int e = threadIdx.x; e < kp; e += blockDim.x) {
+    const float2 v = sym_value(a, e / pxh, e % pxh, py, px, pxh);
+    acc += v.x * v.x + v.y * v.y;
+  }
+  const float tot = block_sum_f(acc, red);
+  const float s = tot > 0.f ? sqrtf((float)kp / tot) : 0.f;
+  __half2* so = reinterpret_cast<__half2*>(s16 + (size_t)blockIdx.x * 2 * kp);
+  __half* po = p16 + (size_t)blockIdx.x * kp;
+  for (int e = threadIdx.x; e < kp; e += blockDim.x) {
+    const float2 v = sym_value(a, e / pxh, e % pxh, py, px, pxh);
+    so[e] = __floats2half2_rn(s * v.x, s * v.y);
+    po[e] = __float2half_rn(s * s * (v.x * v.x + v.y * v.y));
+  }
+}
+
+// Per observed image (block): Y16 = (w conj(m) O) / yinv, Z16 = (w |m|^2) / zinv
+// with yinv, zinv the rows' RMS, and oo = sum w |O|^2.
+__global__ void k_pack_observed(const float2* __restrict__ obs, const cjx_image_params* __restrict__ params, int py,
+                                int px, uint32_t flags, __half* __restrict__ y16, __half* __restrict__ z16,
+                                float* __restrict__ oo, float* __restrict__ yinv, float* __restrict__ zinv) {
+  __shared__ float red[32];
+  const int pxh = px / 2 + 1;
+  const int kp = py * pxh;
+  const float2* o = obs + (size_t)blockIdx.x * kp;
+  const ImageConsts c = load_image_consts(params + blockIdx.x, 1.0f, py, px);
+  float ay = 0.f, az = 0.f, ao = 0.f;
+  for (int e = threadIdx.x; e < kp; e += blockDim.x) {
+    const int i = e / pxh, j = e - (e / pxh) * pxh;
+    const float w = (i == 0 && j == 0) ? 0.f : (self_conj_col(j, px) ? 1.f : 2.f);
+    const float2 m = apply_epilogue(make_float2(1.f, 0.f), i, j, py, px, flags, c);
+    const float2 v = o[e];
+    const float yx = w * (m.x * v.x + m.y * v.y), yy = w * (m.x * v.y - m.y * v.x);
+    const float z = w * (m.x * m.x + m.y * m.y);
+    ay += yx * yx + yy * yy;
+    az += z * z;
+    ao += w * (v.x * v.x + v.y * v.y);
+  }
+  const float ty = block_sum_f(ay, red), tz = block_sum_f(az, red), to = block_sum_f(ao, red);
+  const float ry = ty > 0.f ? sqrtf(ty / (2.f * kp)) : 1.f, rz = tz > 0.f ? sqrtf(tz / kp) : 1.f;
+  if (threadIdx.x == 0) {
+    oo[blockIdx.x] = to;
+    yinv[blockIdx.x] = ry;
+    zinv[blockIdx.x] = rz;
+  }
+  __half2* yo = reinterpret_cast<__half2*>(y16 + (size_t)blockIdx.x * 2 * kp);
+  __half* zo = z16 + (size_t)blockIdx.x * kp;
+  const float sy = 1.f / ry, sz = 1.f / rz;
+  for (int e = threadIdx.x; e < kp; e += blockDim.x) {
+    const int i = e / pxh, j = e - (e / pxh) * pxh;
+    const float w = (i == 0 && j == 0) ? 0.f : (self_conj_col(j, px) ? 1.f : 2.f);
+    const float2 m = apply_epilogue(make_float2(1.f, 0.f), i, j, py, px, flags, c);
+    const float2 v = o[e];
+    yo[e] = __floats2half2_rn(sy * w * (m.x * v.x + m.y * v.y), sy * w * (m.x * v.y - m.y * v.x));
+    zo[e] = __float2half_rn(sz * w * (m.x * m.x + m.y * m.y));
+  }
+}
+
+// Per image row (block): NCC over the T templates and its argmax (ties ->
+// lowest index); optional scores out.
+__global__ void k_ncc_argmax(const float* __restrict__ num, const float* __restrict__ den, int64_t ld,
+                             int64_t T, const float* __restrict__ oo, const float* __restrict__ yinv,
+                             const float* __restrict__ zinv, int64_t t0, float* __restrict__ scores,
+                             int64_t ld_scores, float* __restrict__ best_score, int32_t* __restrict__ best_orient,
+                             int accumulate_best) {
+  __shared__ float sv[32];
+  __shared__ int64_t si[32];
+  const int64_t b = blockIdx.x;
+  const float yr = yinv[b], zr = zinv[b], o2 = oo[b];
+  float bv = -INFINITY;
+  int64_t bi = INT64_MAX;
+  for (int64_t t = threadIdx.x; t < T; t += blockDim.x) {
+    const float n = num[b * ld + t] * yr, d = den[b * ld + t] * zr;
+    const float s = (d > 0.f && o2 > 0.f) ? n * rsqrtf(d * o2) : 0.f;
+    if (scores) scores[b * ld_scores + t0 + t] = s;
+    if (s > bv) {  // t increases per thread: strict ">" keeps the lowest index
+      bv = s;
+      bi = t0 + t;
+    }
+  }
+  for (int s = 16; s > 0; s >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, s);
+    const int64_t oi = __shfl_xor_sync(0xffffffffu, bi, s);
+    if (ov > bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sv[w] = bv;
+    si[w] = bi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
+      if (sv[k] > bv || (sv[k] == bv && si[k] < bi)) {
+        bv = sv[k];
+        bi = si[k];
+      }
+    if (bi == INT64_MAX) bi = t0;
+    if (!accumulate_best || bv > best_score[b] || (bv == best_score[b] && bi < best_orient[b])) {
+      best_score[b] = bv;
+      best_orient[b] = (int32_t)bi;
+    }
+  }
+}
+
+}  // namespace cjx
+
+extern "C" {
+
+int cjx_pack_templates(const void* images, int64_t n, int py, int px, void* s16, void* p16, void* stream) {
+  if (n < 0 || py < 2 || px < 2) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_templates: bad shape");
+  if (n == 0) return CJX_OK;
+  if (!images || !s16 || !p16) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_templates: NULL pointer");
+  if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "pack_templates: too many templates");
+  cjx::k_pack_templates<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const float2*>(images), py, px, static_cast<__half*>(s16), static_cast<__half*>(p16));
+  return cjx::check_cuda(cudaGetLastError(), "pack_templates launch");
+}
+
+int cjx_pack_observed(const void* observed, const cjx_image_params* params, int64_t n, int py, int px, int flags,
+                      void* y16, void* z16, float* oo, float* yinv, float* zinv, void* stream) {
+  if (n < 0 || py < 2 || px < 2) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_observed: bad shape");
+  if (n == 0) return CJX_OK;
+  if (!observed || !params || !y16 || !z16 || !oo || !yinv || !zinv)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_observed: NULL pointer");
+  if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "pack_observed: too many images");
+  cjx::k_pack_observed<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const float2*>(observed), params, py, px, (uint32_t)flags, static_cast<__half*>(y16),
+      static_cast<__half*>(z16), oo, yinv, zinv);
+  return cjx::check_cuda(cudaGetLastError(), "pack_observed launch");
+}
+
+int cjx_ncc_argmax(const float* num, const float* den, int64_t ld, int64_t n, int64_t T, const float* oo,
+                   const float* yinv, const float* zinv, int64_t t0, float* scores, int64_t ld_scores,
+                   float* best_score, int32_t* best_orientation, int accumulate_best, void* stream) {
+  if (n < 0 || T < 1 || ld < T || t0 < 0 || t0 + T > 2147483647LL)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_argmax: bad sizes");
+  if (n == 0) return CJX_OK;
+  if (!num || !den || !oo || !yinv || !zinv || !best_score || !best_orientation)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_argmax: NULL pointer");
+  cjx::k_ncc_argmax<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      num, den, ld, T, oo, yinv, zinv, t0, scores, ld_scores, best_score, best_orientation, accumulate_best);
+  return cjx::check_cuda(cudaGetLastError(), "ncc_argmax launch");
+}
+
+}  // extern "C"

@@ -191,3 +191,95 @@ class LearnedPoseSearch:
         self.threshold = float(np.nextafter(np.float32(s[allowed]), np.float32(np.inf))) if len(s) > allowed else \
             float("-inf")
         return self.threshold
+
+
+class TemplateSharingSearch:
+    """Exhaustive NCC search through CTF-free templates shared by all images.
+
+    Each orientation's central slice is simulated once without CTF; every
+    image's CTF (and shifts, envelope, scale) moves onto its observed image,
+    and the numerator and denominator of all (image, orientation) NCCs are
+    two FP16 tensor-core GEMMs (see cjx_pack_templates / cjx_pack_observed /
+    cjx_ncc_argmax).  Exact in real arithmetic; FP16 operands make the scores
+    approximate (about 1e-3 relative), so near-ties may resolve differently
+    from PoseSearch.  Needs padded_shape == shape and Py a multiple of 8.
+    """
+
+    def __init__(self, rotations, *, device="cuda", template_chunk=4096, image_chunk=4096):
+        torch = _torch()
+        self.rot = np.ascontiguousarray(np.asarray(rotations, np.float64).reshape(-1, 9))
+        self.n_orientations = self.rot.shape[0]
+        self.device = torch.device(device)
+        self.template_chunk = template_chunk
+        self.image_chunk = image_chunk
+        self.s16 = self.p16 = None
+        self._key = None
+
+    def build_templates(self, image_model):
+        """Simulate and pack the CTF-free templates of every orientation (cached per volume and shape)."""
+        torch = _torch()
+        from .constants import wavelength_from_kilovolts
+
+        cfg = image_model.image_config
+        if tuple(cfg.padded_shape) != tuple(cfg.shape):
+            raise NotImplementedError("the NCC search needs padded_shape == shape")
+        vol = image_model.volume_parametrization.get_representation()
+        py, px = cfg.padded_shape
+        if py % 8:
+            raise NotImplementedError("TemplateSharingSearch needs Py to be a multiple of 8")
+        key = (id(vol.fourier_voxel_grid), py, px, float(np.ravel(cfg.pixel_size)[0]))
+        if key == self._key and self.s16 is not None:
+            return
+        kp = py * (px // 2 + 1)
+        T = self.n_orientations
+        self.s16 = torch.empty((T, 2 * kp), dtype=torch.float16, device=self.device)
+        self.p16 = torch.empty((T, kp), dtype=torch.float16, device=self.device)
+        integ = image_model.volume_integrator
+        p = nat.empty_params(T)
+        p[:, 0:9] = self.rot
+        p[:, nat.P_PIXEL_SIZE] = float(np.ravel(cfg.pixel_size)[0])
+        p[:, nat.P_WAVELENGTH] = wavelength_from_kilovolts(float(np.ravel(cfg.voltage_in_kilovolts)[0]))
+        p[:, nat.P_SCALE] = 1.0
+        pd = torch.as_tensor(p, device=self.device)
+        tc = min(self.template_chunk, T)
+        buf = torch.empty((tc, py, px // 2 + 1), dtype=torch.complex64, device=self.device)
+        ws = None
+        for s in range(0, T, tc):
+            e = min(T, s + tc)
+            out = buf[:e - s]
+            integ.run(vol, cfg, None, 0, params_device=pd[s:e], out=out, workspace=ws, n=e - s)
+            nat.pack_templates(out, py, px, self.s16[s:e], self.p16[s:e])
+        self._key = key
+
+    def run(self, image_model, observed, *, observed_is_fourier=False, image_params_device=None,
+            return_scores=False) -> SearchResult:
+        torch = _torch()
+        self.build_templates(image_model)
+        cfg = image_model.image_config
+        py, px = cfg.padded_shape
+        kp = py * (px // 2 + 1)
+        obs_f = observed if observed_is_fourier else observed_to_fourier(observed)
+        n = obs_f.shape[0]
+        pd = image_params_device if image_params_device is not None else torch.as_tensor(
+            image_model.image_params(), device=self.device)
+        flags = image_model._flags()
+        T = self.n_orientations
+        dev = self.device
+        y16 = torch.empty((n, 2 * kp), dtype=torch.float16, device=dev)
+        z16 = torch.empty((n, kp), dtype=torch.float16, device=dev)
+        oo, yinv, zinv = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+        nat.pack_observed(obs_f, pd, py, px, flags, y16, z16, oo, yinv, zinv)
+        best_score = torch.empty(n, dtype=torch.float32, device=dev)
+        best = torch.empty(n, dtype=torch.int32, device=dev)
+        scores = torch.empty((n, T), dtype=torch.float32, device=dev) if return_scores else None
+        mc = min(self.image_chunk, n)
+        num = torch.empty((mc, T), dtype=torch.float32, device=dev)
+        den = torch.empty((mc, T), dtype=torch.float32, device=dev)
+        for s in range(0, n, mc):
+            e = min(n, s + mc)
+            m = e - s
+            nat.gemm(y16[s:e], self.s16, num, m=m, n=T, k=2 * kp, flags=nat.CJX_GEMM_F16)
+            nat.gemm(z16[s:e], self.p16, den, m=m, n=T, k=kp, flags=nat.CJX_GEMM_F16)
+            nat.ncc_argmax(num, den, m, T, oo[s:e], yinv[s:e], zinv[s:e], best_score[s:e], best[s:e],
+                           scores=None if scores is None else scores[s:e])
+        return SearchResult(best.cpu().numpy().astype(np.int64), best_score.cpu().numpy(), scores, None)

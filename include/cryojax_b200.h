@@ -304,6 +304,36 @@ CJX_API int cjx_profile_enable(int on);
 CJX_API int cjx_profile_read(char* names, int64_t* counts, double* total_ms,
                              int max_kernels, int* n_kernels);
 
+/* ---- template-sharing exhaustive search --------------------------------- */
+/* The NCC of every (image, orientation) pair from two FP16 tensor-core
+ * GEMMs (cjx_gemm with CJX_GEMM_F16): num = Y S^T over K = 2 Py (Px/2+1)
+ * and den = Z P^T over K = Py (Px/2+1), where S_t is the CTF-free slice of
+ * orientation t (Hermitian-fixed columns), P_t = |S_t|^2, Y_b = w conj(m_b)
+ * O_b and Z_b = w |m_b|^2 (m_b: image b's CTF, envelope, translation and
+ * scale; w: Parseval weights, 0 at DC).  Rows are FP16 at unit RMS; Py must
+ * be a multiple of 8 (the rows are the GEMM operands).  No counterpart in
+ * the reference (its grid search simulates every pair).                    */
+/* images: complex64 [n][Py][Px/2+1] CTF-free slices -> s16 [n][2 Py (Px/2+1)],
+ * p16 [n][Py (Px/2+1)] (FP16).                                             */
+CJX_API int cjx_pack_templates(const void* images, int64_t n, int py, int px, void* s16,
+                               void* p16, void* stream);
+/* observed: complex64 [n][Py][Px/2+1] (rfftn of the observed images);
+ * params: the images' records (rotation ignored); flags: the CJX_APPLY_*
+ * bits of the image model -> y16, z16 (FP16 rows), oo = sum w |O|^2 and
+ * the rows' RMS scales yinv, zinv.                                         */
+CJX_API int cjx_pack_observed(const void* observed, const cjx_image_params* params, int64_t n,
+                              int py, int px, int flags, void* y16, void* z16, float* oo,
+                              float* yinv, float* zinv, void* stream);
+/* NCC(b, t0 + t) = num[b][t] yinv[b] / sqrt(den[b][t] zinv[b] oo[b]) for t
+ * in [0, T) (num, den: FP32 [n][ld]); writes scores[b][t0 + t] when scores
+ * is non-NULL and the row's best (ties -> lowest index) into best_score /
+ * best_orientation, or merges it with their current values when
+ * accumulate_best != 0 (orientation blocks processed in increasing t0).    */
+CJX_API int cjx_ncc_argmax(const float* num, const float* den, int64_t ld, int64_t n, int64_t T,
+                           const float* oo, const float* yinv, const float* zinv, int64_t t0,
+                           float* scores, int64_t ld_scores, float* best_score,
+                           int32_t* best_orientation, int accumulate_best, void* stream);
+
 /* ---- tensor-core GEMM (pose-proposal network) -------------------------- */
 #define CJX_GEMM_OUT_BF16 1   /* store C as BF16 (default FP32)              */
 #define CJX_GEMM_BIAS 2       /* C[:, n] += bias[n] (FP32)                    */

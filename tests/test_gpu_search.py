@@ -121,3 +121,30 @@ def test_search_rejects_bad_candidates(cuda_device):
     obs = _observed(grid, fs, specs, 3, None)
     with pytest.raises(ValueError):
         PoseSearch(og.rotation_matrices()).run(_model(grid, specs), obs, candidates=np.full((2, 3), og.size))
+
+
+@pytest.mark.parametrize("shift", [0.0, 4.0])
+def test_template_sharing_search_matches_plain_scores(cuda_device, shift):
+    """FP16 GEMM scores within 2e-3 of the plain FP32 scorer; same argmax unless near-tied."""
+    from cryojax_b200.healpix import OrientationGrid
+    from cryojax_b200.search import PoseSearch, TemplateSharingSearch
+
+    og = OrientationGrid(nside=2, n_inplane=8)  # 384 orientations
+    quats = og.quaternions()
+    _, grid, fs = make_volume(48, 60, seed=21)
+    rng = np.random.default_rng(4)
+    specs = _specs(12, 5, (64, 64), quats[rng.choice(og.size, 12, replace=False)])
+    for s in specs:
+        s.offset_in_angstroms = rng.uniform(-shift, shift, 2)
+    obs = _observed(grid, fs, specs, 6, 0.3)
+    model = _model(grid, specs)
+    plain = PoseSearch(og.rotation_matrices()).run(model, obs, return_scores=True)
+    shared = TemplateSharingSearch(og.rotation_matrices(), template_chunk=100, image_chunk=5).run(
+        model, obs, return_scores=True)
+    a, b = plain.scores.cpu().numpy(), shared.scores.cpu().numpy()
+    assert np.abs(a - b).max() <= 2e-3, np.abs(a - b).max()
+    for k in range(12):
+        srt = np.sort(a[k])[::-1]
+        if srt[0] - srt[1] > 4e-3:
+            assert shared.best_orientation[k] == plain.best_orientation[k]
+        assert abs(shared.best_score[k] - b[k].max()) == 0
