@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--pad-scale", type=float, default=2.0)
     ap.add_argument("--chunk", type=int, default=0, help="images per workspace chunk (0 = library default)")
     ap.add_argument("--ilp", type=int, default=0, help="gather ILP (1, 2, 4; 0 = library default)")
+    ap.add_argument("--layout", choices=["pairs", "bricked", "linear"], default="pairs",
+                    help="device layout of the volume the gather reads")
     ap.add_argument("--order", choices=["orientation", "none"], default="orientation",
                     help="image processing order (orientation-sorted for L2 reuse, or as given)")
     ap.add_argument("--cpu-sample", type=int, default=6, help="images in the bounded CPU sample")
@@ -76,6 +78,9 @@ def config_dict(args, world):
         "l2_flush": "not needed: volume (1.07 GB) and output (6.75 GB per step) exceed the 126 MB L2",
         "parallelism": f"replicas x{world} (images sharded, no collective)",
         "processing_order": args.order,
+        "volume_layout": {"pairs": "x-pair bricked (16-byte entries g(x), g(x+1))",
+                          "bricked": "bricked (8^3 blocks, Morton order inside)",
+                          "linear": "C-order [z][y][x]"}[args.layout],
     }
 
 
@@ -582,6 +587,8 @@ def main():
         order_d = torch.as_tensor(S.orientation_order(pose.rotation_matrices()), device=dev)
     flags = model._flags()
     integ = model.volume_integrator
+    integ.use_bricked_layout = args.layout != "linear"
+    integ.pair_layout = args.layout == "pairs"
     py, px = cfg.padded_shape
     out = torch.empty((args.images, py, px // 2 + 1), dtype=torch.complex64, device=dev)
     desc = nat.make_desc(n, py, px, flags, integ.fill_value, args.chunk)

@@ -27,6 +27,7 @@ CJX_APPLY_TRANSLATION = 1 << 1
 CJX_APPLY_ENVELOPE = 1 << 2
 CJX_ZERO_FILL_NEGATIVE = 1 << 3
 CJX_GRID_BRICKED = 1 << 4
+CJX_GRID_BRICKED_PAIRS = 1 << 5
 
 CJX_MAX_SIDE = 1024
 CJX_TUNE_GATHER_ILP = 1
@@ -173,6 +174,7 @@ _SIGNATURES = {
     ),
     "cjx_tuning_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64]),
     "cjx_tuning_get": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
+    "cjx_brick_volume_pairs": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cjx_gemm": (
         ctypes.c_int,
         [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
@@ -614,6 +616,12 @@ def probe_read_bandwidth(buf, passes, sink, stream=None) -> None:
     )
 
 
+def brick_volume_pairs(n: int, grid, pairs, stream=None) -> None:
+    """x-pair bricked copy (CJX_GRID_BRICKED_PAIRS) of a complex64 N^3 grid into `pairs`."""
+    _check(load_library().cjx_brick_volume_pairs(int(n), _cuda_ptr(grid, "grid"), _cuda_ptr(pairs, "pairs"),
+                                                 _stream_ptr(stream)))
+
+
 def bricked_volume_size(n: int) -> int:
     out = ctypes.c_size_t(0)
     _check(load_library().cjx_bricked_volume_size(int(n), ctypes.byref(out)))
@@ -630,6 +638,18 @@ def brick_volume(grid, stream=None):
     out = torch.empty(bricked_volume_size(n) // 8, dtype=torch.complex64, device=grid.device)
     _check(load_library().cjx_brick_volume(int(n), _cuda_ptr(grid, "grid"), _cuda_ptr(out, "bricked"),
                                            _stream_ptr(stream)))
+    return out
+
+
+def brick_volume_pairs_new(grid, stream=None):
+    """x-pair bricked copy (CJX_GRID_BRICKED_PAIRS; 16 bytes per entry) of a complex64 [N, N, N] grid."""
+    import torch
+
+    n = grid.shape[0]
+    if grid.dtype != torch.complex64 or tuple(grid.shape) != (n, n, n):
+        raise ValueError("grid must be complex64 [N, N, N]")
+    out = torch.empty(2 * bricked_volume_size(n) // 8, dtype=torch.complex64, device=grid.device)
+    brick_volume_pairs(n, grid.contiguous(), out, stream)
     return out
 
 

@@ -73,7 +73,8 @@ def autotune(model, *, n_sample=1024, repeats=2, candidates=None, use_cache=True
     vol = model.volume_parametrization
     cfg = model.image_config
     integ = model.volume_integrator
-    flags = model._flags() | integ._base_flags() | (nat.CJX_GRID_BRICKED if integ.use_bricked_layout else 0)
+    grid, layout = integ.device_grid(vol)
+    flags = model._flags() | integ._base_flags() | layout
     n = vol.shape[0]
     py, px = cfg.padded_shape
     key = _key(n, py, px, flags)
@@ -87,7 +88,6 @@ def autotune(model, *, n_sample=1024, repeats=2, candidates=None, use_cache=True
     m = min(n_sample, params.shape[0])
     pd = torch.as_tensor(params[:m], device=vol.fourier_voxel_grid.device)
     out = torch.empty((m, py, px // 2 + 1), dtype=torch.complex64, device=pd.device)
-    grid = vol.bricked_grid() if integ.use_bricked_layout else vol.fourier_voxel_grid
     old = (nat.tuning_get(nat.CJX_TUNE_GATHER_ILP), nat.tuning_get(nat.CJX_TUNE_GATHER_TILE),
            nat.tuning_get(nat.CJX_TUNE_CHUNK_BYTES))
     best, best_ms = None, float("inf")
@@ -148,11 +148,8 @@ class BatchedSimulator:
             vol = model.volume_parametrization
             cfg = model.image_config
             integ = model.volume_integrator
-            flags = model._flags() | integ._base_flags()
-            grid = vol.fourier_voxel_grid
-            if integ.use_bricked_layout:
-                grid = vol.bricked_grid()
-                flags |= nat.CJX_GRID_BRICKED
+            grid, layout = integ.device_grid(vol)
+            flags = model._flags() | integ._base_flags() | layout
             params = model.image_params()
             dev = grid.device
             pd = torch.as_tensor(params, device=dev)

@@ -496,6 +496,8 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
   if (s_loss > 227 * 1024 || s_rows > 227 * 1024 || s_cols > 227 * 1024)
     return fail(CJX_ERR_UNSUPPORTED, "loss gradient shared-memory footprint above 227 KB for these sizes");
   if (int e = ensure_adjoint_smem_attrs()) return e;
+  if (g.flags & CJX_GRID_BRICKED_PAIRS)
+    return fail(CJX_ERR_UNSUPPORTED, "the adjoint reads the grid in the linear or bricked layout, not x-pairs");
   const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);

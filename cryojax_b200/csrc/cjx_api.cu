@@ -29,6 +29,7 @@ int tuning_set(int key, int64_t value);
 int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
 size_t bricked_elements(int n);
 int launch_brick_volume(int n, const float2* grid, float2* bricked, cudaStream_t stream);
+int launch_brick_volume_pairs(int n, const float2* grid, float4* out, cudaStream_t stream);
 
 static thread_local std::string g_last_error;
 
@@ -164,6 +165,14 @@ int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream) {
   if (grid == bricked) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and bricked must not alias");
   return launch_brick_volume(n, static_cast<const float2*>(grid), static_cast<float2*>(bricked),
                              static_cast<cudaStream_t>(stream));
+}
+
+int cjx_brick_volume_pairs(int n, const void* grid, void* pairs, void* stream) {
+  if (n < 2 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE]");
+  if (!grid || !pairs) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and pairs must be non-NULL");
+  if (grid == pairs) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and pairs must not alias");
+  return launch_brick_volume_pairs(n, static_cast<const float2*>(grid), static_cast<float4*>(pairs),
+                                   static_cast<cudaStream_t>(stream));
 }
 
 int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_images, size_t* bytes) {

@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <type_traits>
 
 #include "../../include/cryojax_b200.h"
 #include "cjx_fft.cuh"
@@ -254,6 +255,89 @@ __device__ __forceinline__ void sample_trilinear_batch_fast(const float2* __rest
     }
     out[s] = acc;
   }
+}
+
+// x-pair layout: the bricked (Morton-in-8^3-block) order of BrickLayout with
+// 16-byte entries holding (g(x, y, z), g(x + 1, y, z)) (the second half is 0
+// at x = N - 1).  An interior trilinear sample reads its 8 corners with 4
+// vector loads.  The grid pointer is float4; entry e's first half is g at
+// e's own coordinates, so single-corner reads use the float2 view at 2 e.
+struct PairLayout : BrickLayout {
+  __host__ __device__ explicit PairLayout(int n) : BrickLayout(n) {}
+};
+
+template <int S>
+__device__ __forceinline__ void sample_trilinear_batch_pairs(const float4* __restrict__ grid, int n,
+                                                             const PairLayout& L, const float* ox, const float* oy,
+                                                             const float* oz, const bool* active, bool wrap_negative,
+                                                             float2 fill, float2* out) {
+  float2 v[S][8];
+  float w[S][6];
+  const int h = n / 2;
+  const float2* g2 = reinterpret_cast<const float2*>(grid);
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const float fx = floorf(ox[s]), fy = floorf(oy[s]), fz = floorf(oz[s]);
+    w[s][1] = ox[s] - fx; w[s][0] = 1.0f - w[s][1];
+    w[s][3] = oy[s] - fy; w[s][2] = 1.0f - w[s][3];
+    w[s][5] = oz[s] - fz; w[s][4] = 1.0f - w[s][5];
+    const int ix0 = (int)fx + h, iy0 = (int)fy + h, iz0 = (int)fz + h;
+    const bool interior = (unsigned)ix0 < (unsigned)(n - 1) && (unsigned)iy0 < (unsigned)(n - 1) &&
+                          (unsigned)iz0 < (unsigned)(n - 1);
+    if (interior) {
+      if (active[s]) {
+        const int x0 = L.ax(ix0);
+        const int y0 = L.ay(iy0), y1 = L.ay(iy0 + 1);
+        const int z0 = L.az(iz0), z1 = L.az(iz0 + 1);
+        const float4 a = __ldg(grid + z0 + y0 + x0);
+        const float4 b = __ldg(grid + z0 + y1 + x0);
+        const float4 c = __ldg(grid + z1 + y0 + x0);
+        const float4 d = __ldg(grid + z1 + y1 + x0);
+        v[s][0] = make_float2(a.x, a.y); v[s][1] = make_float2(a.z, a.w);
+        v[s][2] = make_float2(b.x, b.y); v[s][3] = make_float2(b.z, b.w);
+        v[s][4] = make_float2(c.x, c.y); v[s][5] = make_float2(c.z, c.w);
+        v[s][6] = make_float2(d.x, d.y); v[s][7] = make_float2(d.z, d.w);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[s][c] = make_float2(0.f, 0.f);
+      }
+    } else {
+      const AxisNodes ax = axis_nodes(ox[s], n, wrap_negative);
+      const AxisNodes ay = axis_nodes(oy[s], n, wrap_negative);
+      const AxisNodes az = axis_nodes(oz[s], n, wrap_negative);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+        const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
+        const bool ok = active[s] && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
+        v[s][c] = ok ? __ldg(&g2[2 * (L.az(iz) + L.ay(iy) + L.ax(ix))]) : fill;
+      }
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+      const float wt = (w[s][4 + dz] * w[s][2 + dy]) * w[s][dx];
+      acc.x = fmaf(wt, v[s][c].x, acc.x);
+      acc.y = fmaf(wt, v[s][c].y, acc.y);
+    }
+    out[s] = acc;
+  }
+}
+
+// Trilinear samples from a grid in any of the three layouts.
+template <int S, typename Layout>
+__device__ __forceinline__ void gather_samples(const float2* __restrict__ grid, int n, const Layout& L,
+                                               const float* ox, const float* oy, const float* oz,
+                                               const bool* active, bool wrap_negative, float2 fill, float2* out) {
+  if constexpr (std::is_same<Layout, PairLayout>::value)
+    sample_trilinear_batch_pairs<S>(reinterpret_cast<const float4*>(grid), n, L, ox, oy, oz, active, wrap_negative,
+                                    fill, out);
+  else
+    sample_trilinear_batch_fast<S>(grid, n, L, ox, oy, oz, active, wrap_negative, fill, out);
 }
 
 // Lane -> sample mapping inside a CTA's 16 x 16 patch of the plane (MAP):

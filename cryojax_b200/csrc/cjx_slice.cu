@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kWarps * 32)
         oy[s] = fmaf(r11, vy, by);
         oz[s] = fmaf(r21, vy, bz);
       }
-      sample_trilinear_batch_fast<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
+      gather_samples<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
 #pragma unroll
       for (int s = 0; s < S; ++s)
         if (act[s]) a[i0 + 32 * s] = val[s];
@@ -110,8 +110,13 @@ __global__ void __launch_bounds__(kWarps * 32)
 // half-plane slice H[kx][ky] to an L2-resident buffer, then a column kernel
 // that runs the Hermitian fix, inverse FFT and window on H.
 // ---------------------------------------------------------------------------
+// Minimum resident CTAs per SM the compiler must allow for (register cap).
+#ifndef CJX_GATHER_MIN_BLOCKS
+#define CJX_GATHER_MIN_BLOCKS 1
+#endif
+
 template <int S, typename Layout, int MAP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, CJX_GATHER_MIN_BLOCKS)
     k_gather_slice(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
                    const int32_t* __restrict__ order, float2* __restrict__ hbuf, SliceGeom g, int64_t k0) {
   const Layout L(g.n);
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(256)
     oy[s] = fmaf(r11, vy, by);
     oz[s] = fmaf(r21, vy, bz);
   }
-  sample_trilinear_batch_fast<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
+  gather_samples<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
   float2* col = hbuf + ((size_t)blockIdx.z * g.nxh + u) * g.ldh;
 #pragma unroll
   for (int s = 0; s < S; ++s)
@@ -509,7 +514,7 @@ __global__ void __launch_bounds__(256)
     const float ox = fmaf(r01, vy, r00 * ux), oy = fmaf(r11, vy, r10 * ux), oz = fmaf(r21, vy, r20 * ux);
     const bool act = true;
     float2 v;
-    sample_trilinear_batch_fast<1>(grid, n, L, &ox, &oy, &oz, &act, wrap, g.fill, &v);
+    gather_samples<1>(grid, n, L, &ox, &oy, &oz, &act, wrap, g.fill, &v);
     // convert_fftn_to_rfftn(mode="real")  (cryojax/ndimage/_fourier_utils.py:6-57)
     if ((n % 2 == 0) && ((i == h && j == 0) || (i == 0 && j == h) || (i == h && j == h))) v.y = 0.f;
     dst[e] = apply_epilogue(v, i, j, n, n, g.flags, c);
@@ -542,8 +547,11 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
   if (d->n > CJX_MAX_SIDE || d->py > CJX_MAX_SIDE || d->px > CJX_MAX_SIDE)
     return fail(CJX_ERR_UNSUPPORTED, "volume side and image sides are limited to CJX_MAX_SIDE");
   const uint32_t known =
-      CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE | CJX_GRID_BRICKED;
+      CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE | CJX_GRID_BRICKED |
+      CJX_GRID_BRICKED_PAIRS;
   if (d->flags & ~known) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown flag bits");
+  if ((d->flags & CJX_GRID_BRICKED) && (d->flags & CJX_GRID_BRICKED_PAIRS))
+    return fail(CJX_ERR_INVALID_ARGUMENT, "CJX_GRID_BRICKED and CJX_GRID_BRICKED_PAIRS are exclusive");
   g->n = d->n;
   g->py = d->py;
   g->px = d->px;
@@ -655,7 +663,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
                          const Tuning& tn) {
   if (int e = ensure_smem_attrs()) return e;
   const int64_t ilp = tn.ilp;
-  const bool split = tn.gather_mode == 1;
+  const bool split = tn.gather_mode == 1 || (g.flags & CJX_GRID_BRICKED_PAIRS);  // the fused kernel has no pair path
   const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
   const bool fast = tn.fft_mode == 1;
   const size_t sa = smem_a(g), sb = smem_b(g);
@@ -666,9 +674,12 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
       const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
       const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
+      const bool pairs = (g.flags & CJX_GRID_BRICKED_PAIRS) != 0;
       const int64_t map = tn.tile;
 #define CJX_GSM(S, M)                                                                               \
-  if (bricked)                                                                                      \
+  if (pairs)                                                                                        \
+    k_gather_slice<S, PairLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);   \
+  else if (bricked)                                                                                 \
     k_gather_slice<S, BrickLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);  \
   else                                                                                              \
     k_gather_slice<S, LinearLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);
@@ -755,7 +766,9 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
       const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
       prof_begin(stream);
-      if (g.flags & CJX_GRID_BRICKED)
+      if (g.flags & CJX_GRID_BRICKED_PAIRS)
+        k_slice_direct<PairLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      else if (g.flags & CJX_GRID_BRICKED)
         k_slice_direct<BrickLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
       else
         k_slice_direct<LinearLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
@@ -812,6 +825,36 @@ __global__ void k_brick_volume(const float2* __restrict__ grid, float2* __restri
     const int z = bz * 8 + (((w >> 2) & 1) | ((w >> 4) & 2) | ((w >> 6) & 4));
     bricked[e] = (x < n && y < n && z < n) ? grid[((int64_t)z * n + y) * n + x] : make_float2(0.f, 0.f);
   }
+}
+
+// x-pair entries (g(x), g(x + 1)) in the same bricked order; 0 beyond the volume.
+__global__ void k_brick_volume_pairs(const float2* __restrict__ grid, float4* __restrict__ out, int n, int nb) {
+  const int64_t total = (int64_t)nb * nb * nb * 512;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(e & 511);
+    const int64_t blk = e >> 9;
+    const int bx = (int)(blk % nb), by = (int)((blk / nb) % nb), bz = (int)(blk / ((int64_t)nb * nb));
+    const int x = bx * 8 + ((w & 1) | ((w >> 2) & 2) | ((w >> 4) & 4));
+    const int y = by * 8 + (((w >> 1) & 1) | ((w >> 3) & 2) | ((w >> 5) & 4));
+    const int z = bz * 8 + (((w >> 2) & 1) | ((w >> 4) & 2) | ((w >> 6) & 4));
+    float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+    if (y < n && z < n) {
+      const int64_t row = ((int64_t)z * n + y) * n;
+      if (x < n) a = grid[row + x];
+      if (x + 1 < n) b = grid[row + x + 1];
+    }
+    out[e] = make_float4(a.x, a.y, b.x, b.y);
+  }
+}
+
+int launch_brick_volume_pairs(int n, const float2* grid, float4* out, cudaStream_t stream) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  prof_begin(stream);
+  k_brick_volume_pairs<<<sms * 8, 256, 0, stream>>>(grid, out, n, brick_blocks(n));
+  prof_end("k_brick_volume_pairs", stream);
+  return check_cuda(cudaGetLastError(), "k_brick_volume_pairs launch");
 }
 
 size_t bricked_elements(int n) {

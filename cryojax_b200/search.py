@@ -65,11 +65,8 @@ class PoseSearch:
             raise NotImplementedError("the NCC search needs padded_shape == shape")
         integ = image_model.volume_integrator
         vol = image_model.volume_parametrization.get_representation()
-        flags = image_model._flags() | integ._base_flags()
-        grid = vol.fourier_voxel_grid
-        if integ.use_bricked_layout:
-            grid = vol.bricked_grid()
-            flags |= nat.CJX_GRID_BRICKED
+        grid, layout = integ.device_grid(vol)
+        flags = image_model._flags() | integ._base_flags() | layout
         py, px = cfg.padded_shape
         sdesc = nat.SearchDesc()
         sdesc.slice = nat.make_desc(vol.shape[0], py, px, flags, integ.fill_value)

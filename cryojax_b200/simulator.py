@@ -264,7 +264,7 @@ class FourierVoxelGridVolume:
     is generated in the kernel from the pose).
     """
 
-    def __init__(self, fourier_voxel_grid, rotation=None, *, bricked=None):
+    def __init__(self, fourier_voxel_grid, rotation=None, *, bricked=None, pairs=None):
         torch = _torch()
         g = fourier_voxel_grid
         if not isinstance(g, torch.Tensor):
@@ -273,13 +273,20 @@ class FourierVoxelGridVolume:
             raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
         self.fourier_voxel_grid = g
         self.rotation = rotation  # AbstractPose attached by rotate_to_pose
-        self._bricked = bricked   # device re-layout for the gather (built on first use)
+        self._bricked = bricked   # device re-layouts for the gather (built on first use)
+        self._pairs = pairs
 
     def bricked_grid(self):
         """The grid in the library's bricked layout (cached; same values)."""
         if self._bricked is None:
             self._bricked = nat.brick_volume(self.fourier_voxel_grid.contiguous())
         return self._bricked
+
+    def pair_grid(self):
+        """The grid in the x-pair bricked layout (cached; twice the grid's bytes)."""
+        if self._pairs is None:
+            self._pairs = nat.brick_volume_pairs_new(self.fourier_voxel_grid.contiguous())
+        return self._pairs
 
     @property
     def shape(self):
@@ -323,9 +330,8 @@ class FourierVoxelGridVolume:
         if inverse:
             pose = QuaternionPose(*np.moveaxis(pose.offset_in_angstroms[..., :2], -1, 0),
                                   wxyz=rot.quat_inverse(pose.quaternion()))
-        if self._bricked is None and self.fourier_voxel_grid.is_cuda:
-            self.bricked_grid()
-        return FourierVoxelGridVolume(self.fourier_voxel_grid, rotation=pose, bricked=self._bricked)
+        return FourierVoxelGridVolume(self.fourier_voxel_grid, rotation=pose, bricked=self._bricked,
+                                      pairs=self._pairs)
 
     def get_representation(self, rng_key=None):
         return self
@@ -445,7 +451,7 @@ class FourierSliceExtraction:
     is_projection_approximation = True
 
     def __init__(self, *, outputs_integral: bool = True, correction_mask=None, out_of_bounds_mode: str = "fill",
-                 fill_value: complex = 0.0 + 0.0j, use_bricked_layout: bool = True):
+                 fill_value: complex = 0.0 + 0.0j, use_bricked_layout: bool = True, pair_layout: bool = True):
         if correction_mask is not None:
             raise NotImplementedError("correction_mask is not implemented on the device")
         if out_of_bounds_mode not in ("fill", "zero_fill_negative"):
@@ -455,6 +461,21 @@ class FourierSliceExtraction:
         self.out_of_bounds_mode = out_of_bounds_mode
         self.fill_value = complex(fill_value)
         self.use_bricked_layout = use_bricked_layout
+        self.pair_layout = pair_layout
+
+    def device_grid(self, volume):
+        """(grid tensor, layout flag) the forward and search kernels read.
+
+        Bricked layouts are cached on the volume: the x-pair copy when
+        ``pair_layout`` (default), else the plain bricked copy; without
+        ``use_bricked_layout`` the reference's C-order array itself.
+        """
+        grid = volume.fourier_voxel_grid
+        if not (self.use_bricked_layout and grid.is_cuda):
+            return grid, 0
+        if self.pair_layout:
+            return volume.pair_grid(), nat.CJX_GRID_BRICKED_PAIRS
+        return volume.bricked_grid(), nat.CJX_GRID_BRICKED
 
     def _base_flags(self):
         return nat.CJX_ZERO_FILL_NEGATIVE if self.out_of_bounds_mode == "zero_fill_negative" else 0
@@ -469,11 +490,9 @@ class FourierSliceExtraction:
         when not supplied.
         """
         torch = _torch()
-        grid = volume.fourier_voxel_grid
-        n_vol = grid.shape[0]
-        if self.use_bricked_layout and grid.is_cuda:
-            grid = volume.bricked_grid()
-            flags = flags | nat.CJX_GRID_BRICKED
+        n_vol = volume.fourier_voxel_grid.shape[0]
+        grid, layout = self.device_grid(volume)
+        flags = flags | layout
         if image_config.pad_mode != "constant":
             raise NotImplementedError("only constant padding is implemented on the device")
         py, px = image_config.padded_shape

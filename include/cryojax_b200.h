@@ -62,6 +62,11 @@ extern "C" {
 /* `grid` is in the bricked layout written by cjx_brick_volume instead of
  * the reference's C-order array.                                          */
 #define CJX_GRID_BRICKED (1u << 4)
+/* `grid` is in the x-pair layout written by cjx_brick_volume_pairs: the
+ * bricked order with 16-byte entries (g(x), g(x+1)), so that an interior
+ * trilinear sample reads its 8 corners with 4 vector loads.  Forward and
+ * search entry points only (not cjx_slice_ctf_loss_grad).                 */
+#define CJX_GRID_BRICKED_PAIRS (1u << 5)
 
 /* ---- per-image parameters (one record per image, device memory) ------
  * 32 doubles (256 bytes).  Built on the host from a pose, a CTF and an
@@ -260,6 +265,9 @@ CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void
  * cjx_brick_volume: write it (stream-ordered; grid and bricked distinct).  */
 CJX_API int cjx_bricked_volume_size(int n, size_t* bytes);
 CJX_API int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream);
+/* The x-pair copy (CJX_GRID_BRICKED_PAIRS): twice cjx_bricked_volume_size
+ * bytes; entry (x, y, z) = (g(x, y, z), g(x+1, y, z)), zero past the edge. */
+CJX_API int cjx_brick_volume_pairs(int n, const void* grid, void* pairs, void* stream);
 
 /* Batched complex-to-complex FFTs of `count` contiguous rows of n complex64
  * values (direction -1: forward, numpy.fft.fft; +1: unnormalised inverse,

@@ -157,9 +157,41 @@ def test_linear_and_bricked_layouts_match_oracle(cuda_device, box, pad_scale, sh
     vol, grid, fs = make_volume(box, 60, seed=box + 3, pad_scale=pad_scale)
     specs = random_specs(4, seed=box + 5, shape=shape)
     ref = _oracle(grid, fs, specs)
-    for bricked in (False, True):
-        got = _run_model(grid, specs, integrator_kw=dict(use_bricked_layout=bricked))
-        assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL, bricked
+    outs = {}
+    for bricked, pairs in ((False, False), (True, False), (True, True)):
+        got = _run_model(grid, specs, integrator_kw=dict(use_bricked_layout=bricked, pair_layout=pairs))
+        assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL, (bricked, pairs)
+        outs[(bricked, pairs)] = got
+    # the x-pair layout reads the same values in the same order as the bricked one
+    np.testing.assert_array_equal(outs[(True, True)], outs[(True, False)])
+
+
+def test_brick_volume_pairs_layout(cuda_device):
+    """cjx_brick_volume_pairs: entry (z, y, x) = (g(z, y, x), g(z, y, x + 1)) at the bricked address."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    n = 21
+    g = (np.arange(n**3, dtype=np.float32) + 1j * np.arange(n**3, dtype=np.float32)[::-1]).reshape(n, n, n)
+    gt = torch.as_tensor(g.astype(np.complex64)).cuda()
+    b = nat.brick_volume(gt).cpu().numpy()
+    p = nat.brick_volume_pairs_new(gt).cpu().numpy()
+    assert p.size == 2 * b.size
+    np.testing.assert_array_equal(p[0::2], b)  # first halves: the bricked copy
+    nb = (n + 7) // 8
+
+    def addr(z, y, x):
+        def spread(i):
+            return (i & 1) | ((i & 2) << 2) | ((i & 4) << 4)
+        blk = ((z >> 3) * nb + (y >> 3)) * nb + (x >> 3)
+        return blk * 512 + spread(x & 7) + (spread(y & 7) << 1) + (spread(z & 7) << 2)
+
+    rng = np.random.default_rng(0)
+    for z, y, x in rng.integers(0, n, (50, 3)):
+        e = addr(z, y, x)
+        assert p[2 * e] == g[z, y, x]
+        assert p[2 * e + 1] == (g[z, y, x + 1] if x + 1 < n else 0)
 
 
 def test_brick_volume_layout(cuda_device):
