@@ -187,6 +187,11 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float,
          ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "cjx_area_downsample": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+         ctypes.c_void_p],
+    ),
     "cjx_cnn_im2col": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
@@ -518,6 +523,14 @@ def cnn_noisy_normalize(images, out, *, index=None, snr=0.0, seed=0, n=None, str
     _check(load_library().cjx_cnn_noisy_normalize(
         _cuda_ptr(images, "images"), _opt_ptr(index, "index"), int(n), int(h), int(w), float(snr),
         ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), _cuda_ptr(out, "out"), _stream_ptr(stream)))
+
+
+def area_downsample(src, dst, stream=None) -> None:
+    """dst (n, h, w) FP32 = area-weighted downsample of src (n, H, W) FP32 (CUDA tensors)."""
+    n, H, W = src.shape
+    h, w = dst.shape[-2], dst.shape[-1]
+    _check(load_library().cjx_area_downsample(_cuda_ptr(src, "src"), int(n), int(H), int(W), _cuda_ptr(dst, "dst"),
+                                              int(h), int(w), _stream_ptr(stream)))
 
 
 def cnn_im2col(x, B, H, W, C, col, ldk, stream=None) -> None:

@@ -85,6 +85,34 @@ __global__ void k_noisy_normalize(const float* __restrict__ img, const int64_t* 
     o[i] = __float2bfloat16_rn((x[i] + (sigma > 0.f ? sigma * normal_draw(seed, src, i) : 0.f) - mean) * inv);
 }
 
+// Area-weighted downsampling: output pixel (i, j) of an h x w image is the
+// mean of the input over [i H/h, (i+1) H/h) x [j W/w, (j+1) W/w), input
+// pixels weighted by their overlap.
+__device__ __forceinline__ float overlap(float a0, float a1, int p) {
+  return fmaxf(0.f, fminf(a1, (float)(p + 1)) - fmaxf(a0, (float)p));
+}
+
+__global__ void k_area_downsample(const float* __restrict__ src, int H, int W, float* __restrict__ dst, int h, int w,
+                                  int64_t n) {
+  const float fy = (float)H / h, fx = (float)W / w;
+  const float inv = 1.f / (fy * fx);
+  const int64_t total = n * h * w;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(e % w);
+    const int64_t t = e / w;
+    const int i = (int)(t % h);
+    const int64_t b = t / h;
+    const float y0 = i * fy, y1 = (i + 1) * fy, x0 = j * fx, x1 = (j + 1) * fx;
+    const float* s = src + (size_t)b * H * W;
+    float acc = 0.f;
+    for (int y = (int)floorf(y0); y < min(H, (int)ceilf(y1)); ++y) {
+      const float wy = overlap(y0, y1, y);
+      for (int x = (int)floorf(x0); x < min(W, (int)ceilf(x1)); ++x) acc += wy * overlap(x0, x1, x) * s[(size_t)y * W + x];
+    }
+    dst[e] = acc * inv;
+  }
+}
+
 // col[p][k] for a 3x3, stride-2, pad-1 convolution of x [B][H][W][C]:
 // p = (b Ho + oy) Wo + ox, k = (3 ky + kx) C + c, zero in [9C, ldk).
 template <bool VEC>
@@ -350,6 +378,16 @@ int cjx_cnn_noisy_normalize(const float* images, const int64_t* index, int64_t n
   cjx::k_noisy_normalize<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       images, index, h * w, snr, seed, static_cast<bf16*>(out));
   return cjx::check_cuda(cudaGetLastError(), "noisy_normalize launch");
+}
+
+int cjx_area_downsample(const float* src, int64_t n, int H, int W, float* dst, int h, int w, void* stream) {
+  if (n < 0 || h < 1 || w < 1 || H < h || W < w)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "area_downsample needs 1 <= h <= H and 1 <= w <= W");
+  if (n == 0) return CJX_OK;
+  if (!src || !dst) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "src and dst must be non-NULL");
+  cjx::k_area_downsample<<<cjx::grid_for(n * h * w, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      src, H, W, dst, h, w, n);
+  return cjx::check_cuda(cudaGetLastError(), "area_downsample launch");
 }
 
 int cjx_cnn_im2col(const void* x, int64_t B, int H, int W, int C, void* col, int64_t ldk, void* stream) {

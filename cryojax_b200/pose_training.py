@@ -37,12 +37,18 @@ def direction_neighbours(nside: int, k: int = 8) -> np.ndarray:
     return np.argsort(-cos, axis=1, kind="stable")[:, :k].astype(np.int32)
 
 
-def simulate_clean_images(volume, image_config, wxyz, defocus, *, chunk=8192, amplitude_contrast=0.1):
-    """Real-space float32 CUDA images (n, P, P) at the given poses and defoci (no offsets, no noise)."""
+def simulate_clean_images(volume, image_config, wxyz, defocus, *, chunk=8192, amplitude_contrast=0.1, out_size=None):
+    """Real-space float32 CUDA images (n, P, P) at the given poses and defoci (no offsets, no noise).
+
+    With ``out_size`` each image is area-downsampled to out_size x out_size
+    on the device (cjx_area_downsample) as it is made, so only the small
+    images are kept.
+    """
     torch = _torch()
     n = len(wxyz)
     py, px = image_config.padded_shape
-    out = torch.empty((n, py, px), dtype=torch.float32, device=volume.fourier_voxel_grid.device)
+    oy, ox = (py, px) if out_size is None else (out_size, out_size)
+    out = torch.empty((n, oy, ox), dtype=torch.float32, device=volume.fourier_voxel_grid.device)
     from . import _postprocess
 
     for s in range(0, n, chunk):
@@ -54,12 +60,16 @@ def simulate_clean_images(volume, image_config, wxyz, defocus, *, chunk=8192, am
         pose = S.QuaternionPose(np.zeros(m), np.zeros(m), wxyz=np.asarray(wxyz[s:e], np.float64))
         model = S.make_image_model(volume, image_config, pose, tt)
         f = model.compute_fourier_image()
-        out[s:e] = _postprocess.irfftn(f, (py, px)).float()
+        img = _postprocess.irfftn(f, (py, px)).float().contiguous()
+        if out_size is None:
+            out[s:e] = img
+        else:
+            nat.area_downsample(img, out[s:e])
     return out
 
 
 class TrainingSet:
-    def __init__(self, volume, image_config, n, *, seed=0, defocus_range=(8000.0, 20000.0), nside=8):
+    def __init__(self, volume, image_config, n, *, seed=0, defocus_range=(8000.0, 20000.0), nside=8, out_size=None):
         rng = np.random.default_rng(seed)
         self.wxyz = rot.sample_uniform_quaternions(rng, n)
         self.defocus = rng.uniform(*defocus_range, n)
@@ -69,7 +79,7 @@ class TrainingSet:
         torch = _torch()
         dev = volume.fourier_voxel_grid.device
         self.labels = torch.as_tensor(self.labels_np, device=dev)
-        self.images = simulate_clean_images(volume, image_config, self.wxyz, self.defocus)
+        self.images = simulate_clean_images(volume, image_config, self.wxyz, self.defocus, out_size=out_size)
         self.n = n
 
 

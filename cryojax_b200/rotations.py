@@ -91,3 +91,41 @@ def sample_uniform_quaternions(rng: np.random.Generator, n: int):
     a = np.sqrt(1.0 - u1)
     b = np.sqrt(u1)
     return np.stack([a * np.sin(u2), a * np.cos(u2), b * np.sin(u3), b * np.cos(u3)], -1)
+
+
+def matrix_to_quat(R):
+    """Unit quaternions (w, x, y, z) of rotation matrices (..., 3, 3), w >= 0.
+
+    Shepperd's method (S. W. Shepperd, "Quaternion from rotation matrix",
+    J. Guidance and Control 1, 1978): take the square root of the largest of
+    4 w^2, 4 x^2, 4 y^2, 4 z^2 from the trace and diagonal, then the other
+    components from the off-diagonal sums and differences.
+    """
+    R = np.asarray(R, np.float64)
+    shp = R.shape[:-2]
+    R = R.reshape(-1, 3, 3)
+    tr = R[:, 0, 0] + R[:, 1, 1] + R[:, 2, 2]
+    cand = np.stack([1 + tr, 1 + 2 * R[:, 0, 0] - tr, 1 + 2 * R[:, 1, 1] - tr, 1 + 2 * R[:, 2, 2] - tr], -1)
+    k = np.argmax(cand, axis=1)
+    q = np.empty((R.shape[0], 4))
+    s = np.sqrt(np.maximum(cand[np.arange(len(k)), k], 0.0))  # = 2 |component k|
+    for idx in range(4):
+        m = k == idx
+        if not np.any(m):
+            continue
+        r, ss = R[m], s[m]
+        if idx == 0:
+            q[m] = np.stack([ss / 2, (r[:, 2, 1] - r[:, 1, 2]) / (2 * ss), (r[:, 0, 2] - r[:, 2, 0]) / (2 * ss),
+                             (r[:, 1, 0] - r[:, 0, 1]) / (2 * ss)], -1)
+        elif idx == 1:
+            q[m] = np.stack([(r[:, 2, 1] - r[:, 1, 2]) / (2 * ss), ss / 2, (r[:, 0, 1] + r[:, 1, 0]) / (2 * ss),
+                             (r[:, 0, 2] + r[:, 2, 0]) / (2 * ss)], -1)
+        elif idx == 2:
+            q[m] = np.stack([(r[:, 0, 2] - r[:, 2, 0]) / (2 * ss), (r[:, 0, 1] + r[:, 1, 0]) / (2 * ss), ss / 2,
+                             (r[:, 1, 2] + r[:, 2, 1]) / (2 * ss)], -1)
+        else:
+            q[m] = np.stack([(r[:, 1, 0] - r[:, 0, 1]) / (2 * ss), (r[:, 0, 2] + r[:, 2, 0]) / (2 * ss),
+                             (r[:, 1, 2] + r[:, 2, 1]) / (2 * ss), ss / 2], -1)
+    q *= np.where(q[:, :1] < 0, -1.0, 1.0)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return q.reshape(shp + (4,))

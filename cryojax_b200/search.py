@@ -160,7 +160,12 @@ class LearnedPoseSearch:
         obs = obs.to(device=self.search.rotations.device, dtype=torch.float32).contiguous()
         obs_f = observed_to_fourier(obs)
         pd = torch.as_tensor(image_model.image_params(), device=obs.device)
-        dirs, cand = self.net.propose(obs, k=self.top_k, n_inplane=self.grid.n_inplane, batch=batch)
+        x = obs
+        if obs.shape[-1] != self.net.image_size or obs.shape[-2] != self.net.image_size:
+            x = torch.empty((obs.shape[0], self.net.image_size, self.net.image_size), dtype=torch.float32,
+                            device=obs.device)
+            nat.area_downsample(obs, x)  # the network's input size
+        dirs, cand = self.net.propose(x, k=self.top_k, n_inplane=self.grid.n_inplane, batch=batch)
         res = self.search.run(image_model, obs_f, candidates=cand, observed_is_fourier=True, image_params_device=pd)
         best, score = res.best_orientation.copy(), res.best_score.copy()
         low = score < self.threshold

@@ -375,6 +375,11 @@ CJX_API int cjx_device_status(int* status, int reset, void* stream);
 CJX_API int cjx_cnn_noisy_normalize(const float* images, const int64_t* index, int64_t n,
                                     int h, int w, float snr, uint64_t seed, void* out,
                                     void* stream);
+/* dst[b] (FP32 [h][w]) = area-weighted mean of src[b] (FP32 [H][W]) over
+ * each output pixel's footprint (H/h x W/w input pixels, fractional overlaps
+ * weighted): the network's input size from any observed image size.        */
+CJX_API int cjx_area_downsample(const float* src, int64_t n, int H, int W, float* dst, int h,
+                                int w, void* stream);
 /* col[p][k] (BF16, row pitch ldk >= 9C, ldk % 8 == 0) of x [B][H][W][C]:
  * p = (b H/2 + oy) W/2 + ox, k = (3 ky + kx) C + c, zeros in [9C, ldk).    */
 CJX_API int cjx_cnn_im2col(const void* x, int64_t B, int H, int W, int C, void* col,

@@ -108,3 +108,28 @@ def test_orientation_order_is_a_locality_preserving_permutation():
         return np.mean(np.arccos(np.clip(np.abs(np.sum(a * b, 1)), 0, 1)))
 
     assert mean_step(order) < 0.2 * mean_step(np.arange(4096))
+
+
+def test_matrix_to_quat_round_trip():
+    from cryojax_b200 import rotations as rot
+
+    rng = np.random.default_rng(0)
+    q = rot.sample_uniform_quaternions(rng, 500)
+    q = np.concatenate([q, [[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1], [0.5, 0.5, -0.5, 0.5]]])
+    q2 = rot.matrix_to_quat(rot.quat_to_matrix(q))
+    q = q * np.where(q[:, :1] < 0, -1.0, 1.0)
+    np.testing.assert_allclose(np.abs(np.sum(q * q2, 1)), 1.0, atol=1e-12)
+    np.testing.assert_allclose(rot.quat_to_matrix(q2), rot.quat_to_matrix(q), atol=1e-12)
+
+
+def test_area_downsample_reference_weights():
+    """The host restatement of cjx_area_downsample's weights sums each footprint exactly."""
+    H, h = 320, 128
+    f = H / h
+    w = np.zeros((h, H))
+    for i in range(h):
+        y0, y1 = i * f, (i + 1) * f
+        for y in range(int(np.floor(y0)), min(H, int(np.ceil(y1)))):
+            w[i, y] = max(0.0, min(y1, y + 1) - max(y0, y))
+    np.testing.assert_allclose(w.sum(1), f)
+    np.testing.assert_allclose(w.sum(0), 1.0)
