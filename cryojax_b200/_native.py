@@ -246,6 +246,11 @@ _SIGNATURES = {
          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
          ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
     ),
+    "cjx_ncc_topk": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -608,6 +613,12 @@ def ncc_argmax(num, den, n, T, oo, yinv, zinv, best_score, best_orientation, *, 
         _cuda_ptr(yinv, "yinv"), _cuda_ptr(zinv, "zinv"), int(t0), _opt_ptr(scores, "scores"),
         int(scores.stride(0)) if scores is not None else 0, _cuda_ptr(best_score, "best_score"),
         _cuda_ptr(best_orientation, "best_orientation"), 1 if accumulate_best else 0, _stream_ptr(stream)))
+
+
+def ncc_topk(num, den, n, T, oo, yinv, zinv, k, indices, stream=None) -> None:
+    _check(load_library().cjx_ncc_topk(
+        _cuda_ptr(num, "num"), _cuda_ptr(den, "den"), int(num.stride(0)), int(n), int(T), _cuda_ptr(oo, "oo"),
+        _cuda_ptr(yinv, "yinv"), _cuda_ptr(zinv, "zinv"), int(k), _cuda_ptr(indices, "indices"), _stream_ptr(stream)))
 
 
 def device_status(reset: bool = True, stream=None) -> int:

@@ -159,6 +159,89 @@ __global__ void k_ncc_argmax(const float* __restrict__ num, const float* __restr
   }
 }
 
+// Per image row (block of 256): the m <= 16 highest NCCs over the T
+// templates (descending; ties -> lower index) -> idx_out[b][0..m).  Each
+// thread keeps a sorted list of its best m, the block merges the lists in
+// shared memory and one warp selects the final m.
+constexpr int kTopMMax = 16;
+
+__device__ __forceinline__ bool key_gt(float a, int32_t ia, float b, int32_t ib) {
+  return a > b || (a == b && ia < ib);
+}
+
+__global__ void __launch_bounds__(256)
+    k_ncc_topm(const float* __restrict__ num, const float* __restrict__ den, int64_t ld, int64_t T,
+               const float* __restrict__ oo, const float* __restrict__ yinv, const float* __restrict__ zinv, int m,
+               int32_t* __restrict__ idx_out) {
+  __shared__ float sv[256 * kTopMMax];
+  __shared__ int32_t si[256 * kTopMMax];
+  const int64_t b = blockIdx.x;
+  const float yr = yinv[b], zr = zinv[b], o2 = oo[b];
+  float v[kTopMMax];
+  int32_t ix[kTopMMax];
+#pragma unroll
+  for (int k = 0; k < kTopMMax; ++k) {
+    v[k] = -INFINITY;
+    ix[k] = INT32_MAX;
+  }
+  for (int64_t t = threadIdx.x; t < T; t += blockDim.x) {
+    const float n = num[b * ld + t] * yr, d = den[b * ld + t] * zr;
+    const float s = (d > 0.f && o2 > 0.f) ? n * rsqrtf(d * o2) : 0.f;
+    if (!key_gt(s, (int32_t)t, v[m - 1], ix[m - 1])) continue;
+    // insert into the sorted list (registers: unrolled compare-and-shift)
+    float cs = s;
+    int32_t ci = (int32_t)t;
+#pragma unroll
+    for (int k = 0; k < kTopMMax; ++k) {
+      if (k < m && key_gt(cs, ci, v[k], ix[k])) {
+        const float tv = v[k];
+        const int32_t ti = ix[k];
+        v[k] = cs;
+        ix[k] = ci;
+        cs = tv;
+        ci = ti;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kTopMMax; ++k) {
+    sv[threadIdx.x * kTopMMax + k] = k < m ? v[k] : -INFINITY;
+    si[threadIdx.x * kTopMMax + k] = k < m ? ix[k] : INT32_MAX;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (int r = 0; r < m; ++r) {
+      float bv = -INFINITY;
+      int32_t bi = INT32_MAX;
+      int bp = -1;
+      for (int p = lane; p < 256 * kTopMMax; p += 32) {
+        if (key_gt(sv[p], si[p], bv, bi)) {
+          bv = sv[p];
+          bi = si[p];
+          bp = p;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+        if (key_gt(ov, oi, bv, bi)) {
+          bv = ov;
+          bi = oi;
+          bp = op;
+        }
+      }
+      if (lane == 0) {
+        idx_out[b * m + r] = (bi == INT32_MAX) ? r : bi;
+        if (bp >= 0) sv[bp] = -INFINITY;
+        if (bp >= 0) si[bp] = INT32_MAX;
+      }
+      __syncwarp();
+    }
+  }
+}
+
 }  // namespace cjx
 
 extern "C" {
@@ -197,6 +280,18 @@ int cjx_ncc_argmax(const float* num, const float* den, int64_t ld, int64_t n, in
   cjx::k_ncc_argmax<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       num, den, ld, T, oo, yinv, zinv, t0, scores, ld_scores, best_score, best_orientation, accumulate_best);
   return cjx::check_cuda(cudaGetLastError(), "ncc_argmax launch");
+}
+
+int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t n, int64_t T, const float* oo,
+                 const float* yinv, const float* zinv, int k, int32_t* indices, void* stream) {
+  if (n < 0 || T < 1 || ld < T || T > 2147483647LL || k < 1 || k > cjx::kTopMMax || k > T)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_topk: need 1 <= k <= min(16, T), ld >= T");
+  if (n == 0) return CJX_OK;
+  if (!num || !den || !oo || !yinv || !zinv || !indices)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_topk: NULL pointer");
+  cjx::k_ncc_topm<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(num, den, ld, T, oo, yinv, zinv, k,
+                                                                            indices);
+  return cjx::check_cuda(cudaGetLastError(), "ncc_topk launch");
 }
 
 }  // extern "C"

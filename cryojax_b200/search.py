@@ -254,8 +254,13 @@ class TemplateSharingSearch:
         self._key = key
 
     def run(self, image_model, observed, *, observed_is_fourier=False, image_params_device=None,
-            return_scores=False) -> SearchResult:
+            return_scores=False, rerank_top=0) -> SearchResult:
+        """Best orientation per image; with ``rerank_top`` = k (<= 16) the k best FP16 candidates of
+        each image are rescored by the FP32 scorer (PoseSearch with candidate lists) and the best of
+        those is returned, which is the exhaustive FP32 answer whenever it is among them."""
         torch = _torch()
+        if rerank_top < 0 or rerank_top > 16:
+            raise ValueError("rerank_top must be in [0, 16]")
         self.build_templates(image_model)
         cfg = image_model.image_config
         py, px = cfg.padded_shape
@@ -274,6 +279,7 @@ class TemplateSharingSearch:
         best_score = torch.empty(n, dtype=torch.float32, device=dev)
         best = torch.empty(n, dtype=torch.int32, device=dev)
         scores = torch.empty((n, T), dtype=torch.float32, device=dev) if return_scores else None
+        top = torch.empty((n, rerank_top), dtype=torch.int32, device=dev) if rerank_top else None
         mc = min(self.image_chunk, n)
         num = torch.empty((mc, T), dtype=torch.float32, device=dev)
         den = torch.empty((mc, T), dtype=torch.float32, device=dev)
@@ -284,4 +290,11 @@ class TemplateSharingSearch:
             nat.gemm(z16[s:e], self.p16, den, m=m, n=T, k=kp, flags=nat.CJX_GEMM_F16)
             nat.ncc_argmax(num, den, m, T, oo[s:e], yinv[s:e], zinv[s:e], best_score[s:e], best[s:e],
                            scores=None if scores is None else scores[s:e])
-        return SearchResult(best.cpu().numpy().astype(np.int64), best_score.cpu().numpy(), scores, None)
+            if top is not None:
+                nat.ncc_topk(num, den, m, T, oo[s:e], yinv[s:e], zinv[s:e], rerank_top, top[s:e])
+        if top is None:
+            return SearchResult(best.cpu().numpy().astype(np.int64), best_score.cpu().numpy(), scores, None)
+        if getattr(self, "_plain", None) is None:
+            self._plain = PoseSearch(self.rot, device=dev)
+        exact = self._plain.run(image_model, obs_f, candidates=top, observed_is_fourier=True, image_params_device=pd)
+        return SearchResult(exact.best_orientation, exact.best_score, scores, top)

@@ -342,6 +342,15 @@ CJX_API int cjx_ncc_argmax(const float* num, const float* den, int64_t ld, int64
                            float* scores, int64_t ld_scores, float* best_score,
                            int32_t* best_orientation, int accumulate_best, void* stream);
 
+/* The k <= 16 highest NCCs of each row (same formula as cjx_ncc_argmax) as
+ * template indices, descending, ties -> lower index: indices[b][0..k).
+ * Rescoring them with cjx_search (candidate lists, FP32) makes the
+ * template-sharing search's answer exact whenever the FP32 optimum is among
+ * them.                                                                    */
+CJX_API int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t n, int64_t T,
+                         const float* oo, const float* yinv, const float* zinv, int k,
+                         int32_t* indices, void* stream);
+
 /* ---- tensor-core GEMM (pose-proposal network) -------------------------- */
 #define CJX_GEMM_OUT_BF16 1   /* store C as BF16 (default FP32)              */
 #define CJX_GEMM_BIAS 2       /* C[:, n] += bias[n] (FP32)                    */

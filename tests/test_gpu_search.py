@@ -148,3 +148,33 @@ def test_template_sharing_search_matches_plain_scores(cuda_device, shift):
         if srt[0] - srt[1] > 4e-3:
             assert shared.best_orientation[k] == plain.best_orientation[k]
         assert abs(shared.best_score[k] - b[k].max()) == 0
+
+
+def test_template_sharing_rerank_equals_plain_exhaustive(cuda_device):
+    """FP16 top-8 per image rescored in FP32: the plain exhaustive answer and score, bit for bit."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.healpix import OrientationGrid
+    from cryojax_b200.search import PoseSearch, TemplateSharingSearch
+
+    og = OrientationGrid(nside=2, n_inplane=8)
+    quats = og.quaternions()
+    _, grid, fs = make_volume(48, 60, seed=23)
+    rng = np.random.default_rng(8)
+    specs = _specs(10, 9, (64, 64), quats[rng.choice(og.size, 10, replace=False)])
+    obs = _observed(grid, fs, specs, 10, 0.1)
+    model = _model(grid, specs)
+    plain = PoseSearch(og.rotation_matrices()).run(model, obs, return_scores=True)
+    ts = TemplateSharingSearch(og.rotation_matrices())
+    rr = ts.run(model, obs, rerank_top=8, return_scores=True)
+    np.testing.assert_array_equal(rr.best_orientation, plain.best_orientation)
+    np.testing.assert_array_equal(rr.best_score, plain.best_score)
+    # the top-k indices are the k best FP16 scores, descending
+    fp16_scores = rr.scores.cpu().numpy()
+    top = rr.candidates.cpu().numpy()
+    for b in range(10):
+        ref = np.argsort(-fp16_scores[b], kind="stable")[:8]
+        np.testing.assert_array_equal(np.sort(top[b]), np.sort(ref))
+        assert np.all(np.diff(fp16_scores[b, top[b]]) <= 0)
+    assert nat.device_status() == 0
