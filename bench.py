@@ -62,6 +62,8 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the mixed-size batch measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the loss-gradient measurement")
     ap.add_argument("--no-search", action="store_true", help="skip the pose-search (learned vs grid) measurement")
+    ap.add_argument("--probe", choices=["gemm", "search", "cnn"], default=None,
+                    help="run one small workload of that kernel family (for a profiler), print its timing, exit")
     ap.add_argument("--no-refine", action="store_true",
                     help="skip the search + refinement measurement (320^2 images, N=512)")
     ap.add_argument("--refine-images", type=int, default=512, help="images in the learned arm of that measurement")
@@ -683,10 +685,87 @@ def ncu_traffic(kernel):
         return None
 
 
+def run_probe(kind, seed):
+    """Small fixed workloads for ncu captures: few launches before the one of interest."""
+    import numpy as np
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    dev = torch.device("cuda", 0)
+    out = {"probe": kind}
+
+    def ev_time(fn, reps=1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    if kind == "gemm":
+        g = torch.Generator(device=dev).manual_seed(seed)
+        for name, (m, n, k, dt, flags) in {
+            "bf16_8192^3": (8192, 8192, 8192, torch.bfloat16, 0),
+            "fp16_template_ncc_1024x36864x16640": (1024, 36864, 16640, torch.float16, nat.CJX_GEMM_F16),
+        }.items():
+            a = torch.randn((m, k), generator=g, device=dev).to(dt)
+            b = torch.randn((n, k), generator=g, device=dev).to(dt)
+            c = torch.empty((m, n), device=dev)
+            for _ in range(2):
+                nat.gemm(a, b, c, flags=flags)
+            ms = ev_time(lambda: nat.gemm(a, b, c, flags=flags))
+            out[name] = {"ms": ms, "tflops": 2.0 * m * n * k / ms / 1e9}
+            del a, b, c
+    elif kind == "search":
+        from cryojax_b200 import simulator as S
+        from cryojax_b200 import synthetic
+        from cryojax_b200.healpix import OrientationGrid
+        from cryojax_b200.search import PoseSearch
+
+        vol = S.FourierVoxelGridVolume.from_real_voxel_grid(synthetic.gaussian_sum_volume(128, 800, seed),
+                                                            pad_scale=2.0, device=str(dev))
+        b = synthetic.image_batch(8, seed + 1, max_offset=0.0, defocus_range=(8000.0, 20000.0))
+        cfg = S.BasicImageConfig((128, 128), 2.0, 300.0)
+        model = S.make_image_model(vol, cfg, S.QuaternionPose(b.offsets[:, 0], b.offsets[:, 1], wxyz=b.wxyz),
+                                   S.ContrastTransferTheory(S.AstigmaticCTF(b.defocus, b.astigmatism,
+                                                                            b.astigmatism_angle)))
+        obs = model.simulate()
+        grid = OrientationGrid(8, 48)
+        ps = PoseSearch(grid.rotation_matrices())
+        ms = ev_time(lambda: ps.run(model, obs))
+        out["plain_exhaustive_8_images"] = {"ms": ms, "candidates_per_s": 8 * grid.size / (ms / 1000.0)}
+    else:
+        from cryojax_b200.pose_net import PoseProposalNet
+
+        net = PoseProposalNet(128, 768, max_batch=256, seed=seed)
+        g = torch.Generator(device=dev).manual_seed(seed)
+        imgs = torch.randn((256, 128, 128), generator=g, device=dev)
+        labels = torch.randint(0, 768, (256,), generator=g, device=dev, dtype=torch.int32)
+
+        def step():
+            nat.cnn_noisy_normalize(imgs, net.x0, snr=0.05, seed=1)
+            net.forward(B=256)
+            net.backward(labels, B=256)
+            net.adam_step(1e-3)
+
+        for _ in range(2):
+            step()
+        ms = ev_time(step)
+        out["train_step_batch256"] = {"ms": ms, "images_per_s": 256 / (ms / 1000.0)}
+    out["device_status"] = nat.device_status()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.probe:
+        return run_probe(args.probe, args.seed)
 
     import numpy as np
     import torch
