@@ -769,20 +769,17 @@ def main():
 
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     from cryojax_b200 import _native as nat
     from cryojax_b200 import simulator as S
     from cryojax_b200 import synthetic
     from cryojax_b200.pipeline import HostStreamingSimulator
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    from cryojax_b200 import replicas
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    info = replicas.rank_info()
+    rank, world, local = info.rank, info.world, info.local_rank
+    replicas.init("nccl", info)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     nat.load_library()
@@ -791,7 +788,7 @@ def main():
     vol_np = synthetic.gaussian_sum_volume(args.box, args.gaussians, args.seed, sigma_range=(1.0, 3.0))
     volume = S.FourierVoxelGridVolume.from_real_voxel_grid(vol_np, pad_scale=args.pad_scale, device=str(dev))
     n = volume.shape[0]
-    batch = synthetic.image_batch(args.images, args.seed + 1 + 1000 * rank)
+    batch = synthetic.image_batch(args.images, replicas.image_seed(args.seed, rank))
     pose = S.QuaternionPose(batch.offsets[:, 0], batch.offsets[:, 1], wxyz=batch.wxyz)
     tt = S.ContrastTransferTheory(S.AstigmaticCTF(batch.defocus, batch.astigmatism, batch.astigmatism_angle))
     cfg = S.BasicImageConfig((args.image, args.image), 2.0, 300.0)
@@ -819,8 +816,7 @@ def main():
                   images_per_chunk=args.chunk, order=order_d)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(info)
 
     for _ in range(args.warmup):
         step()
@@ -839,12 +835,8 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    t_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_ms = float(t.item())
-    value = args.images * world * args.steps / (t_ms / 1000.0)
+    t_ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), info, dev)
+    value = replicas.job_rate(args.images, info, args.steps, t_ms)
 
     # ---- per-kernel timing (one extra profiled step, not part of `value`)
     nat.profile_enable(True)
@@ -903,10 +895,8 @@ def main():
             sim.run(ph, oh)
         e1.record(stream)
         torch.cuda.synchronize()
-        et = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        e2e = {"value": args.images * world * e_steps / (float(et.item()) / 1000.0), "unit": UNIT,
+        et_ms = replicas.max_over_ranks(e0.elapsed_time(e1), info, dev)
+        e2e = {"value": replicas.job_rate(args.images, info, e_steps, et_ms), "unit": UNIT,
                "h2d_bytes_per_step": int(ph.numel() * ph.element_size()),
                "d2h_bytes_per_step": int(oh.numel() * oh.element_size()),
                "path": "HostStreamingSimulator: pinned host params -> H2D -> cjx_slice_ctf_forward -> D2H "
@@ -988,8 +978,7 @@ def main():
             "search_refine": search_refine,
         }
         print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.shutdown(info)
     return 0
 
 
