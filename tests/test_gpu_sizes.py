@@ -56,4 +56,5 @@ def test_resize_path_sizes(cuda_device, n, shape, padded):
     got = model.compute_fourier_image().cpu().numpy()
     ref = np.stack([O.compute_fourier_image(grid, fs, s) for s in specs])
     errs = rel_l2_per_image(got, ref)
+    print(f"N={n} shape={shape} padded={padded}: max rel-L2 {max(errs):.3e}")  # shown with pytest -s
     assert max(errs) <= IMAGE_REL_L2_TOL, errs
