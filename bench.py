@@ -965,7 +965,12 @@ def main():
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg * images_per_launch,
                          "gather_distinct_voxels_per_image": gather_voxels,
-                         "avg_launch_ms": top_ms / top_count, "launches_per_step": top_count},
+                         "avg_launch_ms": top_ms / top_count, "launches_per_step": top_count,
+                         # DRAM bytes the kernel actually moves (ncu, scaled per launch) over its live launch
+                         # time: how close it runs to the HBM bandwidth it is bound by
+                         "traffic_gbs": ((trf * images_per_launch) / (top_ms / top_count) / 1e6 if trf else None),
+                         "traffic_frac": ((trf * images_per_launch) / (top_ms / top_count) / 1e6 / hbm_peak
+                                          if trf else None)},
             "l2": l2,
             "kernels_per_step": {k: {"launches": c, "ms": ms} for k, (c, ms) in prof.items()},
             "gpu_launches": launches_per_step * args.steps,

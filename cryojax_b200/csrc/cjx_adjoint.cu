@@ -374,14 +374,19 @@ __global__ void __launch_bounds__(kWarps * 32)
 // ---------------------------------------------------------------------------
 // Trilinear scatter-add of the slice gradient and d/dR.
 // ---------------------------------------------------------------------------
-template <typename Layout>
+// VEC: the two x-corners of a (y, z) corner row land in one 16-byte
+// float4 atomic when both are valid, adjacent and 16-byte aligned in the
+// gradient array (about half the rows); otherwise each corner takes an
+// 8-byte float2 atomic.  The scatter is bound by the L2's atomic units, so
+// fewer atomic operations is what shortens it.
+template <typename Layout, bool VEC>
 __global__ void __launch_bounds__(256)
     k_scatter_slice(const float2* __restrict__ grid, const float2* __restrict__ gh,
                     const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
                     float2* __restrict__ grad_grid, double* __restrict__ grads, SliceGeom g, int64_t k0) {
   const Layout L(g.n);
   __shared__ float red[8][6];
-  const int n = g.n, h = n / 2;
+  const int n = g.n;
   const int64_t k = k0 + blockIdx.z;
   const int64_t img = order ? (int64_t)order[k] : k;
   const double* Rm = params[img].rot;
@@ -415,9 +420,28 @@ __global__ void __launch_bounds__(256)
       dH[0][0] += gwx * val.x; dH[0][1] += gwx * val.y;
       dH[1][0] += gwy * val.x; dH[1][1] += gwy * val.y;
       dH[2][0] += gwz * val.x; dH[2][1] += gwz * val.y;
-      if (ok && grad_grid) {
+      if (!VEC && ok && grad_grid) {
         const float w = (wz * wy) * wx;
         atomicAdd(&grad_grid[((size_t)iz * n + iy) * n + ix], make_float2(w * gs.x, w * gs.y));
+      }
+    }
+    if (VEC && grad_grid) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {  // corner rows (dz, dy); x-corners 0 and 1
+        const int dz = r >> 1, dy = r & 1;
+        if (!((dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0))) continue;
+        const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0;
+        const float wyz = (dz ? az.w1 : az.w0) * (dy ? ay.w1 : ay.w0);
+        const size_t row = ((size_t)iz * n + iy) * n;
+        const float2 c0 = make_float2(wyz * ax.w0 * gs.x, wyz * ax.w0 * gs.y);
+        const float2 c1 = make_float2(wyz * ax.w1 * gs.x, wyz * ax.w1 * gs.y);
+        const size_t e0 = row + ax.i0;
+        if (ax.v0 && ax.v1 && ax.i1 == ax.i0 + 1 && (e0 & 1) == 0) {
+          atomicAdd(reinterpret_cast<float4*>(grad_grid + e0), make_float4(c0.x, c0.y, c1.x, c1.y));
+        } else {
+          if (ax.v0) atomicAdd(&grad_grid[e0], c0);
+          if (ax.v1) atomicAdd(&grad_grid[row + ax.i1], c1);
+        }
       }
     }
 #pragma unroll
@@ -534,10 +558,16 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
     prof_end("k_colfft_adj", stream);
     prof_begin(stream);
     const dim3 gs((g.nxh + 15) / 16, (g.n + 15) / 16, cnt);
-    if (bricked)
-      k_scatter_slice<BrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
-    else
-      k_scatter_slice<LinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    const bool agg = tn.scatter_vec != 0;
+    if (bricked && agg) {
+      k_scatter_slice<BrickLayout, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    } else if (bricked) {
+      k_scatter_slice<BrickLayout, false><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    } else if (agg) {
+      k_scatter_slice<LinearLayout, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    } else {
+      k_scatter_slice<LinearLayout, false><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    }
     prof_end("k_scatter_slice", stream);
   }
   return check_cuda(cudaGetLastError(), "loss gradient launch");

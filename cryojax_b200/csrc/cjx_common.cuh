@@ -467,6 +467,7 @@ struct Tuning {
   int tile;         // gather lane tile (0, 1, 2)
   int gather_mode;  // 1 = separate gather kernel, 0 = fused gather + column FFT
   int fft_mode;     // 1 = register FFTs where possible
+  int scatter_vec;  // 1 = adjoint grid scatter merges aligned x-corner pairs into 16-byte atomics
 };
 Tuning current_tuning();
 

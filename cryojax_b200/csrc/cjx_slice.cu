@@ -537,6 +537,7 @@ static std::atomic<int64_t> g_chunk_bytes{512ll << 20};
 static std::atomic<int64_t> g_gather_mode{1};
 static std::atomic<int64_t> g_fft_mode{1};
 static std::atomic<int64_t> g_gather_tile{1};
+static std::atomic<int64_t> g_scatter_vec{1};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -599,6 +600,7 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_GATHER_MODE) return g_gather_mode.load();
   if (key == CJX_TUNE_FFT_MODE) return g_fft_mode.load();
   if (key == CJX_TUNE_GATHER_TILE) return g_gather_tile.load();
+  if (key == CJX_TUNE_SCATTER_VEC) return g_scatter_vec.load();
   return -1;
 }
 
@@ -626,6 +628,11 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_GATHER_TILE) {
     if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather tile must be 0, 1 or 2");
     g_gather_tile = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_SCATTER_VEC) {
+    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "scatter vector mode must be 0 or 1");
+    g_scatter_vec = value;
     return CJX_OK;
   }
   return fail(CJX_ERR_INVALID_ARGUMENT, "unknown tuning key");
@@ -753,7 +760,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 
 Tuning current_tuning() {
   return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
-                (int)g_fft_mode.load()};
+                (int)g_fft_mode.load(), (int)g_scatter_vec.load()};
 }
 
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,

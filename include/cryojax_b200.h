@@ -286,12 +286,16 @@ CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
  * (R in 1-6, 8, 10, 12, 16), 0 = shared-memory Stockham FFTs everywhere.
  * CJX_TUNE_GATHER_TILE: lanes of a gather warp cover 2 x 16 (0), 4 x 8 (1)
- * or 8 x 4 (2) samples (columns x rows) of the slice plane.                 */
+ * or 8 x 4 (2) samples (columns x rows) of the slice plane.
+ * CJX_TUNE_SCATTER_VEC: 1 (default) = the adjoint's grid scatter-add puts
+ * the two x-corners of a corner row into one 16-byte atomic when they are
+ * adjacent and aligned; 0 = one 8-byte atomic per (sample, corner).        */
 #define CJX_TUNE_GATHER_ILP 1
 #define CJX_TUNE_CHUNK_BYTES 2
 #define CJX_TUNE_GATHER_MODE 3
 #define CJX_TUNE_FFT_MODE 4
 #define CJX_TUNE_GATHER_TILE 5
+#define CJX_TUNE_SCATTER_VEC 6
 CJX_API int cjx_tuning_set(int key, int64_t value);
 CJX_API int cjx_tuning_get(int key, int64_t* value);
 

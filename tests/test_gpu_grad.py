@@ -170,3 +170,23 @@ def test_bricked_and_linear_layouts_give_same_gradients(cuda_device):
         np.testing.assert_allclose(out[0][key], out[1][key], rtol=1e-5, atol=1e-8 * np.abs(out[1][key]).max())
     a, b = out[0]["d_grid"].cpu().numpy(), out[1]["d_grid"].cpu().numpy()
     assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max()
+
+
+def test_vector_atomic_scatter_matches_per_corner_atomics(cuda_device):
+    """16-byte x-pair atomics in the grid scatter give the per-corner 8-byte atomics' gradient."""
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.gradients import squared_residual_and_grad
+
+    grid, fs, specs, obs = _setup(box=48, shape=(64, 64), seed=17, n=3)
+    out = []
+    old = nat.tuning_get(nat.CJX_TUNE_SCATTER_VEC)
+    try:
+        for agg in (1, 0):
+            nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, agg)
+            model, _ = _model(grid, specs)
+            out.append(squared_residual_and_grad(model, obs, grid_grad=True))
+    finally:
+        nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, old)
+    a, b = out[0]["d_grid"].cpu().numpy(), out[1]["d_grid"].cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max()
+    np.testing.assert_array_equal(out[0]["loss"], out[1]["loss"])
