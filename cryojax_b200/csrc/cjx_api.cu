@@ -65,7 +65,7 @@ int cjx_slice_ctf_workspace_size(const cjx_slice_desc* desc, int64_t n_images, s
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   SliceGeom g;
   if (int e = make_geom(desc, &g)) return e;
-  *bytes = needs_resize(g) ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
+  *bytes = (needs_resize(g) && n_images > 0) ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
   return CJX_OK;
 }
 
@@ -91,8 +91,9 @@ int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cj
 static int group_plan(const cjx_slice_group& gr, SliceGeom* g, int64_t* chunk, size_t* need) {
   if (int e = make_geom(&gr.desc, g)) return e;
   if (gr.n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "group n_images < 0");
-  *chunk = needs_resize(*g) ? chunk_for(*g, &gr.desc, gr.n_images) : 0;
-  *need = needs_resize(*g) ? (size_t)*chunk * workspace_per_image(*g) : 0;
+  const bool resize = needs_resize(*g) && gr.n_images > 0;  // an empty group needs no scratch
+  *chunk = resize ? chunk_for(*g, &gr.desc, gr.n_images) : 0;
+  *need = resize ? (size_t)*chunk * workspace_per_image(*g) : 0;
   return CJX_OK;
 }
 
@@ -181,7 +182,7 @@ int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_imag
   SliceGeom g;
   if (int e = make_geom(desc, &g)) return e;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
-  *bytes = (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g);
+  *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
   return CJX_OK;
 }
 

@@ -46,6 +46,8 @@ def test_workspace_size_and_validation():
     # per image: Py * round8(N/2+1) + Py * round8(Px/2+1) + (N/2+1) * round8(N) complex64
     assert ws == 10 * 8 * (32 * 40 + 32 * 24 + 33 * 64)
     assert nat.workspace_size(nat.make_desc(64, 64, 64, 0), 10) == 0  # no resize stage
+    assert nat.workspace_size(d, 0) == 0  # no images, no scratch
+    assert nat.loss_workspace_size(d, 0) == 0
     with pytest.raises(nat.CryojaxB200Error) as e:
         nat.workspace_size(nat.make_desc(1, 32, 32, 0), 1)
     assert e.value.code == nat.CJX_ERR_INVALID_ARGUMENT
@@ -97,3 +99,11 @@ def test_search_workspace_plan():
     with pytest.raises(nat.CryojaxB200Error) as e:
         nat.search_workspace_size(_search_desc(64, 32, 32, 2, 0, 0))
     assert e.value.code == nat.CJX_ERR_INVALID_ARGUMENT
+
+
+def test_empty_groups_need_no_workspace():
+    d = nat.make_desc(64, 32, 32, nat.CJX_APPLY_CTF)
+    empty = nat.make_groups([{"desc": d, "n_images": 0}])
+    assert nat.multi_workspace_size(empty) == 0
+    one = nat.make_groups([{"desc": d, "n_images": 0}, {"desc": d, "n_images": 3}])
+    assert nat.multi_workspace_size(one) == nat.workspace_size(d, 3)
