@@ -183,6 +183,7 @@ _SIGNATURES = {
          ctypes.c_void_p],
     ),
     "cjx_device_status": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_void_p]),
+    "cjx_selftest_bounded_wait": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
     "cjx_cnn_noisy_normalize": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_float,
@@ -620,6 +621,12 @@ def ncc_topk(num, den, n, T, oo, yinv, zinv, k, indices, stream=None) -> None:
     _check(load_library().cjx_ncc_topk(
         _cuda_ptr(num, "num"), _cuda_ptr(den, "den"), int(num.stride(0)), int(n), int(T), _cuda_ptr(oo, "oo"),
         _cuda_ptr(yinv, "yinv"), _cuda_ptr(zinv, "zinv"), int(k), _cuda_ptr(indices, "indices"), _stream_ptr(stream)))
+
+
+def selftest_bounded_wait(limit_ns: int, status, stream=None) -> None:
+    """Launch the bounded-wait self-test; `status` is a zeroed int32 CUDA tensor of one element."""
+    _check(load_library().cjx_selftest_bounded_wait(ctypes.c_uint64(int(limit_ns)), _cuda_ptr(status, "status"),
+                                                    _stream_ptr(stream)))
 
 
 def device_status(reset: bool = True, stream=None) -> int:

@@ -94,6 +94,18 @@ __global__ void __launch_bounds__(128, 1)
   ml.teardown(tmem, issued, &g_tc_status);
 }
 
+// One thread waits on an mbarrier that nothing ever arrives on: the bounded
+// wait must give up after limit_ns and record kErrSelfTest in *status.
+__global__ void k_selftest_bounded_wait(uint64_t limit_ns, int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(tc::smem_u32(&bar), 1);
+    tc::fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) tc::mbar_wait(tc::smem_u32(&bar), 0, nullptr, status, tc::kErrSelfTest, limit_ns);
+}
+
 // ---- host side -------------------------------------------------------------
 
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -203,6 +215,14 @@ extern "C" {
 int cjx_gemm(int64_t M, int64_t N, int64_t K, const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
              int64_t ldc, const float* bias, int flags, int split_k, void* stream) {
   return cjx::launch_gemm(M, N, K, A, lda, B, ldb, C, ldc, bias, flags, split_k, static_cast<cudaStream_t>(stream));
+}
+
+int cjx_selftest_bounded_wait(uint64_t limit_ns, int* device_status, void* stream) {
+  if (!device_status) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "device_status is NULL");
+  if (limit_ns < 1000 || limit_ns > cjx::tc::kWaitLimitNs)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "limit_ns must be in [1 us, 2 s]");
+  cjx::k_selftest_bounded_wait<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(limit_ns, device_status);
+  return cjx::check_cuda(cudaGetLastError(), "selftest launch");
 }
 
 int cjx_device_status(int* status, int reset, void* stream) {

@@ -26,7 +26,7 @@ constexpr int BK = 64;   // 16-bit elements per k-block (one 128-byte swizzle ro
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
 // Error codes written to the status word by a kernel that gave up.
-constexpr int kErrWaitFull = 101, kErrWaitEmpty = 102, kErrWaitDone = 103, kErrDrain = 104;
+constexpr int kErrWaitFull = 101, kErrWaitEmpty = 102, kErrWaitDone = 103, kErrDrain = 104, kErrSelfTest = 105;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -66,13 +66,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 // false) when another thread of the CTA raised `abort_flag`, or after
 // kWaitLimitNs, in which case it raises the flag and records `code`.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* status,
-                                          int code) {
+                                          int code, uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (abort_flag && *abort_flag) return false;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) {
+    if (globaltimer_ns() - t0 > limit_ns) {
       if (abort_flag) *abort_flag = 1;
       if (status) atomicCAS(status, 0, code);
       return false;

@@ -375,6 +375,12 @@ CJX_API int cjx_gemm(int64_t M, int64_t N, int64_t K, const void* A, int64_t lda
 /* First error code recorded by a device-side wait that gave up (0 = none);
  * synchronises `stream`; reset != 0 clears it.                             */
 CJX_API int cjx_device_status(int* status, int reset, void* stream);
+/* Failure-path self-test of the tensor-core kernels' bounded waits: one
+ * thread waits on an mbarrier that nothing arrives on; after limit_ns
+ * (1 us .. 2 s) the wait gives up and writes 105 into *device_status (a
+ * device int the caller zeroed) if it is still 0.  The kernel returns
+ * normally; the context stays usable.                                      */
+CJX_API int cjx_selftest_bounded_wait(uint64_t limit_ns, int* device_status, void* stream);
 
 /* ---- pose-proposal network kernels (no counterpart in the reference) --- */
 /* Activations are NHWC BF16; a 3x3 stride-2 pad-1 convolution is

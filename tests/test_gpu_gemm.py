@@ -117,3 +117,28 @@ def test_gemm_argument_errors(cuda_device):
     a = torch.zeros((128, 64), device="cuda", dtype=torch.bfloat16)
     with pytest.raises(nat.CryojaxB200Error):  # split-K without accumulate
         nat.gemm(a, a, c, split_k=2)
+
+
+def test_bounded_wait_gives_up_and_reports(cuda_device):
+    """A wait on a barrier nothing arrives on ends after its limit with status 105; the GPU stays usable."""
+    import time
+
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nat.selftest_bounded_wait(50_000_000, status)  # 50 ms
+    torch.cuda.synchronize()
+    assert time.perf_counter() - t0 >= 0.05
+    assert int(status.item()) == 105
+    # the context is still good: a GEMM right after runs and records no error
+    a = torch.randn((128, 64), device="cuda").to(torch.bfloat16)
+    c = torch.empty((128, 128), device="cuda")
+    nat.gemm(a, a, c)
+    assert nat.device_status() == 0
+    torch.testing.assert_close(c, (a.float() @ a.float().T), rtol=1e-3, atol=1e-3)
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.selftest_bounded_wait(10_000_000_000, status)  # beyond the 2 s cap
