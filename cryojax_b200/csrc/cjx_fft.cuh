@@ -440,4 +440,49 @@ __host__ __device__ inline int reg_fft_radix(int n) {
   }
 }
 
+// 512-point warp FFT as 16 x 32 with one shared-memory transpose:
+// x[n] = x[l + 32 n1] (l = lane), X[k] = X[k1 + 16 k2].
+//   1. a 16-point DFT over n1 in registers, twiddle W_512^(l k1);
+//   2. transpose through shared memory so that lane (k1, e) = (lane >> 1,
+//      lane & 1) holds the 16 values z[2m + e] of column k1;
+//   3. a 16-point DFT over m in registers (the even / odd half of the
+//      32-point DFT over l), then one cross-lane radix-2 step with W_32^q:
+//      X[k1 + 16 q] = Y0 + W Y1 (e = 0), X[k1 + 16 (q + 16)] = Y0 - W Y1 (e = 1).
+// About 40 % fewer instructions than the five-shuffle-stage network of
+// warp_fft_reg<16> (32 shuffles per lane instead of 160).
+// Input: x[n1] = data[32 n1 + lane] (natural lane order, unlike
+// warp_fft_reg).  Output: x[q] = X[fft512_t_out(q, lane)].  tab is the
+// build_reg_twiddles(n = 512) table, w32 the build_w32 table, scr a
+// per-warp shared buffer of >= 16 * 34 values (overwritten).
+__device__ __forceinline__ int fft512_t_out(int q, int lane) { return (lane >> 1) + 16 * (q + 16 * (lane & 1)); }
+
+template <int DIR>
+__device__ __forceinline__ void warp_fft512_t(float2 (&x)[16], const float2* __restrict__ tab,
+                                              const float2* __restrict__ w32, float2* __restrict__ scr, int lane) {
+  constexpr int kStride = 34;  // row stride: conflict-free 8-byte reads within each half-warp
+  RegDft<16, DIR>::run(x);
+  const int bl = brev5(lane);
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1) x[k1] = cmul(x[k1], twiddle<DIR>(tab, k1 * 32 + bl));  // W_512^(lane k1)
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) scr[k1 * kStride + lane] = x[k1];
+  __syncwarp();
+  const int c = lane >> 1, e = lane & 1;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) x[m] = scr[c * kStride + 2 * m + e];
+  __syncwarp();
+  RegDft<16, DIR>::run(x);
+  const float sg = e ? -1.f : 1.f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    float2 w = e ? w32[q] : make_float2(1.f, 0.f);
+    if (DIR > 0) w = cconj(w);
+    const float2 v = cmul(x[q], w);
+    float2 p;
+    p.x = __shfl_xor_sync(0xffffffffu, v.x, 1);
+    p.y = __shfl_xor_sync(0xffffffffu, v.y, 1);
+    x[q] = make_float2(fmaf(sg, v.x, p.x), fmaf(sg, v.y, p.y));
+  }
+}
+
 }  // namespace cjx

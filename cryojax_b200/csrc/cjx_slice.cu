@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 // ---------------------------------------------------------------------------
 
 // Pass A (split): column inverse FFT + window of the gathered slice H.
-template <int R>
+template <int R, bool T512 = false>
 __global__ void __launch_bounds__(kWarps * 32)
     k_colifft_window_reg(const float2* __restrict__ hbuf, float2* __restrict__ t1, SliceGeom g) {
   constexpr int n = 32 * R;
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   if (j < g.nxh) {
     const LaneTwiddles lt = make_lane_twiddles(w32, lane);
     const float2* col = hbuf + ((size_t)blockIdx.y * g.nxh + j) * g.ldh;
-    const int bl = brev5(lane);
+    const int bl = T512 ? lane : brev5(lane);  // the transpose FFT takes natural lane order
     float2 x[R];
     const bool sym = (j == 0) || (j == n / 2);
 #pragma unroll
@@ -338,9 +338,16 @@ __global__ void __launch_bounds__(kWarps * 32)
       }
       x[n1] = v;
     }
-    warp_fft_reg<R, +1>(x, tab, lt, lane);
+    if constexpr (T512) {
+      static_assert(R == 16, "the transpose FFT is 512-point");
+      warp_fft512_t<+1>(x, tab, w32, buf, lane);
 #pragma unroll
-    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+      for (int q = 0; q < R; ++q) buf[pad16(fft512_t_out(q, lane))] = x[q];
+    } else {
+      warp_fft_reg<R, +1>(x, tab, lt, lane);
+#pragma unroll
+      for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+    }
   }
   __syncthreads();
   const int ncols = min(kWarps, g.nxh - j0);
@@ -535,7 +542,7 @@ static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py
 static std::atomic<int64_t> g_gather_ilp{2};
 static std::atomic<int64_t> g_chunk_bytes{512ll << 20};
 static std::atomic<int64_t> g_gather_mode{1};
-static std::atomic<int64_t> g_fft_mode{1};
+static std::atomic<int64_t> g_fft_mode{2};
 static std::atomic<int64_t> g_gather_tile{1};
 static std::atomic<int64_t> g_scatter_vec{1};
 
@@ -621,7 +628,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_FFT_MODE) {
-    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "FFT mode must be 0 or 1");
+    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "FFT mode must be 0, 1 or 2");
     g_fft_mode = value;
     return CJX_OK;
   }
@@ -672,7 +679,8 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
   const int64_t ilp = tn.ilp;
   const bool split = tn.gather_mode == 1 || (g.flags & CJX_GRID_BRICKED_PAIRS);  // the fused kernel has no pair path
   const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
-  const bool fast = tn.fft_mode == 1;
+  const bool fast = tn.fft_mode >= 1;
+  const bool t512 = tn.fft_mode == 2 && rn == 16;  // 512-point column transforms through the transpose FFT
   const size_t sa = smem_a(g), sb = smem_b(g);
   const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
   const size_t sb_reg =
@@ -710,7 +718,9 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
       prof_end("k_gather_slice", stream);
       prof_begin(stream);
       const dim3 gc((g.nxh + kWarps - 1) / kWarps, cnt);
-      if (fast && rn) {
+      if (fast && t512) {
+        k_colifft_window_reg<16, true><<<gc, kWarps * 32, sa_reg, stream>>>(hb, t1, g);
+      } else if (fast && rn) {
         switch (rn) {
 #define CJX_A_CASE(R) \
   case R: k_colifft_window_reg<R><<<gc, kWarps * 32, sa_reg, stream>>>(hb, t1, g); break;
@@ -792,7 +802,7 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   const int rpy = reg_fft_radix(g.py);
-  const bool fast = tn.fft_mode == 1;
+  const bool fast = tn.fft_mode >= 1;
   const size_t sc_reg = sizeof(float2) * (size_t)(g.py + kWarps * (pad16(g.py) + 1));
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);

@@ -284,7 +284,10 @@ CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t
  * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
  * column-FFT kernel, 0 = one fused gather + column-FFT kernel.
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
- * (R in 1-6, 8, 10, 12, 16), 0 = shared-memory Stockham FFTs everywhere.
+ * (R in 1-6, 8, 10, 12, 16), 2 (default) = the same, with the 512-point
+ * column transforms of the resize stage done as 16 x 32 through one
+ * shared-memory transpose instead of five shuffle stages, 0 = shared-memory
+ * Stockham FFTs everywhere.
  * CJX_TUNE_GATHER_TILE: lanes of a gather warp cover 2 x 16 (0), 4 x 8 (1)
  * or 8 x 4 (2) samples (columns x rows) of the slice plane.
  * CJX_TUNE_SCATTER_VEC: 1 (default) = the adjoint's grid scatter-add puts

@@ -79,6 +79,12 @@ def test_tuning_knobs():
         nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, 3)
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(99, 1)
+    assert nat.tuning_get(nat.CJX_TUNE_FFT_MODE) == 2  # transpose FFT for 512-point column passes
+    assert nat.tuning_get(nat.CJX_TUNE_SCATTER_VEC) == 1
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(nat.CJX_TUNE_FFT_MODE, 3)
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, 2)
 
 
 def _search_desc(n, py, px, n_img, n_orient, k):

@@ -58,3 +58,27 @@ def test_resize_path_sizes(cuda_device, n, shape, padded):
     errs = rel_l2_per_image(got, ref)
     print(f"N={n} shape={shape} padded={padded}: max rel-L2 {max(errs):.3e}")  # shown with pytest -s
     assert max(errs) <= IMAGE_REL_L2_TOL, errs
+
+
+@pytest.mark.parametrize("fft_mode", [0, 1, 2])
+def test_fft_modes_at_the_benchmark_shape(cuda_device, fft_mode):
+    """N = 512 -> 320^2 through each FFT implementation (Stockham, shuffle network, 512-point transpose)."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+
+    n, shape = 512, (320, 320)
+    grid = synthetic_grid(n, seed=77)
+    fs = O.make_frequency_slice((n, n), outputs_rfftfreqs=False)
+    specs = random_specs(2, seed=78, shape=shape)
+    pose, tt, cfg = specs_to_model_args(specs)
+    vol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+    old = nat.tuning_get(nat.CJX_TUNE_FFT_MODE)
+    try:
+        nat.tuning_set(nat.CJX_TUNE_FFT_MODE, fft_mode)
+        got = S.make_image_model(vol, cfg, pose, tt).compute_fourier_image().cpu().numpy()
+    finally:
+        nat.tuning_set(nat.CJX_TUNE_FFT_MODE, old)
+    ref = np.stack([O.compute_fourier_image(grid, fs, s) for s in specs])
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
