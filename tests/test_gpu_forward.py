@@ -238,3 +238,56 @@ def test_from_real_voxel_grid_matches_oracle(cuda_device):
     dvol = S.FourierVoxelGridVolume.from_real_voxel_grid(vol, pad_scale=1.3)
     assert dvol.shape == grid.shape
     assert O.relative_l2(dvol.fourier_voxel_grid.cpu().numpy(), grid) < 1e-6
+
+
+def _golden_volume():
+    import json
+    import os
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    vol = np.load(os.path.join(here, "3j9g_potential_ps4_4.npy")).astype(np.float64)
+    return vol, json.load(open(os.path.join(here, "3j9g_potential_ps4_4.json")))["voxel_size_A"]
+
+
+def test_reference_fixture_volume_and_config(cuda_device):
+    """The reference's image-model fixture: its 64^3 map at pad 1.3 (N = 83, prime), images 74^2 padded
+    to 83^2, default CTF; identity and random poses; Fourier image and cropped real-space image."""
+    import torch
+
+    from cryojax_b200 import simulator as S
+
+    vol, voxel = _golden_volume()
+    grid, fs = O.fourier_voxel_grid_from_real_voxel_grid(vol, pad_scale=1.3)
+    n = grid.shape[0]
+    rng = np.random.default_rng(3)
+    q = np.concatenate([[[1.0, 0.0, 0.0, 0.0]], O.uniform_poses(4, 5, 0.0)[0]])
+    specs = [O.ImageSpec(shape=(int(0.9 * n), int(0.9 * n)), padded_shape=(n, n), pixel_size=voxel, wxyz=qq,
+                         offset_in_angstroms=rng.uniform(-8, 8, 2)) for qq in q]
+    pose, tt, cfg = specs_to_model_args(specs)
+    V = S.FourierVoxelGridVolume.from_real_voxel_grid(torch.as_tensor(vol), pad_scale=1.3)
+    model = S.make_image_model(V, cfg, pose, tt)
+    got_f = model.compute_fourier_image().cpu().numpy()
+    ref_f = np.stack([O.compute_fourier_image(grid, fs, s) for s in specs])
+    assert max(rel_l2_per_image(got_f, ref_f)) <= IMAGE_REL_L2_TOL
+    got = model.simulate().cpu().numpy()
+    ref = np.stack([O.simulate(grid, fs, s) for s in specs])
+    assert got.shape == (5, 74, 74)
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+@pytest.mark.parametrize("extra_y, extra_x", [(1, 1), (1, 0), (0, 1)])
+def test_even_vs_odd_image_shape_on_the_device(cuda_device, extra_y, extra_x):
+    """cryojax tests/test_image_model.py:83-105 through the device path (odd-N resize, N = 83)."""
+    import torch
+
+    from cryojax_b200 import simulator as S
+
+    vol, voxel = _golden_volume()
+    V = S.FourierVoxelGridVolume.from_real_voxel_grid(torch.as_tensor(vol), pad_scale=1.3)
+    n = V.shape[0]
+    control, test = (n, n), (n + extra_y, n + extra_x)
+    pose = S.EulerAnglePose()
+    tt = S.ContrastTransferTheory(S.AstigmaticCTF())
+    a = S.make_image_model(V, S.BasicImageConfig(test, voxel, 300.0), pose, tt).simulate().cpu().numpy()
+    b = S.make_image_model(V, S.BasicImageConfig(control, voxel, 300.0), pose, tt).simulate().cpu().numpy()
+    np.testing.assert_allclose(O.crop_to_shape(a, control), b, atol=1e-4)
