@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the mixed-size batch measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the loss-gradient measurement")
     ap.add_argument("--no-search", action="store_true", help="skip the pose-search (learned vs grid) measurement")
-    ap.add_argument("--probe", choices=["gemm", "search", "cnn"], default=None,
+    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline"], default=None,
                     help="run one small workload of that kernel family (for a profiler), print its timing, exit")
     ap.add_argument("--no-refine", action="store_true",
                     help="skip the search + refinement measurement (320^2 images, N=512)")
@@ -737,6 +737,37 @@ def run_probe(kind, seed):
         ps = PoseSearch(grid.rotation_matrices())
         ms = ev_time(lambda: ps.run(model, obs))
         out["plain_exhaustive_8_images"] = {"ms": ms, "candidates_per_s": 8 * grid.size / (ms / 1000.0)}
+    elif kind == "spline":
+        from cryojax_b200 import simulator as S
+        from cryojax_b200 import synthetic
+
+        # FourierVoxelSplineVolume at the benchmark shape (N = 512 -> 320^2), 64 images, x-pair coefficients
+        grid = S.FourierVoxelGridVolume.from_real_voxel_grid(synthetic.gaussian_sum_volume(256, 6000, seed),
+                                                             pad_scale=2.0, device=str(dev)).fourier_voxel_grid
+        n = grid.shape[0]
+        ws = torch.empty(nat.spline_coefficients_workspace_size(n), dtype=torch.uint8, device=dev)
+        coef = torch.empty((n + 2,) * 3, dtype=torch.complex64, device=dev)
+        nat.spline_coefficients(grid, coef, ws)
+        out["coefficients_ms_N512"] = ev_time(lambda: nat.spline_coefficients(grid, coef, ws))
+        del grid, ws
+        torch.cuda.empty_cache()
+        vol = S.FourierVoxelSplineVolume(coef)
+        b = synthetic.image_batch(64, seed + 1)
+        cfg = S.BasicImageConfig((320, 320), 2.0, 300.0)
+        model = S.make_image_model(vol, cfg, S.QuaternionPose(b.offsets[:, 0], b.offsets[:, 1], wxyz=b.wxyz),
+                                   S.ContrastTransferTheory(S.AstigmaticCTF(b.defocus, b.astigmatism,
+                                                                            b.astigmatism_angle)))
+        integ = model.volume_integrator
+        pd = torch.as_tensor(model.image_params(), device=dev)
+        o = torch.empty((64, 320, 161), dtype=torch.complex64, device=dev)
+
+        def fwd():
+            integ.run(vol, cfg, None, model._flags(), params_device=pd, out=o)
+
+        for _ in range(3):
+            fwd()
+        ms = ev_time(fwd)
+        out["spline_forward_64_images"] = {"ms": ms, "images_per_s": 64 / (ms / 1000.0)}
     else:
         from cryojax_b200.pose_net import PoseProposalNet
 

@@ -28,6 +28,7 @@ CJX_APPLY_ENVELOPE = 1 << 2
 CJX_ZERO_FILL_NEGATIVE = 1 << 3
 CJX_GRID_BRICKED = 1 << 4
 CJX_GRID_BRICKED_PAIRS = 1 << 5
+CJX_GRID_SPLINE = 1 << 6
 
 CJX_MAX_SIDE = 1024
 CJX_TUNE_GATHER_ILP = 1
@@ -36,6 +37,7 @@ CJX_TUNE_GATHER_MODE = 3
 CJX_TUNE_FFT_MODE = 4
 CJX_TUNE_GATHER_TILE = 5
 CJX_TUNE_SCATTER_VEC = 6
+CJX_TUNE_SPLINE_ILP = 7
 PARAMS_DOUBLES = 32  # sizeof(cjx_image_params) / 8
 
 # field offsets (in doubles) of cjx_image_params
@@ -103,6 +105,11 @@ class CryojaxB200Error(RuntimeError):
 # Every exported symbol of include/cryojax_b200.h with (restype, argtypes).
 _SIGNATURES = {
     "cjx_get_version": (ctypes.c_int, []),
+    "cjx_spline_coefficients_workspace_size": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "cjx_spline_coefficients": (
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+    ),
     "cjx_get_last_error": (ctypes.c_char_p, []),
     "cjx_slice_ctf_workspace_size": (
         ctypes.c_int,
@@ -682,6 +689,37 @@ def brick_volume_pairs_new(grid, stream=None):
         raise ValueError("grid must be complex64 [N, N, N]")
     out = torch.empty(2 * bricked_volume_size(n) // 8, dtype=torch.complex64, device=grid.device)
     brick_volume_pairs(n, grid.contiguous(), out, stream)
+    return out
+
+
+def spline_coefficients_workspace_size(n: int) -> int:
+    out = ctypes.c_size_t(0)
+    _check(load_library().cjx_spline_coefficients_workspace_size(int(n), ctypes.byref(out)))
+    return int(out.value)
+
+
+def spline_coefficients(grid, out=None, workspace=None, stream=None):
+    """Cubic-spline coefficients ((N+2)^3 complex64) of a centred complex64 [N, N, N] CUDA grid.
+
+    cryojax/ndimage/_map_coordinates.py:71-82 (compute_spline_coefficients).
+    """
+    import torch
+
+    n = grid.shape[0]
+    if grid.dtype != torch.complex64 or tuple(grid.shape) != (n, n, n):
+        raise ValueError("grid must be complex64 [N, N, N]")
+    grid = grid.contiguous()
+    m = n + 2
+    if out is None:
+        out = torch.empty((m, m, m), dtype=torch.complex64, device=grid.device)
+    elif out.dtype != torch.complex64 or tuple(out.shape) != (m, m, m) or not out.is_contiguous():
+        raise ValueError("out must be contiguous complex64 [N+2, N+2, N+2]")
+    need = spline_coefficients_workspace_size(n)
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
+        workspace = torch.empty(need, dtype=torch.uint8, device=grid.device)
+    _check(load_library().cjx_spline_coefficients(int(n), _cuda_ptr(grid, "grid"), _cuda_ptr(out, "coefficients"),
+                                                  _cuda_ptr(workspace, "workspace"),
+                                                  workspace.numel() * workspace.element_size(), _stream_ptr(stream)))
     return out
 
 

@@ -86,7 +86,7 @@ def autotune(model, *, n_sample=1024, repeats=2, candidates=None, use_cache=True
             return hit
     params = model.image_params()
     m = min(n_sample, params.shape[0])
-    pd = torch.as_tensor(params[:m], device=vol.fourier_voxel_grid.device)
+    pd = torch.as_tensor(params[:m], device=vol.device)
     out = torch.empty((m, py, px // 2 + 1), dtype=torch.complex64, device=pd.device)
     old = (nat.tuning_get(nat.CJX_TUNE_GATHER_ILP), nat.tuning_get(nat.CJX_TUNE_GATHER_TILE),
            nat.tuning_get(nat.CJX_TUNE_CHUNK_BYTES))

@@ -30,6 +30,8 @@ int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cud
 size_t bricked_elements(int n);
 int launch_brick_volume(int n, const float2* grid, float2* bricked, cudaStream_t stream);
 int launch_brick_volume_pairs(int n, const float2* grid, float4* out, cudaStream_t stream);
+size_t spline_workspace_elements(int n);
+int launch_spline_coefficients(int n, const float2* grid, float2* coef, float2* work, cudaStream_t stream);
 
 static thread_local std::string g_last_error;
 
@@ -143,7 +145,10 @@ int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, voi
     group_plan(gr, &g, &chunk, &need);
     Tuning tn = base;
     if (gr.tuning_valid) {
-      tn.ilp = gr.gather_ilp;
+      if (gr.desc.flags & CJX_GRID_SPLINE)
+        tn.spline_ilp = gr.gather_ilp;
+      else
+        tn.ilp = gr.gather_ilp;
       tn.tile = gr.gather_tile;
     }
     if (int e = launch_forward(g, static_cast<const float2*>(gr.grid), gr.params, gr.order, gr.n_images,
@@ -155,13 +160,13 @@ int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, voi
 
 int cjx_bricked_volume_size(int n, size_t* bytes) {
   if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
-  if (n < 2 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE]");
+  if (n < 2 || n > CJX_MAX_SIDE + 2) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE + 2]");
   *bytes = bricked_elements(n) * sizeof(float2);
   return CJX_OK;
 }
 
 int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream) {
-  if (n < 2 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE]");
+  if (n < 2 || n > CJX_MAX_SIDE + 2) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE + 2]");
   if (!grid || !bricked) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and bricked must be non-NULL");
   if (grid == bricked) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and bricked must not alias");
   return launch_brick_volume(n, static_cast<const float2*>(grid), static_cast<float2*>(bricked),
@@ -169,11 +174,29 @@ int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream) {
 }
 
 int cjx_brick_volume_pairs(int n, const void* grid, void* pairs, void* stream) {
-  if (n < 2 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE]");
+  if (n < 2 || n > CJX_MAX_SIDE + 2) return fail(CJX_ERR_UNSUPPORTED, "n must be in [2, CJX_MAX_SIDE + 2]");
   if (!grid || !pairs) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and pairs must be non-NULL");
   if (grid == pairs) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and pairs must not alias");
   return launch_brick_volume_pairs(n, static_cast<const float2*>(grid), static_cast<float4*>(pairs),
                                    static_cast<cudaStream_t>(stream));
+}
+
+int cjx_spline_coefficients_workspace_size(int n, size_t* bytes) {
+  if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  if (n < 4 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [4, CJX_MAX_SIDE]");
+  *bytes = spline_workspace_elements(n) * sizeof(float2);
+  return CJX_OK;
+}
+
+int cjx_spline_coefficients(int n, const void* grid, void* coefficients, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+  if (n < 4 || n > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "n must be in [4, CJX_MAX_SIDE]");
+  if (!grid || !coefficients) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and coefficients must be non-NULL");
+  if (grid == coefficients) return fail(CJX_ERR_INVALID_ARGUMENT, "grid and coefficients must not alias");
+  if (!workspace || workspace_bytes < spline_workspace_elements(n) * sizeof(float2))
+    return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_spline_coefficients_workspace_size()");
+  return launch_spline_coefficients(n, static_cast<const float2*>(grid), static_cast<float2*>(coefficients),
+                                    static_cast<float2*>(workspace), static_cast<cudaStream_t>(stream));
 }
 
 int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_images, size_t* bytes) {
@@ -182,6 +205,7 @@ int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_imag
   SliceGeom g;
   if (int e = make_geom(desc, &g)) return e;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
+  if (g.flags & CJX_GRID_SPLINE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of spline volumes is not implemented");
   *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
   return CJX_OK;
 }
@@ -194,6 +218,7 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   if (n_images == 0) return CJX_OK;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
+  if (g.flags & CJX_GRID_SPLINE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of spline volumes is not implemented");
   if (!grid || !params || !observed || !image_grads)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");
   const int64_t chunk = chunk_for(g, desc, n_images);

@@ -328,12 +328,160 @@ __device__ __forceinline__ void sample_trilinear_batch_pairs(const float4* __res
   }
 }
 
-// Trilinear samples from a grid in any of the three layouts.
+// ---------------------------------------------------------------------------
+// Cubic-spline sampling from a FourierVoxelSplineVolume's coefficient array
+// (side m = N + 2), cryojax/ndimage/_map_coordinates.py:126-142, 217-250:
+// for the logical coordinate c = off + N/2 the taps are the coefficient
+// indices i = floor(c) + t, t = 0..3, each weighted by basis(c - i + 1) with
+// basis(u) = 4 - 6u^2 + 3|u|^3 (|u| <= 1), (2 - |u|)^3 (1 <= |u| <= 2).
+// With f = c - floor(c) the four weights are (1-f)^3, 4 - 6f^2 + 3f^3,
+// 4 - 6(1-f)^2 + 3(1-f)^3 and f^3.  Each tap is read with the same
+// `.at[idx].get(mode="fill")` rule as the trilinear corners, on side m.
+// The layouts address the coefficient array on side N + 2.
+// ---------------------------------------------------------------------------
+struct SplineLinearLayout : LinearLayout {
+  __host__ __device__ explicit SplineLinearLayout(int n) : LinearLayout(n + 2) {}
+};
+struct SplineBrickLayout : BrickLayout {
+  __host__ __device__ explicit SplineBrickLayout(int n) : BrickLayout(n + 2) {}
+};
+// x-pair entries (c(x), c(x + 1)) in the bricked order on side N + 2: a row
+// of 4 x-taps is two 16-byte loads (entries x0 and x0 + 2).
+struct SplinePairLayout : BrickLayout {
+  __host__ __device__ explicit SplinePairLayout(int n) : BrickLayout(n + 2) {}
+};
+template <typename Layout>
+struct is_spline_layout
+    : std::integral_constant<bool, std::is_same<Layout, SplineLinearLayout>::value ||
+                                       std::is_same<Layout, SplineBrickLayout>::value ||
+                                       std::is_same<Layout, SplinePairLayout>::value> {};
+
+struct SplineAxis {
+  int i[4];    // wrapped tap indices (0 when invalid)
+  bool v[4];   // tap inside [0, m)
+  float w[4];  // basis weights
+};
+
+__device__ __forceinline__ void spline_weights(float f, float* w) {
+  const float g = 1.0f - f;
+  w[0] = g * g * g;
+  w[1] = fmaf(fmaf(3.0f, f, -6.0f), f * f, 4.0f);
+  w[2] = fmaf(fmaf(3.0f, g, -6.0f), g * g, 4.0f);
+  w[3] = f * f * f;
+}
+
+__device__ __forceinline__ SplineAxis spline_axis(float off, int n, bool wrap_negative) {
+  SplineAxis a;
+  const float fl = floorf(off);
+  spline_weights(off - fl, a.w);
+  const int m = n + 2;
+  const int i0 = (int)fl + n / 2;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    int i = i0 + t;
+    if (wrap_negative && i < 0) i += m;
+    a.v[t] = (unsigned)i < (unsigned)m;
+    a.i[t] = a.v[t] ? i : 0;
+  }
+  return a;
+}
+
+// S cubic-spline samples.  A sample whose 64 taps all lie inside the
+// coefficient array (every sample away from the faces) reads them at the
+// layout's offsets with no per-tap checks; samples near the faces take the
+// general rule.  The taps are summed as x rows (4 taps), each row weighted
+// by its (z, y) weight.
+template <int S, typename Layout>
+__device__ __forceinline__ void sample_spline_batch(const float2* __restrict__ coef, int n, const Layout& L,
+                                                    const float* ox, const float* oy, const float* oz,
+                                                    const bool* active, bool wrap_negative, float2 fill,
+                                                    float2* out) {
+  const int h = n / 2;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    float2 acc = make_float2(0.f, 0.f);
+    if (active[s]) {
+      const float fx = floorf(ox[s]), fy = floorf(oy[s]), fz = floorf(oz[s]);
+      float wx[4], wy[4], wz[4];
+      spline_weights(ox[s] - fx, wx);
+      spline_weights(oy[s] - fy, wy);
+      spline_weights(oz[s] - fz, wz);
+      const int ix0 = (int)fx + h, iy0 = (int)fy + h, iz0 = (int)fz + h;
+      // taps i0..i0+3 inside [0, N + 2) on every axis
+      const bool interior = (unsigned)ix0 < (unsigned)(n - 1) && (unsigned)iy0 < (unsigned)(n - 1) &&
+                            (unsigned)iz0 < (unsigned)(n - 1);
+      if (interior) {
+        int xo[4], yo[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          xo[t] = L.ax(ix0 + t);
+          yo[t] = L.ay(iy0 + t);
+        }
+#pragma unroll
+        for (int dz = 0; dz < 4; ++dz) {
+          const int zo = L.az(iz0 + dz);
+#pragma unroll
+          for (int dy = 0; dy < 4; ++dy) {
+            float2 c0, c1, c2, c3;
+            if constexpr (std::is_same<Layout, SplinePairLayout>::value) {
+              const float4* row = reinterpret_cast<const float4*>(coef) + zo + yo[dy];
+              const float4 p = __ldg(row + xo[0]), q = __ldg(row + xo[2]);
+              c0 = make_float2(p.x, p.y); c1 = make_float2(p.z, p.w);
+              c2 = make_float2(q.x, q.y); c3 = make_float2(q.z, q.w);
+            } else {
+              const float2* row = coef + zo + yo[dy];
+              c0 = __ldg(row + xo[0]); c1 = __ldg(row + xo[1]);
+              c2 = __ldg(row + xo[2]); c3 = __ldg(row + xo[3]);
+            }
+            float2 r;
+            r.x = fmaf(wx[3], c3.x, fmaf(wx[2], c2.x, fmaf(wx[1], c1.x, wx[0] * c0.x)));
+            r.y = fmaf(wx[3], c3.y, fmaf(wx[2], c2.y, fmaf(wx[1], c1.y, wx[0] * c0.y)));
+            const float wzy = wz[dz] * wy[dy];
+            acc.x = fmaf(wzy, r.x, acc.x);
+            acc.y = fmaf(wzy, r.y, acc.y);
+          }
+        }
+      } else {
+        const SplineAxis ax = spline_axis(ox[s], n, wrap_negative);
+        const SplineAxis ay = spline_axis(oy[s], n, wrap_negative);
+        const SplineAxis az = spline_axis(oz[s], n, wrap_negative);
+#pragma unroll
+        for (int dz = 0; dz < 4; ++dz) {
+#pragma unroll
+          for (int dy = 0; dy < 4; ++dy) {
+            const bool vzy = az.v[dz] && ay.v[dy];
+            const int zy = L.az(az.i[dz]) + L.ay(ay.i[dy]);
+            float2 r = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int dx = 0; dx < 4; ++dx) {
+              // a pair entry's first half is the coefficient at the entry's own coordinates
+              const int e = zy + L.ax(ax.i[dx]);
+              const float2 c = (vzy && ax.v[dx])
+                                   ? __ldg(coef + (std::is_same<Layout, SplinePairLayout>::value ? 2 * e : e))
+                                   : fill;
+              r.x = fmaf(ax.w[dx], c.x, r.x);
+              r.y = fmaf(ax.w[dx], c.y, r.y);
+            }
+            const float wzy = az.w[dz] * ay.w[dy];
+            acc.x = fmaf(wzy, r.x, acc.x);
+            acc.y = fmaf(wzy, r.y, acc.y);
+          }
+        }
+      }
+    }
+    out[s] = acc;
+  }
+}
+
+// Samples from a grid in any of the layouts: trilinear from a voxel grid,
+// cubic spline from a coefficient array.
 template <int S, typename Layout>
 __device__ __forceinline__ void gather_samples(const float2* __restrict__ grid, int n, const Layout& L,
                                                const float* ox, const float* oy, const float* oz,
                                                const bool* active, bool wrap_negative, float2 fill, float2* out) {
-  if constexpr (std::is_same<Layout, PairLayout>::value)
+  if constexpr (is_spline_layout<Layout>::value)
+    sample_spline_batch<S>(grid, n, L, ox, oy, oz, active, wrap_negative, fill, out);
+  else if constexpr (std::is_same<Layout, PairLayout>::value)
     sample_trilinear_batch_pairs<S>(reinterpret_cast<const float4*>(grid), n, L, ox, oy, oz, active, wrap_negative,
                                     fill, out);
   else
@@ -468,6 +616,7 @@ struct Tuning {
   int gather_mode;  // 1 = separate gather kernel, 0 = fused gather + column FFT
   int fft_mode;     // 1 = register FFTs where possible
   int scatter_vec;  // 1 = adjoint grid scatter merges aligned x-corner pairs into 16-byte atomics
+  int spline_ilp;   // samples per lane in the cubic-spline gather (1, 2, 4)
 };
 Tuning current_tuning();
 

@@ -115,8 +115,14 @@ __global__ void __launch_bounds__(kWarps * 32)
 #define CJX_GATHER_MIN_BLOCKS 1
 #endif
 
+// Spline instances: 64 taps per sample would take ~170 registers if every
+// load were hoisted; two resident CTAs per SM cap them at 128.
+#ifndef CJX_SPLINE_MIN_BLOCKS
+#define CJX_SPLINE_MIN_BLOCKS 2
+#endif
+
 template <int S, typename Layout, int MAP>
-__global__ void __launch_bounds__(256, CJX_GATHER_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, is_spline_layout<Layout>::value ? CJX_SPLINE_MIN_BLOCKS : CJX_GATHER_MIN_BLOCKS)
     k_gather_slice(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
                    const int32_t* __restrict__ order, float2* __restrict__ hbuf, SliceGeom g, int64_t k0) {
   const Layout L(g.n);
@@ -545,6 +551,7 @@ static std::atomic<int64_t> g_gather_mode{1};
 static std::atomic<int64_t> g_fft_mode{2};
 static std::atomic<int64_t> g_gather_tile{1};
 static std::atomic<int64_t> g_scatter_vec{1};
+static std::atomic<int64_t> g_spline_ilp{4};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -556,7 +563,7 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
     return fail(CJX_ERR_UNSUPPORTED, "volume side and image sides are limited to CJX_MAX_SIDE");
   const uint32_t known =
       CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE | CJX_GRID_BRICKED |
-      CJX_GRID_BRICKED_PAIRS;
+      CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE;
   if (d->flags & ~known) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown flag bits");
   if ((d->flags & CJX_GRID_BRICKED) && (d->flags & CJX_GRID_BRICKED_PAIRS))
     return fail(CJX_ERR_INVALID_ARGUMENT, "CJX_GRID_BRICKED and CJX_GRID_BRICKED_PAIRS are exclusive");
@@ -608,6 +615,7 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_FFT_MODE) return g_fft_mode.load();
   if (key == CJX_TUNE_GATHER_TILE) return g_gather_tile.load();
   if (key == CJX_TUNE_SCATTER_VEC) return g_scatter_vec.load();
+  if (key == CJX_TUNE_SPLINE_ILP) return g_spline_ilp.load();
   return -1;
 }
 
@@ -635,6 +643,11 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_GATHER_TILE) {
     if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather tile must be 0, 1 or 2");
     g_gather_tile = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_SPLINE_ILP) {
+    if (value != 1 && value != 2 && value != 4) return fail(CJX_ERR_INVALID_ARGUMENT, "spline ILP must be 1, 2 or 4");
+    g_spline_ilp = value;
     return CJX_OK;
   }
   if (key == CJX_TUNE_SCATTER_VEC) {
@@ -676,8 +689,9 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
                          int64_t k0, int cnt, float2* t1, float2* t2, float2* hb, cudaStream_t stream,
                          const Tuning& tn) {
   if (int e = ensure_smem_attrs()) return e;
-  const int64_t ilp = tn.ilp;
-  const bool split = tn.gather_mode == 1 || (g.flags & CJX_GRID_BRICKED_PAIRS);  // the fused kernel has no pair path
+  const int64_t ilp = (g.flags & CJX_GRID_SPLINE) ? tn.spline_ilp : tn.ilp;
+  // the fused kernel has no pair or spline path
+  const bool split = tn.gather_mode == 1 || (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE));
   const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
   const bool fast = tn.fft_mode >= 1;
   const bool t512 = tn.fft_mode == 2 && rn == 16;  // 512-point column transforms through the transpose FFT
@@ -690,9 +704,16 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
       prof_begin(stream);
       const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
       const bool pairs = (g.flags & CJX_GRID_BRICKED_PAIRS) != 0;
+      const bool spline = (g.flags & CJX_GRID_SPLINE) != 0;
       const int64_t map = tn.tile;
-#define CJX_GSM(S, M)                                                                               \
-  if (pairs)                                                                                        \
+#define CJX_GSM(S, M)                                                                                   \
+  if (spline && pairs)                                                                                  \
+    k_gather_slice<S, SplinePairLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);   \
+  else if (spline && bricked)                                                                           \
+    k_gather_slice<S, SplineBrickLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);  \
+  else if (spline)                                                                                      \
+    k_gather_slice<S, SplineLinearLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0); \
+  else if (pairs)                                                                                   \
     k_gather_slice<S, PairLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);   \
   else if (bricked)                                                                                 \
     k_gather_slice<S, BrickLayout, M><<<gg, 256, 0, stream>>>(grid, params, order, hb, g, k0);  \
@@ -770,7 +791,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 
 Tuning current_tuning() {
   return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
-                (int)g_fft_mode.load(), (int)g_scatter_vec.load()};
+                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load()};
 }
 
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
@@ -783,7 +804,13 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
       const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
       prof_begin(stream);
-      if (g.flags & CJX_GRID_BRICKED_PAIRS)
+      if ((g.flags & CJX_GRID_SPLINE) && (g.flags & CJX_GRID_BRICKED_PAIRS))
+        k_slice_direct<SplinePairLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      else if ((g.flags & CJX_GRID_SPLINE) && (g.flags & CJX_GRID_BRICKED))
+        k_slice_direct<SplineBrickLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      else if (g.flags & CJX_GRID_SPLINE)
+        k_slice_direct<SplineLinearLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
+      else if (g.flags & CJX_GRID_BRICKED_PAIRS)
         k_slice_direct<PairLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);
       else if (g.flags & CJX_GRID_BRICKED)
         k_slice_direct<BrickLayout><<<dim3(blocks, cnt), 256, 0, stream>>>(grid, params, order, out, g, k0);

@@ -138,6 +138,8 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
     integ = model.volume_integrator
     params = model.image_params()
     n = params.shape[0]
+    if not hasattr(vol, "fourier_voxel_grid"):
+        raise NotImplementedError("gradients through spline volumes are not implemented on the device")
     dev = vol.fourier_voxel_grid.device
     flags = model._flags() | integ._base_flags()
     grid = vol.fourier_voxel_grid

@@ -52,7 +52,7 @@ class GaussianWhiteNoiseModel:
         py, px = cfg.padded_shape
         n = self.image_model.batch_size
         lead = () if n is None else (n,)
-        dev = self.image_model.volume_parametrization.fourier_voxel_grid.device
+        dev = self.image_model.volume_parametrization.device
         z = torch.randn(lead + (py, px // 2 + 1), generator=generator, device=dev, dtype=torch.float64)
         z[..., 0, 0] = 0.0
         var = torch.as_tensor(np.asarray(self.variance, np.float64), device=dev)

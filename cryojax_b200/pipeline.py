@@ -30,7 +30,7 @@ class HostStreamingSimulator:
         self.chunk = images_per_chunk
         self.sort = sort_orientations
         self.order_d = [None, None]
-        dev = volume.fourier_voxel_grid.device
+        dev = volume.device
         py, px = image_config.padded_shape
         self.out_shape = (py, px // 2 + 1)
         self.streams = [torch.cuda.Stream(device=dev) for _ in range(2)]

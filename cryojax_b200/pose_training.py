@@ -48,7 +48,7 @@ def simulate_clean_images(volume, image_config, wxyz, defocus, *, chunk=8192, am
     n = len(wxyz)
     py, px = image_config.padded_shape
     oy, ox = (py, px) if out_size is None else (out_size, out_size)
-    out = torch.empty((n, oy, ox), dtype=torch.float32, device=volume.fourier_voxel_grid.device)
+    out = torch.empty((n, oy, ox), dtype=torch.float32, device=volume.device)
     from . import _postprocess
 
     for s in range(0, n, chunk):
@@ -77,7 +77,7 @@ class TrainingSet:
         R = rot.quat_to_matrix(self.wxyz)
         self.labels_np = self.grid.direction_of(R).astype(np.int32)
         torch = _torch()
-        dev = volume.fourier_voxel_grid.device
+        dev = volume.device
         self.labels = torch.as_tensor(self.labels_np, device=dev)
         self.images = simulate_clean_images(volume, image_config, self.wxyz, self.defocus, out_size=out_size)
         self.n = n

@@ -70,6 +70,8 @@ def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_s
         raise NotImplementedError("refinement needs padded_shape == shape")
     vol = image_model.volume_parametrization.get_representation()
     integ = image_model.volume_integrator
+    if not hasattr(vol, "fourier_voxel_grid"):
+        raise NotImplementedError("gradients through spline volumes are not implemented on the device")
     dev = vol.fourier_voxel_grid.device
     params = image_model.image_params().copy()
     n = params.shape[0]

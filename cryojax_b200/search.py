@@ -229,7 +229,8 @@ class TemplateSharingSearch:
         py, px = cfg.padded_shape
         if py % 8:
             raise NotImplementedError("TemplateSharingSearch needs Py to be a multiple of 8")
-        key = (id(vol.fourier_voxel_grid), py, px, float(np.ravel(cfg.pixel_size)[0]))
+        integ = image_model.volume_integrator
+        key = (id(integ.device_grid(vol)[0]), py, px, float(np.ravel(cfg.pixel_size)[0]))
         if key == self._key and self.s16 is not None:
             return
         kp = py * (px // 2 + 1)

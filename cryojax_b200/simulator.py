@@ -16,7 +16,8 @@ Covered (reference file:line):
   ContrastTransferTheory      cryojax/simulator/_transfer_theory/transfer_theory.py:21-119
   FourierGaussian (envelope)  cryojax/ndimage/operators/_fourier_operator.py:183-234
   FourierVoxelGridVolume      cryojax/simulator/_volume/representations/voxel_volume.py:40-119
-  FourierSliceExtraction      cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-146
+  FourierVoxelSplineVolume    cryojax/simulator/_volume/representations/voxel_volume.py:122-203
+  FourierSliceExtraction      cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-183
   WeakPhaseScatteringTheory   cryojax/simulator/_scattering_theory/weak_phase_scattering_theory.py:13-80
   LinearImageModel, ProjectionImageModel
                               cryojax/simulator/_image_model/base_image_model.py:216-432
@@ -255,6 +256,34 @@ def _torch():
     return torch
 
 
+def _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype):
+    """pad -> ifftshift -> fftn -> fftshift, complex64 on ``device``
+    (cryojax/simulator/_volume/representations/voxel_volume.py:69-119, 163-203)."""
+    torch = _torch()
+    if pad_scale < 1.0:
+        raise ValueError("`pad_scale` must be greater than 1.0")
+    if pad_mode != "constant":
+        raise NotImplementedError("only constant padding is implemented")
+    real = real_voxel_grid
+    if not isinstance(real, torch.Tensor):
+        real = torch.as_tensor(np.asarray(real, np.float64))
+    real = real.to(device=device, dtype=fft_dtype or torch.float64)
+    shape = tuple(int(s * pad_scale) for s in real.shape)
+    pads = []
+    for s, d in zip(reversed(shape), reversed(real.shape)):
+        pad = s - d
+        if s % 2 == 1 and d % 2 == 0:
+            lr = (pad // 2, pad // 2 + 1)
+        elif s % 2 == 0 and d % 2 == 1:
+            lr = (pad // 2 + 1, pad // 2)
+        else:
+            lr = (pad // 2, pad // 2)
+        pads.extend(lr)
+    padded = torch.nn.functional.pad(real, pads, mode="constant", value=0.0)
+    ft = torch.fft.fftn(torch.fft.ifftshift(padded))
+    return torch.fft.fftshift(ft).to(torch.complex64).contiguous()
+
+
 class FourierVoxelGridVolume:
     """Centred full 3-D FFT grid of a padded real volume (complex64, CUDA).
 
@@ -292,6 +321,10 @@ class FourierVoxelGridVolume:
     def shape(self):
         return tuple(self.fourier_voxel_grid.shape)
 
+    @property
+    def device(self):
+        return self.fourier_voxel_grid.device
+
     @classmethod
     def from_real_voxel_grid(cls, real_voxel_grid, *, pad_scale: float = 1.0, pad_mode: str = "constant",
                              device: str = "cuda", fft_dtype=None):
@@ -300,30 +333,7 @@ class FourierVoxelGridVolume:
         The FFT runs in float64 on ``device`` and the grid is stored as
         complex64 (one-time volume preparation, not part of the image path).
         """
-        torch = _torch()
-        if pad_scale < 1.0:
-            raise ValueError("`pad_scale` must be greater than 1.0")
-        if pad_mode != "constant":
-            raise NotImplementedError("only constant padding is implemented")
-        real = real_voxel_grid
-        if not isinstance(real, torch.Tensor):
-            real = torch.as_tensor(np.asarray(real, np.float64))
-        real = real.to(device=device, dtype=fft_dtype or torch.float64)
-        shape = tuple(int(s * pad_scale) for s in real.shape)
-        pads = []
-        for s, d in zip(reversed(shape), reversed(real.shape)):
-            pad = s - d
-            if s % 2 == 1 and d % 2 == 0:
-                lr = (pad // 2, pad // 2 + 1)
-            elif s % 2 == 0 and d % 2 == 1:
-                lr = (pad // 2 + 1, pad // 2)
-            else:
-                lr = (pad // 2, pad // 2)
-            pads.extend(lr)
-        padded = torch.nn.functional.pad(real, pads, mode="constant", value=0.0)
-        ft = torch.fft.fftn(torch.fft.ifftshift(padded))
-        grid = torch.fft.fftshift(ft).to(torch.complex64).contiguous()
-        return cls(grid)
+        return cls(_centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype))
 
     def rotate_to_pose(self, pose: AbstractPose, inverse: bool = False):
         """Attach the pose (the frequency slice is rotated inside the kernel)."""
@@ -332,6 +342,72 @@ class FourierVoxelGridVolume:
                                   wxyz=rot.quat_inverse(pose.quaternion()))
         return FourierVoxelGridVolume(self.fourier_voxel_grid, rotation=pose, bricked=self._bricked,
                                       pairs=self._pairs)
+
+    def get_representation(self, rng_key=None):
+        return self
+
+
+class FourierVoxelSplineVolume:
+    """Cubic-spline coefficients ((N+2)^3 complex64, CUDA) of a centred
+    Fourier voxel grid.
+
+    cryojax/simulator/_volume/representations/voxel_volume.py:122-203.  The
+    slice is cubic-spline interpolated from the coefficients
+    (fourier_voxel_extract.py:148-183); ``shape`` is the voxel grid's.
+    """
+
+    def __init__(self, spline_coefficients, rotation=None, *, bricked=None, pairs=None):
+        torch = _torch()
+        c = spline_coefficients
+        if not isinstance(c, torch.Tensor):
+            c = torch.as_tensor(np.asarray(c))
+        if c.dim() != 3 or len(set(c.shape)) != 1:
+            raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
+        self.spline_coefficients = c
+        self.rotation = rotation
+        self._bricked = bricked
+        self._pairs = pairs
+
+    def bricked_grid(self):
+        """The coefficients in the library's bricked layout on side N + 2 (cached)."""
+        if self._bricked is None:
+            self._bricked = nat.brick_volume(self.spline_coefficients.contiguous())
+        return self._bricked
+
+    def pair_grid(self):
+        """The coefficients in the x-pair bricked layout on side N + 2 (cached; twice their bytes)."""
+        if self._pairs is None:
+            self._pairs = nat.brick_volume_pairs_new(self.spline_coefficients.contiguous())
+        return self._pairs
+
+    @property
+    def shape(self):
+        return tuple(s - 2 for s in self.spline_coefficients.shape)
+
+    @property
+    def device(self):
+        return self.spline_coefficients.device
+
+    @classmethod
+    def from_real_voxel_grid(cls, real_voxel_grid, *, pad_scale: float = 1.0, pad_mode: str = "constant",
+                             device: str = "cuda", fft_dtype=None):
+        """Fourier grid as FourierVoxelGridVolume.from_real_voxel_grid, then its
+        spline coefficients on the device (voxel_volume.py:163-203)."""
+        grid = _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype)
+        return cls(nat.spline_coefficients(grid))
+
+    @classmethod
+    def from_fourier_voxel_grid(cls, volume: FourierVoxelGridVolume):
+        """Spline coefficients of an existing FourierVoxelGridVolume's grid."""
+        return cls(nat.spline_coefficients(volume.fourier_voxel_grid.contiguous()))
+
+    def rotate_to_pose(self, pose: AbstractPose, inverse: bool = False):
+        """Attach the pose (the frequency slice is rotated inside the kernel)."""
+        if inverse:
+            pose = QuaternionPose(*np.moveaxis(pose.offset_in_angstroms[..., :2], -1, 0),
+                                  wxyz=rot.quat_inverse(pose.quaternion()))
+        return FourierVoxelSplineVolume(self.spline_coefficients, rotation=pose, bricked=self._bricked,
+                                        pairs=self._pairs)
 
     def get_representation(self, rng_key=None):
         return self
@@ -441,9 +517,9 @@ def orientation_order(rotations: np.ndarray, bits: int = 8) -> np.ndarray:
 class FourierSliceExtraction:
     """Fourier-slice projection of a FourierVoxelGridVolume on the B200.
 
-    cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-146
-    (trilinear grid path; ``correction_mask`` and spline volumes are not
-    implemented).  ``out_of_bounds_mode="fill"`` with ``fill_value`` follows
+    cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-183
+    (trilinear sampling of a FourierVoxelGridVolume, cubic-spline sampling
+    of a FourierVoxelSplineVolume; ``correction_mask`` is not implemented).  ``out_of_bounds_mode="fill"`` with ``fill_value`` follows
     the reference; ``"zero_fill_negative"`` fills negative indices too
     (not the reference's rule, see CJX_ZERO_FILL_NEGATIVE).
     """
@@ -468,8 +544,17 @@ class FourierSliceExtraction:
 
         Bricked layouts are cached on the volume: the x-pair copy when
         ``pair_layout`` (default), else the plain bricked copy; without
-        ``use_bricked_layout`` the reference's C-order array itself.
+        ``use_bricked_layout`` the reference's C-order array itself.  A
+        FourierVoxelSplineVolume gives its coefficients (CJX_GRID_SPLINE) in
+        the same three layouts.
         """
+        if isinstance(volume, FourierVoxelSplineVolume):
+            coef = volume.spline_coefficients
+            if not (self.use_bricked_layout and coef.is_cuda):
+                return coef, nat.CJX_GRID_SPLINE
+            if self.pair_layout:
+                return volume.pair_grid(), nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED_PAIRS
+            return volume.bricked_grid(), nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED
         grid = volume.fourier_voxel_grid
         if not (self.use_bricked_layout and grid.is_cuda):
             return grid, 0
@@ -490,7 +575,7 @@ class FourierSliceExtraction:
         when not supplied.
         """
         torch = _torch()
-        n_vol = volume.fourier_voxel_grid.shape[0]
+        n_vol = volume.shape[0]
         grid, layout = self.device_grid(volume)
         flags = flags | layout
         if image_config.pad_mode != "constant":
@@ -668,11 +753,12 @@ class ContrastImageModel(AbstractImageModel):
 def make_image_model(volume_parametrization, image_config, pose, transfer_theory=None, volume_integrator=None,
                      detector=None, *, applies_translation=True, normalizes_signal=False, signal_region=None,
                      simulates_quantity=False, quantity_mode="contrast", translate_mode="fft"):
-    """cryojax/simulator/_api_utils.py:36-223 (FourierVoxelGridVolume routes)."""
-    if not isinstance(volume_parametrization, FourierVoxelGridVolume):
+    """cryojax/simulator/_api_utils.py:36-223 (Fourier voxel volume routes)."""
+    if not isinstance(volume_parametrization, (FourierVoxelGridVolume, FourierVoxelSplineVolume)):
         raise ValueError(
             "Could not select default integrator for volume of type "
-            f"{type(volume_parametrization).__name__}: only FourierVoxelGridVolume runs on the device")
+            f"{type(volume_parametrization).__name__}: only FourierVoxelGridVolume and FourierVoxelSplineVolume "
+            "run on the device")
     if volume_integrator is None:
         volume_integrator = FourierSliceExtraction(outputs_integral=simulates_quantity)
     kw = dict(applies_translation=applies_translation, normalizes_signal=normalizes_signal,

@@ -67,6 +67,17 @@ extern "C" {
  * trilinear sample reads its 8 corners with 4 vector loads.  Forward and
  * search entry points only (not cjx_slice_ctf_loss_grad).                 */
 #define CJX_GRID_BRICKED_PAIRS (1u << 5)
+/* `grid` holds the cubic-spline coefficients of a FourierVoxelSplineVolume
+ * (side N + 2: C order, bricked on side N + 2 with CJX_GRID_BRICKED,
+ * or x-pair bricked on side N + 2 with CJX_GRID_BRICKED_PAIRS, as written
+ * by cjx_brick_volume / cjx_brick_volume_pairs with n = N + 2)
+ * instead of the voxel grid, and every sample is the reference's 4x4x4-tap
+ * cubic-spline interpolation
+ * (cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:148-183,
+ * 453-462, 531-534; cryojax/ndimage/_map_coordinates.py:126-142, 217-250).
+ * desc->n stays the voxel grid's side N.  Forward, multi, no-alloc and
+ * search entry points; not cjx_slice_ctf_loss_grad (CJX_ERR_UNSUPPORTED).  */
+#define CJX_GRID_SPLINE (1u << 6)
 
 /* ---- per-image parameters (one record per image, device memory) ------
  * 32 doubles (256 bytes).  Built on the host from a pose, a CTF and an
@@ -256,7 +267,8 @@ CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void
                                           int64_t n_images, void* out, void* stream);
 
 /* Bricked volume layout (no counterpart in the reference; a device-side
- * re-layout of FourierVoxelGridVolume.fourier_voxel_grid).  8x8x8 blocks in
+ * re-layout of FourierVoxelGridVolume.fourier_voxel_grid, or of a
+ * FourierVoxelSplineVolume's coefficients with n = N + 2).  8x8x8 blocks in
  * C order; inside a block the voxels are in Morton order, so every 2x2x2
  * brick is 64 contiguous bytes.  A slice plane at any orientation then reads
  * compact voxel clusters per DRAM burst.  Sides are padded to a multiple of
@@ -266,8 +278,25 @@ CJX_API int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const void
 CJX_API int cjx_bricked_volume_size(int n, size_t* bytes);
 CJX_API int cjx_brick_volume(int n, const void* grid, void* bricked, void* stream);
 /* The x-pair copy (CJX_GRID_BRICKED_PAIRS): twice cjx_bricked_volume_size
- * bytes; entry (x, y, z) = (g(x, y, z), g(x+1, y, z)), zero past the edge. */
+ * bytes; entry (x, y, z) = (g(x, y, z), g(x+1, y, z)), zero past the edge.
+ * n may be up to CJX_MAX_SIDE + 2 (a spline coefficient array's side).      */
 CJX_API int cjx_brick_volume_pairs(int n, const void* grid, void* pairs, void* stream);
+
+/* Cubic-spline coefficients of a centred Fourier voxel grid: `grid` N^3
+ * complex64 (C order) -> `coefficients` (N + 2)^3 complex64 (C order).
+ * Replaces compute_spline_coefficients
+ * (cryojax/ndimage/_map_coordinates.py:71-82, 179-215) as called by
+ * FourierVoxelSplineVolume.from_real_voxel_grid
+ * (cryojax/simulator/_volume/representations/voxel_volume.py:163-203):
+ * along x, then y, then z, each line of length L gets c2 = d[0]/6,
+ * c_{L+1} = d[L-1]/6, the tridiag(1, 4, 1) solve for the interior and the
+ * two end extrapolations.  Solved in double precision, stored complex64.
+ * N in [4, CJX_MAX_SIDE]; grid and coefficients distinct; scratch of
+ * cjx_spline_coefficients_workspace_size bytes (N (N + 2)^2 complex64).
+ * Stream-ordered.                                                          */
+CJX_API int cjx_spline_coefficients_workspace_size(int n, size_t* bytes);
+CJX_API int cjx_spline_coefficients(int n, const void* grid, void* coefficients, void* workspace,
+                                    size_t workspace_bytes, void* stream);
 
 /* Batched complex-to-complex FFTs of `count` contiguous rows of n complex64
  * values (direction -1: forward, numpy.fft.fft; +1: unnormalised inverse,
@@ -292,13 +321,16 @@ CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t
  * or 8 x 4 (2) samples (columns x rows) of the slice plane.
  * CJX_TUNE_SCATTER_VEC: 1 (default) = the adjoint's grid scatter-add puts
  * the two x-corners of a corner row into one 16-byte atomic when they are
- * adjacent and aligned; 0 = one 8-byte atomic per (sample, corner).        */
+ * adjacent and aligned; 0 = one 8-byte atomic per (sample, corner).
+ * CJX_TUNE_SPLINE_ILP: samples per lane in the cubic-spline gather
+ * (CJX_GRID_SPLINE; 1, 2 or 4, default 4).                                 */
 #define CJX_TUNE_GATHER_ILP 1
 #define CJX_TUNE_CHUNK_BYTES 2
 #define CJX_TUNE_GATHER_MODE 3
 #define CJX_TUNE_FFT_MODE 4
 #define CJX_TUNE_GATHER_TILE 5
 #define CJX_TUNE_SCATTER_VEC 6
+#define CJX_TUNE_SPLINE_ILP 7
 CJX_API int cjx_tuning_set(int key, int64_t value);
 CJX_API int cjx_tuning_get(int key, int64_t* value);
 

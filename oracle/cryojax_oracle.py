@@ -372,6 +372,74 @@ def map_coordinates_linear(grid, coordinates, cval=0.0, wrap_negative=True):
     return np.asarray(out).astype(grid.dtype)
 
 
+def compute_spline_coefficients(data):
+    """Cubic B-spline coefficients, one tridiagonal solve per axis line.
+
+    cryojax/ndimage/_map_coordinates.py:71-82, 179-215: along each axis
+    (last axis first) a line d of length n gets c2 = d[0] / 6,
+    c_{n+2} = d[-1] / 6, the interior cs from tridiag(1, 4, 1) cs = d[1:-1]
+    with d[1] -= c2 and d[-2] -= c_{n+2} (a banded solve here, lineax's
+    TridiagonalLinearOperator there), then c1 = 2 c2 - cs[0] and
+    c_{n+3} = 2 c_{n+2} - cs[-1]: n + 2 coefficients per line.
+    """
+    from scipy.linalg import solve_banded
+
+    out = np.asarray(data, np.complex128)
+    for axis in reversed(range(out.ndim)):
+        x = np.moveaxis(out, axis, 0)
+        n = x.shape[0]
+        rest = x.shape[1:]
+        x = x.reshape(n, -1)
+        c2, cnp2 = x[0] / 6.0, x[-1] / 6.0
+        y = x[1:-1].copy()
+        y[0] -= c2
+        y[-1] -= cnp2
+        m = n - 2
+        ab = np.zeros((3, m))
+        ab[0, 1:] = 1.0
+        ab[1, :] = 4.0
+        ab[2, :-1] = 1.0
+        cs = solve_banded((1, 1), ab, y)
+        res = np.concatenate([(2 * c2 - cs[0])[None], c2[None], cs, cnp2[None], (2 * cnp2 - cs[-1])[None]], 0)
+        out = np.moveaxis(res.reshape((n + 2,) + rest), 0, axis)
+    return out
+
+
+def spline_basis(t):
+    """cryojax/ndimage/_map_coordinates.py:217-225 (unnormalised cubic B-spline: 4 at 0, 1 at +-1)."""
+    at = np.abs(t)
+    return np.where(at >= 1, np.where(at <= 2, (2 - at) ** 3, 0.0), 4 - 6 * at**2 + 3 * at**3)
+
+
+def map_coordinates_spline(coefficients, coordinates, cval=0.0, wrap_negative=True):
+    """Cubic-spline sampling, mode="fill".
+
+    cryojax/ndimage/_map_coordinates.py:48-68, 126-142, 228-250: for a
+    coordinate c the taps are the coefficient indices floor(c) + {0, 1, 2, 3}
+    along each axis with weights spline_basis(c - i + 1); each tap is read
+    with ``.at[idx].get(mode="fill", fill_value=cval)`` (an index in [-n, 0)
+    wraps once, anything else outside [0, n) reads cval).
+    """
+    axes = []
+    for c in coordinates:
+        c = np.asarray(c, np.float64)
+        f = np.floor(c).astype(np.int64)
+        axes.append([(f + t, spline_basis(c - (f + t) + 1)) for t in range(4)])
+    out = 0.0
+    for items in itertools.product(*axes):
+        valid = True
+        idx = []
+        weight = 1.0
+        for axis, (i, w) in enumerate(items):
+            n = coefficients.shape[axis]
+            j = np.where(i < 0, i + n, i) if wrap_negative else i
+            valid = valid & (j >= 0) & (j < n)
+            idx.append(np.clip(j, 0, n - 1))
+            weight = weight * w
+        out = out + weight * np.where(valid, coefficients[tuple(idx)], cval)
+    return np.asarray(out).astype(np.complex128)
+
+
 # ---------------------------------------------------------------------------
 # Volume and Fourier-slice extraction
 # (cryojax/simulator/_volume/representations/voxel_volume.py,
@@ -403,19 +471,26 @@ def rotate_frequency_slice(frequency_slice, wxyz):
     return quat_apply(wxyz, frequency_slice)
 
 
-def extract_surface_from_voxel_grid(grid, frequency_coordinates, cval=0.0, wrap_negative=True):
-    """cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:519-544."""
+def extract_surface_from_voxel_grid(grid, frequency_coordinates, cval=0.0, wrap_negative=True, spline=False):
+    """cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:519-544.
+
+    With ``spline`` the grid holds cubic-spline coefficients ((N+2)^3) and
+    the surface is sampled with map_coordinates_spline (:531-534).
+    """
     n = frequency_coordinates.shape[1]
     logical = frequency_coordinates * n + n // 2
     k_z, k_y, k_x = np.moveaxis(logical, -1, 0)
-    surface = map_coordinates_linear(grid, (k_x, k_y, k_z), cval, wrap_negative)[0]
+    if spline:
+        surface = map_coordinates_spline(grid, (k_x, k_y, k_z), cval, wrap_negative)[0]
+    else:
+        surface = map_coordinates_linear(grid, (k_x, k_y, k_z), cval, wrap_negative)[0]
     return np.fft.ifftshift(surface)
 
 
-def extract_slice(grid, frequency_coordinates, cval=0.0, wrap_negative=True):
-    """cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:428-443."""
+def extract_slice(grid, frequency_coordinates, cval=0.0, wrap_negative=True, spline=False):
+    """cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:428-457 (grid and spline)."""
     return convert_fftn_to_rfftn(
-        extract_surface_from_voxel_grid(grid, frequency_coordinates, cval, wrap_negative),
+        extract_surface_from_voxel_grid(grid, frequency_coordinates, cval, wrap_negative, spline),
         mode="real",
     )
 
@@ -431,15 +506,18 @@ def fourier_slice_integrate(
     cval=0.0,
     outputs_real_space=False,
     wrap_negative=True,
+    spline=False,
 ):
-    """FourierSliceExtraction.integrate for a FourierVoxelGridVolume.
+    """FourierSliceExtraction.integrate for a FourierVoxelGridVolume
+    (or, with ``spline``, a FourierVoxelSplineVolume's coefficients).
 
     cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:78-146.
     """
     n = rotated_frequency_slice.shape[1]
-    if grid.shape != (n, n, n):
+    m = n + 2 if spline else n
+    if grid.shape != (m, m, m):
         raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
-    proj = extract_slice(grid, rotated_frequency_slice, cval, wrap_negative)
+    proj = extract_slice(grid, rotated_frequency_slice, cval, wrap_negative, spline)
     if tuple(padded_shape) != (n, n):
         proj = rfftn(resize_with_crop_or_pad(irfftn(proj, s=(n, n)), tuple(padded_shape), pad_mode))
     if outputs_integral:
@@ -585,6 +663,7 @@ def compute_fourier_image(
     apply_ctf=True,
     cval=0.0,
     wrap_negative=True,
+    spline=False,
 ):
     """LinearImageModel / ContrastImageModel.compute_fourier_image.
 
@@ -605,6 +684,7 @@ def compute_fourier_image(
         pad_mode=spec.pad_mode,
         cval=cval,
         wrap_negative=wrap_negative,
+        spline=spline,
     )
     if simulates_quantity:
         proj = interaction_constant_from_kilovolts(spec.voltage_in_kilovolts) * proj
@@ -691,7 +771,7 @@ def normalized_cross_correlation(simulated, observed):
     return float(np.mean(normalize_image(simulated) * normalize_image(observed)))
 
 
-def grid_search_orientations(grid, frequency_slice, specs, observed, quaternions):
+def grid_search_orientations(grid, frequency_slice, specs, observed, quaternions, **kw):
     """Exhaustive orientation search: best (max NCC) grid index per image.
 
     For each image b, simulate spec b at every orientation of the grid (its
@@ -700,6 +780,7 @@ def grid_search_orientations(grid, frequency_slice, specs, observed, quaternions
     running argmin of MinimumSearchMethod.batch_update applied to -NCC
     (cryojax/jax_util/_grid_search/search_method.py:237-265,
     search_loop.py:24-158).  Returns (best_index (n,), scores (n, T)).
+    ``kw`` goes to compute_fourier_image (e.g. ``spline=True``).
     """
     import copy
 
@@ -709,7 +790,7 @@ def grid_search_orientations(grid, frequency_slice, specs, observed, quaternions
         for k, q in enumerate(quaternions):
             s = copy.copy(spec)
             s.wxyz = np.asarray(q, np.float64)
-            scores[b, k] = normalized_cross_correlation(simulate(grid, frequency_slice, s), observed[b])
+            scores[b, k] = normalized_cross_correlation(simulate(grid, frequency_slice, s, **kw), observed[b])
     best = np.empty(n, np.int64)
     for b in range(n):
         cur, idx = np.inf, 0

@@ -81,6 +81,9 @@ def test_tuning_knobs():
         nat.tuning_set(99, 1)
     assert nat.tuning_get(nat.CJX_TUNE_FFT_MODE) == 2  # transpose FFT for 512-point column passes
     assert nat.tuning_get(nat.CJX_TUNE_SCATTER_VEC) == 1
+    assert nat.tuning_get(nat.CJX_TUNE_SPLINE_ILP) == 4
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(nat.CJX_TUNE_SPLINE_ILP, 3)
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(nat.CJX_TUNE_FFT_MODE, 3)
     with pytest.raises(nat.CryojaxB200Error):
@@ -113,3 +116,22 @@ def test_empty_groups_need_no_workspace():
     assert nat.multi_workspace_size(empty) == 0
     one = nat.make_groups([{"desc": d, "n_images": 0}, {"desc": d, "n_images": 3}])
     assert nat.multi_workspace_size(one) == nat.workspace_size(d, 3)
+
+
+def test_spline_flag_validation():
+    d = nat.make_desc(64, 32, 32, nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED)
+    assert nat.workspace_size(d, 2) == nat.workspace_size(nat.make_desc(64, 32, 32, 0), 2)
+    assert nat.workspace_size(nat.make_desc(64, 32, 32, nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED_PAIRS), 1) > 0
+    with pytest.raises(nat.CryojaxB200Error) as e:
+        nat.loss_workspace_size(nat.make_desc(64, 32, 32, nat.CJX_GRID_SPLINE), 1)
+    assert e.value.code == nat.CJX_ERR_UNSUPPORTED
+    # coefficient solve: N in [4, CJX_MAX_SIDE], scratch N (N + 2)^2 complex64
+    assert nat.spline_coefficients_workspace_size(64) == 8 * 64 * 66 * 66
+    for bad in (3, nat.CJX_MAX_SIDE + 1):
+        with pytest.raises(nat.CryojaxB200Error) as e:
+            nat.spline_coefficients_workspace_size(bad)
+        assert e.value.code == nat.CJX_ERR_UNSUPPORTED
+    lib = nat.load_library()
+    assert lib.cjx_spline_coefficients(8, None, None, None, 0, None) == nat.CJX_ERR_INVALID_ARGUMENT
+    # a coefficient array (side N + 2) can be bricked up to N = CJX_MAX_SIDE
+    assert nat.bricked_volume_size(nat.CJX_MAX_SIDE + 2) > 0

@@ -111,3 +111,34 @@ def test_map_coordinates_out_of_bounds_rule():
     assert O.map_coordinates_linear(g, (np.array([3.5]),), cval=10.0)[0] == pytest.approx(0.5 * 3 + 0.5 * 10)
     assert O.map_coordinates_linear(g, (np.array([-0.5]),), wrap_negative=False)[0] == pytest.approx(0.0)
     assert O.map_coordinates_linear(g, (np.array([-0.5]),))[0] == pytest.approx(0.5 * 3 + 0.5 * 0)
+
+
+def test_spline_coefficients_interpolate_the_grid():
+    """The cubic spline through the coefficients passes through every grid value
+    (c_{i-1} + 4 c_i + c_{i+1} = d_i in each axis), and sampling at grid points returns the grid."""
+    rng = np.random.default_rng(2)
+    g = rng.standard_normal((9, 10, 11)) + 1j * rng.standard_normal((9, 10, 11))
+    c = O.compute_spline_coefficients(g)
+    assert c.shape == (11, 12, 13)
+    z, y, x = np.meshgrid(np.arange(9), np.arange(10), np.arange(11), indexing="ij")
+    v = O.map_coordinates_spline(c, (z, y, x))
+    np.testing.assert_allclose(v, g, atol=1e-12 * np.abs(g).max())
+    # 1-D: the end conditions of the reference's solve (c2 = d0 / 6 and c1 = 2 c2 - c3)
+    d = rng.standard_normal(7)
+    c1 = O.compute_spline_coefficients(d)
+    np.testing.assert_allclose(c1[1], d[0] / 6)
+    np.testing.assert_allclose(c1[0], 2 * c1[1] - c1[2])
+    np.testing.assert_allclose(c1[1:-3] + 4 * c1[2:-2] + c1[3:-1], d[1:-1], atol=1e-12)
+
+
+def test_spline_slice_of_a_smooth_volume_is_close_to_the_linear_one():
+    vol = O.gaussian_sum_volume(16, 20, seed=3, sigma_range=(2.0, 3.0))
+    grid, fs = O.fourier_voxel_grid_from_real_voxel_grid(vol, pad_scale=2.0)
+    coeffs = O.compute_spline_coefficients(grid)
+    q = O.uniform_poses(1, 4, 0.0)[0][0]
+    rot = O.rotate_frequency_slice(fs, q)
+    lin = O.extract_slice(grid, rot)
+    spl = O.extract_slice(coeffs, rot, spline=True)
+    # both interpolate the same band-limited grid; they agree to the interpolation error
+    assert np.linalg.norm(spl - lin) <= 0.1 * np.linalg.norm(lin)
+    assert np.linalg.norm(spl - lin) > 1e-6 * np.linalg.norm(lin)
