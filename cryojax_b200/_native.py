@@ -29,6 +29,7 @@ CJX_ZERO_FILL_NEGATIVE = 1 << 3
 CJX_GRID_BRICKED = 1 << 4
 CJX_GRID_BRICKED_PAIRS = 1 << 5
 CJX_GRID_SPLINE = 1 << 6
+CJX_EWALD_SPHERE = 1 << 7
 
 CJX_MAX_SIDE = 1024
 CJX_TUNE_GATHER_ILP = 1
@@ -54,6 +55,8 @@ P_PIXEL_SIZE = 17
 P_SCALE = 18
 P_ENV_AMP = 19
 P_ENV_B = 20
+P_AC = 21
+P_PHASE_SHIFT = 22
 
 
 class SliceDesc(ctypes.Structure):

@@ -65,6 +65,7 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_verbose: boo
     objs = []
     tmp_dir = os.path.join(LIB_DIR, "obj")
     os.makedirs(tmp_dir, exist_ok=True)
+    cmds = []
     for src in _sources():
         obj = os.path.join(tmp_dir, os.path.basename(src)[:-3] + ".o")
         cmd = [nvcc, *ARCH_FLAGS, *NVCC_FLAGS, "-I", INCLUDE, "-c", src, "-o", obj]
@@ -72,8 +73,15 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_verbose: boo
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # one nvcc per translation unit, run side by side
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp_lib = LIB_PATH + ".tmp"
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", tmp_lib, *objs, "-lcudart"]
     if verbose:

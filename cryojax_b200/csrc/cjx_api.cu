@@ -206,6 +206,7 @@ int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_imag
   if (int e = make_geom(desc, &g)) return e;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
   if (g.flags & CJX_GRID_SPLINE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of spline volumes is not implemented");
+  if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
   *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
   return CJX_OK;
 }
@@ -219,6 +220,7 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (n_images == 0) return CJX_OK;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
   if (g.flags & CJX_GRID_SPLINE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of spline volumes is not implemented");
+  if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
   if (!grid || !params || !observed || !image_grads)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");
   const int64_t chunk = chunk_for(g, desc, n_images);
@@ -233,6 +235,7 @@ static int search_plan(const cjx_search_desc* d, SliceGeom* g, int* K, int64_t* 
   if (!d) return fail(CJX_ERR_INVALID_ARGUMENT, "desc is NULL");
   if (int e = make_geom(&d->slice, g)) return e;
   if (!needs_resize(*g)) return fail(CJX_ERR_UNSUPPORTED, "search needs the resize path ((Py, Px) != (N, N))");
+  if (g->flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "search scores projection images only");
   if (d->n_images < 0 || d->n_orientations < 1 || d->candidates_per_image < 0)
     return fail(CJX_ERR_INVALID_ARGUMENT, "need n_images >= 0, n_orientations >= 1, candidates_per_image >= 0");
   if (d->n_orientations > 2147483647LL) return fail(CJX_ERR_UNSUPPORTED, "too many orientations");

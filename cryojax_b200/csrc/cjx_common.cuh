@@ -21,6 +21,7 @@ struct SliceGeom {
   int n;            // volume side N
   int py, px;       // padded image shape
   int nxh;          // N/2 + 1 (half-plane columns of the slice)
+  int ncols;        // slice columns sampled: N/2 + 1, or N for the Ewald sphere's full surface
   int pxh;          // Px/2 + 1
   int ld1, ld2;     // row pitch (complex elements) of workspace T1, T2
   int ldh;          // column pitch of the slice buffer H ([kx][ky], split gather)
@@ -520,6 +521,8 @@ struct ImageConsts {
   float cos2a, sin2a;   // cos / sin of 2 * astigmatism_angle
   float scale;
   float env_amp, env_quarter_b;
+  double ps_cycles;     // phase_shift / (2 pi)        (Ewald contrast)
+  float w1, w2;         // ac, sqrt(1 - ac^2)          (Ewald contrast)
 };
 
 __device__ __forceinline__ ImageConsts load_image_consts(const cjx_image_params* __restrict__ p, float extra_scale,
@@ -543,7 +546,18 @@ __device__ __forceinline__ ImageConsts load_image_consts(const cjx_image_params*
   c.scale = (float)(p->scale * (double)extra_scale);
   c.env_amp = (float)p->envelope_amplitude;
   c.env_quarter_b = (float)(0.25 * p->envelope_b_factor);
+  c.ps_cycles = p->phase_shift * 0.15915494309189533577;
+  const double ac = p->amplitude_contrast_ratio;
+  c.w1 = (float)ac;
+  c.w2 = (float)sqrt(1.0 - ac * ac);
   return c;
+}
+
+// The Ewald surface's third coordinate per squared pixel frequency index:
+// N q_z = N (lambda / pixel_size) |q|^2 / 2 with q = (kx, ky) / N
+// (cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:489-516).
+__device__ __forceinline__ float ewald_w(const cjx_image_params* __restrict__ p, int n) {
+  return (float)(p->wavelength / (2.0 * (double)n * p->pixel_size));
 }
 
 // Value at rfft-grid entry (i, j) of a (py, px) image.
@@ -559,6 +573,46 @@ __device__ __forceinline__ ImageConsts load_image_consts(const cjx_image_params*
 //   before the single-precision sinpi, so large defocus keeps full accuracy.
 //   Translation: zero the even-size Nyquist self-conjugates, then multiply
 //   by exp(-2 pi i (qx tx + qy ty))  (cryojax/simulator/_pose.py:68-114).
+// chi / (2 pi) without the constant phase: -1/2 df(theta) lambda k^2 + 1/4 Cs lambda^3 k^4.
+__device__ __forceinline__ double aberration_cycles(double qx, double qy, double k2, const ImageConsts& c) {
+  // angle terms only scale the astigmatism (|astig| / 2 <~ 1e3 A), so
+  // single precision is ample for them
+  float c2t = 1.0f, s2t = 0.0f;
+  if (k2 > 0.0) {
+    const float qxf = (float)qx, qyf = (float)qy;
+    const float inv = 1.0f / (float)k2;
+    c2t = (qyf * qyf - qxf * qxf) * inv;
+    s2t = 2.0f * qxf * qyf * inv;
+  }
+  const double df = c.defocus + c.half_astig * (double)(c2t * c.cos2a + s2t * c.sin2a);
+  return (c.c_def * df + c.c_sph * k2) * k2;
+}
+
+// Envelope and translation of an rfft-grid value (shared by both epilogues).
+__device__ __forceinline__ float2 envelope_translate(float2 v, int i, int j, int py, int px, double qx, double qy,
+                                                    double k2, uint32_t flags, const ImageConsts& c) {
+  if (flags & CJX_APPLY_ENVELOPE) {
+    const float e = c.env_amp * expf(-c.env_quarter_b * (float)k2);
+    v.x *= e;
+    v.y *= e;
+  }
+  if (flags & CJX_APPLY_TRANSLATION) {
+    const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
+    const bool self_conj = (ey && i == py / 2 && j == 0) || (ex && i == 0 && j == px / 2) ||
+                           (ey && ex && i == py / 2 && j == px / 2);
+    if (self_conj) {
+      v = make_float2(0.f, 0.f);
+    } else {
+      const double ph = qx * c.tx + qy * c.ty;
+      const float r = (float)(ph - rint(ph));
+      float s, co;
+      sincospif(2.0f * r, &s, &co);
+      v = make_float2(fmaf(v.x, co, v.y * s), fmaf(v.y, co, -v.x * s));
+    }
+  }
+  return v;
+}
+
 __device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
                                                  const ImageConsts& c) {
   v.x *= c.scale;
@@ -568,43 +622,56 @@ __device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py,
     const double qx = (double)j * c.qx_step;
     const double k2 = qx * qx + qy * qy;
     if (flags & CJX_APPLY_CTF) {
-      // angle terms only scale the astigmatism (|astig| / 2 <~ 1e3 A), so
-      // single precision is ample for them
-      float c2t = 1.0f, s2t = 0.0f;
-      if (k2 > 0.0) {
-        const float qxf = (float)qx, qyf = (float)qy;
-        const float inv = 1.0f / (float)k2;
-        c2t = (qyf * qyf - qxf * qxf) * inv;
-        s2t = 2.0f * qxf * qyf * inv;
-      }
-      const double df = c.defocus + c.half_astig * (double)(c2t * c.cos2a + s2t * c.sin2a);
-      const double arg = (c.c_def * df + c.c_sph * k2) * k2 - c.phase_cycles;
+      const double arg = aberration_cycles(qx, qy, k2, c) - c.phase_cycles;
       const float r = (float)(arg - rint(arg));
       const float ctf = sinpif(2.0f * r);
       v.x *= ctf;
       v.y *= ctf;
     }
-    if (flags & CJX_APPLY_ENVELOPE) {
-      const float e = c.env_amp * expf(-c.env_quarter_b * (float)k2);
-      v.x *= e;
-      v.y *= e;
-    }
-    if (flags & CJX_APPLY_TRANSLATION) {
-      const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
-      const bool self_conj = (ey && i == py / 2 && j == 0) || (ex && i == 0 && j == px / 2) ||
-                             (ey && ex && i == py / 2 && j == px / 2);
-      if (self_conj) {
-        v = make_float2(0.f, 0.f);
-      } else {
-        const double ph = qx * c.tx + qy * c.ty;
-        const float r = (float)(ph - rint(ph));
-        float s, co;
-        sincospif(2.0f * r, &s, &co);
-        v = make_float2(fmaf(v.x, co, v.y * s), fmaf(v.y, co, -v.x * s));
-      }
-    }
+    v = envelope_translate(v, i, j, py, px, qx, qy, k2, flags, c);
   }
   return v;
+}
+
+// Ewald-sphere contrast at rfft-grid entry (i, j) of a (py, px) image from
+// the full object spectrum's a = O[i, j] and b = O[-i, -j]
+// (cryojax/simulator/_transfer_theory/transfer_theory.py:165-255):
+//   K(pos, neg) = 1/2 [ (w2 (p+n)_r + w1 (p+n)_i) sin + (w2 (p+n)_i - w1 (p+n)_r) cos
+//                   + i ((w2 (p-n)_i + w1 (n-p)_r) sin + (w2 (n-p)_r + w1 (n-p)_i) cos) ],
+//   sin, cos of chi - deg2rad(phase_shift), w1 = ac, w2 = sqrt(1 - ac^2);
+//   pos = a, neg = b, except the even-size Nyquist column (pos = conj(b)) and
+//   the x = 0 column's even-size Nyquist row (conj(K(conj(a), a))).  Rows
+//   y > Py/2 of the x = 0 column equal conj(K) of their mirror row, which is
+//   K itself since K's imaginary part is odd in (pos, neg).
+__device__ __forceinline__ float2 ewald_epilogue(float2 a, float2 b, int i, int j, int py, int px, uint32_t flags,
+                                                 const ImageConsts& c) {
+  a.x *= c.scale;
+  a.y *= c.scale;
+  b.x *= c.scale;
+  b.y *= c.scale;
+  const double qy = (double)fft_index(i, py) * c.qy_step;
+  const double qx = (double)j * c.qx_step;
+  const double k2 = qx * qx + qy * qy;
+  const double arg = aberration_cycles(qx, qy, k2, c) - c.ps_cycles;
+  const float r = (float)(arg - rint(arg));
+  float s, co;
+  sincospif(2.0f * r, &s, &co);
+  float2 pos = a, neg = b;
+  bool conj_out = false;
+  if ((px % 2 == 0) && j == px / 2) {
+    pos = make_float2(b.x, -b.y);
+  } else if (j == 0 && (py % 2 == 0) && i == py / 2) {
+    pos = make_float2(a.x, -a.y);
+    neg = a;
+    conj_out = true;
+  }
+  const float sr = pos.x + neg.x, si = pos.y + neg.y;
+  const float dr = neg.x - pos.x, di = pos.y - neg.y;
+  float2 v;
+  v.x = 0.5f * ((c.w2 * sr + c.w1 * si) * s + (c.w2 * si - c.w1 * sr) * co);
+  v.y = 0.5f * ((c.w2 * di + c.w1 * dr) * s + (c.w2 * dr - c.w1 * di) * co);
+  if (conj_out) v.y = -v.y;
+  return envelope_translate(v, i, j, py, px, qx, qy, k2, flags, c);
 }
 
 // ---------------------------------------------------------------------------

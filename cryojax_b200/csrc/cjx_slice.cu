@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256, is_spline_layout<Layout>::value ? CJX_SPL
   int du, dv;
   gather_lane_offsets<MAP>(warp, lane, du, dv);
   const int u = blockIdx.x * 16 + du;
-  if (u >= g.nxh) return;
+  if (u >= g.ncols) return;
   const int vbase = blockIdx.y * (16 * S) + dv;
   const float ux = (float)fft_index(u, n);
   const float bx = r00 * ux, by = r10 * ux, bz = r20 * ux;
@@ -155,8 +155,21 @@ __global__ void __launch_bounds__(256, is_spline_layout<Layout>::value ? CJX_SPL
     oy[s] = fmaf(r11, vy, by);
     oz[s] = fmaf(r21, vy, bz);
   }
+  if (g.flags & CJX_EWALD_SPHERE) {
+    // the sphere's third coordinate w = lambda (u^2 + v^2) / (2 N pixel_size), rotated with R's third column
+    const float cw = ewald_w(params + img, n);
+    const float r02 = (float)R[2], r12 = (float)R[5], r22 = (float)R[8];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const float vy = (float)fft_index(act[s] ? vbase + 16 * s : 0, n);
+      const float w = cw * fmaf(ux, ux, vy * vy);
+      ox[s] = fmaf(r02, w, ox[s]);
+      oy[s] = fmaf(r12, w, oy[s]);
+      oz[s] = fmaf(r22, w, oz[s]);
+    }
+  }
   gather_samples<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
-  float2* col = hbuf + ((size_t)blockIdx.z * g.nxh + u) * g.ldh;
+  float2* col = hbuf + ((size_t)blockIdx.z * g.ncols + u) * g.ldh;
 #pragma unroll
   for (int s = 0; s < S; ++s)
     if (act[s]) col[vbase + 16 * s] = val[s];
@@ -176,11 +189,12 @@ __global__ void __launch_bounds__(kWarps * 32)
   const int j = j0 + warp;
   float2* a = bufs + warp * stride;
   float2* b = a + n;
-  if (j < g.nxh) {
-    const float2* col = hbuf + ((size_t)blockIdx.y * g.nxh + j) * g.ldh;
+  const bool ewald = (g.flags & CJX_EWALD_SPHERE) != 0;  // full complex surface: no Hermitian fix
+  if (j < g.ncols) {
+    const float2* col = hbuf + ((size_t)blockIdx.y * g.ncols + j) * g.ldh;
     for (int i = lane; i < n; i += 32) a[i] = col[i];
     __syncwarp();
-    if (j == 0 || ((n % 2 == 0) && j == h)) {
+    if (!ewald && (j == 0 || ((n % 2 == 0) && j == h))) {
       for (int i = lane; i <= n / 2; i += 32) {
         const int i2 = (i == 0) ? 0 : n - i;
         const float2 x = a[i], y = a[i2];
@@ -194,7 +208,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   __syncthreads();
   const int res_off = (g.plan_n.nstages == 0 || (g.plan_n.nstages & 1)) ? n : 0;
-  const int ncols = min(kWarps, g.nxh - j0);
+  const int ncols = min(kWarps, g.ncols - j0);
   float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
   for (int e = threadIdx.x; e < g.py * kWarps; e += blockDim.x) {
     const int m = e / kWarps, jj = e % kWarps;
@@ -328,12 +342,13 @@ __global__ void __launch_bounds__(kWarps * 32)
   const int j0 = blockIdx.x * kWarps;
   const int j = j0 + warp;
   float2* buf = bufs + warp * stride;
-  if (j < g.nxh) {
+  if (j < g.ncols) {
     const LaneTwiddles lt = make_lane_twiddles(w32, lane);
-    const float2* col = hbuf + ((size_t)blockIdx.y * g.nxh + j) * g.ldh;
+    const float2* col = hbuf + ((size_t)blockIdx.y * g.ncols + j) * g.ldh;
     const int bl = T512 ? lane : brev5(lane);  // the transpose FFT takes natural lane order
     float2 x[R];
-    const bool sym = (j == 0) || (j == n / 2);
+    // the Ewald sphere's full complex surface takes no Hermitian fix
+    const bool sym = !(g.flags & CJX_EWALD_SPHERE) && ((j == 0) || (j == n / 2));
 #pragma unroll
     for (int n1 = 0; n1 < R; ++n1) {
       const int idx = 32 * n1 + bl;
@@ -356,7 +371,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     }
   }
   __syncthreads();
-  const int ncols = min(kWarps, g.nxh - j0);
+  const int ncols = min(kWarps, g.ncols - j0);
   float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
   for (int e = threadIdx.x; e < g.py * kWarps; e += blockDim.x) {
     const int m = e / kWarps, jj = e % kWarps;
@@ -563,8 +578,12 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
     return fail(CJX_ERR_UNSUPPORTED, "volume side and image sides are limited to CJX_MAX_SIDE");
   const uint32_t known =
       CJX_APPLY_CTF | CJX_APPLY_TRANSLATION | CJX_APPLY_ENVELOPE | CJX_ZERO_FILL_NEGATIVE | CJX_GRID_BRICKED |
-      CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE;
+      CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE;
   if (d->flags & ~known) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown flag bits");
+  if ((d->flags & CJX_EWALD_SPHERE) && !(d->flags & CJX_APPLY_CTF) &&
+      (d->flags & (CJX_APPLY_ENVELOPE | CJX_APPLY_TRANSLATION)))
+    return fail(CJX_ERR_INVALID_ARGUMENT,
+                "CJX_EWALD_SPHERE without CJX_APPLY_CTF outputs the full spectrum: no envelope or translation");
   if ((d->flags & CJX_GRID_BRICKED) && (d->flags & CJX_GRID_BRICKED_PAIRS))
     return fail(CJX_ERR_INVALID_ARGUMENT, "CJX_GRID_BRICKED and CJX_GRID_BRICKED_PAIRS are exclusive");
   g->n = d->n;
@@ -572,8 +591,10 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
   g->px = d->px;
   g->nxh = d->n / 2 + 1;
   g->pxh = d->px / 2 + 1;
-  g->ld1 = round_up(g->nxh, 8);
-  g->ld2 = round_up(g->pxh, 8);
+  const bool ewald = (d->flags & CJX_EWALD_SPHERE) != 0;
+  g->ncols = ewald ? d->n : g->nxh;
+  g->ld1 = round_up(g->ncols, 8);
+  g->ld2 = round_up(ewald ? d->px : g->pxh, 8);
   g->ldh = round_up(g->n, 8);
   auto left_pad = [](int pad_dim, int image_dim) {
     const int pad = pad_dim - image_dim;
@@ -592,9 +613,9 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
 
 bool needs_resize(const SliceGeom& g) { return !(g.py == g.n && g.px == g.n); }
 
-// Per image: T1 [Py][ld1], T2 [Py][ld2] and the split gather's H [N/2+1][ldh].
+// Per image: T1 [Py][ld1], T2 [Py][ld2] and the split gather's H [ncols][ldh].
 size_t workspace_per_image(const SliceGeom& g) {
-  return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2 + (size_t)g.nxh * g.ldh);
+  return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2 + (size_t)g.ncols * g.ldh);
 }
 
 // Default chunk: about 64 MB of intermediates, so a chunk stays in L2.
@@ -683,6 +704,12 @@ static int ensure_smem_attrs() {
   return err;
 }
 
+int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream);
+int launch_ewald_colfft(const SliceGeom& g, const float2* t2, const cjx_image_params* params, const int32_t* order,
+                        float2* out, int64_t k0, int cnt, cudaStream_t stream);
+int launch_ewald_direct(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                        int64_t n_images, float2* out, cudaStream_t stream);
+
 // Passes up to T2 (gather, column inverse FFT + window, rows) for one chunk of
 // `cnt` images starting at processing index k0.
 int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
@@ -690,8 +717,9 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
                          const Tuning& tn) {
   if (int e = ensure_smem_attrs()) return e;
   const int64_t ilp = (g.flags & CJX_GRID_SPLINE) ? tn.spline_ilp : tn.ilp;
-  // the fused kernel has no pair or spline path
-  const bool split = tn.gather_mode == 1 || (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE));
+  // the fused kernel has no pair, spline or Ewald path
+  const bool split =
+      tn.gather_mode == 1 || (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE));
   const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
   const bool fast = tn.fft_mode >= 1;
   const bool t512 = tn.fft_mode == 2 && rn == 16;  // 512-point column transforms through the transpose FFT
@@ -700,7 +728,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
   const size_t sb_reg =
       sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
     if (split) {
-      const dim3 gg((g.nxh + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
+      const dim3 gg((g.ncols + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
       const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
       const bool pairs = (g.flags & CJX_GRID_BRICKED_PAIRS) != 0;
@@ -738,7 +766,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 #undef CJX_GSM
       prof_end("k_gather_slice", stream);
       prof_begin(stream);
-      const dim3 gc((g.nxh + kWarps - 1) / kWarps, cnt);
+      const dim3 gc((g.ncols + kWarps - 1) / kWarps, cnt);
       if (fast && t512) {
         k_colifft_window_reg<16, true><<<gc, kWarps * 32, sa_reg, stream>>>(hb, t1, g);
       } else if (fast && rn) {
@@ -772,6 +800,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 #undef CJX_GC
       prof_end("k_gather_colifft", stream);
     }
+    if (g.flags & CJX_EWALD_SPHERE) return launch_ewald_rows(g, t1, t2, cnt, stream);
     prof_begin(stream);
     const dim3 gb((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt);
     if (fast && rn && rpx) {
@@ -798,6 +827,8 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
                    int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
                    const Tuning& tn) {
   if (n_images == 0) return CJX_OK;
+  if (!needs_resize(g) && (g.flags & CJX_EWALD_SPHERE))
+    return launch_ewald_direct(g, grid, params, order, n_images, out, stream);
   if (!needs_resize(g)) {
     const int total = g.n * g.nxh;
     const int blocks = std::min((total + 255) / 256, 1024);
@@ -834,6 +865,10 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
+    if (g.flags & CJX_EWALD_SPHERE) {
+      if (int e = launch_ewald_colfft(g, t2, params, order, out, k0, cnt, stream)) return e;
+      continue;
+    }
     prof_begin(stream);
     const dim3 gcc((g.pxh + kWarps - 1) / kWarps, cnt);
     if (fast && rpy) {

@@ -18,6 +18,7 @@ Covered (reference file:line):
   FourierVoxelGridVolume      cryojax/simulator/_volume/representations/voxel_volume.py:40-119
   FourierVoxelSplineVolume    cryojax/simulator/_volume/representations/voxel_volume.py:122-203
   FourierSliceExtraction      cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-183
+  EwaldSphereExtraction       cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:225-516
   WeakPhaseScatteringTheory   cryojax/simulator/_scattering_theory/weak_phase_scattering_theory.py:13-80
   LinearImageModel, ProjectionImageModel
                               cryojax/simulator/_image_model/base_image_model.py:216-432
@@ -457,6 +458,8 @@ def pack_image_params(pose: AbstractPose, image_config: BasicImageConfig,
         ac = _per_image(transfer_theory.amplitude_contrast_ratio, n)
         p[:, nat.P_PHASE_TOTAL] = np.deg2rad(_per_image(transfer_theory.phase_shift, n)) + np.arctan(
             ac / np.sqrt(1.0 - ac**2))
+        p[:, nat.P_AC] = ac
+        p[:, nat.P_PHASE_SHIFT] = np.deg2rad(_per_image(transfer_theory.phase_shift, n))
         if transfer_theory.envelope is not None:
             p[:, nat.P_ENV_AMP] = _per_image(transfer_theory.envelope.amplitude, n)
             p[:, nat.P_ENV_B] = _per_image(transfer_theory.envelope.b_factor, n)
@@ -565,6 +568,9 @@ class FourierSliceExtraction:
     def _base_flags(self):
         return nat.CJX_ZERO_FILL_NEGATIVE if self.out_of_bounds_mode == "zero_fill_negative" else 0
 
+    def _out_columns(self, px, flags):
+        return px // 2 + 1
+
     def run(self, volume: FourierVoxelGridVolume, image_config: BasicImageConfig, params: np.ndarray | None,
             flags: int, *, params_device=None, out=None, workspace=None, stream=None, images_per_chunk=0,
             n=None, order=None):
@@ -587,7 +593,7 @@ class FourierSliceExtraction:
         if params_device is None:
             params_device = torch.as_tensor(params, dtype=torch.float64, device=grid.device)
         if out is None:
-            out = torch.empty((n, py, px // 2 + 1), dtype=torch.complex64, device=grid.device)
+            out = torch.empty((n, py, self._out_columns(px, flags)), dtype=torch.complex64, device=grid.device)
         ws_bytes = nat.workspace_size(desc, n)
         if ws_bytes and (workspace is None or workspace.numel() * workspace.element_size() < ws_bytes):
             workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=grid.device)
@@ -609,6 +615,43 @@ class FourierSliceExtraction:
             from . import _postprocess
 
             return _postprocess.irfftn(out, image_config.padded_shape)
+        return out
+
+
+class EwaldSphereExtraction(FourierSliceExtraction):
+    """Ewald-sphere surface extraction on the B200.
+
+    cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:225-516:
+    the surface R (q + (lambda / pixel_size) |q|^2 zhat / 2) of a
+    FourierVoxelGridVolume (trilinear) or FourierVoxelSplineVolume (cubic
+    spline), not reduced to an rfft half plane.  ``integrate`` returns the
+    full [Py, Px] spectrum; in an image model with a ContrastTransferTheory
+    the contrast follows the reference's non-projection branch
+    (cryojax/simulator/_transfer_theory/transfer_theory.py:100-111, 165-255).
+    """
+
+    is_projection_approximation = False
+
+    def _base_flags(self):
+        return super()._base_flags() | nat.CJX_EWALD_SPHERE
+
+    def _out_columns(self, px, flags):
+        return px // 2 + 1 if flags & nat.CJX_APPLY_CTF else px
+
+    def integrate(self, volume_representation, image_config: BasicImageConfig, outputs_real_space: bool = False):
+        """cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:269-324."""
+        pose = volume_representation.rotation or QuaternionPose()
+        scale = image_config.pixel_size if self.outputs_integral else 1.0
+        params = pack_image_params(pose, image_config, None, scale=scale)
+        out = self.run(volume_representation, image_config, params, 0)
+        if pose.batch_size is None and _batch_size(image_config.pixel_size) is None:
+            out = out[0]
+        if outputs_real_space:
+            from . import _postprocess
+
+            # irfftn of the full spectrum reads its first Px//2 + 1 columns
+            return _postprocess.irfftn(out[..., : image_config.padded_shape[1] // 2 + 1].contiguous(),
+                                       image_config.padded_shape)
         return out
 
 
@@ -651,6 +694,9 @@ class AbstractImageModel:
             if self.translate_mode != "fft":
                 raise ValueError("translate_mode='atom' needs an atom volume, not a FourierVoxelGridVolume")
             f |= nat.CJX_APPLY_TRANSLATION
+        if not self.volume_integrator.is_projection_approximation and not (f & nat.CJX_APPLY_CTF):
+            raise NotImplementedError("an Ewald-sphere image needs a transfer theory (the integrator alone "
+                                      "gives the full spectrum: use EwaldSphereExtraction.integrate)")
         return f
 
     def image_params(self) -> np.ndarray:

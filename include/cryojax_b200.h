@@ -78,6 +78,20 @@ extern "C" {
  * desc->n stays the voxel grid's side N.  Forward, multi, no-alloc and
  * search entry points; not cjx_slice_ctf_loss_grad (CJX_ERR_UNSUPPORTED).  */
 #define CJX_GRID_SPLINE (1u << 6)
+/* EwaldSphereExtraction instead of FourierSliceExtraction
+ * (cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:225-516):
+ * the full N x N surface at R (kx, ky, lambda (kx^2 + ky^2) / (2 N
+ * pixel_size)) (pixel frequency indices) is sampled, with no rfft-half
+ * conversion, and resized with complex FFTs.  With CJX_APPLY_CTF the output
+ * is ContrastTransferTheory's non-projection contrast
+ * (cryojax/simulator/_transfer_theory/transfer_theory.py:100-111, 165-255),
+ * [Py][Px/2+1], from amplitude_contrast_ratio and phase_shift of the
+ * parameter record; CJX_APPLY_ENVELOPE and CJX_APPLY_TRANSLATION as usual.
+ * Without CJX_APPLY_CTF the output is the integrator's full spectrum
+ * [Py][Px] (scale applied; no envelope or translation allowed).  Any grid
+ * layout, trilinear or spline.  Forward, multi and no-alloc entry points
+ * (not search or loss_grad).                                              */
+#define CJX_EWALD_SPHERE (1u << 7)
 
 /* ---- per-image parameters (one record per image, device memory) ------
  * 32 doubles (256 bytes).  Built on the host from a pose, a CTF and an
@@ -100,7 +114,9 @@ typedef struct cjx_image_params {
                                  contrast model, else 1                      */
   double envelope_amplitude;  /* used with CJX_APPLY_ENVELOPE               */
   double envelope_b_factor;   /* Angstrom^2                                 */
-  double reserved[11];
+  double amplitude_contrast_ratio; /* CJX_EWALD_SPHERE with CJX_APPLY_CTF  */
+  double phase_shift;         /* radians: deg2rad(phase_shift), same use    */
+  double reserved[9];
 } cjx_image_params;
 
 /* ---- geometry of one launch ------------------------------------------- */

@@ -226,11 +226,13 @@ def sample_uniform_quaternion(u1, u2, u3):
 
 def fftn(x, s=None, axes=None):
     """cryojax/ndimage/_fft.py:34-55."""
+    axes = _axes_for(x, s, axes)
     return np.fft.fftn(np.fft.ifftshift(x, axes=axes), s=s, axes=axes)
 
 
 def ifftn(ft, s=None, axes=None):
     """cryojax/ndimage/_fft.py:11-31."""
+    axes = _axes_for(ft, s, axes)
     return np.fft.fftshift(np.fft.ifftn(ft, s=s, axes=axes), axes=axes)
 
 
@@ -525,6 +527,102 @@ def fourier_slice_integrate(
     return irfftn(proj, s=tuple(padded_shape)) if outputs_real_space else proj
 
 
+def ewald_sphere_frequencies(rotated_frequency_slice, voxel_size, wavelength):
+    """Ewald-sphere surface through a rotated frequency slice (cycles/pixel).
+
+    cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:489-516:
+    zhat = xhat x yhat from the slice's own (unit-normalised) in-plane axes,
+    q_surface = q + (wavelength / voxel_size) |q|^2 zhat / 2.
+    """
+    corner = np.fft.ifftshift(rotated_frequency_slice, axes=(0, 1, 2))
+    xhat, yhat = corner[0, 0, 1, :], corner[0, 1, 0, :]
+    xhat = xhat / np.linalg.norm(xhat)
+    yhat = yhat / np.linalg.norm(yhat)
+    zhat = np.cross(xhat, yhat)
+    q_squared = np.sum(rotated_frequency_slice**2, axis=-1)
+    return rotated_frequency_slice + (wavelength / voxel_size) * (q_squared[..., None] * zhat) / 2
+
+
+def ewald_integrate(
+    grid,
+    rotated_frequency_slice,
+    padded_shape,
+    pixel_size,
+    wavelength,
+    *,
+    outputs_integral=True,
+    pad_mode="constant",
+    cval=0.0,
+    wrap_negative=True,
+    spline=False,
+):
+    """EwaldSphereExtraction.integrate: the full (not rfft) complex surface.
+
+    cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:269-324,
+    455-486: sample the curved surface (trilinear, or cubic spline from
+    coefficients), then for padded_shape != (N, N)
+    fftn(crop_or_pad(ifftn(surface))) and the pixel-size factor.
+    """
+    n = rotated_frequency_slice.shape[1]
+    m = n + 2 if spline else n
+    if grid.shape != (m, m, m):
+        raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
+    freqs = ewald_sphere_frequencies(rotated_frequency_slice, pixel_size, wavelength)
+    surface = extract_surface_from_voxel_grid(grid, freqs, cval, wrap_negative, spline)
+    if tuple(padded_shape) != (n, n):
+        surface = fftn(resize_with_crop_or_pad(ifftn(surface, s=(n, n)), tuple(padded_shape), pad_mode))
+    if outputs_integral:
+        surface = surface * pixel_size
+    return surface
+
+
+def _ewald_propagate(pos, neg, ac, sin, cos):
+    """cryojax/simulator/_transfer_theory/transfer_theory.py:245-255."""
+    w1, w2 = ac, np.sqrt(1.0 - ac**2)
+    sr, si = pos.real + neg.real, pos.imag + neg.imag
+    dr, di = neg.real - pos.real, pos.imag - neg.imag
+    return 0.5 * ((w2 * sr + w1 * si) * sin + (w2 * si - w1 * sr) * cos
+                  + 1.0j * ((w2 * di + w1 * dr) * sin + (w2 * dr - w1 * di) * cos))
+
+
+def compute_contrast_from_ewald_sphere(object_spectrum, phase_shifts, amplitude_contrast_ratio, padded_shape):
+    """Contrast (rfft half plane) from a full Ewald-sphere object spectrum.
+
+    cryojax/simulator/_transfer_theory/transfer_theory.py:165-242: every
+    half-plane frequency pairs the spectrum at +q with the spectrum at -q;
+    the even-size Nyquist column uses conj(O[-y, Nyq]) as its +q partner,
+    the x = 0 column is filled from its y > 0 half by Hermitian symmetry
+    (its even-size Nyquist row likewise from conj(O[Ny, 0])).
+    ``phase_shifts`` are chi(q) - deg2rad(phase_shift) on the rfft grid.
+    """
+    ny, nx = padded_shape
+    ac = float(amplitude_contrast_ratio)
+    sin, cos = np.sin(phase_shifts), np.cos(phase_shifts)
+    hx, hy = nx // 2 + nx % 2, ny // 2 + ny % 2  # first negative-frequency index
+    out = np.empty((ny, nx // 2 + 1), np.complex128)
+    # y >= 1, x >= 1
+    pos = object_spectrum[1:, 1:hx]
+    neg = object_spectrum[1:, hx:][::-1, ::-1]
+    if nx % 2 == 0:
+        pos = np.concatenate([pos, np.conj(neg[:, -1:])], axis=1)
+    out[1:, 1:] = _ewald_propagate(pos, neg, ac, sin[1:, 1:], cos[1:, 1:])
+    # y = 0, x >= 1
+    pos0 = object_spectrum[0, 1:hx]
+    neg0 = object_spectrum[0, hx:][::-1]
+    if nx % 2 == 0:
+        pos0 = np.concatenate([pos0, np.conj(neg0[-1:])])
+    out[0, 1:] = _ewald_propagate(pos0, neg0, ac, sin[0, 1:nx // 2 + 1], cos[0, 1:nx // 2 + 1])
+    # x = 0
+    posy = object_spectrum[1:hy, 0]
+    negy = object_spectrum[hy:, 0][::-1]
+    if ny % 2 == 0:
+        posy = np.concatenate([posy, np.conj(negy[-1:])])
+    cy = _ewald_propagate(posy, negy, ac, sin[1:ny // 2 + 1, 0], cos[1:ny // 2 + 1, 0])
+    c00 = _ewald_propagate(object_spectrum[0, 0], object_spectrum[0, 0], ac, sin[0, 0], cos[0, 0])
+    out[:, 0] = np.concatenate([[c00], cy if ny % 2 == 1 else cy[:-1], np.conj(cy[::-1])])
+    return out
+
+
 # ---------------------------------------------------------------------------
 # CTF and transfer theory  (cryojax/simulator/_transfer_theory/)
 # ---------------------------------------------------------------------------
@@ -664,6 +762,7 @@ def compute_fourier_image(
     cval=0.0,
     wrap_negative=True,
     spline=False,
+    ewald=False,
 ):
     """LinearImageModel / ContrastImageModel.compute_fourier_image.
 
@@ -672,9 +771,15 @@ def compute_fourier_image(
     cryojax/simulator/_scattering_theory/weak_phase_scattering_theory.py:37-80
     (contrast: integral times the interaction constant).  ``apply_ctf=False``
     is ProjectionImageModel (:412-432).  Order: rotate -> integrate -> CTF ->
-    translate.
+    translate.  ``ewald``: EwaldSphereExtraction as the integrator and
+    ContrastTransferTheory's non-projection branch
+    (cryojax/simulator/_transfer_theory/transfer_theory.py:100-111); without
+    the CTF it returns EwaldSphereExtraction.integrate's full spectrum.
     """
     rotated = rotate_frequency_slice(frequency_slice, quaternion_pose_rotation(spec.wxyz))
+    if ewald:
+        return _compute_fourier_image_ewald(grid, rotated, spec, outputs_integral, simulates_quantity,
+                                            applies_translation, apply_ctf, cval, wrap_negative, spline)
     proj = fourier_slice_integrate(
         grid,
         rotated,
@@ -708,6 +813,32 @@ def compute_fourier_image(
     if applies_translation:
         proj = translate_image(proj, translation_operator(freqs, spec.offset_in_angstroms), spec.padded_shape)
     return proj
+
+
+def _compute_fourier_image_ewald(grid, rotated, spec, outputs_integral, simulates_quantity, applies_translation,
+                                 apply_ctf, cval, wrap_negative, spline):
+    wavelength = wavelength_from_kilovolts(spec.voltage_in_kilovolts)
+    obj = ewald_integrate(grid, rotated, spec.padded_shape, spec.pixel_size, wavelength,
+                          outputs_integral=outputs_integral, pad_mode=spec.pad_mode, cval=cval,
+                          wrap_negative=wrap_negative, spline=spline)
+    if simulates_quantity:
+        obj = interaction_constant_from_kilovolts(spec.voltage_in_kilovolts) * obj
+    if not apply_ctf:
+        if applies_translation:
+            raise NotImplementedError("the Ewald spectrum is a full plane; translation applies to the contrast")
+        return obj
+    freqs = padded_frequency_grid_in_angstroms(spec.padded_shape, spec.pixel_size)
+    offset_z = spec.offset_in_angstroms[2] if spec.offset_in_angstroms.shape[0] == 3 else None
+    defocus = spec.defocus_in_angstroms if offset_z is None else spec.defocus_in_angstroms + offset_z
+    chi = compute_phase_shifts_with_spherical_aberration(
+        freqs, defocus, spec.astigmatism_in_angstroms, np.deg2rad(spec.astigmatism_angle), wavelength,
+        spec.spherical_aberration_in_mm * 1e7) - np.deg2rad(spec.phase_shift)
+    img = compute_contrast_from_ewald_sphere(obj, chi, spec.amplitude_contrast_ratio, spec.padded_shape)
+    if spec.envelope_b_factor is not None:
+        img = img * fourier_gaussian_envelope(freqs, spec.envelope_amplitude, spec.envelope_b_factor)
+    if applies_translation:
+        img = translate_image(img, translation_operator(freqs, spec.offset_in_angstroms), spec.padded_shape)
+    return img
 
 
 def postprocess(fourier_image, spec: ImageSpec, *, outputs_real_space=True, normalizes_signal=False):
