@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the mixed-size batch measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the loss-gradient measurement")
     ap.add_argument("--no-search", action="store_true", help="skip the pose-search (learned vs grid) measurement")
-    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline"], default=None,
+    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline", "ewald"], default=None,
                     help="run one small workload of that kernel family (for a profiler), print its timing, exit")
     ap.add_argument("--no-refine", action="store_true",
                     help="skip the search + refinement measurement (320^2 images, N=512)")
@@ -70,6 +70,7 @@ def parse_args():
     ap.add_argument("--refine-exhaustive-images", type=int, default=64,
                     help="images in its exhaustive arm (36,864 simulations each)")
     ap.add_argument("--no-spline", action="store_true", help="skip the spline-volume measurement")
+    ap.add_argument("--no-ewald", action="store_true", help="skip the Ewald-sphere measurement")
     ap.add_argument("--search-images", type=int, default=1024,
                     help="observed images in the pose-search measurement (the configuration has 4096)")
     return ap.parse_args()
@@ -747,6 +748,72 @@ def measure_spline(dev, grid, batch, cfg, steps, warmup, n_images, cpu_images):
     return res
 
 
+def measure_ewald(dev, volume, batch, cfg, steps, warmup, n_images, cpu_images):
+    """EwaldSphereExtraction + ContrastTransferTheory (non-projection contrast) on the headline volume and
+    images: `n_images` of them, x-pair bricked trilinear grid."""
+    import numpy as np
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+
+    sl = slice(0, n_images)
+    pose = S.QuaternionPose(batch.offsets[sl, 0], batch.offsets[sl, 1], wxyz=batch.wxyz[sl])
+    tt = S.ContrastTransferTheory(S.AstigmaticCTF(batch.defocus[sl], batch.astigmatism[sl],
+                                                  batch.astigmatism_angle[sl]))
+    integ = S.EwaldSphereExtraction(outputs_integral=False)
+    model = S.make_image_model(volume, cfg, pose, tt, volume_integrator=integ)
+    flags = model._flags()
+    n = volume.shape[0]
+    py, px = cfg.padded_shape
+    pd = torch.as_tensor(model.image_params(), device=dev)
+    order = torch.as_tensor(S.orientation_order(pose.rotation_matrices()), device=dev)
+    out = torch.empty((n_images, py, px // 2 + 1), dtype=torch.complex64, device=dev)
+    desc = nat.make_desc(n, py, px, flags | integ._base_flags() | integ.device_grid(volume)[1])
+    ws = torch.empty(max(nat.workspace_size(desc, n_images), 1), dtype=torch.uint8, device=dev)
+
+    def step():
+        integ.run(volume, cfg, None, flags, params_device=pd, out=out, workspace=ws, order=order)
+
+    for _ in range(warmup):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nat.profile_enable(True)
+    step()
+    torch.cuda.synchronize()
+    prof = nat.profile_read()
+    nat.profile_enable(False)
+    res = {"value": n_images / (ms / 1000.0), "unit": UNIT, "images": n_images, "ms_per_step": ms,
+           "layout": "x-pair bricked grid, trilinear",
+           "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()}}
+    del out, ws, pd
+    if cpu_images:
+        from oracle import cryojax_oracle as O
+
+        grid_h = volume.fourier_voxel_grid.cpu().numpy().astype(np.complex128)
+        fs = O.make_frequency_slice((n, n), outputs_rfftfreqs=False)
+        t0 = time.perf_counter()
+        for b in range(cpu_images):
+            spec = O.ImageSpec(shape=cfg.shape, pixel_size=2.0, voltage_in_kilovolts=300.0, wxyz=batch.wxyz[b],
+                               offset_in_angstroms=batch.offsets[b], defocus_in_angstroms=batch.defocus[b],
+                               astigmatism_in_angstroms=batch.astigmatism[b],
+                               astigmatism_angle=batch.astigmatism_angle[b])
+            O.compute_fourier_image(grid_h, fs, spec, ewald=True)
+        wall = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": cpu_images / wall, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"{cpu_images} images through the float64 NumPy oracle's Ewald-sphere "
+                                         f"restatement, 1 process ({wall:.1f} s)"}
+        del grid_h
+    return res
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -819,6 +886,30 @@ def run_probe(kind, seed):
         ps = PoseSearch(grid.rotation_matrices())
         ms = ev_time(lambda: ps.run(model, obs))
         out["plain_exhaustive_8_images"] = {"ms": ms, "candidates_per_s": 8 * grid.size / (ms / 1000.0)}
+    elif kind == "ewald":
+        from cryojax_b200 import simulator as S
+        from cryojax_b200 import synthetic
+
+        # EwaldSphereExtraction + CTF at the benchmark shape (N = 512 -> 320^2), 64 images
+        vol = S.FourierVoxelGridVolume.from_real_voxel_grid(synthetic.gaussian_sum_volume(256, 6000, seed),
+                                                            pad_scale=2.0, device=str(dev))
+        b = synthetic.image_batch(64, seed + 1)
+        cfg = S.BasicImageConfig((320, 320), 2.0, 300.0)
+        integ = S.EwaldSphereExtraction(outputs_integral=False)
+        model = S.make_image_model(vol, cfg, S.QuaternionPose(b.offsets[:, 0], b.offsets[:, 1], wxyz=b.wxyz),
+                                   S.ContrastTransferTheory(S.AstigmaticCTF(b.defocus, b.astigmatism,
+                                                                            b.astigmatism_angle)),
+                                   volume_integrator=integ)
+        pd = torch.as_tensor(model.image_params(), device=dev)
+        o = torch.empty((64, 320, 161), dtype=torch.complex64, device=dev)
+
+        def fwd():
+            integ.run(vol, cfg, None, model._flags(), params_device=pd, out=o)
+
+        for _ in range(3):
+            fwd()
+        ms = ev_time(fwd)
+        out["ewald_forward_64_images"] = {"ms": ms, "images_per_s": 64 / (ms / 1000.0)}
     elif kind == "spline":
         from cryojax_b200 import simulator as S
         from cryojax_b200 import synthetic
@@ -1064,6 +1155,16 @@ def main():
         except Exception as e:
             spline = {"error": repr(e)}
 
+    # ---- Ewald-sphere extraction at the headline shape
+    ewald = None
+    if not args.no_ewald and world == 1:
+        try:
+            torch.cuda.empty_cache()
+            ewald = measure_ewald(dev, volume, batch, cfg, max(3, min(args.steps, 10)), 3, min(4096, args.images),
+                                  0 if args.no_cpu_baseline else 2)
+        except Exception as e:
+            ewald = {"error": repr(e)}
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1105,6 +1206,7 @@ def main():
             "pose_search": pose_search,
             "search_refine": search_refine,
             "spline": spline,
+            "ewald": ewald,
         }
         print(json.dumps(line))
     replicas.shutdown(info)

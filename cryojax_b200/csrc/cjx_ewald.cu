@@ -106,6 +106,148 @@ __global__ void __launch_bounds__(kEwWarps * 32)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-FFT forms (N, Px, Py = 32 R): the same data flow with the
+// transforms in registers (cjx_fft.cuh); shared memory holds the twiddle
+// tables and the transposes, so loads and stores stay coalesced.
+// ---------------------------------------------------------------------------
+template <int RN, int RP>
+__device__ __forceinline__ void ewald_row_reg(const float2* __restrict__ row, float2* __restrict__ dst, float2* buf,
+                                              const float2* tabN, const float2* tabP, const LaneTwiddles& lt,
+                                              int lane, const int* winx) {
+  constexpr int px = 32 * RP;
+  const int bl = brev5(lane);
+  float2 z[RN];
+#pragma unroll
+  for (int n1 = 0; n1 < RN; ++n1) z[n1] = row[32 * n1 + bl];
+  warp_fft_reg<RN, +1>(z, tabN, lt, lane);
+#pragma unroll
+  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+  __syncwarp();
+  float2 w[RP];
+#pragma unroll
+  for (int n1 = 0; n1 < RP; ++n1) {
+    const int src = winx[32 * n1 + bl];
+    w[n1] = (src >= 0) ? buf[pad16(src)] : make_float2(0.f, 0.f);
+  }
+  __syncwarp();
+  warp_fft_reg<RP, -1>(w, tabP, lt, lane);
+#pragma unroll
+  for (int k1 = 0; k1 < RP; ++k1) buf[pad16(k1 + RP * lane)] = w[k1];
+  __syncwarp();
+  for (int k = lane; k < px; k += 32) dst[k] = buf[pad16(k)];
+}
+
+template <int RN>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
+  constexpr int n = 32 * RN;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int px = g.px;
+  const int stride = pad16(max(n, px)) + 1;
+  float2* tabN = smem;
+  float2* tabP = tabN + n;
+  float2* bufs = tabP + px;
+  int* winx = reinterpret_cast<int*>(bufs + kWarps * stride);
+  build_reg_twiddles(tabN, n);
+  build_reg_twiddles(tabP, px);
+  build_w32(w32);
+  for (int m = threadIdx.x; m < px; m += blockDim.x) winx[m] = win_src(m, n, px, g.pad_left_x);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kWarps + warp;
+  if (r >= g.py) return;
+  const float2* row = t1 + ((size_t)blockIdx.y * g.py + r) * g.ld1;
+  float2* dst = t2 + ((size_t)blockIdx.y * g.py + r) * g.ld2;
+  float2* buf = bufs + warp * stride;
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  switch (rp) {
+#define CJX_EROW_CASE(RPV) \
+  case RPV: ewald_row_reg<RN, RPV>(row, dst, buf, tabN, tabP, lt, lane, winx); break;
+    CJX_EROW_CASE(1) CJX_EROW_CASE(2) CJX_EROW_CASE(3) CJX_EROW_CASE(4) CJX_EROW_CASE(5)
+    CJX_EROW_CASE(6) CJX_EROW_CASE(8) CJX_EROW_CASE(10) CJX_EROW_CASE(12) CJX_EROW_CASE(16)
+#undef CJX_EROW_CASE
+    default: break;
+  }
+}
+
+// Column pass: a CTA takes kWarps consecutive output columns and (with the
+// CTF) their mirror columns (Px - x) mod Px; each warp transforms its column
+// and its mirror, forms the contrast in place, and the CTA stores rows of
+// kWarps values.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_colfft_reg(const float2* __restrict__ t2, const cjx_image_params* __restrict__ params,
+                       const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0,
+                       float norm) {
+  constexpr int py = 32 * R;
+  constexpr int stride = pad16(py) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  float2* tab = smem;
+  float2* bufs = smem + py;  // columns [0, kWarps): own, [kWarps, 2 kWarps): mirrors
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  const int px = g.px;
+  const bool ctf = (g.flags & CJX_APPLY_CTF) != 0;
+  const int pitch = ctf ? g.pxh : px;
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, pitch - j0);
+  const float2* src = t2 + (size_t)blockIdx.y * py * g.ld2;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld2 + j0 + jj];
+      if (ctf) bufs[(kWarps + jj) * stride + pad16(m)] = src[(size_t)m * g.ld2 + (px - j0 - jj) % px];
+    }
+  }
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  const ImageConsts c = load_image_consts(params + img, norm, py, px);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) {
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const int bl = brev5(lane);
+    float2* A = bufs + warp * stride;
+    float2* B = bufs + (kWarps + warp) * stride;
+    float2 x[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = A[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(x, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) A[pad16(k1 + R * lane)] = x[k1];
+    if (ctf) {
+#pragma unroll
+      for (int n1 = 0; n1 < R; ++n1) x[n1] = B[pad16(32 * n1 + bl)];
+      warp_fft_reg<R, -1>(x, tab, lt, lane);
+      __syncwarp();
+#pragma unroll
+      for (int k1 = 0; k1 < R; ++k1) B[pad16(k1 + R * lane)] = x[k1];
+    }
+    __syncwarp();
+    const int col = j0 + warp;
+    for (int i = lane; i < py; i += 32) {
+      float2 v = A[pad16(i)];
+      if (ctf) {
+        v = ewald_epilogue(v, B[pad16((py - i) % py)], i, col, py, px, g.flags, c);
+      } else {
+        v.x *= c.scale;
+        v.y *= c.scale;
+      }
+      A[pad16(i)] = v;
+    }
+  }
+  __syncthreads();
+  float2* dst = out + (size_t)img * py * pitch + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) dst[(size_t)m * pitch + jj] = bufs[jj * stride + pad16(m)];
+  }
+}
+
 // Offset from the grid centre of surface entry (i, j) (pixel frequency
 // indices v, u): R (u, v, cw (u^2 + v^2)).
 struct SurfaceFrame {
@@ -184,34 +326,72 @@ static int ensure_ewald_smem() {
   if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
   int err = CJX_OK;
   std::call_once(flags[dev & 63], [&] {
-    cudaError_t e = cudaFuncSetAttribute(k_ewald_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_ewald_colfft, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    const int kMax = 227 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_ewald_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ewald_colfft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
+    // the register kernels also hold a static 32-entry twiddle table
+    const int kMaxReg = kMax - 1024;
+#define CJX_EW_ATTR(R)                                                                                        \
+  if (e == cudaSuccess)                                                                                       \
+    e = cudaFuncSetAttribute(k_ewald_colfft_reg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxReg);     \
+  if (e == cudaSuccess)                                                                                       \
+    e = cudaFuncSetAttribute(k_ewald_rows_reg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxReg);
+    CJX_EW_ATTR(1) CJX_EW_ATTR(2) CJX_EW_ATTR(3) CJX_EW_ATTR(4) CJX_EW_ATTR(5)
+    CJX_EW_ATTR(6) CJX_EW_ATTR(8) CJX_EW_ATTR(10) CJX_EW_ATTR(12) CJX_EW_ATTR(16)
+#undef CJX_EW_ATTR
     if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
   });
   return err;
 }
 
-int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream) {
+int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream,
+                      const Tuning& tn) {
   if (int e = ensure_ewald_smem()) return e;
-  const size_t sm = ewald_rows_smem(g);
-  if (sm > 227 * 1024) return fail(CJX_ERR_UNSUPPORTED, "Ewald row pass: shared memory exceeds 227 KB");
+  const dim3 gd((g.py + kWarps - 1) / kWarps, cnt);
+  const int rn = reg_fft_radix(g.n), rp = reg_fft_radix(g.px);
   prof_begin(stream);
-  k_ewald_rows<<<dim3((g.py + kWarps - 1) / kWarps, cnt), kWarps * 32, sm, stream>>>(t1, t2, g);
+  if (tn.fft_mode >= 1 && rn && rp) {
+    const size_t sm = sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) +
+                      sizeof(int) * (size_t)g.px;
+    switch (rn) {
+#define CJX_ER_CASE(R) \
+  case R: k_ewald_rows_reg<R><<<gd, kWarps * 32, sm, stream>>>(t1, t2, g, rp); break;
+      CJX_ER_CASE(1) CJX_ER_CASE(2) CJX_ER_CASE(3) CJX_ER_CASE(4) CJX_ER_CASE(5)
+      CJX_ER_CASE(6) CJX_ER_CASE(8) CJX_ER_CASE(10) CJX_ER_CASE(12) CJX_ER_CASE(16)
+#undef CJX_ER_CASE
+    }
+  } else {
+    const size_t sm = ewald_rows_smem(g);
+    if (sm > 227 * 1024) return fail(CJX_ERR_UNSUPPORTED, "Ewald row pass: shared memory exceeds 227 KB");
+    k_ewald_rows<<<gd, kWarps * 32, sm, stream>>>(t1, t2, g);
+  }
   prof_end("k_ewald_rows", stream);
   return check_cuda(cudaGetLastError(), "k_ewald_rows launch");
 }
 
 int launch_ewald_colfft(const SliceGeom& g, const float2* t2, const cjx_image_params* params, const int32_t* order,
-                        float2* out, int64_t k0, int cnt, cudaStream_t stream) {
+                        float2* out, int64_t k0, int cnt, cudaStream_t stream, const Tuning& tn) {
   if (int e = ensure_ewald_smem()) return e;
-  const size_t sm = ewald_cols_smem(g);
-  if (sm > 227 * 1024) return fail(CJX_ERR_UNSUPPORTED, "Ewald column pass: shared memory exceeds 227 KB");
   const int cols = (g.flags & CJX_APPLY_CTF) ? g.pxh : g.px;
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
+  const int ry = reg_fft_radix(g.py);
   prof_begin(stream);
-  k_ewald_colfft<<<dim3((cols + kEwWarps - 1) / kEwWarps, cnt), kEwWarps * 32, sm, stream>>>(t2, params, order, out,
-                                                                                               g, k0, norm);
+  if (tn.fft_mode >= 1 && ry) {
+    const dim3 gd((cols + kWarps - 1) / kWarps, cnt);
+    const size_t sm = sizeof(float2) * (size_t)(g.py + 2 * kWarps * (pad16(g.py) + 1));
+    switch (ry) {
+#define CJX_EC_CASE(R) \
+  case R: k_ewald_colfft_reg<R><<<gd, kWarps * 32, sm, stream>>>(t2, params, order, out, g, k0, norm); break;
+      CJX_EC_CASE(1) CJX_EC_CASE(2) CJX_EC_CASE(3) CJX_EC_CASE(4) CJX_EC_CASE(5)
+      CJX_EC_CASE(6) CJX_EC_CASE(8) CJX_EC_CASE(10) CJX_EC_CASE(12) CJX_EC_CASE(16)
+#undef CJX_EC_CASE
+    }
+  } else {
+    const size_t sm = ewald_cols_smem(g);
+    if (sm > 227 * 1024) return fail(CJX_ERR_UNSUPPORTED, "Ewald column pass: shared memory exceeds 227 KB");
+    k_ewald_colfft<<<dim3((cols + kEwWarps - 1) / kEwWarps, cnt), kEwWarps * 32, sm, stream>>>(t2, params, order,
+                                                                                                 out, g, k0, norm);
+  }
   prof_end("k_ewald_colfft", stream);
   return check_cuda(cudaGetLastError(), "k_ewald_colfft launch");
 }

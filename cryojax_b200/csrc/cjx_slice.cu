@@ -704,9 +704,10 @@ static int ensure_smem_attrs() {
   return err;
 }
 
-int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream);
+int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream,
+                      const Tuning& tn);
 int launch_ewald_colfft(const SliceGeom& g, const float2* t2, const cjx_image_params* params, const int32_t* order,
-                        float2* out, int64_t k0, int cnt, cudaStream_t stream);
+                        float2* out, int64_t k0, int cnt, cudaStream_t stream, const Tuning& tn);
 int launch_ewald_direct(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                         int64_t n_images, float2* out, cudaStream_t stream);
 
@@ -800,7 +801,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 #undef CJX_GC
       prof_end("k_gather_colifft", stream);
     }
-    if (g.flags & CJX_EWALD_SPHERE) return launch_ewald_rows(g, t1, t2, cnt, stream);
+    if (g.flags & CJX_EWALD_SPHERE) return launch_ewald_rows(g, t1, t2, cnt, stream, tn);
     prof_begin(stream);
     const dim3 gb((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt);
     if (fast && rn && rpx) {
@@ -866,7 +867,7 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
     if (g.flags & CJX_EWALD_SPHERE) {
-      if (int e = launch_ewald_colfft(g, t2, params, order, out, k0, cnt, stream)) return e;
+      if (int e = launch_ewald_colfft(g, t2, params, order, out, k0, cnt, stream, tn)) return e;
       continue;
     }
     prof_begin(stream);

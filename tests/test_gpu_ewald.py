@@ -150,3 +150,42 @@ def test_ewald_rejections(cuda_device):
         nat.loss_workspace_size(nat.make_desc(32, 16, 16, nat.CJX_EWALD_SPHERE | nat.CJX_APPLY_CTF), 1)
     assert e.value.code == nat.CJX_ERR_UNSUPPORTED
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("spline", [False, True])
+def test_register_fft_passes_match_oracle(cuda_device, spline):
+    """N = 128 -> 96^2 (register transforms of 128 and 96 points in the row and column passes)."""
+    _, grid, fs = make_volume(64, 120, seed=41)
+    specs = _specs(3, seed=43, shape=(96, 96), kv=40.0)
+    model = _model(_volume(grid, spline), specs, _integrator("pairs", outputs_integral=False))
+    got = model.compute_fourier_image().cpu().numpy()
+    og = _oracle_grid(grid, spline)
+    ref = np.stack([O.compute_fourier_image(og, fs, s, ewald=True, spline=spline) for s in specs])
+    assert max(rel_l2_per_image(got, ref)) <= IMAGE_REL_L2_TOL
+
+
+def test_fft_modes_agree_at_the_benchmark_shape(cuda_device):
+    """N = 512 -> 320^2: register-FFT passes (default) against the shared-memory Stockham passes."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+    from cryojax_b200 import synthetic
+
+    vol = S.FourierVoxelGridVolume.from_real_voxel_grid(synthetic.gaussian_sum_volume(256, 2000, 3),
+                                                        pad_scale=2.0)
+    b = synthetic.image_batch(16, 5)
+    pose = S.QuaternionPose(b.offsets[:, 0], b.offsets[:, 1], wxyz=b.wxyz)
+    tt = S.ContrastTransferTheory(S.AstigmaticCTF(b.defocus, b.astigmatism, b.astigmatism_angle))
+    cfg = S.BasicImageConfig((320, 320), 2.0, 300.0)
+    model = S.make_image_model(vol, cfg, pose, tt, volume_integrator=S.EwaldSphereExtraction(outputs_integral=False))
+    old = nat.tuning_get(nat.CJX_TUNE_FFT_MODE)
+    try:
+        outs = {}
+        for mode in (0, 2):
+            nat.tuning_set(nat.CJX_TUNE_FFT_MODE, mode)
+            outs[mode] = model.compute_fourier_image().cpu().numpy()
+    finally:
+        nat.tuning_set(nat.CJX_TUNE_FFT_MODE, old)
+    torch.cuda.synchronize()
+    assert max(rel_l2_per_image(outs[2], outs[0])) <= 1e-5
