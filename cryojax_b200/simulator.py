@@ -15,6 +15,7 @@ Covered (reference file:line):
   AstigmaticCTF               cryojax/simulator/_transfer_theory/transfer_function.py:84-169
   ContrastTransferTheory      cryojax/simulator/_transfer_theory/transfer_theory.py:21-119
   FourierGaussian (envelope)  cryojax/ndimage/operators/_fourier_operator.py:183-234
+  Constant (envelope)         cryojax/ndimage/operators/_base_operator.py:53-67
   FourierVoxelGridVolume      cryojax/simulator/_volume/representations/voxel_volume.py:40-119
   FourierVoxelSplineVolume    cryojax/simulator/_volume/representations/voxel_volume.py:122-203
   FourierSliceExtraction      cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-183
@@ -230,16 +231,30 @@ class FourierGaussian:
         self.b_factor = _arr(b_factor)
 
 
+class Constant:
+    """A constant envelope (RELION's scale factor alone).  cryojax/ndimage/operators/_base_operator.py:53-67."""
+
+    def __init__(self, value):
+        self.value = _arr(value)
+
+
+def _envelope_amp_b(envelope):
+    """(amplitude, b_factor) of a device envelope: a Constant is amplitude * exp(-0 k^2 / 4)."""
+    if isinstance(envelope, Constant):
+        return envelope.value, np.zeros_like(envelope.value)
+    return envelope.amplitude, envelope.b_factor
+
+
 class ContrastTransferTheory:
     """cryojax/simulator/_transfer_theory/transfer_theory.py:21-119 (projection branch)."""
 
-    def __init__(self, ctf: AstigmaticCTF, envelope: FourierGaussian | None = None, amplitude_contrast_ratio=0.1,
-                 phase_shift=0.0):
+    def __init__(self, ctf: AstigmaticCTF, envelope: FourierGaussian | Constant | None = None,
+                 amplitude_contrast_ratio=0.1, phase_shift=0.0):
         ac = _arr(amplitude_contrast_ratio)
         if np.any(ac < 0) or np.any(ac > 1):
             raise ValueError("`amplitude_contrast_ratio` must be in [0, 1]")
-        if envelope is not None and not isinstance(envelope, FourierGaussian):
-            raise NotImplementedError("only FourierGaussian envelopes run on the device")
+        if envelope is not None and not isinstance(envelope, (FourierGaussian, Constant)):
+            raise NotImplementedError("only FourierGaussian and Constant envelopes run on the device")
         self.ctf = ctf
         self.envelope = envelope
         self.amplitude_contrast_ratio = ac
@@ -431,7 +446,7 @@ def pack_image_params(pose: AbstractPose, image_config: BasicImageConfig,
                   ctf.spherical_aberration_in_mm, transfer_theory.amplitude_contrast_ratio,
                   transfer_theory.phase_shift]
         if transfer_theory.envelope is not None:
-            cands += [transfer_theory.envelope.amplitude, transfer_theory.envelope.b_factor]
+            cands += list(_envelope_amp_b(transfer_theory.envelope))
     if n is None:
         n = _batch_size(*cands) or 1
     p = nat.empty_params(n)
@@ -461,8 +476,9 @@ def pack_image_params(pose: AbstractPose, image_config: BasicImageConfig,
         p[:, nat.P_AC] = ac
         p[:, nat.P_PHASE_SHIFT] = np.deg2rad(_per_image(transfer_theory.phase_shift, n))
         if transfer_theory.envelope is not None:
-            p[:, nat.P_ENV_AMP] = _per_image(transfer_theory.envelope.amplitude, n)
-            p[:, nat.P_ENV_B] = _per_image(transfer_theory.envelope.b_factor, n)
+            amp, b = _envelope_amp_b(transfer_theory.envelope)
+            p[:, nat.P_ENV_AMP] = _per_image(amp, n)
+            p[:, nat.P_ENV_B] = _per_image(b, n)
     return p
 
 

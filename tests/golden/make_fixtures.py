@@ -1,4 +1,4 @@
-"""Write the reference's own test volume as a NumPy fixture (run where the reference tree exists).
+"""Write the reference's own test data as fixtures (run where the reference tree exists).
 
 The reference's image-model tests use the real-space potential
 tests/data/3j9g_potential_ps4_4.mrc (a 64^3 float32 map, 4.4 A voxels;
@@ -9,13 +9,18 @@ cell lengths in A at 40-51, extended-header size nsymbt at 92), then the
 data with x fastest, which is the [z][y][x] array mrcfile returns.
 
 Output: tests/golden/3j9g_potential_ps4_4.npy and
-tests/golden/3j9g_potential_ps4_4.json (voxel size, source).
+tests/golden/3j9g_potential_ps4_4.json (voxel size, source).  Given the
+reference's tests/data directory instead of the MRC path, it also copies
+the RELION fixtures byte for byte into tests/golden/relion/: the STAR file
+test_starfile.star (3 particles, one optics group) and the 3-image 16 x 16
+stack 000000.mrcs it names (cryojax tests/test_relion_dataset.py:47-62).
 
-    python tests/golden/make_fixtures.py /root/reference/tests/data/3j9g_potential_ps4_4.mrc
+    python tests/golden/make_fixtures.py /root/reference/tests/data
 """
 
 import json
 import os
+import shutil
 import struct
 import sys
 
@@ -37,6 +42,11 @@ def read_mrc(path):
 
 def main(src):
     here = os.path.dirname(os.path.abspath(__file__))
+    if os.path.isdir(src):
+        os.makedirs(os.path.join(here, "relion"), exist_ok=True)
+        for name in ("test_starfile.star", "000000.mrcs"):
+            shutil.copyfile(os.path.join(src, name), os.path.join(here, "relion", name))
+        src = os.path.join(src, "3j9g_potential_ps4_4.mrc")
     vol, voxel = read_mrc(src)
     np.save(os.path.join(here, "3j9g_potential_ps4_4.npy"), vol)
     with open(os.path.join(here, "3j9g_potential_ps4_4.json"), "w") as f:
