@@ -71,6 +71,7 @@ def parse_args():
                     help="images in its exhaustive arm (36,864 simulations each)")
     ap.add_argument("--no-spline", action="store_true", help="skip the spline-volume measurement")
     ap.add_argument("--no-ewald", action="store_true", help="skip the Ewald-sphere measurement")
+    ap.add_argument("--no-relion", action="store_true", help="skip the RELION particle-stack measurement")
     ap.add_argument("--search-images", type=int, default=1024,
                     help="observed images in the pose-search measurement (the configuration has 4096)")
     return ap.parse_args()
@@ -814,6 +815,71 @@ def measure_ewald(dev, volume, batch, cfg, steps, warmup, n_images, cpu_images):
     return res
 
 
+def measure_relion_stack(dev, volume, cfg, n_particles, seed):
+    """simulate_particle_stack end to end: a RELION STAR file of `n_particles` (random Euler poses, CTFs and
+    origins) is read, simulated in batches of 1024 through the device launch and written as MRC stacks of 1024
+    images.  Host wall clock; the split into device and I/O time is measured inside."""
+    import pathlib
+    import shutil
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    from cryojax_b200 import relion
+    from cryojax_b200 import simulator as S
+
+    rng = np.random.default_rng(seed)
+    n = n_particles
+    ox, oy = rng.uniform(-20, 20, n), rng.uniform(-20, 20, n)
+    rot, psi = rng.uniform(-180, 180, n), rng.uniform(-180, 180, n)
+    tilt = np.rad2deg(np.arccos(rng.uniform(-1, 1, n)))
+    df, astig, ang = rng.uniform(5000, 25000, n), rng.uniform(0, 500, n), rng.uniform(0, 180, n)
+    root = pathlib.Path(tempfile.mkdtemp(prefix="relion_bench_"))
+
+    def write_star(path, k):
+        pf = relion.RelionParticleParameterFile(path, mode="w")
+        pf.append({"image_config": S.BasicImageConfig(cfg.shape, 2.0, 300.0),
+                   "pose": S.EulerAnglePose(ox[:k], oy[:k], rot[:k], tilt[:k], psi[:k]),
+                   "transfer_theory": S.ContrastTransferTheory(S.AstigmaticCTF(df[:k], astig[:k], ang[:k], 2.7))})
+        pf.save()
+
+    device_s = [0.0]
+
+    def compute(parameters, vol, _):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        model = S.make_image_model(vol, parameters["image_config"], parameters["pose"], parameters["transfer_theory"])
+        dimg = model.simulate()
+        img = torch.empty(dimg.shape, dtype=dimg.dtype, pin_memory=True)
+        img.copy_(dimg)
+        device_s[0] += time.perf_counter() - t
+        return img
+
+    def run(star_in, project, batch):
+        pf = relion.RelionParticleParameterFile(star_in)
+        pf.path_to_starfile = project / "sim.star"
+        ds = relion.RelionParticleStackDataset(pf, project, mode="w")
+        relion.simulate_particle_stack(ds, compute, constant_args=volume, batch_size=batch, images_per_file=batch)
+
+    try:
+        write_star(root / "warm.star", 64)
+        write_star(root / "in.star", n)
+        run(root / "warm.star", root / "warm", 64)
+        device_s[0] = 0.0
+        t0 = time.perf_counter()
+        run(root / "in.star", root / "out", 1024)
+        wall = time.perf_counter() - t0
+        written = sum(f.stat().st_size for f in (root / "out").iterdir())
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    return {"value": n / wall, "unit": UNIT, "particles": n, "wall_s": wall,
+            "device_simulate_and_d2h_s": device_s[0], "host_io_and_parsing_s": wall - device_s[0],
+            "bytes_written": written,
+            "path": "STAR read -> RelionParticleParameterFile[batch] -> make_image_model(...).simulate() on the "
+                    "device (batches of 1024) -> D2H -> MRC stacks of 1024 images + STAR write"}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -1165,6 +1231,15 @@ def main():
         except Exception as e:
             ewald = {"error": repr(e)}
 
+    # ---- RELION particle stack: STAR in, MRC stacks out
+    relion_stack = None
+    if not args.no_relion and world == 1:
+        try:
+            torch.cuda.empty_cache()
+            relion_stack = measure_relion_stack(dev, volume, cfg, 4096, args.seed + 60)
+        except Exception as e:
+            relion_stack = {"error": repr(e)}
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1207,6 +1282,7 @@ def main():
             "search_refine": search_refine,
             "spline": spline,
             "ewald": ewald,
+            "relion_stack": relion_stack,
         }
         print(json.dumps(line))
     replicas.shutdown(info)

@@ -121,9 +121,9 @@ def _write(array, spacing, filename, kind, overwrite):
         mx, my = nx, ny
         mz, ispg = (1, 0) if kind == "image_stack" else (nz, 1)
     d = float(np.asarray(spacing))
-    as64 = data.astype(np.float64)
-    dmin, dmax, dmean = float(as64.min()), float(as64.max()), float(as64.mean())
-    rms = float(as64.std())
+    dmin, dmax = float(data.min()), float(data.max())
+    dmean = float(data.mean(dtype=np.float64))
+    rms = float(data.std(dtype=np.float64))
     header = bytearray(_HEADER_BYTES)
     struct.pack_into("<10i", header, 0, nx, ny, nz, 2, 0, 0, 0, mx, my, mz)
     struct.pack_into("<6f", header, 40, d * mx, d * my, d * mz, 90.0, 90.0, 90.0)
@@ -139,9 +139,11 @@ def _write(array, spacing, filename, kind, overwrite):
     label = b"Created by cryojax_b200"
     header[224:224 + len(label)] = label
     header[224 + len(label):224 + 80] = b" " * (80 - len(label))
+    if data.dtype.byteorder == ">":
+        data = data.astype("<f4")
     with open(filename, "wb") as f:
         f.write(bytes(header))
-        f.write(data.astype("<f4").tobytes())
+        f.write(memoryview(data).cast("B"))
 
 
 def _no_compression(compression):

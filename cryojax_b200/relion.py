@@ -541,6 +541,16 @@ class RelionParticleStackDataset:
 
     def write_images(self, index_array, images, parameters=None):
         """relion.py:756-833: one stack file per call, named after the previous one."""
+        path, images, pixel = self._prepare_write(index_array, images, parameters)
+        self._write_stack(path, images, pixel)
+
+    def _write_stack(self, path, images, pixel):
+        path.parent.mkdir(parents=True, exist_ok=True)
+        _mrc.write_image_stack_to_mrc(images, pixel, path, overwrite=self.mrcfile_settings["overwrite"],
+                                      compression=self.mrcfile_settings["compression"])
+
+    def _prepare_write(self, index_array, images, parameters=None):
+        """Validate, name the particles' images in the STAR table and return (path, float32 images, pixel size)."""
         pf = self.parameter_file
         particles, optics = pf.starfile_data["particles"], pf.starfile_data["optics"]
         index_array = np.atleast_1d(np.asarray(index_array, dtype=int))
@@ -561,10 +571,7 @@ class RelionParticleStackDataset:
         if "rlnImageName" not in particles.columns:
             particles["rlnImageName"] = pd.Series([None] * len(particles), index=particles.index, dtype=object)
         particles.loc[particles.index[index_array], "rlnImageName"] = names
-        path.parent.mkdir(parents=True, exist_ok=True)
-        _mrc.write_image_stack_to_mrc(images.astype(np.float32), pixel, path,
-                                      overwrite=self.mrcfile_settings["overwrite"],
-                                      compression=self.mrcfile_settings["compression"])
+        return path, np.asarray(images, dtype=np.float32), pixel
 
 
 def _to_numpy(images):
@@ -609,21 +616,34 @@ def simulate_particle_stack(dataset: RelionParticleStackDataset, compute_image_f
     if dataset.mode == "r":
         raise ValueError("Found that the `dataset` was in reading mode (`mode = 'r'`), but this must be "
                          "instantiated in writing mode (`mode = 'w'`).")
+    from concurrent.futures import ThreadPoolExecutor
+
     n = len(dataset)
     per_file = n if images_per_file is None else int(images_per_file)
     pf = dataset.parameter_file
-    for start in range(0, n, max(per_file, 1)):
-        index = np.arange(start, min(start + per_file, n))
-        parameters = pf[index]
-        chunks = []
-        if batch_size is None:
-            for i, k in enumerate(index):
-                img = compute_image_fn(pf[int(k)], constant_args, _index_per_particle(k, per_particle_args))
-                chunks.append(_to_numpy(img)[None])
-        else:
-            for b0 in range(0, index.size, int(batch_size)):
-                sub = index[b0:b0 + int(batch_size)]
-                img = _to_numpy(compute_image_fn(pf[sub], constant_args, _index_per_particle(sub, per_particle_args)))
-                chunks.append(img.reshape((-1,) + img.shape[-2:]))
-        dataset.write_images(index, np.concatenate(chunks, axis=0), parameters)
+    # each finished stack is written on a background thread while the next one is simulated;
+    # the STAR table's image names are assigned in order on this thread
+    with ThreadPoolExecutor(max_workers=1) as writer:
+        pending = None
+        for start in range(0, n, max(per_file, 1)):
+            index = np.arange(start, min(start + per_file, n))
+            parameters = pf[index]
+            chunks = []
+            if batch_size is None:
+                for k in index:
+                    img = compute_image_fn(pf[int(k)], constant_args, _index_per_particle(k, per_particle_args))
+                    chunks.append(_to_numpy(img)[None])
+            else:
+                for b0 in range(0, index.size, int(batch_size)):
+                    sub = index[b0:b0 + int(batch_size)]
+                    img = _to_numpy(compute_image_fn(pf[sub], constant_args,
+                                                     _index_per_particle(sub, per_particle_args)))
+                    chunks.append(img.reshape((-1,) + img.shape[-2:]))
+            images = chunks[0] if len(chunks) == 1 else np.concatenate(chunks, axis=0)
+            job = dataset._prepare_write(index, images, parameters)
+            if pending is not None:
+                pending.result()
+            pending = writer.submit(dataset._write_stack, *job)
+        if pending is not None:
+            pending.result()
     pf.save(**kwargs)
