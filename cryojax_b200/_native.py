@@ -59,6 +59,23 @@ P_AC = 21
 P_PHASE_SHIFT = 22
 
 
+CJX_RENDER_ACCUMULATE = 1
+CJX_RENDER_MAX_GAUSSIANS = 8
+
+
+class RenderDesc(ctypes.Structure):
+    _fields_ = [
+        ("nz", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("nx", ctypes.c_int32),
+        ("n_gaussians", ctypes.c_int32),
+        ("voxel_size", ctypes.c_float),
+        ("cutoff_sigmas", ctypes.c_float),
+        ("flags", ctypes.c_uint32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class SliceDesc(ctypes.Structure):
     _fields_ = [
         ("n", ctypes.c_int32),
@@ -109,6 +126,11 @@ class CryojaxB200Error(RuntimeError):
 _SIGNATURES = {
     "cjx_get_version": (ctypes.c_int, []),
     "cjx_spline_coefficients_workspace_size": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "cjx_render_gaussians": (
+        ctypes.c_int,
+        [ctypes.POINTER(RenderDesc), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "cjx_spline_coefficients": (
         ctypes.c_int,
         [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
@@ -723,6 +745,32 @@ def spline_coefficients(grid, out=None, workspace=None, stream=None):
     _check(load_library().cjx_spline_coefficients(int(n), _cuda_ptr(grid, "grid"), _cuda_ptr(out, "coefficients"),
                                                   _cuda_ptr(workspace, "workspace"),
                                                   workspace.numel() * workspace.element_size(), _stream_ptr(stream)))
+    return out
+
+
+def render_gaussians(shape, voxel_size, positions, amplitudes, variances, out=None, accumulate=False,
+                     cutoff_sigmas=0.0, stream=None):
+    """Voxel-averaged Gaussian mixture on a float32 [nz, ny, nx] CUDA grid (cjx_render_gaussians)."""
+    import torch
+
+    nz, ny, nx = (int(v) for v in shape)
+    dev = positions.device
+    pos = positions.to(torch.float32).contiguous()
+    amp = amplitudes.to(torch.float32).contiguous()
+    var = variances.to(torch.float32).contiguous()
+    n = pos.shape[0]
+    if pos.shape != (n, 3) or amp.dim() != 2 or amp.shape[0] != n or var.shape != amp.shape:
+        raise ValueError("positions [n, 3], amplitudes and variances [n, n_gaussians]")
+    if out is None:
+        out = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev)
+    elif out.dtype != torch.float32 or tuple(out.shape) != (nz, ny, nx) or not out.is_contiguous():
+        raise ValueError("out must be contiguous float32 [nz, ny, nx]")
+    d = RenderDesc(nz, ny, nx, int(amp.shape[1]), float(voxel_size), float(cutoff_sigmas),
+                   CJX_RENDER_ACCUMULATE if accumulate else 0, 0)
+    null = ctypes.c_void_p(0)
+    _check(load_library().cjx_render_gaussians(
+        ctypes.byref(d), _cuda_ptr(pos, "positions") if n else null, _cuda_ptr(amp, "amplitudes") if n else null,
+        _cuda_ptr(var, "variances") if n else null, n, _cuda_ptr(out, "grid"), _stream_ptr(stream)))
     return out
 
 

@@ -30,3 +30,13 @@ def lorentz_factor_from_kilovolts(voltage_in_kilovolts):
 def interaction_constant_from_kilovolts(voltage_in_kilovolts):
     """lambda * gamma (:52-109)."""
     return wavelength_from_kilovolts(voltage_in_kilovolts) * lorentz_factor_from_kilovolts(voltage_in_kilovolts)
+
+
+def b_factor_to_variance(b_factor):
+    """variance = B / (8 pi^2).  cryojax/constants/_conventions.py:6-27."""
+    return np.asarray(b_factor, np.float64) / (8.0 * np.pi**2)
+
+
+def variance_to_b_factor(variance):
+    """B = 8 pi^2 variance.  cryojax/constants/_conventions.py:30-50."""
+    return 8.0 * np.pi**2 * np.asarray(variance, np.float64)

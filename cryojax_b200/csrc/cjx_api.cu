@@ -31,6 +31,8 @@ size_t bricked_elements(int n);
 int launch_brick_volume(int n, const float2* grid, float2* bricked, cudaStream_t stream);
 int launch_brick_volume_pairs(int n, const float2* grid, float4* out, cudaStream_t stream);
 size_t spline_workspace_elements(int n);
+int launch_render_gaussians(const cjx_render_desc* d, const float* positions, const float* amplitudes,
+                            const float* variances, int64_t n_atoms, float* grid, cudaStream_t stream);
 int launch_spline_coefficients(int n, const float2* grid, float2* coef, float2* work, cudaStream_t stream);
 
 static thread_local std::string g_last_error;
@@ -197,6 +199,24 @@ int cjx_spline_coefficients(int n, const void* grid, void* coefficients, void* w
     return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_spline_coefficients_workspace_size()");
   return launch_spline_coefficients(n, static_cast<const float2*>(grid), static_cast<float2*>(coefficients),
                                     static_cast<float2*>(workspace), static_cast<cudaStream_t>(stream));
+}
+
+int cjx_render_gaussians(const cjx_render_desc* desc, const float* positions, const float* amplitudes,
+                         const float* variances, int64_t n_atoms, float* grid, void* stream) {
+  if (!desc) return fail(CJX_ERR_INVALID_ARGUMENT, "desc is NULL");
+  if (desc->nz < 1 || desc->ny < 1 || desc->nx < 1 || desc->nz > 4096 || desc->ny > 4096 || desc->nx > 4096)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "grid sides must be in [1, 4096]");
+  if (desc->n_gaussians < 1 || desc->n_gaussians > CJX_RENDER_MAX_GAUSSIANS)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "n_gaussians must be in [1, CJX_RENDER_MAX_GAUSSIANS]");
+  if (!(desc->voxel_size > 0.f) || desc->cutoff_sigmas < 0.f)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "need voxel_size > 0 and cutoff_sigmas >= 0");
+  if (desc->flags & ~CJX_RENDER_ACCUMULATE) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown flag bits");
+  if (n_atoms < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_atoms < 0");
+  if (!grid) return fail(CJX_ERR_INVALID_ARGUMENT, "grid must be non-NULL");
+  if (n_atoms > 0 && (!positions || !amplitudes || !variances))
+    return fail(CJX_ERR_INVALID_ARGUMENT, "positions, amplitudes and variances must be non-NULL");
+  return launch_render_gaussians(desc, positions, amplitudes, variances, n_atoms, grid,
+                                 static_cast<cudaStream_t>(stream));
 }
 
 int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_images, size_t* bytes) {

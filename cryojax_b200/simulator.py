@@ -16,6 +16,8 @@ Covered (reference file:line):
   ContrastTransferTheory      cryojax/simulator/_transfer_theory/transfer_theory.py:21-119
   FourierGaussian (envelope)  cryojax/ndimage/operators/_fourier_operator.py:183-234
   Constant (envelope)         cryojax/ndimage/operators/_base_operator.py:53-67
+  GaussianMixtureVolume       cryojax/simulator/_volume/representations/gaussian_volume.py:21-204
+  GaussianMixtureRenderFn     cryojax/simulator/_volume_rendering/gaussian_rendering.py:24-336
   FourierVoxelGridVolume      cryojax/simulator/_volume/representations/voxel_volume.py:40-119
   FourierVoxelSplineVolume    cryojax/simulator/_volume/representations/voxel_volume.py:122-203
   FourierSliceExtraction      cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:26-183
@@ -427,6 +429,106 @@ class FourierVoxelSplineVolume:
 
     def get_representation(self, rng_key=None):
         return self
+
+
+class GaussianMixtureVolume:
+    """Atoms as mixtures of isotropic Gaussians.
+
+    cryojax/simulator/_volume/representations/gaussian_volume.py:21-204:
+    ``positions`` [n, 3] (Angstrom), ``amplitudes`` and ``variances``
+    (Angstrom^2) scalars, [n] or [n, n_gaussians], broadcast to
+    [n, n_gaussians]; variances must be positive.  Rendered to a voxel grid
+    on the device by GaussianMixtureRenderFn.
+    """
+
+    def __init__(self, positions, amplitudes=1.0, variances=1.0):
+        pos = np.asarray(positions, np.float64)
+        if pos.ndim != 2 or pos.shape[1] != 3:
+            raise ValueError("`positions` must have shape (n_positions, 3)")
+        n = pos.shape[0]
+
+        def as_2d(name, v):
+            v = np.asarray(v, np.float64)
+            if v.ndim == 0:
+                v = v[None, None]
+            elif v.ndim == 1:
+                v = v[:, None]
+            elif v.ndim != 2:
+                raise ValueError(f"`{name}` must be of shape (), (n_positions,) or (n_positions, n_gaussians)")
+            return v
+
+        amp, var = as_2d("amplitudes", amplitudes), as_2d("variances", variances)
+        g = max(amp.shape[1], var.shape[1])
+        self.positions = pos
+        self.amplitudes = np.broadcast_to(amp, (n, g)).copy()
+        self.variances = np.broadcast_to(var, (n, g)).copy()
+        if np.any(self.variances <= 0):
+            raise ValueError("`variances` must be positive")
+
+    @classmethod
+    def from_tabulated_parameters(cls, atom_positions, parameters, extra_b_factors=None):
+        """gaussian_volume.py:144-183: amplitudes a, variances (b + extra B) / (8 pi^2) (Peng et al. 1996)."""
+        a = np.asarray(parameters.a if hasattr(parameters, "a") else parameters["a"], np.float64)
+        b = np.asarray(parameters.b if hasattr(parameters, "b") else parameters["b"], np.float64)
+        if extra_b_factors is not None:
+            extra = np.asarray(extra_b_factors, np.float64)
+            b = b + (extra[:, None] if extra.ndim == 1 else extra)
+        return cls(atom_positions, a, C.b_factor_to_variance(b))
+
+    def rotate_to_pose(self, pose: AbstractPose, inverse: bool = False):
+        """gaussian_volume.py:185-192: positions rotated by the pose's rotation (or its inverse)."""
+        R = pose.rotation_matrices()
+        if R.ndim != 2:
+            raise ValueError("rotate a GaussianMixtureVolume with one pose at a time")
+        if inverse:
+            R = R.T
+        return GaussianMixtureVolume(self.positions @ R.T, self.amplitudes, self.variances)
+
+    def translate_to_pose(self, pose: AbstractPose):
+        """gaussian_volume.py:194-204."""
+        o = np.asarray(pose.offset_in_angstroms, np.float64)
+        if o.ndim != 1:
+            raise ValueError("translate a GaussianMixtureVolume with one pose at a time")
+        if o.shape[0] == 2:
+            o = np.concatenate([o, [0.0]])
+        return GaussianMixtureVolume(self.positions + o, self.amplitudes, self.variances)
+
+
+class GaussianMixtureRenderFn:
+    """Render a GaussianMixtureVolume to a voxel grid on the device.
+
+    cryojax/simulator/_volume_rendering/gaussian_rendering.py:24-197: the
+    voxel-averaged potential (error-function integrals per axis), here
+    splatted atom by atom (cjx_render_gaussians).  ``batch_options`` are
+    accepted for API compatibility and have no effect (the device kernel
+    needs no batching over z-planes or atoms).
+    """
+
+    def __init__(self, shape, voxel_size, *, batch_options: dict | None = None):
+        self.shape = tuple(int(s) for s in shape)
+        if len(self.shape) != 3:
+            raise ValueError("`shape` must be (z_dim, y_dim, x_dim)")
+        _require_positive("voxel_size", voxel_size)
+        self.voxel_size = float(voxel_size)
+        self.batch_options = dict(batch_options or {})
+
+    def __call__(self, volume_representation: GaussianMixtureVolume, *, outputs_real_space: bool = True,
+                 outputs_rfft: bool = False, fftshifted: bool = False, device: str = "cuda"):
+        torch = _torch()
+        v = volume_representation
+        if v.amplitudes.shape[1] > nat.CJX_RENDER_MAX_GAUSSIANS:
+            raise NotImplementedError(f"at most {nat.CJX_RENDER_MAX_GAUSSIANS} Gaussians per position")
+        t = lambda a: torch.as_tensor(a, dtype=torch.float32, device=device)
+        real = nat.render_gaussians(self.shape, self.voxel_size, t(v.positions), t(v.amplitudes), t(v.variances))
+        if outputs_real_space:
+            return real
+        # cryojax.ndimage fftn / rfftn transform ifftshift(x) (the origin moved to the corner first)
+        x = torch.fft.ifftshift(real.to(torch.float64))
+        if outputs_rfft:
+            ft = torch.fft.rfftn(x)
+            return torch.fft.fftshift(ft, dim=(0, 1)) if fftshifted else ft
+        ft = torch.fft.fftn(x)
+        return torch.fft.fftshift(ft) if fftshifted else ft
 
 
 # ---------------------------------------------------------------------------

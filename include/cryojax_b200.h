@@ -314,6 +314,32 @@ CJX_API int cjx_spline_coefficients_workspace_size(int n, size_t* bytes);
 CJX_API int cjx_spline_coefficients(int n, const void* grid, void* coefficients, void* workspace,
                                     size_t workspace_bytes, void* stream);
 
+/* ---- Gaussian-mixture rendering ----------------------------------------
+ * GaussianMixtureRenderFn (cryojax/simulator/_volume_rendering/
+ * gaussian_rendering.py:24-336) for a GaussianMixtureVolume
+ * (cryojax/simulator/_volume/representations/gaussian_volume.py:21-180):
+ * grid[z][y][x] (float32, device) = sum over atoms and their Gaussians of
+ * amplitude / (2 dx)^3 times, per axis, erf(s (L - p + dx)) - erf(s (L - p)),
+ * s = 1 / sqrt(2 variance), L = (i - D/2) dx - dx/2.  positions [n][3]
+ * (x, y, z, Angstrom), amplitudes and variances [n][n_gaussians] (variances
+ * in Angstrom^2, positive), all float32 device arrays.  Each atom adds to
+ * the voxels within cutoff_sigmas standard deviations (plus one voxel) of
+ * it (0 = the default 7), with float atomics (summation order varies run
+ * to run at rounding level).  The grid is zeroed first unless
+ * CJX_RENDER_ACCUMULATE.  Stream-ordered.                                   */
+#define CJX_RENDER_ACCUMULATE 1u
+#define CJX_RENDER_MAX_GAUSSIANS 8
+typedef struct cjx_render_desc {
+  int32_t nz, ny, nx;        /* grid shape                                  */
+  int32_t n_gaussians;       /* per atom, 1..CJX_RENDER_MAX_GAUSSIANS       */
+  float voxel_size;          /* Angstrom                                    */
+  float cutoff_sigmas;       /* 0 = default (7)                              */
+  uint32_t flags;            /* CJX_RENDER_*                                */
+  int32_t reserved;
+} cjx_render_desc;
+CJX_API int cjx_render_gaussians(const cjx_render_desc* desc, const float* positions, const float* amplitudes,
+                                 const float* variances, int64_t n_atoms, float* grid, void* stream);
+
 /* Batched complex-to-complex FFTs of `count` contiguous rows of n complex64
  * values (direction -1: forward, numpy.fft.fft; +1: unnormalised inverse,
  * n * numpy.fft.ifft), with the same warp FFTs the resize stage uses.  No

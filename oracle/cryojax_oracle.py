@@ -623,6 +623,40 @@ def compute_contrast_from_ewald_sphere(object_spectrum, phase_shifts, amplitude_
     return out
 
 
+def make_1d_coordinate_grid(size, grid_spacing=1.0):
+    """(i - size//2) * spacing.  cryojax/coordinates/_make_coordinate_grids.py:201-223, 301-317."""
+    return np.fft.fftshift(np.fft.fftfreq(size, 1.0 / grid_spacing)) * size
+
+
+def render_gaussian_mixture(shape, voxel_size, positions, amplitudes, variances):
+    """Voxel-averaged Gaussian mixture on a real-space grid (z, y, x).
+
+    cryojax/simulator/_volume_rendering/gaussian_rendering.py:196-336:
+    B = 8 pi^2 variance, s = 2 pi / sqrt(B); per axis the integral of each
+    Gaussian over voxel i is erf(s (L_i - p + dx)) - erf(s (L_i - p)) with
+    L_i = c_i - dx / 2 the voxel's left edge; the voxel value is
+    sum over atoms and Gaussians of a / (2 dx)^3 times the three axis
+    integrals.  Evaluated densely (every voxel, every Gaussian) in float64.
+    """
+    from scipy.special import erf
+
+    positions = np.asarray(positions, np.float64).reshape(-1, 3)
+    amplitudes = np.asarray(amplitudes, np.float64).reshape(positions.shape[0], -1)
+    variances = np.broadcast_to(np.asarray(variances, np.float64).reshape(positions.shape[0], -1), amplitudes.shape)
+    b_factors = 8.0 * np.pi**2 * variances
+    scaling = 2.0 * np.pi / np.sqrt(b_factors)  # (n, g)
+    nz, ny, nx = shape
+    integrals = []
+    for axis, size in ((0, nx), (1, ny), (2, nz)):
+        left = make_1d_coordinate_grid(size, voxel_size) - voxel_size / 2
+        delta = left[:, None] - positions[None, :, axis]  # (size, n)
+        integrals.append(erf(scaling[None] * (delta + voxel_size)[:, :, None])
+                         - erf(scaling[None] * delta[:, :, None]))  # (size, n, g)
+    gx, gy, gz = integrals
+    prefactor = amplitudes / (2.0 * voxel_size) ** 3
+    return np.einsum("xng,yng,zng,ng->zyx", gx, gy, gz, prefactor, optimize=True)
+
+
 # ---------------------------------------------------------------------------
 # CTF and transfer theory  (cryojax/simulator/_transfer_theory/)
 # ---------------------------------------------------------------------------

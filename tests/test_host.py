@@ -133,3 +133,24 @@ def test_area_downsample_reference_weights():
             w[i, y] = max(0.0, min(y1, y + 1) - max(y0, y))
     np.testing.assert_allclose(w.sum(1), f)
     np.testing.assert_allclose(w.sum(0), 1.0)
+
+
+def test_gaussian_mixture_volume_shapes_and_pose():
+    import numpy as np
+
+    from cryojax_b200 import simulator as S
+
+    v = S.GaussianMixtureVolume(np.zeros((4, 3)), 2.0, [1.0, 2.0, 3.0, 4.0])
+    assert v.amplitudes.shape == (4, 1) and v.variances[:, 0].tolist() == [1.0, 2.0, 3.0, 4.0]
+    with pytest.raises(ValueError):
+        S.GaussianMixtureVolume(np.zeros((2, 3)), 1.0, -1.0)
+    params = {"a": np.ones((3, 5)), "b": np.full((3, 5), 8 * np.pi**2)}
+    t = S.GaussianMixtureVolume.from_tabulated_parameters(np.zeros((3, 3)), params, extra_b_factors=np.zeros(3))
+    np.testing.assert_allclose(t.variances, 1.0)
+    pose = S.EulerAnglePose(1.0, -2.0, 30.0, 40.0, 50.0)
+    p = np.random.default_rng(0).standard_normal((5, 3))
+    r = S.GaussianMixtureVolume(p).rotate_to_pose(pose)
+    np.testing.assert_allclose(r.positions, p @ pose.rotation_matrices().T)
+    back = r.rotate_to_pose(pose, inverse=True)
+    np.testing.assert_allclose(back.positions, p, atol=1e-12)
+    np.testing.assert_allclose(S.GaussianMixtureVolume(p).translate_to_pose(pose).positions, p + [1.0, -2.0, 0.0])

@@ -208,3 +208,20 @@ def test_ewald_surface_at_zero_wavelength_is_the_slice():
     # a positive wavelength bends the surface: the result moves
     bent = O.ewald_integrate(grid, rot, (24, 24), 2.0, 0.5)
     assert np.abs(bent - full).max() > 1e-3 * np.abs(full).max()
+
+
+def test_gaussian_rendering_integrates_to_the_amplitudes():
+    """The axis integrals telescope to erf(inf) - erf(-inf) = 2 when the grid holds the whole mass, so
+    sum(V) dx^3 = sum of the amplitudes; a wide Gaussian's voxel averages approach its point values."""
+    rng = np.random.default_rng(4)
+    pos = rng.uniform(-3, 3, (6, 3))
+    amp = rng.uniform(0.5, 2.0, (6, 2))
+    var = rng.uniform(0.3, 1.0, (6, 2))
+    v = O.render_gaussian_mixture((40, 36, 32), 0.7, pos, amp, var)
+    np.testing.assert_allclose(v.sum() * 0.7**3, amp.sum(), rtol=1e-10)
+    # wide single Gaussian: voxel average = point value to O(dx^2 / sigma^2)
+    v1 = O.render_gaussian_mixture((32, 32, 32), 0.25, np.zeros((1, 3)), np.ones((1, 1)), np.full((1, 1), 4.0))
+    c = O.make_1d_coordinate_grid(32, 0.25)
+    zz, yy, xx = np.meshgrid(c, c, c, indexing="ij")
+    point = np.exp(-(xx**2 + yy**2 + zz**2) / 8.0) / (2 * np.pi * 4.0) ** 1.5
+    assert np.abs(v1 - point).max() <= 2e-3 * point.max()
