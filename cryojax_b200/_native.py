@@ -154,6 +154,21 @@ _SIGNATURES = {
             ctypes.c_void_p,
         ],
     ),
+    "cjx_slice_ctf_forward_filtered": (
+        ctypes.c_int,
+        [
+            ctypes.POINTER(SliceDesc),
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_int64,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_void_p,
+            ctypes.c_size_t,
+            ctypes.c_void_p,
+        ],
+    ),
     "cjx_slice_ctf_loss_workspace_size": (
         ctypes.c_int,
         [ctypes.POINTER(SliceDesc), ctypes.c_int64, ctypes.POINTER(ctypes.c_size_t)],
@@ -378,8 +393,13 @@ def _order_ptr(order, n_images):
     return _cuda_ptr(order, "order")
 
 
-def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream=None, order=None) -> None:
-    """Launch cjx_slice_ctf_forward on torch CUDA tensors (stream-ordered)."""
+def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream=None, order=None,
+                      filter=None) -> None:
+    """Launch cjx_slice_ctf_forward on torch CUDA tensors (stream-ordered).
+
+    ``filter``: an optional float32 CUDA array with one image's output shape, multiplied into every
+    output image inside the epilogue (cjx_slice_ctf_forward_filtered).
+    """
     import torch
 
     n_images = params.shape[0]
@@ -394,6 +414,15 @@ def slice_ctf_forward(desc: SliceDesc, grid, params, out, workspace=None, stream
     if workspace is not None:
         ws_ptr = _cuda_ptr(workspace, "workspace")
         ws_bytes = workspace.numel() * workspace.element_size()
+    if filter is not None:
+        if filter.dtype != torch.float32 or tuple(filter.shape) != tuple(out.shape[-2:]):
+            raise ValueError(f"filter must be float32 {tuple(out.shape[-2:])} (one output image's shape)")
+        _check(
+            load_library().cjx_slice_ctf_forward_filtered(
+                ctypes.byref(desc), _cuda_ptr(grid, "grid"), _cuda_ptr(params, "params"),
+                _order_ptr(order, n_images), int(n_images), _cuda_ptr(filter, "filter"), _cuda_ptr(out, "out"),
+                ws_ptr, ws_bytes, _stream_ptr(stream)))
+        return
     _check(
         load_library().cjx_slice_ctf_forward(
             ctypes.byref(desc),

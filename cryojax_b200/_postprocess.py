@@ -6,8 +6,8 @@ the inverse transforms the leading axis as complex and keeps only the real
 part of the DC and (even size) Nyquist bins of the last axis; the columns
 kx = 0 and kx = Px/2 are made Hermitian in ky first so the library C2R sees
 a well-defined input.  postprocess mirrors
-cryojax/simulator/_image_model/base_image_model.py:107-158 without masks or
-filters.
+cryojax/simulator/_image_model/base_image_model.py:107-158 (the filter is
+applied earlier, inside the device launch).
 """
 
 from __future__ import annotations
@@ -49,8 +49,9 @@ def rfftn(image):
     return torch.fft.rfftn(torch.fft.ifftshift(image, dim=(-2, -1)), dim=(-2, -1))
 
 
-def postprocess(fourier_image, shape, padded_shape, *, outputs_real_space=True, normalizes_signal=False):
-    if tuple(padded_shape) == tuple(shape) and not normalizes_signal:
+def postprocess(fourier_image, shape, padded_shape, *, outputs_real_space=True, normalizes_signal=False,
+                mask=None):
+    if mask is None and tuple(padded_shape) == tuple(shape) and not normalizes_signal:
         return irfftn(fourier_image, shape) if outputs_real_space else fourier_image
     image = irfftn(fourier_image, padded_shape)
     if tuple(padded_shape) != tuple(shape):
@@ -59,4 +60,6 @@ def postprocess(fourier_image, shape, padded_shape, *, outputs_real_space=True, 
         mean = image.mean(dim=(-2, -1), keepdim=True)
         std = image.std(dim=(-2, -1), keepdim=True, unbiased=False)
         image = (image - mean) / std
+    if mask is not None:
+        image = mask(image)
     return image if outputs_real_space else rfftn(image)

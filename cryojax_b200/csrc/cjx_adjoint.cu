@@ -464,6 +464,96 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
+// Cubic-spline scatter-add (FourierVoxelSplineVolume) and d/dR.
+// ---------------------------------------------------------------------------
+// The transpose of sample_spline_batch: every one of a sample's 64 taps
+// receives weight * cotangent in the C-order (N+2)^3 coefficient gradient,
+// and d(sample)/d(coordinate) uses the basis derivatives, per axis
+//   -3 (1-f)^2,  -12 f + 9 f^2,  12 (1-f) - 9 (1-f)^2,  3 f^2
+// (d/dc of basis(c - i + 1) for taps i = floor(c) + 0..3; floor has zero
+// derivative), with fill-valued taps included as the forward reads them.
+__device__ __forceinline__ void spline_dweights(float f, float* dw) {
+  const float g = 1.0f - f;
+  dw[0] = -3.0f * g * g;
+  dw[1] = f * fmaf(9.0f, f, -12.0f);
+  dw[2] = g * fmaf(-9.0f, g, 12.0f);
+  dw[3] = 3.0f * f * f;
+}
+
+template <typename Layout>
+__global__ void __launch_bounds__(256)
+    k_scatter_slice_spline(const float2* __restrict__ coef, const float2* __restrict__ gh,
+                           const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
+                           float2* __restrict__ grad_coef, double* __restrict__ grads, SliceGeom g, int64_t k0) {
+  const Layout L(g.n);
+  __shared__ float red[8][6];
+  const int n = g.n, m = n + 2;
+  const int64_t k = k0 + blockIdx.z;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  const double* Rm = params[img].rot;
+  const float r00 = (float)Rm[0], r01 = (float)Rm[1];
+  const float r10 = (float)Rm[3], r11 = (float)Rm[4];
+  const float r20 = (float)Rm[6], r21 = (float)Rm[7];
+  const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int du, dv;
+  gather_lane_offsets<1>(warp, lane, du, dv);
+  const int u = blockIdx.x * 16 + du;
+  const int v = blockIdx.y * 16 + dv;
+  float gr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (u < g.nxh && v < n) {
+    const float2 gs = gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v];
+    const float ux = (float)fft_index(u, n), vy = (float)fft_index(v, n);
+    const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    const SplineAxis ax = spline_axis(o[0], n, wrap);
+    const SplineAxis ay = spline_axis(o[1], n, wrap);
+    const SplineAxis az = spline_axis(o[2], n, wrap);
+    float dwx[4], dwy[4], dwz[4];
+    spline_dweights(o[0] - floorf(o[0]), dwx);
+    spline_dweights(o[1] - floorf(o[1]), dwy);
+    spline_dweights(o[2] - floorf(o[2]), dwz);
+    float dH[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+    for (int dz = 0; dz < 4; ++dz) {
+      for (int dy = 0; dy < 4; ++dy) {
+        const bool vzy = az.v[dz] && ay.v[dy];
+        const int zy = L.az(az.i[dz]) + L.ay(ay.i[dy]);
+        const size_t row = ((size_t)az.i[dz] * m + ay.i[dy]) * m;
+        const float wzy = az.w[dz] * ay.w[dy];
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+          const bool ok = vzy && ax.v[dx];
+          const float2 val = ok ? __ldg(coef + zy + L.ax(ax.i[dx])) : g.fill;
+          const float gwx = dwx[dx] * wzy, gwy = ax.w[dx] * dwy[dy] * az.w[dz], gwz = ax.w[dx] * ay.w[dy] * dwz[dz];
+          dH[0][0] += gwx * val.x; dH[0][1] += gwx * val.y;
+          dH[1][0] += gwy * val.x; dH[1][1] += gwy * val.y;
+          dH[2][0] += gwz * val.x; dH[2][1] += gwz * val.y;
+          if (ok && grad_coef) {
+            const float w = wzy * ax.w[dx];
+            atomicAdd(&grad_coef[row + ax.i[dx]], make_float2(w * gs.x, w * gs.y));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float dLdo = gs.x * dH[a][0] + gs.y * dH[a][1];
+      gr[2 * a] = dLdo * ux;
+      gr[2 * a + 1] = dLdo * vy;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) gr[q] = warp_sum(gr[q]);
+  if (lane == 0)
+    for (int q = 0; q < 6; ++q) red[warp][q] = gr[q];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double acc = 0.0;
+    for (int w = 0; w < 8; ++w) acc += (double)red[w][threadIdx.x];
+    atomicAdd(&grads[img * 16 + kGradRot + threadIdx.x], acc);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host launcher
 // ---------------------------------------------------------------------------
 int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
@@ -559,7 +649,13 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
     prof_begin(stream);
     const dim3 gs((g.nxh + 15) / 16, (g.n + 15) / 16, cnt);
     const bool agg = tn.scatter_vec != 0;
-    if (bricked && agg) {
+    if ((g.flags & CJX_GRID_SPLINE) && bricked) {
+      k_scatter_slice_spline<SplineBrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
+                                                                        k0);
+    } else if (g.flags & CJX_GRID_SPLINE) {
+      k_scatter_slice_spline<SplineLinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads,
+                                                                         g, k0);
+    } else if (bricked && agg) {
       k_scatter_slice<BrickLayout, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
     } else if (bricked) {
       k_scatter_slice<BrickLayout, false><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);

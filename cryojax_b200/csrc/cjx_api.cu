@@ -92,6 +92,25 @@ int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cj
                         workspace, chunk, static_cast<cudaStream_t>(stream), current_tuning());
 }
 
+int cjx_slice_ctf_forward_filtered(const cjx_slice_desc* desc, const void* grid, const cjx_image_params* params,
+                                   const int32_t* order, int64_t n_images, const float* filter, void* out,
+                                   void* workspace, size_t workspace_bytes, void* stream) {
+  SliceGeom g;
+  if (int e = make_geom(desc, &g)) return e;
+  if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
+  if (n_images == 0) return CJX_OK;
+  if (!grid || !params || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params and out must be non-NULL");
+  g.filter = filter;
+  int64_t chunk = 0;
+  if (needs_resize(g)) {
+    chunk = chunk_for(g, desc, n_images);
+    if (!workspace || workspace_bytes < (size_t)chunk * workspace_per_image(g))
+      return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_workspace_size()");
+  }
+  return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images, static_cast<float2*>(out),
+                        workspace, chunk, static_cast<cudaStream_t>(stream), current_tuning());
+}
+
 static int group_plan(const cjx_slice_group& gr, SliceGeom* g, int64_t* chunk, size_t* need) {
   if (int e = make_geom(&gr.desc, g)) return e;
   if (gr.n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "group n_images < 0");
@@ -225,7 +244,6 @@ int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_imag
   SliceGeom g;
   if (int e = make_geom(desc, &g)) return e;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
-  if (g.flags & CJX_GRID_SPLINE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of spline volumes is not implemented");
   if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
   *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
   return CJX_OK;
@@ -239,7 +257,6 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   if (n_images == 0) return CJX_OK;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
-  if (g.flags & CJX_GRID_SPLINE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of spline volumes is not implemented");
   if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
   if (!grid || !params || !observed || !image_grads)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");

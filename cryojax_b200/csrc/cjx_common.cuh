@@ -30,7 +30,18 @@ struct SliceGeom {
   uint32_t flags;
   float2 fill;      // out-of-bounds fill value
   FftPlan plan_n, plan_py, plan_px;
+  const float* filter;  // optional Fourier-space filter over the output grid (row pitch = output columns)
 };
+
+// Output entry (i, j) times the optional fused filter.
+__device__ __forceinline__ float2 apply_filter(float2 v, const SliceGeom& g, int i, int j, int pitch) {
+  if (g.filter) {
+    const float f = __ldg(g.filter + (size_t)i * pitch + j);
+    v.x *= f;
+    v.y *= f;
+  }
+  return v;
+}
 
 // ---------------------------------------------------------------------------
 // Index helpers

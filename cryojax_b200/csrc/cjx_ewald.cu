@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kEwWarps * 32)
       v.x *= c.scale;
       v.y *= c.scale;
     }
-    dst[(size_t)i * pitch] = v;
+    dst[(size_t)i * pitch] = apply_filter(v, g, i, x, pitch);
   }
 }
 
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kWarps * 32)
         v.x *= c.scale;
         v.y *= c.scale;
       }
-      A[pad16(i)] = v;
+      A[pad16(i)] = apply_filter(v, g, i, col, pitch);
     }
   }
   __syncthreads();
@@ -302,11 +302,11 @@ __global__ void __launch_bounds__(256)
       surface_offset(f, (n - i) % n, (n - j) % n, n, ox[1], oy[1], oz[1]);
       const bool act[2] = {true, true};
       gather_samples<2>(grid, n, L, ox, oy, oz, act, wrap, g.fill, v);
-      dst[e] = ewald_epilogue(v[0], v[1], i, j, n, n, g.flags, c);
+      dst[e] = apply_filter(ewald_epilogue(v[0], v[1], i, j, n, n, g.flags, c), g, i, j, width);
     } else {
       const bool act = true;
       gather_samples<1>(grid, n, L, ox, oy, oz, &act, wrap, g.fill, v);
-      dst[e] = make_float2(v[0].x * c.scale, v[0].y * c.scale);
+      dst[e] = apply_filter(make_float2(v[0].x * c.scale, v[0].y * c.scale), g, i, j, width);
     }
   }
 }

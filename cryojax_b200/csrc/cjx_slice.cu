@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     float2* a = bufs + warp * stride;
     float2* X = warp_fft<-1>(a, a + py, g.plan_py, tw, lane);
     const int j = j0 + warp;
-    for (int i = lane; i < py; i += 32) X[i] = apply_epilogue(X[i], i, j, py, g.px, g.flags, c);
+    for (int i = lane; i < py; i += 32) X[i] = apply_filter(apply_epilogue(X[i], i, j, py, g.px, g.flags, c), g, i, j, g.pxh);
   }
   __syncthreads();
   const int res_off = (g.plan_py.nstages == 0 || (g.plan_py.nstages & 1)) ? py : 0;
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
       const int i = k1 + R * lane;
-      buf[pad16(i)] = apply_epilogue(x[k1], i, j, py, g.px, g.flags, c);
+      buf[pad16(i)] = apply_filter(apply_epilogue(x[k1], i, j, py, g.px, g.flags, c), g, i, j, g.pxh);
     }
   }
   __syncthreads();
@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(256)
     gather_samples<1>(grid, n, L, &ox, &oy, &oz, &act, wrap, g.fill, &v);
     // convert_fftn_to_rfftn(mode="real")  (cryojax/ndimage/_fourier_utils.py:6-57)
     if ((n % 2 == 0) && ((i == h && j == 0) || (i == 0 && j == h) || (i == h && j == h))) v.y = 0.f;
-    dst[e] = apply_epilogue(v, i, j, n, n, g.flags, c);
+    dst[e] = apply_filter(apply_epilogue(v, i, j, n, n, g.flags, c), g, i, j, g.nxh);
   }
 }
 
@@ -605,6 +605,7 @@ int make_geom(const cjx_slice_desc* d, SliceGeom* g) {
   g->pad_left_x = d->px > d->n ? left_pad(d->px, d->n) : 0;
   g->flags = d->flags;
   g->fill = make_float2(d->fill_re, d->fill_im);
+  g->filter = nullptr;
   g->plan_n = make_fft_plan(d->n);
   g->plan_py = make_fft_plan(d->py);
   g->plan_px = make_fft_plan(d->px);

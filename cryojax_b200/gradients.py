@@ -138,14 +138,21 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
     integ = model.volume_integrator
     params = model.image_params()
     n = params.shape[0]
-    if not hasattr(vol, "fourier_voxel_grid"):
-        raise NotImplementedError("gradients through spline volumes are not implemented on the device")
-    dev = vol.fourier_voxel_grid.device
+    if not integ.is_projection_approximation:
+        raise NotImplementedError("gradients through the Ewald sphere are not implemented on the device")
+    dev = vol.device
     flags = model._flags() | integ._base_flags()
-    grid = vol.fourier_voxel_grid
-    if integ.use_bricked_layout:
-        grid = vol.bricked_grid()
-        flags |= nat.CJX_GRID_BRICKED
+    if hasattr(vol, "spline_coefficients"):  # gradient with respect to the spline coefficients
+        grid, grad_shape = vol.spline_coefficients, tuple(vol.spline_coefficients.shape)
+        flags |= nat.CJX_GRID_SPLINE
+        if integ.use_bricked_layout:
+            grid = vol.bricked_grid()
+            flags |= nat.CJX_GRID_BRICKED
+    else:
+        grid, grad_shape = vol.fourier_voxel_grid, tuple(vol.shape)
+        if integ.use_bricked_layout:
+            grid = vol.bricked_grid()
+            flags |= nat.CJX_GRID_BRICKED
     py, px = cfg.padded_shape
     desc = nat.make_desc(vol.shape[0], py, px, flags, integ.fill_value)
     obs_f = observed if observed_is_fourier else observed_to_fourier(observed)
@@ -156,7 +163,7 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
     if sort_orientations:
         order = torch.as_tensor(orientation_order(params[:, 0:9].reshape(-1, 3, 3)), device=dev)
     grads = torch.empty((n, nat.GRAD_DOUBLES), dtype=torch.float64, device=dev)
-    gg = torch.zeros(vol.shape, dtype=torch.complex64, device=dev) if grid_grad else None
+    gg = torch.zeros(grad_shape, dtype=torch.complex64, device=dev) if grid_grad else None
     ws = torch.empty(max(nat.loss_workspace_size(desc, n), 1), dtype=torch.uint8, device=dev)
     nat.slice_ctf_loss_grad(desc, grid, pd, obs_f, grads, gg, ws, order=order)
     g = grads.cpu().numpy()

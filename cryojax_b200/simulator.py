@@ -232,12 +232,20 @@ class FourierGaussian:
         self.amplitude = _arr(amplitude)
         self.b_factor = _arr(b_factor)
 
+    def __call__(self, frequency_grid):
+        """amplitude * exp(-b |k|^2 / 4) on a (..., 2) frequency grid (cycles / A)."""
+        k2 = np.sum(np.square(np.asarray(frequency_grid, np.float64)), axis=-1)
+        return self.amplitude * np.exp(-0.25 * self.b_factor * k2)
+
 
 class Constant:
     """A constant envelope (RELION's scale factor alone).  cryojax/ndimage/operators/_base_operator.py:53-67."""
 
     def __init__(self, value):
         self.value = _arr(value)
+
+    def __call__(self, frequency_grid=None, *args, **kwargs):
+        return self.value
 
 
 def _envelope_amp_b(envelope):
@@ -691,12 +699,13 @@ class FourierSliceExtraction:
 
     def run(self, volume: FourierVoxelGridVolume, image_config: BasicImageConfig, params: np.ndarray | None,
             flags: int, *, params_device=None, out=None, workspace=None, stream=None, images_per_chunk=0,
-            n=None, order=None):
+            n=None, order=None, filter=None):
         """Launch the batched kernel; returns a complex64 [n, Py, Px//2+1] CUDA tensor.
 
         ``params`` (host float64 [n, 32]) is copied to the device unless
         ``params_device`` is given.  ``out`` and ``workspace`` are allocated
-        when not supplied.
+        when not supplied.  ``filter`` (an AbstractFilter or array over the
+        output grid) is multiplied in inside the kernel's epilogue.
         """
         torch = _torch()
         n_vol = volume.shape[0]
@@ -717,7 +726,16 @@ class FourierSliceExtraction:
             workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=grid.device)
         if order is not None and not isinstance(order, torch.Tensor):
             order = torch.as_tensor(np.asarray(order, np.int32), device=grid.device)
-        nat.slice_ctf_forward(desc, grid, params_device, out, workspace if ws_bytes else None, stream, order)
+        fdev = None
+        if filter is not None:
+            arr = filter.get() if hasattr(filter, "get") else filter
+            fdev = torch.as_tensor(np.asarray(arr) if not isinstance(arr, torch.Tensor) else arr,
+                                   dtype=torch.float32, device=grid.device).contiguous()
+            if tuple(fdev.shape) != tuple(out.shape[-2:]):
+                raise ValueError(f"Found that the `filter` was shape {tuple(fdev.shape)}, but expected it to be "
+                                 f"shape {tuple(out.shape[-2:])} (the padded Fourier image).")
+        nat.slice_ctf_forward(desc, grid, params_device, out, workspace if ws_bytes else None, stream, order,
+                              filter=fdev)
         return out
 
     def integrate(self, volume_representation: FourierVoxelGridVolume, image_config: BasicImageConfig,
@@ -840,31 +858,38 @@ class AbstractImageModel:
     def get_image_config(self):
         return self.image_config
 
-    def compute_fourier_image(self, rng_key=None, *, out=None, workspace=None, stream=None, params_device=None):
-        """One launch for the whole batch: rotate -> integrate -> CTF -> translate.
+    def compute_fourier_image(self, rng_key=None, *, out=None, workspace=None, stream=None, params_device=None,
+                              filter=None):
+        """One launch for the whole batch: rotate -> integrate -> CTF -> translate (-> filter).
 
-        cryojax/simulator/_image_model/base_image_model.py:297-328.
+        cryojax/simulator/_image_model/base_image_model.py:297-328; ``filter``
+        is postprocess's Fourier filter, fused into the same launch.
         """
         params = self.image_params()
         img = self.volume_integrator.run(self.volume_parametrization.get_representation(), self.image_config,
                                          params, self._flags(), out=out, workspace=workspace, stream=stream,
-                                         params_device=params_device)
+                                         params_device=params_device, filter=filter)
         return img if self.batch_size is not None else img[0]
 
     def simulate(self, rng_key=None, *, removes_padding: bool = True, outputs_real_space: bool = True, mask=None,
                  filter=None):
-        """cryojax/simulator/_image_model/base_image_model.py:68-105."""
-        if mask is not None or filter is not None:
-            raise NotImplementedError("masks and filters are not implemented on the device")
-        fourier_image = self.compute_fourier_image(rng_key)
+        """cryojax/simulator/_image_model/base_image_model.py:68-158.
+
+        ``filter`` (over the padded rfft grid) is multiplied into the Fourier
+        image inside the device launch; ``mask`` multiplies the real-space
+        image after the inverse transform, crop and normalisation.  Without
+        ``removes_padding`` neither is applied (as in the reference).
+        """
         from . import _postprocess
 
         cfg = self.image_config
-        if removes_padding:
-            return _postprocess.postprocess(fourier_image, cfg.shape, cfg.padded_shape,
-                                            outputs_real_space=outputs_real_space,
-                                            normalizes_signal=self.normalizes_signal)
-        return _postprocess.irfftn(fourier_image, cfg.padded_shape) if outputs_real_space else fourier_image
+        if not removes_padding:
+            fourier_image = self.compute_fourier_image(rng_key)
+            return _postprocess.irfftn(fourier_image, cfg.padded_shape) if outputs_real_space else fourier_image
+        fourier_image = self.compute_fourier_image(rng_key, filter=filter)
+        return _postprocess.postprocess(fourier_image, cfg.shape, cfg.padded_shape,
+                                        outputs_real_space=outputs_real_space,
+                                        normalizes_signal=self.normalizes_signal, mask=mask)
 
 
 class LinearImageModel(AbstractImageModel):

@@ -76,7 +76,8 @@ extern "C" {
  * (cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:148-183,
  * 453-462, 531-534; cryojax/ndimage/_map_coordinates.py:126-142, 217-250).
  * desc->n stays the voxel grid's side N.  Forward, multi, no-alloc and
- * search entry points; not cjx_slice_ctf_loss_grad (CJX_ERR_UNSUPPORTED).  */
+ * search entry points, and cjx_slice_ctf_loss_grad (C order or bricked;
+ * grid_grad is then the (N + 2)^3 C-order coefficient gradient).           */
 #define CJX_GRID_SPLINE (1u << 6)
 /* EwaldSphereExtraction instead of FourierSliceExtraction
  * (cryojax/simulator/_volume_integrator/fourier_voxel_extract.py:225-516):
@@ -186,6 +187,19 @@ typedef struct cjx_image_grads {
                          pose parameters on the host                         */
   double reserved[6];
 } cjx_image_grads;
+
+/* cjx_slice_ctf_forward with a Fourier-space filter fused into the output
+ * epilogue: every output entry [y][x] is multiplied by filter[y][x]
+ * (float32, device; the output's own layout: [Py][Px/2+1], or [Py][Px]
+ * for the Ewald sphere's full spectrum).  This is
+ * AbstractImageModel.postprocess's `filter` applied to the Fourier image
+ * (cryojax/simulator/_image_model/base_image_model.py:107-158) before the
+ * inverse transform, e.g. cryojax.ndimage's LowpassFilter / HighpassFilter
+ * / CustomFilter arrays.  filter = NULL is cjx_slice_ctf_forward.         */
+CJX_API int cjx_slice_ctf_forward_filtered(const cjx_slice_desc* desc, const void* grid,
+                                           const cjx_image_params* params, const int32_t* order,
+                                           int64_t n_images, const float* filter, void* out,
+                                           void* workspace, size_t workspace_bytes, void* stream);
 
 /* Workspace for cjx_slice_ctf_loss_grad (same per-image need as the
  * forward's resize path).                                                  */

@@ -875,26 +875,35 @@ def _compute_fourier_image_ewald(grid, rotated, spec, outputs_integral, simulate
     return img
 
 
-def postprocess(fourier_image, spec: ImageSpec, *, outputs_real_space=True, normalizes_signal=False):
-    """AbstractImageModel.postprocess without mask or filter.
+def postprocess(fourier_image, spec: ImageSpec, *, outputs_real_space=True, normalizes_signal=False, mask=None,
+                filter=None):
+    """AbstractImageModel.postprocess with optional mask and filter arrays.
 
-    cryojax/simulator/_image_model/base_image_model.py:107-158, 184-192.
+    cryojax/simulator/_image_model/base_image_model.py:107-158, 184-192:
+    filter (times the padded Fourier image) -> irfftn -> crop -> normalise
+    -> mask (times the real-space image).
     """
-    if spec.padded_shape == spec.shape and not normalizes_signal:
+    if filter is not None:
+        fourier_image = fourier_image * filter
+    if mask is None and spec.padded_shape == spec.shape and not normalizes_signal:
         return irfftn(fourier_image, s=spec.shape) if outputs_real_space else fourier_image
     image = irfftn(fourier_image, s=spec.padded_shape)
     if spec.padded_shape != spec.shape:
         image = crop_to_shape(image, spec.shape)
     if normalizes_signal:
         image = (image - image.mean()) / image.std()
+    if mask is not None:
+        image = image * mask
     return image if outputs_real_space else rfftn(image)
 
 
-def simulate(grid, frequency_slice, spec: ImageSpec, *, outputs_real_space=True, removes_padding=True, **kw):
+def simulate(grid, frequency_slice, spec: ImageSpec, *, outputs_real_space=True, removes_padding=True,
+             mask=None, filter=None, normalizes_signal=False, **kw):
     """AbstractImageModel.simulate.  base_image_model.py:68-105, 194-213."""
     fourier_image = compute_fourier_image(grid, frequency_slice, spec, **kw)
     if removes_padding:
-        return postprocess(fourier_image, spec, outputs_real_space=outputs_real_space)
+        return postprocess(fourier_image, spec, outputs_real_space=outputs_real_space, mask=mask, filter=filter,
+                           normalizes_signal=normalizes_signal)
     return irfftn(fourier_image, s=spec.padded_shape) if outputs_real_space else fourier_image
 
 
@@ -919,6 +928,16 @@ def gaussian_white_log_likelihood(simulated, observed, variance):
     """cryojax/simulator/_noise_model/gaussian_noise_model.py:207-255."""
     r = simulated - observed
     return float(np.sum(-(np.abs(r) ** 2 / (2 * variance) + np.log(2 * np.pi * variance) / 2)))
+
+
+def gaussian_colored_log_likelihood(simulated_fourier, observed_fourier, variance_grid, n_pixels):
+    """cryojax/simulator/_noise_model/gaussian_noise_model.py:334-397: per-mode
+    |r|^2 / (2 v) + log(2 pi v) / 2 with v = n_pixels * variance_fn(freqs), summed over
+    the rfft half plane with column 0 (rows >= 1) once and the other columns twice,
+    divided by n_pixels and negated."""
+    v = n_pixels * np.asarray(variance_grid, np.float64)
+    per_mode = np.abs(simulated_fourier - observed_fourier) ** 2 / (2 * v) + np.log(2 * np.pi * v) / 2
+    return float(-(per_mode[1:, 0].sum() + 2 * per_mode[:, 1:].sum()) / n_pixels)
 
 
 def normalize_image(image):

@@ -194,15 +194,3 @@ def test_exhaustive_search_on_a_spline_volume(cuda_device):
     assert np.abs(got - ref_scores).max() <= 5e-5
     np.testing.assert_array_equal(res.best_orientation, true_idx)
     np.testing.assert_array_equal(ref_best, true_idx)
-
-
-def test_spline_volume_rejects_gradients(cuda_device):
-    from cryojax_b200 import gradients
-    from cryojax_b200 import simulator as S
-
-    _, grid, fs = make_volume(16, 20, seed=2)
-    specs = random_specs(2, seed=3, shape=(16, 16))
-    pose, tt, cfg = specs_to_model_args(specs)
-    model = S.make_image_model(_spline_volume(grid), cfg, pose, tt)
-    with pytest.raises(NotImplementedError):
-        gradients.squared_residual_and_grad(model, np.zeros((2, 16, 16), np.float32))
