@@ -41,3 +41,51 @@ def test_masks():
     np.testing.assert_allclose(sq[15, 15], 0.25)  # both edges: product
     img = np.ones((21, 21))
     np.testing.assert_array_equal(T.CircularCosineMask(g, 5.0, 2.0)(img), m)
+
+
+def test_cylinder_rectangle_and_box_masks():
+    g = T.make_coordinate_grid((21, 21), 1.0)
+    band = T.Cylindrical2DCosineMask(g, radius=3.0, rolloff_width=2.0).get()
+    # a horizontal band |y| < 3 (x free), raised-cosine edge to |y| = 5
+    assert band[10, 0] == 1.0 and band[10 + 4, 5] == 0.5 and band[10 + 5, 5] == 0.0
+    rot = T.Cylindrical2DCosineMask(g, radius=3.0, rolloff_width=2.0, in_plane_rotation_angle=90.0).get()
+    np.testing.assert_allclose(rot, band.T, atol=1e-12)  # rotated by 90 degrees: a vertical band
+    rect = T.Rectangular2DCosineMask(g, x_width=10.0, y_width=4.0, rolloff_width=2.0).get()
+    assert rect[10, 15] == 1.0 and rect[10, 16] == 0.5 and rect[12, 10] == 1.0 and rect[13, 10] == 0.5
+    np.testing.assert_allclose(rect[13, 16], 0.25)
+    g3 = T.make_coordinate_grid((9, 11, 13), 1.0)
+    assert g3.shape == (9, 11, 13, 3) and g3[0, 0, 0].tolist() == [-6.0, -5.0, -4.0]
+    box = T.Rectangular3DCosineMask(g3, 6.0, 4.0, 2.0, 2.0).get()
+    assert box[4, 5, 6] == 1.0 and box[4, 5, 10] == 0.5  # x = 4: halfway through the x edge
+    np.testing.assert_allclose(box[6, 8, 10], 0.125)  # three edges at their midpoints
+    sph = T.SphericalCosineMask(g3, 3.0, 2.0).get()
+    assert sph[4, 5, 6] == 1.0 and sph[4, 5, 10] == 0.5
+    inv = T.InverseSincMask(g).get()
+    np.testing.assert_allclose(inv[10, 10], 1.0)
+    np.testing.assert_allclose(inv[10, 15], 1.0 / np.sinc(5 / 21))
+
+
+def test_whitening_filter():
+    rng = np.random.default_rng(0)
+    white = rng.standard_normal((64, 48, 48)) * 3.0
+    f = T.WhiteningFilter(white).get()
+    assert f.shape == (48, 25) and f[0, 0] == 0.0 and f[24, 24] == 0.0
+    inner = f[1:20, 1:20]
+    np.testing.assert_allclose(inner.mean(), 1 / 3.0, rtol=0.03)  # white noise of std 3: flat 1/3
+    sq = T.WhiteningFilter(white, outputs_squared=True).get()
+    np.testing.assert_allclose(sq[1:20, 1:20].mean(), 1 / 9.0, rtol=0.05)
+    # a coloured spectrum: the filter whitens it (a gentle one: the right-closed bins attribute each ring's
+    # mean power to its outer edge, which under-whitens steep spectra by about slope x half a bin)
+    k = np.linalg.norm(T.make_frequency_grid((48, 48)), axis=-1)
+    amp = np.exp(-4 * k**2)
+    noise = np.fft.irfftn(np.fft.rfftn(rng.standard_normal((64, 48, 48)), axes=(1, 2)) * amp, s=(48, 48),
+                          axes=(1, 2))
+    wf = T.WhiteningFilter(noise).get()
+    whitened = np.fft.rfftn(noise, axes=(1, 2)) * wf
+    p = (np.abs(whitened) ** 2).mean(axis=0)
+    ring = lambda r0: p[(k > r0) & (k < r0 + 0.05)].mean()
+    assert abs(ring(0.05) / ring(0.25) - 1.0) < 0.1
+    resized = T.WhiteningFilter(white, shape=(32, 32)).get()
+    assert resized.shape == (32, 17) and resized[0, 0] == 0.0
+    nearest = T.WhiteningFilter(white, interpolation_mode="nearest").get()
+    assert abs(nearest[1:20, 1:20].mean() * 3.0 - 1.0) < 0.03
