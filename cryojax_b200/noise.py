@@ -110,7 +110,7 @@ class GaussianColoredNoiseModel(GaussianWhiteNoiseModel):
         pixel = float(np.ravel(self.image_model.image_config.pixel_size)[0])
         v = np.broadcast_to(np.asarray(self.variance_fn(make_frequency_grid(shape, pixel)), np.float64),
                             (shape[0], shape[1] // 2 + 1))
-        return torch.as_tensor(np.ascontiguousarray(v), device=dev)
+        return torch.as_tensor(np.array(v, dtype=np.float64), device=dev)
 
     def _variance_grid(self, dev):
         return self._variance_on(self.image_model.image_config.padded_shape, dev)

@@ -326,7 +326,7 @@ class FourierVoxelGridVolume:
             g = torch.as_tensor(np.asarray(g))
         if g.dim() != 3 or len(set(g.shape)) != 1:
             raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
-        self.fourier_voxel_grid = g
+        self.fourier_voxel_grid = g.contiguous()  # the kernels read C order
         self.rotation = rotation  # AbstractPose attached by rotate_to_pose
         self._bricked = bricked   # device re-layouts for the gather (built on first use)
         self._pairs = pairs
@@ -389,7 +389,7 @@ class FourierVoxelSplineVolume:
             c = torch.as_tensor(np.asarray(c))
         if c.dim() != 3 or len(set(c.shape)) != 1:
             raise AttributeError("Only cubic boxes are supported for fourier slice extraction.")
-        self.spline_coefficients = c
+        self.spline_coefficients = c.contiguous()  # the kernels read C order
         self.rotation = rotation
         self._bricked = bricked
         self._pairs = pairs

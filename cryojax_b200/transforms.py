@@ -316,7 +316,7 @@ class WhiteningFilter(AbstractFilter):
             spectra.append(p)
         power = interpolate_radial_average_on_grid(np.mean(spectra, axis=0), bins, radial, interpolation_mode)
         if shape is not None:
-            real = np.fft.fftshift(np.fft.irfftn(power, s=(ny, nx)))
+            real = np.fft.fftshift(np.fft.irfftn(power, s=(ny, nx), axes=(0, 1)))
             power = np.fft.rfftn(np.fft.ifftshift(_edge_resize(real, tuple(shape)))).real
             power = np.where(power < 0, 0.0, power)
             new_shape = tuple(shape)

@@ -30,7 +30,7 @@ def _fd(f, h):
     return (f(h) - f(-h)) / (2 * h)
 
 
-def _setup(seed, n=2, box=24):
+def _setup(seed, n=2, box=32):  # N = 64, images 32^2: the loss gradient's register-FFT sizes (32 R)
     rng = np.random.default_rng(seed)
     _, grid, fs = make_volume(box, 50, seed=seed)
     coef = O.compute_spline_coefficients(grid)
