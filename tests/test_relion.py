@@ -199,3 +199,40 @@ def test_mrc_round_trips(tmp_path):
         mrc.write_image_to_mrc(v[0], 2.0, tmp_path / "i.mrc")
     with pytest.raises(OSError):
         mrc.write_image_stack_to_mrc(v, 2.0, tmp_path / "s.mrc")
+
+
+def test_star_edge_cases(tmp_path):
+    p = tmp_path / "e.star"
+    p.write_text("# comment\n\ndata_general\n\n_rlnImageSize 64\n_rlnComment 'two words'\n\n"
+                 "data_particles\n\nloop_\n_rlnA #1\n_rlnName #2\n1\t\"a b\"\n2\tc\n\n")
+    d = star.read_starfile(p)
+    assert d["general"]["rlnImageSize"].tolist() == [64]
+    assert d["particles"]["rlnName"].tolist() == ["a b", "c"] and d["particles"]["rlnA"].dtype == np.int64
+    star.write_starfile(d, tmp_path / "o.star")
+    back = star.read_starfile(tmp_path / "o.star")
+    assert back["particles"]["rlnName"].tolist() == ["a b", "c"]
+    bad = tmp_path / "bad.star"
+    bad.write_text("data_x\nloop_\n_rlnA #1\n_rlnB #2\n1 2 3\n")
+    with pytest.raises(ValueError):
+        star.read_starfile(bad)
+    with pytest.raises(OSError):
+        star.read_starfile(tmp_path / "x.txt")
+
+
+def test_mrc_big_endian_and_modes(tmp_path):
+    import struct
+
+    data = np.arange(2 * 3 * 4, dtype=">i2").reshape(2, 3, 4)
+    header = bytearray(1024)
+    struct.pack_into(">10i", header, 0, 4, 3, 2, 1, 0, 0, 0, 4, 3, 2)
+    struct.pack_into(">3f", header, 40, 8.0, 6.0, 4.0)
+    struct.pack_into(">2i", header, 88, 1, 0)
+    header[208:212] = b"MAP "
+    header[212:216] = b"\x11\x11\x00\x00"
+    (tmp_path / "be.mrc").write_bytes(bytes(header) + data.tobytes())
+    got, d = mrc.read_array_from_mrc(tmp_path / "be.mrc", loads_grid_spacing=True)
+    np.testing.assert_array_equal(got, data.astype(np.float64))
+    assert d == 2.0
+    (tmp_path / "short.mrc").write_bytes(bytes(header) + data.tobytes()[:10])
+    with pytest.raises(ValueError):
+        mrc.read_array_from_mrc(tmp_path / "short.mrc")
