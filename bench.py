@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the mixed-size batch measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the loss-gradient measurement")
     ap.add_argument("--no-search", action="store_true", help="skip the pose-search (learned vs grid) measurement")
-    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline", "ewald"], default=None,
+    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline", "ewald", "render"], default=None,
                     help="run one small workload of that kernel family (for a profiler), print its timing, exit")
     ap.add_argument("--no-refine", action="store_true",
                     help="skip the search + refinement measurement (320^2 images, N=512)")
@@ -1002,6 +1002,17 @@ def run_probe(kind, seed):
         ps = PoseSearch(grid.rotation_matrices())
         ms = ev_time(lambda: ps.run(model, obs))
         out["plain_exhaustive_8_images"] = {"ms": ms, "candidates_per_s": 8 * grid.size / (ms / 1000.0)}
+    elif kind == "render":
+        # GaussianMixtureRenderFn: 50k atoms x 5 Gaussians into 256^3 at 1 A (two warm-up launches, one timed)
+        rng = np.random.default_rng(seed)
+        pos = torch.as_tensor(rng.uniform(-100, 100, (50000, 3)), dtype=torch.float32, device=dev)
+        amp = torch.as_tensor(rng.uniform(0.1, 1.0, (50000, 5)), dtype=torch.float32, device=dev)
+        var = torch.as_tensor(rng.uniform(0.2, 2.0, (50000, 5)), dtype=torch.float32, device=dev)
+        grid = torch.empty((256, 256, 256), dtype=torch.float32, device=dev)
+        for _ in range(2):
+            nat.render_gaussians(grid.shape, 1.0, pos, amp, var, out=grid)
+        ms = ev_time(lambda: nat.render_gaussians(grid.shape, 1.0, pos, amp, var, out=grid))
+        out["render_50k_atoms_256^3"] = {"ms": ms, "atoms_per_s": 50000 / (ms / 1000.0)}
     elif kind == "ewald":
         from cryojax_b200 import simulator as S
         from cryojax_b200 import synthetic

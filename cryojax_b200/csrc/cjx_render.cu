@@ -19,7 +19,6 @@
 
 namespace cjx {
 
-constexpr int kRenderMaxG = 8;    // Gaussians per atom
 constexpr int kRenderChunk = 64;  // sub-box side staged in shared memory
 constexpr int kRenderThreads = 128;
 
@@ -28,18 +27,24 @@ struct RenderGeom {
   float dx, cutoff;
 };
 
+// G (Gaussians per atom) is a template parameter so the per-Gaussian
+// constants and the hoisted y * z products stay in registers.  The splat
+// gives each warp whole (z, y) rows of the sub-box and its lanes the x
+// positions: one integer division per row, G multiply-adds per voxel.
+template <int G>
 __global__ void __launch_bounds__(kRenderThreads)
     k_render_gaussians(const float* __restrict__ positions, const float* __restrict__ amplitudes,
                        const float* __restrict__ variances, int64_t n_atoms, float* __restrict__ grid, RenderGeom rg) {
-  __shared__ float ix[kRenderMaxG][kRenderChunk];
-  __shared__ float iy[kRenderMaxG][kRenderChunk];
-  __shared__ float iz[kRenderMaxG][kRenderChunk];
-  const int G = rg.g;
+  __shared__ float ix[G][kRenderChunk];
+  __shared__ float iy[G][kRenderChunk];
+  __shared__ float iz[G][kRenderChunk];
   const float dx = rg.dx;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n_warps = blockDim.x >> 5;
   for (int64_t atom = blockIdx.x; atom < n_atoms; atom += gridDim.x) {
     const float p[3] = {positions[3 * atom], positions[3 * atom + 1], positions[3 * atom + 2]};
-    float s[kRenderMaxG], pref[kRenderMaxG];
+    float s[G], pref[G];
     float var_max = 0.f;
+#pragma unroll
     for (int g = 0; g < G; ++g) {
       const float v = variances[atom * G + g];
       var_max = fmaxf(var_max, v);
@@ -51,6 +56,7 @@ __global__ void __launch_bounds__(kRenderThreads)
     const int dims[3] = {rg.nx, rg.ny, rg.nz};
     int lo[3], hi[3];
     bool empty = false;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
       // clamped in floating point first, so atoms far outside (or NaN) convert safely: lo in [0, D], hi in [-1, D-1]
       const float half = (float)(dims[a] / 2);
@@ -67,25 +73,32 @@ __global__ void __launch_bounds__(kRenderThreads)
         for (int x0 = lo[0]; x0 <= hi[0]; x0 += kRenderChunk) {
           const int wx = min(kRenderChunk, hi[0] - x0 + 1);
           __syncthreads();  // the previous sub-box's integrals are no longer read
-          for (int e = threadIdx.x; e < G * kRenderChunk * 3; e += blockDim.x) {
-            const int a = e / (G * kRenderChunk), r = e % (G * kRenderChunk);
-            const int g = r / kRenderChunk, i = r % kRenderChunk;
+          for (int e = threadIdx.x; e < 3 * kRenderChunk; e += blockDim.x) {
+            const int a = e / kRenderChunk, i = e % kRenderChunk;
             const int w = a == 0 ? wx : (a == 1 ? wy : wz);
             if (i >= w) continue;
             const int idx = (a == 0 ? x0 : (a == 1 ? y0 : z0)) + i;
-            const float left = (float)(idx - dims[a] / 2) * dx - 0.5f * dx;
-            const float d = left - p[a];
-            float v = erff(s[g] * (d + dx)) - erff(s[g] * d);
-            if (a == 0) v *= pref[g];
-            (a == 0 ? ix : (a == 1 ? iy : iz))[g][i] = v;
+            const float d = (float)(idx - dims[a] / 2) * dx - 0.5f * dx - p[a];
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+              float v = erff(s[g] * (d + dx)) - erff(s[g] * d);
+              if (a == 0) v *= pref[g];
+              (a == 0 ? ix : (a == 1 ? iy : iz))[g][i] = v;
+            }
           }
           __syncthreads();
-          const int n = wx * wy * wz;
-          for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            const int x = e % wx, y = (e / wx) % wy, z = e / (wx * wy);
-            float v = 0.f;
-            for (int g = 0; g < G; ++g) v = fmaf(ix[g][x] * iy[g][y], iz[g][z], v);
-            atomicAdd(grid + ((size_t)(z0 + z) * rg.ny + (y0 + y)) * rg.nx + (x0 + x), v);
+          for (int zy = warp; zy < wz * wy; zy += n_warps) {
+            const int z = zy / wy, y = zy - z * wy;
+            float cyz[G];
+#pragma unroll
+            for (int g = 0; g < G; ++g) cyz[g] = iy[g][y] * iz[g][z];
+            float* row = grid + ((size_t)(z0 + z) * rg.ny + (y0 + y)) * rg.nx + x0;
+            for (int x = lane; x < wx; x += 32) {
+              float v = 0.f;
+#pragma unroll
+              for (int g = 0; g < G; ++g) v = fmaf(ix[g][x], cyz[g], v);
+              atomicAdd(row + x, v);
+            }
           }
         }
       }
@@ -105,7 +118,18 @@ int launch_render_gaussians(const cjx_render_desc* d, const float* positions, co
   RenderGeom rg{d->nz, d->ny, d->nx, d->n_gaussians, d->voxel_size, d->cutoff_sigmas > 0.f ? d->cutoff_sigmas : 7.f};
   const int blocks = (int)std::min<int64_t>(n_atoms, (int64_t)sms * 16);
   prof_begin(stream);
-  k_render_gaussians<<<blocks, kRenderThreads, 0, stream>>>(positions, amplitudes, variances, n_atoms, grid, rg);
+  switch (rg.g) {
+#define CJX_RENDER_CASE(G)                                                                                        \
+  case G:                                                                                                         \
+    k_render_gaussians<G><<<blocks, kRenderThreads, 0, stream>>>(positions, amplitudes, variances, n_atoms, grid, \
+                                                                 rg);                                            \
+    break;
+    CJX_RENDER_CASE(1) CJX_RENDER_CASE(2) CJX_RENDER_CASE(3) CJX_RENDER_CASE(4)
+    CJX_RENDER_CASE(5) CJX_RENDER_CASE(6) CJX_RENDER_CASE(7) CJX_RENDER_CASE(8)
+#undef CJX_RENDER_CASE
+    default:
+      return fail(CJX_ERR_INVALID_ARGUMENT, "n_gaussians must be in [1, CJX_RENDER_MAX_GAUSSIANS]");
+  }
   prof_end("k_render_gaussians", stream);
   return check_cuda(cudaGetLastError(), "k_render_gaussians launch");
 }
