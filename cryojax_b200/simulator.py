@@ -282,9 +282,22 @@ def _torch():
     return torch
 
 
-def _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype):
+def fftn_native(x):
+    """numpy.fft.fftn of a complex64 CUDA tensor [nz, ny, nx] with the library's batched warp FFTs
+    (cjx_fft_c2c): one pass per axis, that axis moved last (one contiguous copy) for its pass."""
+    for axis in (2, 1, 0):
+        x = nat.fft_c2c(x.movedim(axis, -1).contiguous(), -1).movedim(-1, axis)
+    return x.contiguous()
+
+
+def _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype, fft_backend="native"):
     """pad -> ifftshift -> fftn -> fftshift, complex64 on ``device``
-    (cryojax/simulator/_volume/representations/voxel_volume.py:69-119, 163-203)."""
+    (cryojax/simulator/_volume/representations/voxel_volume.py:69-119, 163-203).
+
+    ``fft_backend="native"``: the 3-D transform runs on this library's FFT
+    kernels in single precision; ``"torch"``: torch.fft in ``fft_dtype``
+    (float64 by default), for comparison.
+    """
     torch = _torch()
     if pad_scale < 1.0:
         raise ValueError("`pad_scale` must be greater than 1.0")
@@ -306,6 +319,11 @@ def _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtyp
             lr = (pad // 2, pad // 2)
         pads.extend(lr)
     padded = torch.nn.functional.pad(real, pads, mode="constant", value=0.0)
+    if fft_backend == "native":
+        ft = fftn_native(torch.fft.ifftshift(padded).to(torch.complex64))
+        return torch.fft.fftshift(ft).contiguous()
+    if fft_backend != "torch":
+        raise ValueError("fft_backend must be 'native' or 'torch'")
     ft = torch.fft.fftn(torch.fft.ifftshift(padded))
     return torch.fft.fftshift(ft).to(torch.complex64).contiguous()
 
@@ -353,13 +371,14 @@ class FourierVoxelGridVolume:
 
     @classmethod
     def from_real_voxel_grid(cls, real_voxel_grid, *, pad_scale: float = 1.0, pad_mode: str = "constant",
-                             device: str = "cuda", fft_dtype=None):
+                             device: str = "cuda", fft_dtype=None, fft_backend: str = "native"):
         """pad -> ifftshift -> fftn -> fftshift, as the reference (voxel_volume.py:69-119).
 
-        The FFT runs in float64 on ``device`` and the grid is stored as
-        complex64 (one-time volume preparation, not part of the image path).
+        The 3-D FFT runs on ``device`` with this library's FFT kernels
+        (``fft_backend="torch"``: torch.fft in float64) and the grid is stored
+        as complex64 (one-time volume preparation).
         """
-        return cls(_centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype))
+        return cls(_centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype, fft_backend))
 
     def rotate_to_pose(self, pose: AbstractPose, inverse: bool = False):
         """Attach the pose (the frequency slice is rotated inside the kernel)."""
@@ -416,10 +435,10 @@ class FourierVoxelSplineVolume:
 
     @classmethod
     def from_real_voxel_grid(cls, real_voxel_grid, *, pad_scale: float = 1.0, pad_mode: str = "constant",
-                             device: str = "cuda", fft_dtype=None):
+                             device: str = "cuda", fft_dtype=None, fft_backend: str = "native"):
         """Fourier grid as FourierVoxelGridVolume.from_real_voxel_grid, then its
         spline coefficients on the device (voxel_volume.py:163-203)."""
-        grid = _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype)
+        grid = _centred_fourier_grid(real_voxel_grid, pad_scale, pad_mode, device, fft_dtype, fft_backend)
         return cls(nat.spline_coefficients(grid))
 
     @classmethod
