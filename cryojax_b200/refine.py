@@ -70,12 +70,14 @@ def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_s
         raise NotImplementedError("refinement needs padded_shape == shape")
     vol = image_model.volume_parametrization.get_representation()
     integ = image_model.volume_integrator
-    if not hasattr(vol, "fourier_voxel_grid"):
-        raise NotImplementedError("gradients through spline volumes are not implemented on the device")
-    dev = vol.fourier_voxel_grid.device
+    if not integ.is_projection_approximation:
+        raise NotImplementedError("refinement through the Ewald sphere is not implemented on the device")
+    dev = vol.device
     params = image_model.image_params().copy()
     n = params.shape[0]
     flags = image_model._flags() | integ._base_flags() | nat.CJX_GRID_BRICKED
+    if hasattr(vol, "spline_coefficients"):  # FourierVoxelSplineVolume: cubic-spline samples and gradients
+        flags |= nat.CJX_GRID_SPLINE
     grid = vol.bricked_grid()
     py, px = cfg.padded_shape
     desc = nat.make_desc(vol.shape[0], py, px, flags, integ.fill_value)
