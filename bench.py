@@ -1233,6 +1233,26 @@ def main():
                "path": "HostStreamingSimulator: pinned host params -> H2D -> cjx_slice_ctf_forward -> D2H "
                        "into pinned host images, 2 streams, 2048-image sub-batches"}
         del oh, ph, sim
+        try:  # the host link's own device-to-host rate: the e2e roof when the images dominate the traffic
+            nbytes = 1 << 30
+            src = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            dst = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            for _ in range(2):
+                dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(4):
+                dst.copy_(src, non_blocking=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            link_gbs = 4 * nbytes / (e0.elapsed_time(e1) * 1e6)
+            d2h_gbs = e2e["d2h_bytes_per_step"] * e_steps / (et_ms * 1e6)
+            e2e["host_link"] = {"d2h_probe_gbs": link_gbs, "d2h_achieved_gbs": d2h_gbs,
+                                "frac": d2h_gbs / link_gbs,
+                                "probe": "4 x 1 GiB device -> pinned host copies, CUDA events"}
+            del src, dst
+        except Exception as e:  # measurement helper only
+            e2e["host_link"] = {"error": str(e)}
 
     # ---- mixed-size batch (configuration with four volume sizes)
     batched = None

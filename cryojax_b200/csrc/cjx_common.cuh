@@ -624,6 +624,75 @@ __device__ __forceinline__ float2 envelope_translate(float2 v, int i, int j, int
   return v;
 }
 
+// exp(-2 pi i ph), ph reduced to [-1/2, 1/2] in double before the float sincospi.
+__device__ __forceinline__ float2 phase_factor(double ph) {
+  const float r = (float)(ph - rint(ph));
+  float s, co;
+  sincospif(2.0f * r, &s, &co);
+  return make_float2(co, -s);
+}
+
+// The epilogue of one output column j (the column pass's unit of work),
+// with the per-column terms hoisted:
+//   * the translation factor is separable, exp(-2 pi i qx tx) exp(-2 pi i
+//     qy ty): the column factor is computed once, the row factors come from
+//     a per-CTA table (row_phase[i]);
+//   * chi / (2 pi) needs no angle: cos(2 theta) k^2 = qy^2 - qx^2 and
+//     sin(2 theta) k^2 = 2 qx qy, so
+//     chi / (2 pi) = (c_def df + c_sph k^2) k^2 + c_def (astig / 2)
+//                    ((qy^2 - qx^2) cos 2 alpha + 2 qx qy sin 2 alpha),
+//     the large first term in double, the astigmatic term in float.
+// Same values as apply_epilogue up to rounding.
+struct ColumnEpilogue {
+  double qx, qx2, c_dd;
+  float qxf, c_astig;
+  float2 col_phase;
+};
+
+__device__ __forceinline__ ColumnEpilogue column_epilogue(int j, uint32_t flags, const ImageConsts& c) {
+  ColumnEpilogue e;
+  e.qx = (double)j * c.qx_step;
+  e.qx2 = e.qx * e.qx;
+  e.qxf = (float)e.qx;
+  e.c_dd = c.c_def * c.defocus;
+  e.c_astig = (float)(c.c_def * c.half_astig);
+  e.col_phase = (flags & CJX_APPLY_TRANSLATION) ? phase_factor(e.qx * c.tx) : make_float2(1.f, 0.f);
+  return e;
+}
+
+__device__ __forceinline__ float2 apply_column_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
+                                                        const ImageConsts& c, const ColumnEpilogue& e,
+                                                        const float2* __restrict__ row_phase) {
+  v.x *= c.scale;
+  v.y *= c.scale;
+  if (flags & (CJX_APPLY_CTF | CJX_APPLY_ENVELOPE)) {
+    const double qy = (double)fft_index(i, py) * c.qy_step;
+    const double k2 = fma(qy, qy, e.qx2);
+    if (flags & CJX_APPLY_CTF) {
+      const float qyf = (float)qy;
+      const float astig = e.c_astig * fmaf(fmaf(qyf, qyf, -e.qxf * e.qxf), c.cos2a, 2.0f * e.qxf * qyf * c.sin2a);
+      const double arg = fma(fma(c.c_sph, k2, e.c_dd), k2, (double)astig - c.phase_cycles);
+      const float r = (float)(arg - rint(arg));
+      const float ctf = sinpif(2.0f * r);
+      v.x *= ctf;
+      v.y *= ctf;
+    }
+    if (flags & CJX_APPLY_ENVELOPE) {
+      const float en = c.env_amp * expf(-c.env_quarter_b * (float)k2);
+      v.x *= en;
+      v.y *= en;
+    }
+  }
+  if (flags & CJX_APPLY_TRANSLATION) {
+    const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
+    const bool self_conj = (ey && i == py / 2 && j == 0) || (ex && i == 0 && j == px / 2) ||
+                           (ey && ex && i == py / 2 && j == px / 2);
+    if (self_conj) return make_float2(0.f, 0.f);
+    v = cmul(v, cmul(e.col_phase, row_phase[i]));
+  }
+  return v;
+}
+
 __device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
                                                  const ImageConsts& c) {
   v.x *= c.scale;

@@ -111,15 +111,14 @@ __global__ void __launch_bounds__(kEwWarps * 32)
 // transforms in registers (cjx_fft.cuh); shared memory holds the twiddle
 // tables and the transposes, so loads and stores stay coalesced.
 // ---------------------------------------------------------------------------
+// z holds the row in the lane's bit-reversed order, loaded by the caller
+// before its table copy.
 template <int RN, int RP>
-__device__ __forceinline__ void ewald_row_reg(const float2* __restrict__ row, float2* __restrict__ dst, float2* buf,
+__device__ __forceinline__ void ewald_row_reg(float2 (&z)[RN], float2* __restrict__ dst, float2* buf,
                                               const float2* tabN, const float2* tabP, const LaneTwiddles& lt,
                                               int lane, const int* winx) {
   constexpr int px = 32 * RP;
   const int bl = brev5(lane);
-  float2 z[RN];
-#pragma unroll
-  for (int n1 = 0; n1 < RN; ++n1) z[n1] = row[32 * n1 + bl];
   warp_fft_reg<RN, +1>(z, tabN, lt, lane);
 #pragma unroll
   for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
@@ -150,21 +149,27 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2* tabP = tabN + n;
   float2* bufs = tabP + px;
   int* winx = reinterpret_cast<int*>(bufs + kWarps * stride);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kWarps + warp;
+  float2 z[RN];  // loaded first, so that the load latency overlaps the table copy
+  if (r < g.py) {
+    const float2* row = t1 + ((size_t)blockIdx.y * g.py + r) * g.ld1;
+    const int bl = brev5(lane);
+#pragma unroll
+    for (int n1 = 0; n1 < RN; ++n1) z[n1] = row[32 * n1 + bl];
+  }
   build_reg_twiddles(tabN, n);
   build_reg_twiddles(tabP, px);
   build_w32(w32);
   for (int m = threadIdx.x; m < px; m += blockDim.x) winx[m] = win_src(m, n, px, g.pad_left_x);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r = blockIdx.x * kWarps + warp;
   if (r >= g.py) return;
-  const float2* row = t1 + ((size_t)blockIdx.y * g.py + r) * g.ld1;
   float2* dst = t2 + ((size_t)blockIdx.y * g.py + r) * g.ld2;
   float2* buf = bufs + warp * stride;
   const LaneTwiddles lt = make_lane_twiddles(w32, lane);
   switch (rp) {
 #define CJX_EROW_CASE(RPV) \
-  case RPV: ewald_row_reg<RN, RPV>(row, dst, buf, tabN, tabP, lt, lane, winx); break;
+  case RPV: ewald_row_reg<RN, RPV>(z, dst, buf, tabN, tabP, lt, lane, winx); break;
     CJX_EROW_CASE(1) CJX_EROW_CASE(2) CJX_EROW_CASE(3) CJX_EROW_CASE(4) CJX_EROW_CASE(5)
     CJX_EROW_CASE(6) CJX_EROW_CASE(8) CJX_EROW_CASE(10) CJX_EROW_CASE(12) CJX_EROW_CASE(16)
 #undef CJX_EROW_CASE
@@ -187,25 +192,40 @@ __global__ void __launch_bounds__(kWarps * 32)
   __shared__ float2 w32[32];
   float2* tab = smem;
   float2* bufs = smem + py;  // columns [0, kWarps): own, [kWarps, 2 kWarps): mirrors
-  build_reg_twiddles(tab, py);
-  build_w32(w32);
   const int px = g.px;
   const bool ctf = (g.flags & CJX_APPLY_CTF) != 0;
   const int pitch = ctf ? g.pxh : px;
   const int j0 = blockIdx.x * kWarps;
   const int ncols = min(kWarps, pitch - j0);
   const float2* src = t2 + (size_t)blockIdx.y * py * g.ld2;
-  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
-    const int m = e / kWarps, jj = e % kWarps;
-    if (jj < ncols) {
-      bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld2 + j0 + jj];
-      if (ctf) bufs[(kWarps + jj) * stride + pad16(m)] = src[(size_t)m * g.ld2 + (px - j0 - jj) % px];
+  // staging: thread t moves column t % kWarps (and its mirror), rows
+  // t / kWarps + 32 q; the loads are issued before the table copy
+  static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
+  const int sj = threadIdx.x % kWarps, sm0 = threadIdx.x / kWarps;
+  const int cj = j0 + sj, cm = (px - j0 - sj) % px;
+  float2 st[R], sb[R];
+  if (sj < ncols) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      st[q] = src[(size_t)(sm0 + 32 * q) * g.ld2 + cj];
+      if (ctf) sb[q] = src[(size_t)(sm0 + 32 * q) * g.ld2 + cm];
+    }
+  }
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  if (sj < ncols) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      bufs[sj * stride + pad16(sm0 + 32 * q)] = st[q];
+      if (ctf) bufs[(kWarps + sj) * stride + pad16(sm0 + 32 * q)] = sb[q];
     }
   }
   const int64_t k = k0 + blockIdx.y;
   const int64_t img = order ? (int64_t)order[k] : k;
-  const ImageConsts c = load_image_consts(params + img, norm, py, px);
+  __shared__ ImageConsts sc;  // evaluated once per CTA
+  if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, py, px);
   __syncthreads();
+  const ImageConsts c = sc;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < ncols) {
     const LaneTwiddles lt = make_lane_twiddles(w32, lane);

@@ -5,7 +5,8 @@
 // out).  Radices 8, 4, 2, 3, 5 have hand-written butterflies, radix 7 uses
 // the twiddle table; a length with any other prime factor falls back to a
 // direct O(n^2) DFT.  Twiddles exp(-2 pi i m / n) are computed per launch in
-// double precision and stored as float2 in shared memory.
+// double precision and stored as float2 in shared memory.  The register FFTs
+// (n = 32 R) copy theirs from tables the compiler evaluates.
 //
 // Sign convention: DIR = -1 is the forward transform (numpy.fft.fft),
 // DIR = +1 the unnormalised inverse (n * numpy.fft.ifft).
@@ -273,7 +274,57 @@ constexpr double cos2pi(int m, int R) {
   return taylor_cos(x - 2 * kPi);
 }
 constexpr double sin2pi(int m, int R) { return cos2pi(m * 4 - R, 4 * R); }
+
+// Register-FFT twiddle tables, evaluated by the compiler: for each n = 32 R
+// with R in the register-FFT list, entries k1 * 32 + l = exp(-2 pi i brev5(l)
+// k1 / n) (the layout build_reg_twiddles fills), back to back in the order
+// of that list; then w32[m] = exp(-2 pi i m / 32).
+__host__ __device__ constexpr int reg_table_offset(int R) {
+  switch (R) {
+    case 1: return 0;
+    case 2: return 32;
+    case 3: return 96;
+    case 4: return 192;
+    case 5: return 320;
+    case 6: return 480;
+    case 8: return 672;
+    case 10: return 928;
+    case 12: return 1248;
+    case 16: return 1632;
+    default: return -1;
+  }
+}
+constexpr int kRegTableSize = 2144;  // 32 * (1 + 2 + 3 + 4 + 5 + 6 + 8 + 10 + 12 + 16)
+constexpr int brev5c(int l) {
+  int r = 0;
+  for (int b = 0; b < 5; ++b) r |= ((l >> b) & 1) << (4 - b);
+  return r;
+}
+struct TwiddleTables {
+  float2 reg[kRegTableSize];
+  float2 w32[32];
+};
+constexpr TwiddleTables make_twiddle_tables() {
+  TwiddleTables t{};
+  const int radices[10] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+  for (int q = 0; q < 10; ++q) {
+    const int R = radices[q], n = 32 * R, o = reg_table_offset(R);
+    for (int k1 = 0; k1 < R; ++k1)
+      for (int l = 0; l < 32; ++l) {
+        const int a = brev5c(l) * k1;
+        t.reg[o + k1 * 32 + l] = float2{(float)cos2pi(a, n), (float)-sin2pi(a, n)};
+      }
+  }
+  for (int m = 0; m < 32; ++m) t.w32[m] = float2{(float)cos2pi(m, 32), (float)-sin2pi(m, 32)};
+  return t;
+}
 }  // namespace ct
+
+// In global memory (L2-resident after the first CTAs): every CTA copies its
+// table into shared memory instead of evaluating n double-precision sincospi.
+// Not declared const, so that it stays an ordinary global array read through
+// the L1 (lanes read different entries).
+static __device__ ct::TwiddleTables kTwiddleTables = ct::make_twiddle_tables();
 
 // exp(DIR 2 pi i m / R) as a compile-time constant
 template <int DIR, int M, int R>
@@ -374,11 +425,7 @@ struct LaneTwiddles {
 
 // w32[m] = exp(-2 pi i m / 32), m in [0, 32) (block-cooperative).
 __device__ inline void build_w32(float2* w32) {
-  if (threadIdx.x < 32) {
-    double s, c;
-    sincospi(-(double)threadIdx.x / 16.0, &s, &c);
-    w32[threadIdx.x] = make_float2((float)c, (float)s);
-  }
+  if (threadIdx.x < 32) w32[threadIdx.x] = __ldg(&kTwiddleTables.w32[threadIdx.x]);
 }
 
 __device__ __forceinline__ LaneTwiddles make_lane_twiddles(const float2* w32, int lane) {
@@ -394,6 +441,11 @@ __device__ __forceinline__ LaneTwiddles make_lane_twiddles(const float2* w32, in
 // Fill tab[k1 * 32 + l] = exp(-2 pi i brev5(l) k1 / n), k1 in [0, R) (block-cooperative).
 __device__ inline void build_reg_twiddles(float2* tab, int n) {
   const int R = n / 32;
+  const int o = (n % 32 == 0) ? ct::reg_table_offset(R) : -1;
+  if (o >= 0) {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) tab[e] = __ldg(&kTwiddleTables.reg[o + e]);
+    return;
+  }
   for (int e = threadIdx.x; e < R * 32; e += blockDim.x) {
     const int k1 = e >> 5, l = e & 31;
     double s, c;

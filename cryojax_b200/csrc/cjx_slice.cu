@@ -334,19 +334,15 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2* tab = smem;
   float2* bufs = smem + n;
   int* winy = reinterpret_cast<int*>(bufs + kWarps * stride);
-  build_reg_twiddles(tab, n);
-  build_w32(w32);
-  for (int m = threadIdx.x; m < g.py; m += blockDim.x) winy[m] = win_src(m, n, g.py, g.pad_left_y);
-  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j0 = blockIdx.x * kWarps;
   const int j = j0 + warp;
   float2* buf = bufs + warp * stride;
+  const int bl = T512 ? lane : brev5(lane);  // the transpose FFT takes natural lane order
+  float2 x[R];
+  // the column is loaded first, so that its latency overlaps the table copy
   if (j < g.ncols) {
-    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
     const float2* col = hbuf + ((size_t)blockIdx.y * g.ncols + j) * g.ldh;
-    const int bl = T512 ? lane : brev5(lane);  // the transpose FFT takes natural lane order
-    float2 x[R];
     // the Ewald sphere's full complex surface takes no Hermitian fix
     const bool sym = !(g.flags & CJX_EWALD_SPHERE) && ((j == 0) || (j == n / 2));
 #pragma unroll
@@ -359,6 +355,13 @@ __global__ void __launch_bounds__(kWarps * 32)
       }
       x[n1] = v;
     }
+  }
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  for (int m = threadIdx.x; m < g.py; m += blockDim.x) winy[m] = win_src(m, n, g.py, g.pad_left_y);
+  __syncthreads();
+  if (j < g.ncols) {
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
     if constexpr (T512) {
       static_assert(R == 16, "the transpose FFT is 512-point");
       warp_fft512_t<+1>(x, tab, w32, buf, lane);
@@ -384,14 +387,13 @@ __global__ void __launch_bounds__(kWarps * 32)
 
 // Pass B: two rows per warp.  N-point inverse FFT of A + iB (register form,
 // R = RN), Px window, Px-point forward FFT (register form, RP), split.
-template <int RN, int RP>
-__device__ __forceinline__ void rows_pair_reg(const float2* __restrict__ rowA, const float2* __restrict__ rowB,
-                                              bool has_b, float2* __restrict__ outA, int ld2, float2* buf,
-                                              const float2* tabN, const float2* tabP, const LaneTwiddles& lt,
-                                              int lane, const int* winx) {
-  constexpr int n = 32 * RN, px = 32 * RP, h = n / 2;
+// The load of the packed pair (z = A + iB in the lane's bit-reversed order)
+// is separate, so that a kernel can issue it before its table copy.
+template <int RN>
+__device__ __forceinline__ void rows_pair_load(const float2* __restrict__ rowA, const float2* __restrict__ rowB,
+                                               bool has_b, float2 (&z)[RN], int lane) {
+  constexpr int n = 32 * RN, h = n / 2;
   const int bl = brev5(lane);
-  float2 z[RN];
 #pragma unroll
   for (int n1 = 0; n1 < RN; ++n1) {
     const int idx = 32 * n1 + bl;
@@ -409,6 +411,14 @@ __device__ __forceinline__ void rows_pair_reg(const float2* __restrict__ rowA, c
       z[n1] = make_float2(A.x + B.y, B.x - A.y);
     }
   }
+}
+
+template <int RN, int RP>
+__device__ __forceinline__ void rows_pair_reg(float2 (&z)[RN], bool has_b, float2* __restrict__ outA, int ld2,
+                                              float2* buf, const float2* tabN, const float2* tabP,
+                                              const LaneTwiddles& lt, int lane, const int* winx) {
+  constexpr int px = 32 * RP;
+  const int bl = brev5(lane);
   warp_fft_reg<RN, +1>(z, tabN, lt, lane);  // z = a + i b (the two real rows)
 #pragma unroll
   for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
@@ -444,22 +454,27 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2* tabP = tabN + n;
   float2* bufs = tabP + px;
   int* winx = reinterpret_cast<int*>(bufs + kWarps * stride);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  const bool has_b = (ra + 1) < g.py;
+  // the row pair is loaded first, so that its latency overlaps the table copy
+  float2 z[RN];
+  if (ra < g.py) {
+    const float2* rowA = t1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
+    rows_pair_load<RN>(rowA, rowA + g.ld1, has_b, z, lane);
+  }
   build_reg_twiddles(tabN, n);
   build_reg_twiddles(tabP, px);
   build_w32(w32);
   for (int m = threadIdx.x; m < px; m += blockDim.x) winx[m] = win_src(m, n, px, g.pad_left_x);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ra = 2 * (blockIdx.x * kWarps + warp);
   if (ra >= g.py) return;
-  const bool has_b = (ra + 1) < g.py;
-  const float2* rowA = t1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
   float2* outA = t2 + ((size_t)blockIdx.y * g.py + ra) * g.ld2;
   float2* buf = bufs + warp * stride;
   const LaneTwiddles lt = make_lane_twiddles(w32, lane);
   switch (rp) {
 #define CJX_ROWS_CASE(RPV) \
-  case RPV: rows_pair_reg<RN, RPV>(rowA, rowA + g.ld1, has_b, outA, g.ld2, buf, tabN, tabP, lt, lane, winx); break;
+  case RPV: rows_pair_reg<RN, RPV>(z, has_b, outA, g.ld2, buf, tabN, tabP, lt, lane, winx); break;
     CJX_ROWS_CASE(1) CJX_ROWS_CASE(2) CJX_ROWS_CASE(3) CJX_ROWS_CASE(4) CJX_ROWS_CASE(5)
     CJX_ROWS_CASE(6) CJX_ROWS_CASE(8) CJX_ROWS_CASE(10) CJX_ROWS_CASE(12) CJX_ROWS_CASE(16)
 #undef CJX_ROWS_CASE
@@ -477,20 +492,36 @@ __global__ void __launch_bounds__(kWarps * 32)
   constexpr int stride = pad16(py) + 1;
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
+  __shared__ ImageConsts sc;
   float2* tab = smem;
-  float2* bufs = smem + py;
-  build_reg_twiddles(tab, py);
-  build_w32(w32);
+  float2* row_phase = smem + py;  // exp(-2 pi i qy(i) ty)
+  float2* bufs = smem + 2 * py;
   const int j0 = blockIdx.x * kWarps;
   const int ncols = min(kWarps, g.pxh - j0);
   const float2* src = t2 + (size_t)blockIdx.y * py * g.ld2 + j0;
-  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
-    const int m = e / kWarps, jj = e % kWarps;
-    if (jj < ncols) bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld2 + jj];
+  // staging: thread t moves column t % kWarps, rows t / kWarps + 32 q; all R
+  // loads are issued before the table copy and the shared-memory stores
+  static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
+  const int sj = threadIdx.x % kWarps, sm0 = threadIdx.x / kWarps;
+  float2 st[R];
+  if (sj < ncols) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) st[q] = src[(size_t)(sm0 + 32 * q) * g.ld2 + sj];
+  }
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  if (sj < ncols) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) bufs[sj * stride + pad16(sm0 + 32 * q)] = st[q];
   }
   const int64_t k = k0 + blockIdx.y;
   const int64_t img = order ? (int64_t)order[k] : k;
-  const ImageConsts c = load_image_consts(params + img, norm, g.py, g.px);
+  // the image's constants (double divisions and a sincos) once per CTA, not once per thread
+  if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, g.py, g.px);
+  __syncthreads();
+  const ImageConsts c = sc;
+  if (g.flags & CJX_APPLY_TRANSLATION)
+    for (int i = threadIdx.x; i < py; i += blockDim.x) row_phase[i] = phase_factor((double)fft_index(i, py) * c.qy_step * c.ty);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < ncols) {
@@ -502,11 +533,13 @@ __global__ void __launch_bounds__(kWarps * 32)
     for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
     warp_fft_reg<R, -1>(x, tab, lt, lane);
     const int j = j0 + warp;
+    const ColumnEpilogue ce = column_epilogue(j, g.flags, c);
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
       const int i = k1 + R * lane;
-      buf[pad16(i)] = apply_filter(apply_epilogue(x[k1], i, j, py, g.px, g.flags, c), g, i, j, g.pxh);
+      buf[pad16(i)] =
+          apply_filter(apply_column_epilogue(x[k1], i, j, py, g.px, g.flags, c, ce, row_phase), g, i, j, g.pxh);
     }
   }
   __syncthreads();
@@ -863,7 +896,7 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   const int rpy = reg_fft_radix(g.py);
   const bool fast = tn.fft_mode >= 1;
-  const size_t sc_reg = sizeof(float2) * (size_t)(g.py + kWarps * (pad16(g.py) + 1));
+  const size_t sc_reg = sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1));
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
