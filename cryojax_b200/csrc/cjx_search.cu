@@ -81,25 +81,43 @@ __global__ void __launch_bounds__(kWarps * 32)
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
   __shared__ float red[kWarps][2];
+  __shared__ ImageConsts sc;
   float2* tab = smem;
-  float2* bufs = smem + py;
+  float2* row_phase = smem + py;  // exp(-2 pi i qy(i) ty)
+  float2* bufs = smem + 2 * py;
   float2* obuf = bufs + kWarps * stride;
-  build_reg_twiddles(tab, py);
-  build_w32(w32);
   const int j0 = blockIdx.x * kWarps;
   const int ncols = min(kWarps, g.pxh - j0);
   const int k = blockIdx.y;
   const int64_t img = cimg[k];
   const float2* src = t2 + (size_t)k * py * g.ld2 + j0;
   const float2* ocol = obs + (size_t)img * py * g.pxh + j0;
-  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
-    const int m = e / kWarps, jj = e % kWarps;
-    if (jj < ncols) {
-      bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld2 + jj];
-      obuf[jj * stride + pad16(m)] = ocol[(size_t)m * g.pxh + jj];
+  // staging as in the forward column pass: thread t moves column t % kWarps,
+  // rows t / kWarps + 32 q, loads issued before the table copy
+  static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
+  const int sj = threadIdx.x % kWarps, sm0 = threadIdx.x / kWarps;
+  float2 st[R], so[R];
+  if (sj < ncols) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      st[q] = src[(size_t)(sm0 + 32 * q) * g.ld2 + sj];
+      so[q] = ocol[(size_t)(sm0 + 32 * q) * g.pxh + sj];
     }
   }
-  const ImageConsts c = load_image_consts(cparams + k, norm, g.py, g.px);
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  if (sj < ncols) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      bufs[sj * stride + pad16(sm0 + 32 * q)] = st[q];
+      obuf[sj * stride + pad16(sm0 + 32 * q)] = so[q];
+    }
+  }
+  if (threadIdx.x == 0) sc = load_image_consts(cparams + k, norm, g.py, g.px);
+  __syncthreads();
+  const ImageConsts c = sc;
+  if (g.flags & CJX_APPLY_TRANSLATION)
+    for (int i = threadIdx.x; i < py; i += blockDim.x) row_phase[i] = phase_factor((double)fft_index(i, py) * c.qy_step * c.ty);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float num = 0.f, den = 0.f;
@@ -113,11 +131,12 @@ __global__ void __launch_bounds__(kWarps * 32)
 #pragma unroll
     for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
     warp_fft_reg<R, -1>(x, tab, lt, lane);
+    const ColumnEpilogue ce = column_epilogue(j, g.flags, c);
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
       const int i = k1 + R * lane;
-      buf[pad16(i)] = apply_epilogue(x[k1], i, j, py, g.px, g.flags, c);
+      buf[pad16(i)] = apply_column_epilogue(x[k1], i, j, py, g.px, g.flags, c, ce, row_phase);
     }
     __syncwarp();
     const bool self_col = (j == 0) || ((g.px % 2 == 0) && j == g.px / 2);
@@ -244,7 +263,7 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
   unsigned long long* best = reinterpret_cast<unsigned long long*>(p);
 
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
-  const size_t s_score = sizeof(float2) * (size_t)(g.py + 2 * kWarps * (pad16(g.py) + 1));
+  const size_t s_score = sizeof(float2) * (size_t)(2 * g.py + 2 * kWarps * (pad16(g.py) + 1));
   prof_begin(stream);
   k_fourier_power<<<(unsigned)n_images, 256, 0, stream>>>(obs, oo, g.py, g.px);
   prof_end("k_fourier_power", stream);
