@@ -509,6 +509,8 @@ def measure_pose_search(dev, seed, n_obs):
     res, t_l = timed(lambda: learned.run(model, obs))
     _, t_net = timed(lambda: net.propose(obs, k=16, n_inplane=grid.n_inplane))
     shared = TemplateSharingSearch(grid.rotation_matrices())
+    shared.build_templates(model)  # warm-up: buffer allocation; the timed build below recomputes every template
+    shared._key = None
     _, t_tmpl = timed(lambda: shared.build_templates(model))
     sh, t_sh = timed(lambda: shared.run(model, obs))
     shr, t_shr = timed(lambda: shared.run(model, obs, rerank_top=8))

@@ -111,24 +111,40 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2* tab = smem;
   float2* bufs = smem + py;                  // T2 columns, then F, then g_X
   float2* obuf = bufs + kWarps * stride;     // observed columns
-  build_reg_twiddles(tab, py);
-  build_w32(w32);
+  __shared__ ImageConsts sc;
   const int j0 = blockIdx.x * kWarps;
   const int ncols = min(kWarps, g.pxh - j0);
   const int64_t k = k0 + blockIdx.y;
   const int64_t img = order ? (int64_t)order[k] : k;
   float2* col0 = t2 + (size_t)blockIdx.y * py * g.ld2 + j0;
   const float2* ocol0 = obs + (size_t)img * py * g.pxh + j0;
-  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
-    const int m = e / kWarps, jj = e % kWarps;
-    if (jj < ncols) {
-      bufs[jj * stride + pad16(m)] = col0[(size_t)m * g.ld2 + jj];
-      obuf[jj * stride + pad16(m)] = ocol0[(size_t)m * g.pxh + jj];
+  // staging: thread t moves column t % kWarps, rows t / kWarps + 32 q; the
+  // loads are issued before the table copy
+  static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
+  const int sj = threadIdx.x % kWarps, sm0 = threadIdx.x / kWarps;
+  {
+    float2 st[R], so[R];
+    if (sj < ncols) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        st[q] = col0[(size_t)(sm0 + 32 * q) * g.ld2 + sj];
+        so[q] = ocol0[(size_t)(sm0 + 32 * q) * g.pxh + sj];
+      }
+    }
+    build_reg_twiddles(tab, py);
+    build_w32(w32);
+    if (sj < ncols) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        bufs[sj * stride + pad16(sm0 + 32 * q)] = st[q];
+        obuf[sj * stride + pad16(sm0 + 32 * q)] = so[q];
+      }
     }
   }
-  const ImageConsts c = load_image_consts(params + img, norm, g.py, g.px);
+  if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, g.py, g.px);  // once per CTA
   const double wl = params[img].wavelength;
   __syncthreads();
+  const ImageConsts& c = sc;  // read from shared memory where used (keeps the register count down)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float sl = 0.f, stx = 0.f, sty = 0.f, sdf = 0.f;
   if (warp < ncols) {

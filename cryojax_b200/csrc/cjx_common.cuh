@@ -660,28 +660,23 @@ __device__ __forceinline__ ColumnEpilogue column_epilogue(int j, uint32_t flags,
   return e;
 }
 
-__device__ __forceinline__ float2 apply_column_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
-                                                        const ImageConsts& c, const ColumnEpilogue& e,
-                                                        const float2* __restrict__ row_phase) {
-  v.x *= c.scale;
-  v.y *= c.scale;
-  if (flags & (CJX_APPLY_CTF | CJX_APPLY_ENVELOPE)) {
-    const double qy = (double)fft_index(i, py) * c.qy_step;
-    const double k2 = fma(qy, qy, e.qx2);
-    if (flags & CJX_APPLY_CTF) {
-      const float qyf = (float)qy;
-      const float astig = e.c_astig * fmaf(fmaf(qyf, qyf, -e.qxf * e.qxf), c.cos2a, 2.0f * e.qxf * qyf * c.sin2a);
-      const double arg = fma(fma(c.c_sph, k2, e.c_dd), k2, (double)astig - c.phase_cycles);
-      const float r = (float)(arg - rint(arg));
-      const float ctf = sinpif(2.0f * r);
-      v.x *= ctf;
-      v.y *= ctf;
-    }
-    if (flags & CJX_APPLY_ENVELOPE) {
-      const float en = c.env_amp * expf(-c.env_quarter_b * (float)k2);
-      v.x *= en;
-      v.y *= en;
-    }
+// chi / (2 pi) - const_cycles at (qy, k2) of column e.
+__device__ __forceinline__ double column_aberration_cycles(double qy, double k2, const ImageConsts& c,
+                                                           const ColumnEpilogue& e, double const_cycles) {
+  const float qyf = (float)qy;
+  const float astig = e.c_astig * fmaf(fmaf(qyf, qyf, -e.qxf * e.qxf), c.cos2a, 2.0f * e.qxf * qyf * c.sin2a);
+  return fma(fma(c.c_sph, k2, e.c_dd), k2, (double)astig - const_cycles);
+}
+
+// Envelope and translation in column form (envelope_translate's counterpart).
+__device__ __forceinline__ float2 column_envelope_translate(float2 v, int i, int j, int py, int px, double k2,
+                                                            uint32_t flags, const ImageConsts& c,
+                                                            const ColumnEpilogue& e,
+                                                            const float2* __restrict__ row_phase) {
+  if (flags & CJX_APPLY_ENVELOPE) {
+    const float en = c.env_amp * expf(-c.env_quarter_b * (float)k2);
+    v.x *= en;
+    v.y *= en;
   }
   if (flags & CJX_APPLY_TRANSLATION) {
     const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
@@ -691,6 +686,26 @@ __device__ __forceinline__ float2 apply_column_epilogue(float2 v, int i, int j, 
     v = cmul(v, cmul(e.col_phase, row_phase[i]));
   }
   return v;
+}
+
+__device__ __forceinline__ float2 apply_column_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
+                                                        const ImageConsts& c, const ColumnEpilogue& e,
+                                                        const float2* __restrict__ row_phase) {
+  v.x *= c.scale;
+  v.y *= c.scale;
+  double k2 = 0.0;
+  if (flags & (CJX_APPLY_CTF | CJX_APPLY_ENVELOPE)) {
+    const double qy = (double)fft_index(i, py) * c.qy_step;
+    k2 = fma(qy, qy, e.qx2);
+    if (flags & CJX_APPLY_CTF) {
+      const double arg = column_aberration_cycles(qy, k2, c, e, c.phase_cycles);
+      const float r = (float)(arg - rint(arg));
+      const float ctf = sinpif(2.0f * r);
+      v.x *= ctf;
+      v.y *= ctf;
+    }
+  }
+  return column_envelope_translate(v, i, j, py, px, k2, flags, c, e, row_phase);
 }
 
 __device__ __forceinline__ float2 apply_epilogue(float2 v, int i, int j, int py, int px, uint32_t flags,
@@ -752,6 +767,41 @@ __device__ __forceinline__ float2 ewald_epilogue(float2 a, float2 b, int i, int 
   v.y = 0.5f * ((c.w2 * di + c.w1 * dr) * s + (c.w2 * dr - c.w1 * di) * co);
   if (conj_out) v.y = -v.y;
   return envelope_translate(v, i, j, py, px, qx, qy, k2, flags, c);
+}
+
+// ewald_epilogue in column form: the aberration phase without an angle or
+// a division, the translation from the column factor and the per-CTA row
+// table (same values up to rounding).
+__device__ __forceinline__ float2 ewald_column_epilogue(float2 a, float2 b, int i, int j, int py, int px,
+                                                        uint32_t flags, const ImageConsts& c,
+                                                        const ColumnEpilogue& e,
+                                                        const float2* __restrict__ row_phase) {
+  a.x *= c.scale;
+  a.y *= c.scale;
+  b.x *= c.scale;
+  b.y *= c.scale;
+  const double qy = (double)fft_index(i, py) * c.qy_step;
+  const double k2 = fma(qy, qy, e.qx2);
+  const double arg = column_aberration_cycles(qy, k2, c, e, c.ps_cycles);
+  const float r = (float)(arg - rint(arg));
+  float s, co;
+  sincospif(2.0f * r, &s, &co);
+  float2 pos = a, neg = b;
+  bool conj_out = false;
+  if ((px % 2 == 0) && j == px / 2) {
+    pos = make_float2(b.x, -b.y);
+  } else if (j == 0 && (py % 2 == 0) && i == py / 2) {
+    pos = make_float2(a.x, -a.y);
+    neg = a;
+    conj_out = true;
+  }
+  const float sr = pos.x + neg.x, si = pos.y + neg.y;
+  const float dr = neg.x - pos.x, di = pos.y - neg.y;
+  float2 v;
+  v.x = 0.5f * ((c.w2 * sr + c.w1 * si) * s + (c.w2 * si - c.w1 * sr) * co);
+  v.y = 0.5f * ((c.w2 * di + c.w1 * dr) * s + (c.w2 * dr - c.w1 * di) * co);
+  if (conj_out) v.y = -v.y;
+  return column_envelope_translate(v, i, j, py, px, k2, flags, c, e, row_phase);
 }
 
 // ---------------------------------------------------------------------------

@@ -191,7 +191,8 @@ __global__ void __launch_bounds__(kWarps * 32)
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
   float2* tab = smem;
-  float2* bufs = smem + py;  // columns [0, kWarps): own, [kWarps, 2 kWarps): mirrors
+  float2* row_phase = smem + py;  // exp(-2 pi i qy(i) ty)
+  float2* bufs = smem + 2 * py;   // columns [0, kWarps): own, [kWarps, 2 kWarps): mirrors
   const int px = g.px;
   const bool ctf = (g.flags & CJX_APPLY_CTF) != 0;
   const int pitch = ctf ? g.pxh : px;
@@ -225,7 +226,11 @@ __global__ void __launch_bounds__(kWarps * 32)
   __shared__ ImageConsts sc;  // evaluated once per CTA
   if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, py, px);
   __syncthreads();
-  const ImageConsts c = sc;
+  const ImageConsts& c = sc;  // read from shared memory where used (keeps the register count down)
+  if (ctf && (g.flags & CJX_APPLY_TRANSLATION)) {
+    for (int i = threadIdx.x; i < py; i += blockDim.x) row_phase[i] = phase_factor((double)fft_index(i, py) * c.qy_step * c.ty);
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < ncols) {
     const LaneTwiddles lt = make_lane_twiddles(w32, lane);
@@ -249,10 +254,11 @@ __global__ void __launch_bounds__(kWarps * 32)
     }
     __syncwarp();
     const int col = j0 + warp;
+    const ColumnEpilogue ce = column_epilogue(col, ctf ? g.flags : 0u, c);
     for (int i = lane; i < py; i += 32) {
       float2 v = A[pad16(i)];
       if (ctf) {
-        v = ewald_epilogue(v, B[pad16((py - i) % py)], i, col, py, px, g.flags, c);
+        v = ewald_column_epilogue(v, B[pad16((py - i) % py)], i, col, py, px, g.flags, c, ce, row_phase);
       } else {
         v.x *= c.scale;
         v.y *= c.scale;
@@ -398,7 +404,7 @@ int launch_ewald_colfft(const SliceGeom& g, const float2* t2, const cjx_image_pa
   prof_begin(stream);
   if (tn.fft_mode >= 1 && ry) {
     const dim3 gd((cols + kWarps - 1) / kWarps, cnt);
-    const size_t sm = sizeof(float2) * (size_t)(g.py + 2 * kWarps * (pad16(g.py) + 1));
+    const size_t sm = sizeof(float2) * (size_t)(2 * g.py + 2 * kWarps * (pad16(g.py) + 1));
     switch (ry) {
 #define CJX_EC_CASE(R) \
   case R: k_ewald_colfft_reg<R><<<gd, kWarps * 32, sm, stream>>>(t2, params, order, out, g, k0, norm); break;

@@ -115,7 +115,10 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   if (threadIdx.x == 0) sc = load_image_consts(cparams + k, norm, g.py, g.px);
   __syncthreads();
-  const ImageConsts c = sc;
+  // R <= 8 keeps a register copy (cheaper at 128^2, where registers are not
+  // scarce); larger R reads the shared copy where used (keeps 4 CTAs per SM)
+  const ImageConsts c_reg = sc;
+  const ImageConsts& c = (R <= 8) ? c_reg : sc;
   if (g.flags & CJX_APPLY_TRANSLATION)
     for (int i = threadIdx.x; i < py; i += blockDim.x) row_phase[i] = phase_factor((double)fft_index(i, py) * c.qy_step * c.ty);
   __syncthreads();

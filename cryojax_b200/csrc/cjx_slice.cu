@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   // the image's constants (double divisions and a sincos) once per CTA, not once per thread
   if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, g.py, g.px);
   __syncthreads();
-  const ImageConsts c = sc;
+  const ImageConsts& c = sc;  // read from shared memory where used (keeps the register count down)
   if (g.flags & CJX_APPLY_TRANSLATION)
     for (int i = threadIdx.x; i < py; i += blockDim.x) row_phase[i] = phase_factor((double)fft_index(i, py) * c.qy_step * c.ty);
   __syncthreads();

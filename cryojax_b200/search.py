@@ -235,8 +235,10 @@ class TemplateSharingSearch:
             return
         kp = py * (px // 2 + 1)
         T = self.n_orientations
-        self.s16 = torch.empty((T, 2 * kp), dtype=torch.float16, device=self.device)
-        self.p16 = torch.empty((T, kp), dtype=torch.float16, device=self.device)
+        if self.s16 is None or tuple(self.s16.shape) != (T, 2 * kp):  # a rebuild reuses the buffers
+            self.s16 = self.p16 = None
+            self.s16 = torch.empty((T, 2 * kp), dtype=torch.float16, device=self.device)
+            self.p16 = torch.empty((T, kp), dtype=torch.float16, device=self.device)
         integ = image_model.volume_integrator
         p = nat.empty_params(T)
         p[:, 0:9] = self.rot
