@@ -68,6 +68,8 @@ CASES = [
     (25, 1.0, (25, 25), None, 20.0),       # odd N, no resize
     (32, 1.3, (30, 30), (44, 42), 60.0),   # prime N = 41, padded != shape
     (31, 2.0, (31, 31), None, 300.0),      # N = 62, odd image
+    (32, 2.0, (64, 33), None, 60.0),       # register column pass (Py = 64), odd Px
+    (32, 2.0, (32, 40), None, 300.0),      # register column pass, Px = 40 (shared-memory rows)
 ]
 
 

@@ -50,6 +50,8 @@ CASES = [
     (32, 1.3, (30, 30), (44, 42)), # prime N with pad and padded_shape != shape
     (48, 2.0, (48, 48), None),     # N = 96 = 2^5 * 3
     (40, 2.0, (40, 40), None),     # N = 80 = 2^4 * 5, image 40 = 2^3 * 5
+    (32, 2.0, (64, 33), None),     # register column pass (Py = 64), odd Px: no x-Nyquist column
+    (32, 2.0, (32, 40), None),     # register column pass, Px = 40 through the shared-memory row pass
 ]
 
 
