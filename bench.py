@@ -1233,7 +1233,7 @@ def main():
                "h2d_bytes_per_step": int(ph.numel() * ph.element_size()),
                "d2h_bytes_per_step": int(oh.numel() * oh.element_size()),
                "path": "HostStreamingSimulator: pinned host params -> H2D -> cjx_slice_ctf_forward -> D2H "
-                       "into pinned host images, 2 streams, 2048-image sub-batches"}
+                       "into pinned host images, 2 streams, 2048-image sub-batches after a 256/512/1024 ramp"}
         del oh, ph, sim
         try:  # the host link's own device-to-host rate: the e2e roof when the images dominate the traffic
             nbytes = 1 << 30

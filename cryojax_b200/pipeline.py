@@ -53,6 +53,21 @@ class HostStreamingSimulator:
     def pinned_output(self, n):
         return self.torch.empty((n,) + self.out_shape, dtype=self.torch.complex64, pin_memory=True)
 
+    def sub_batches(self, n):
+        """(start, count) of each sub-batch: sub_batch / 8, / 4, / 2, then full ones.
+
+        Every call is ordered after the caller's stream, so its first
+        device-to-host copy waits for its first sub-batch's simulation; the
+        ramp keeps that wait to a small batch's instead of a full one's.
+        """
+        out, pos, size = [], 0, max(1, self.sub_batch // 8)
+        while pos < n:
+            cnt = min(size, n - pos)
+            out.append((pos, cnt))
+            pos += cnt
+            size = min(self.sub_batch, 2 * size)
+        return out
+
     def run(self, params_host, out_host):
         """params_host: pinned float64 [n, 32]; out_host: pinned complex64 [n, Py, Px//2+1].
 
@@ -61,20 +76,20 @@ class HostStreamingSimulator:
         """
         torch = self.torch
         n = params_host.shape[0]
+        batches = self.sub_batches(n)
         orders = []
         if self.sort:
             from .simulator import orientation_order
 
             rots = params_host[:, 0:9].numpy().reshape(-1, 3, 3)
-            for s0 in range(0, n, self.sub_batch):
-                o = orientation_order(rots[s0:s0 + self.sub_batch])
+            for s0, cnt in batches:
+                o = orientation_order(rots[s0:s0 + cnt])
                 orders.append(torch.from_numpy(o).pin_memory())
         cur = torch.cuda.current_stream()
         for s in self.streams:
             s.wait_stream(cur)
-        for i, s0 in enumerate(range(0, n, self.sub_batch)):
+        for i, (s0, cnt) in enumerate(batches):
             k = i % 2
-            cnt = min(self.sub_batch, n - s0)
             st = self.streams[k]
             with torch.cuda.stream(st):
                 pd = self.params_d[k][:cnt]
