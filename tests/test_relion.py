@@ -236,3 +236,17 @@ def test_mrc_big_endian_and_modes(tmp_path):
     (tmp_path / "short.mrc").write_bytes(bytes(header) + data.tobytes()[:10])
     with pytest.raises(ValueError):
         mrc.read_array_from_mrc(tmp_path / "short.mrc")
+
+
+def test_mrc_header_statistics_match_numpy_float64():
+    """The writer's header min / max / mean / rms against NumPy in float64 (header fields are float32)."""
+    from cryojax_b200.mrc import _header_stats
+
+    rng = np.random.default_rng(3)
+    for shape, offset in [((3, 5), 0.0), ((40, 64, 64), 100.0), ((2, 1000, 1001), -7.5)]:
+        a = (rng.standard_normal(shape) * 3 + offset).astype(np.float32)
+        lo, hi, mean, rms = _header_stats(a)
+        assert lo == float(a.min()) and hi == float(a.max())
+        np.testing.assert_allclose(mean, a.mean(dtype=np.float64), rtol=1e-6, atol=1e-7)
+        np.testing.assert_allclose(rms, a.std(dtype=np.float64), rtol=1e-6)
+    assert _header_stats(np.zeros((0, 4), np.float32)) == (0.0, 0.0, 0.0, 0.0)
