@@ -272,7 +272,8 @@ static int search_plan(const cjx_search_desc* d, SliceGeom* g, int* K, int64_t* 
   if (!d) return fail(CJX_ERR_INVALID_ARGUMENT, "desc is NULL");
   if (int e = make_geom(&d->slice, g)) return e;
   if (!needs_resize(*g)) return fail(CJX_ERR_UNSUPPORTED, "search needs the resize path ((Py, Px) != (N, N))");
-  if (g->flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "search scores projection images only");
+  if ((g->flags & CJX_EWALD_SPHERE) && !(g->flags & CJX_APPLY_CTF))
+    return fail(CJX_ERR_UNSUPPORTED, "search on the Ewald sphere needs the contrast transfer (CJX_APPLY_CTF)");
   if (d->n_images < 0 || d->n_orientations < 1 || d->candidates_per_image < 0)
     return fail(CJX_ERR_INVALID_ARGUMENT, "need n_images >= 0, n_orientations >= 1, candidates_per_image >= 0");
   if (d->n_orientations > 2147483647LL) return fail(CJX_ERR_UNSUPPORTED, "too many orientations");

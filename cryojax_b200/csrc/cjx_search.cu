@@ -174,6 +174,107 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
 }
 
+// Pass C for scoring on the Ewald sphere: each warp transforms a column x of
+// the full object spectrum and its mirror (Px - x) mod Px, forms the
+// contrast that pairs +q with -q (ewald_column_epilogue, the forward's
+// k_ewald_colfft_reg epilogue), then accumulates the two NCC sums against
+// the observed rfft image exactly as k_colfft_score_reg does.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_colfft_score_reg(const float2* __restrict__ t2, const cjx_image_params* __restrict__ cparams,
+                             const int32_t* __restrict__ cimg, const float2* __restrict__ obs,
+                             float* __restrict__ sums, SliceGeom g, float norm) {
+  constexpr int py = 32 * R;
+  constexpr int stride = pad16(py) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  __shared__ float red[kWarps][2];
+  __shared__ ImageConsts sc;
+  float2* tab = smem;
+  float2* row_phase = smem + py;               // exp(-2 pi i qy(i) ty)
+  float2* bufs = smem + 2 * py;                // own columns [0, kWarps), mirrors [kWarps, 2 kWarps)
+  float2* obuf = bufs + 2 * kWarps * stride;   // observed columns
+  const int px = g.px;
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.pxh - j0);
+  const int k = blockIdx.y;
+  const int64_t img = cimg[k];
+  const float2* src = t2 + (size_t)k * py * g.ld2;
+  const float2* ocol = obs + (size_t)img * py * g.pxh + j0;
+  build_reg_twiddles(tab, py);
+  build_w32(w32);
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      bufs[jj * stride + pad16(m)] = src[(size_t)m * g.ld2 + j0 + jj];
+      bufs[(kWarps + jj) * stride + pad16(m)] = src[(size_t)m * g.ld2 + (px - j0 - jj) % px];
+      obuf[jj * stride + pad16(m)] = ocol[(size_t)m * g.pxh + jj];
+    }
+  }
+  if (threadIdx.x == 0) sc = load_image_consts(cparams + k, norm, g.py, g.px);
+  __syncthreads();
+  const ImageConsts& c = sc;
+  if (g.flags & CJX_APPLY_TRANSLATION)
+    for (int i = threadIdx.x; i < py; i += blockDim.x) row_phase[i] = phase_factor((double)fft_index(i, py) * c.qy_step * c.ty);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float num = 0.f, den = 0.f;
+  if (warp < ncols) {
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const int bl = brev5(lane);
+    float2* A = bufs + warp * stride;
+    float2* B = bufs + (kWarps + warp) * stride;
+    const float2* ob = obuf + warp * stride;
+    float2 x[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = A[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(x, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) A[pad16(k1 + R * lane)] = x[k1];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = B[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(x, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) B[pad16(k1 + R * lane)] = x[k1];
+    __syncwarp();
+    const int j = j0 + warp;
+    const ColumnEpilogue ce = column_epilogue(j, g.flags, c);
+    for (int i = lane; i < py; i += 32)  // row i is read and written by this lane only
+      A[pad16(i)] = ewald_column_epilogue(A[pad16(i)], B[pad16((py - i) % py)], i, j, py, px, g.flags, c, ce,
+                                          row_phase);
+    __syncwarp();
+    const bool self_col = (j == 0) || ((px % 2 == 0) && j == px / 2);
+    const float w = self_col ? 1.f : 2.f;
+    for (int i = lane; i < py; i += 32) {
+      if (i == 0 && j == 0) continue;
+      float2 f = A[pad16(i)];
+      if (self_col) {
+        const float2 fm = A[pad16(i == 0 ? 0 : py - i)];
+        f = make_float2(0.5f * (f.x + fm.x), 0.5f * (f.y - fm.y));
+      }
+      const float2 o = ob[pad16(i)];
+      num += w * (o.x * f.x + o.y * f.y);
+      den += w * (f.x * f.x + f.y * f.y);
+    }
+  }
+  for (int s = 16; s > 0; s >>= 1) {
+    num += __shfl_xor_sync(0xffffffffu, num, s);
+    den += __shfl_xor_sync(0xffffffffu, den, s);
+  }
+  if (lane == 0) {
+    red[warp][0] = num;
+    red[warp][1] = den;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    float t = 0.f;
+    for (int w = 0; w < kWarps; ++w) t += red[w][threadIdx.x];
+    sums[((size_t)k * gridDim.x + blockIdx.x) * 2 + threadIdx.x] = t;
+  }
+}
+
 // Orderable 64-bit key: score (monotone bits) in the high word, and the
 // complement of the orientation index in the low word (ties -> lowest index).
 __device__ __forceinline__ unsigned long long score_key(float s, int32_t orient) {
@@ -222,7 +323,9 @@ static cudaError_t search_smem_attrs() {
   std::call_once(once, [&] {
 #define CJX_SA(R)                                                                                              \
   if (err == cudaSuccess)                                                                                      \
-    err = cudaFuncSetAttribute(k_colfft_score_reg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    err = cudaFuncSetAttribute(k_colfft_score_reg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
+  if (err == cudaSuccess)                                                                                      \
+    err = cudaFuncSetAttribute(k_ewald_colfft_score_reg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     CJX_SA(1) CJX_SA(2) CJX_SA(3) CJX_SA(4) CJX_SA(5) CJX_SA(6) CJX_SA(8) CJX_SA(10) CJX_SA(12) CJX_SA(16)
 #undef CJX_SA
   });
@@ -267,6 +370,7 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
 
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   const size_t s_score = sizeof(float2) * (size_t)(2 * g.py + 2 * kWarps * (pad16(g.py) + 1));
+  const size_t s_ewald = sizeof(float2) * (size_t)(2 * g.py + 3 * kWarps * (pad16(g.py) + 1));
   prof_begin(stream);
   k_fourier_power<<<(unsigned)n_images, 256, 0, stream>>>(obs, oo, g.py, g.px);
   prof_end("k_fourier_power", stream);
@@ -281,12 +385,23 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
     if (int e = launch_forward_to_t2(g, grid, cparams, nullptr, 0, cnt, t1, t2, hb, stream, tn)) return e;
     prof_begin(stream);
     const dim3 gs(nparts, cnt);
-    switch (rpy) {
+    if (g.flags & CJX_EWALD_SPHERE) {
+      switch (rpy) {
+#define CJX_S_CASE(R)                                                                                                  \
+  case R:                                                                                                              \
+    k_ewald_colfft_score_reg<R><<<gs, kWarps * 32, s_ewald, stream>>>(t2, cparams, cimg, obs, sums, g, norm); break;
+        CJX_S_CASE(1) CJX_S_CASE(2) CJX_S_CASE(3) CJX_S_CASE(4) CJX_S_CASE(5)
+        CJX_S_CASE(6) CJX_S_CASE(8) CJX_S_CASE(10) CJX_S_CASE(12) CJX_S_CASE(16)
+#undef CJX_S_CASE
+      }
+    } else {
+      switch (rpy) {
 #define CJX_S_CASE(R) \
   case R: k_colfft_score_reg<R><<<gs, kWarps * 32, s_score, stream>>>(t2, cparams, cimg, obs, sums, g, norm); break;
-      CJX_S_CASE(1) CJX_S_CASE(2) CJX_S_CASE(3) CJX_S_CASE(4) CJX_S_CASE(5)
-      CJX_S_CASE(6) CJX_S_CASE(8) CJX_S_CASE(10) CJX_S_CASE(12) CJX_S_CASE(16)
+        CJX_S_CASE(1) CJX_S_CASE(2) CJX_S_CASE(3) CJX_S_CASE(4) CJX_S_CASE(5)
+        CJX_S_CASE(6) CJX_S_CASE(8) CJX_S_CASE(10) CJX_S_CASE(12) CJX_S_CASE(16)
 #undef CJX_S_CASE
+      }
     }
     prof_end("k_colfft_score", stream);
     prof_begin(stream);

@@ -230,6 +230,9 @@ class TemplateSharingSearch:
         if py % 8:
             raise NotImplementedError("TemplateSharingSearch needs Py to be a multiple of 8")
         integ = image_model.volume_integrator
+        if not integ.is_projection_approximation:
+            # the Ewald contrast pairs +q with -q, so the CTF cannot be moved onto the observed image
+            raise NotImplementedError("TemplateSharingSearch needs a projection integrator; use PoseSearch")
         key = (id(integ.device_grid(vol)[0]), py, px, float(np.ravel(cfg.pixel_size)[0]))
         if key == self._key and self.s16 is not None:
             return

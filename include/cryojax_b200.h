@@ -90,8 +90,9 @@ extern "C" {
  * parameter record; CJX_APPLY_ENVELOPE and CJX_APPLY_TRANSLATION as usual.
  * Without CJX_APPLY_CTF the output is the integrator's full spectrum
  * [Py][Px] (scale applied; no envelope or translation allowed).  Any grid
- * layout, trilinear or spline.  Forward, multi and no-alloc entry points
- * (not search or loss_grad).                                              */
+ * layout, trilinear or spline.  Forward, multi and no-alloc entry points,
+ * and cjx_search with CJX_APPLY_CTF (the scores are the contrast images'
+ * NCC); not loss_grad.                                                    */
 #define CJX_EWALD_SPHERE (1u << 7)
 
 /* ---- per-image parameters (one record per image, device memory) ------

@@ -178,3 +178,40 @@ def test_template_sharing_rerank_equals_plain_exhaustive(cuda_device):
         np.testing.assert_array_equal(np.sort(top[b]), np.sort(ref))
         assert np.all(np.diff(fp16_scores[b, top[b]]) <= 0)
     assert nat.device_status() == 0
+
+
+@pytest.mark.parametrize("kv,layout", [(300.0, "pairs"), (20.0, "linear")])
+def test_ewald_search_scores_match_oracle(cuda_device, kv, layout):
+    """PoseSearch on EwaldSphereExtraction + ContrastTransferTheory against the oracle's grid search
+    on the Ewald contrast (every pair simulated in float64); 20 kV gives a strongly curved surface."""
+    import torch
+
+    from cryojax_b200 import simulator as S
+    from cryojax_b200.healpix import OrientationGrid
+    from cryojax_b200.search import PoseSearch, TemplateSharingSearch
+
+    og = OrientationGrid(nside=1, n_inplane=4)  # 48 orientations
+    quats = og.quaternions()
+    _, grid, fs = make_volume(32, 40, seed=61)
+    rng = np.random.default_rng(62)
+    true_idx = rng.choice(og.size, 2, replace=False)
+    specs = [O.ImageSpec(shape=(32, 32), pixel_size=2.0, voltage_in_kilovolts=kv, wxyz=quats[t],
+                         offset_in_angstroms=rng.uniform(-4, 4, 2), defocus_in_angstroms=rng.uniform(8000, 20000),
+                         astigmatism_in_angstroms=rng.uniform(0, 300), astigmatism_angle=rng.uniform(0, 180),
+                         amplitude_contrast_ratio=0.1, phase_shift=rng.uniform(0, 20)) for t in true_idx]
+    obs = np.stack([O.simulate(grid, fs, s, ewald=True) for s in specs])
+    _, ref_scores = O.grid_search_orientations(grid, fs, specs, obs, quats, ewald=True)
+
+    pose, tt, cfg = specs_to_model_args(specs)
+    vol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+    integ = S.EwaldSphereExtraction(use_bricked_layout=layout != "linear", pair_layout=layout == "pairs")
+    model = S.make_image_model(vol, cfg, pose, tt, volume_integrator=integ)
+    res = PoseSearch(og.rotation_matrices()).run(model, obs, return_scores=True)
+    got = res.scores.cpu().numpy()
+    assert got.shape == ref_scores.shape
+    err = np.abs(got - ref_scores).max()
+    assert err <= NCC_ABS_TOL, err
+    _check_best(res.best_orientation, ref_scores)
+    np.testing.assert_array_equal(res.best_orientation, true_idx)  # noiseless images at grid orientations
+    with pytest.raises(NotImplementedError):
+        TemplateSharingSearch(og.rotation_matrices()).run(model, obs)
