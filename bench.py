@@ -507,6 +507,11 @@ def measure_pose_search(dev, seed, n_obs):
     learned.run(model, obs, fallback=False)  # warm-up
     ex, t_ex = timed(lambda: search.run(model, obs))
     res, t_l = timed(lambda: learned.run(model, obs))
+    nat.profile_enable(True)  # one extra, profiled run of the learned arm (not part of its value)
+    learned.run(model, obs)
+    torch.cuda.synchronize()
+    learned_kernels = {k: {"launches": c, "ms": t} for k, (c, t) in nat.profile_read().items()}
+    nat.profile_enable(False)
     _, t_net = timed(lambda: net.propose(obs, k=16, n_inplane=grid.n_inplane))
     shared = TemplateSharingSearch(grid.rotation_matrices())
     shared.build_templates(model)  # warm-up: buffer allocation; the timed build below recomputes every template
@@ -522,7 +527,8 @@ def measure_pose_search(dev, seed, n_obs):
         "plain_exhaustive": {"value": n_obs / t_ex, "seconds": t_ex, "candidates_per_image": grid.size,
                              "candidates_per_s": n_obs * grid.size / t_ex},
         "learned": {"value": n_obs / t_l, "seconds": t_l, "candidates_per_image": 16 * grid.n_inplane,
-                    "network_seconds": t_net, "fallback_fraction": float(res.fallback.mean()), "threshold": thr},
+                    "network_seconds": t_net, "fallback_fraction": float(res.fallback.mean()), "threshold": thr,
+                    "kernels_per_run": learned_kernels},
         "template_sharing_exhaustive": {
             "value": n_obs / (t_tmpl + t_sh), "seconds": t_tmpl + t_sh, "template_seconds": t_tmpl,
             "gemm_search_seconds": t_sh,
