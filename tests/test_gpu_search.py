@@ -123,9 +123,11 @@ def test_search_rejects_bad_candidates(cuda_device):
         PoseSearch(og.rotation_matrices()).run(_model(grid, specs), obs, candidates=np.full((2, 3), og.size))
 
 
-@pytest.mark.parametrize("shift", [0.0, 4.0])
-def test_template_sharing_search_matches_plain_scores(cuda_device, shift):
-    """FP16 GEMM scores within 2e-3 of the plain FP32 scorer; same argmax unless near-tied."""
+@pytest.mark.parametrize("shift,spline", [(0.0, False), (4.0, False), (4.0, True)])
+def test_template_sharing_search_matches_plain_scores(cuda_device, shift, spline):
+    """FP16 GEMM scores within 2e-3 of the plain FP32 scorer; same argmax unless near-tied
+    (trilinear volumes, and a FourierVoxelSplineVolume for both searches)."""
+    from cryojax_b200 import simulator as S
     from cryojax_b200.healpix import OrientationGrid
     from cryojax_b200.search import PoseSearch, TemplateSharingSearch
 
@@ -138,6 +140,10 @@ def test_template_sharing_search_matches_plain_scores(cuda_device, shift):
         s.offset_in_angstroms = rng.uniform(-shift, shift, 2)
     obs = _observed(grid, fs, specs, 6, 0.3)
     model = _model(grid, specs)
+    if spline:
+        vol = S.FourierVoxelSplineVolume.from_fourier_voxel_grid(model.volume_parametrization.get_representation())
+        pose, tt, cfg = specs_to_model_args(specs)
+        model = S.make_image_model(vol, cfg, pose, tt)
     plain = PoseSearch(og.rotation_matrices()).run(model, obs, return_scores=True)
     shared = TemplateSharingSearch(og.rotation_matrices(), template_chunk=100, image_chunk=5).run(
         model, obs, return_scores=True)
