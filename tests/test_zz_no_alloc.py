@@ -33,26 +33,26 @@ def _inputs(seed, n_images, shape):
     return dvol.fourier_voxel_grid, params, model._flags(), cfg.padded_shape
 
 
-def _allocating(grid, params, flags, padded):
+def _allocating(grid, params, flags, padded, n=None):
     import torch
 
     from cryojax_b200 import _native as nat
 
     py, px = padded
-    desc = nat.make_desc(grid.shape[0], py, px, flags)
+    desc = nat.make_desc(grid.shape[0] if n is None else n, py, px, flags)
     ws = torch.empty(max(nat.workspace_size(desc, params.shape[0]), 1), dtype=torch.uint8, device="cuda")
     out = torch.empty((params.shape[0], py, px // 2 + 1), dtype=torch.complex64, device="cuda")
     nat.slice_ctf_forward(desc, grid, params, out, ws)
     return out
 
 
-def _noalloc(grid, params, flags, padded, images_per_chunk=0):
+def _noalloc(grid, params, flags, padded, images_per_chunk=0, n=None):
     import torch
 
     from cryojax_b200 import _native as nat
 
     py, px = padded
-    desc = nat.make_desc(grid.shape[0], py, px, flags, images_per_chunk=images_per_chunk)
+    desc = nat.make_desc(grid.shape[0] if n is None else n, py, px, flags, images_per_chunk=images_per_chunk)
     out = torch.empty((params.shape[0], py, px // 2 + 1), dtype=torch.complex64, device="cuda")
     nat.slice_ctf_forward_noalloc(desc, grid, params, out)
     return out
@@ -86,3 +86,27 @@ def test_noalloc_rejects_chunks_beyond_its_scratch(cuda_device):
         _noalloc(g, p, f, s, images_per_chunk=too_many)
     assert e.value.code == nat.CJX_ERR_UNSUPPORTED
     assert "CJX_NOALLOC_SCRATCH_BYTES" in str(e.value)
+
+
+@pytest.mark.parametrize("variant", ["ewald", "spline"])
+def test_noalloc_ewald_and_spline_match_allocating_entry_point(cuda_device, variant):
+    """The Ewald sphere's contrast (CJX_EWALD_SPHERE with the CTF) and C-order spline coefficients
+    (CJX_GRID_SPLINE, desc.n = coefficient side - 2) through the allocation-free entry point."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    g, p, f, s = _inputs(404, 5, (32, 32))
+    n = g.shape[0]
+    if variant == "ewald":
+        f = f | nat.CJX_EWALD_SPHERE
+    else:
+        coef = torch.empty((n + 2,) * 3, dtype=torch.complex64, device="cuda")
+        ws = torch.empty(nat.spline_coefficients_workspace_size(n), dtype=torch.uint8, device="cuda")
+        nat.spline_coefficients(g, coef, ws)
+        g, f = coef, f | nat.CJX_GRID_SPLINE
+    got = _noalloc(g, p, f, s, n=n)
+    ref = _allocating(g, p, f, s, n=n)
+    torch.cuda.synchronize()
+    err = rel_l2_per_image(got.cpu().numpy(), ref.cpu().numpy())
+    assert max(err) <= IMAGE_REL_L2_TOL, err
