@@ -141,7 +141,7 @@ class LearnedPoseSearch:
     are simulated and scored exactly as in the exhaustive search
     (PoseSearch with a candidate list), and images whose best score falls
     below ``threshold`` are searched exhaustively.  The exhaustive grid
-    search therefore stays both the fallback and the judge of the result.
+    search therefore stays both the fallback and the scorer of every result.
     """
 
     def __init__(self, net, grid, *, top_k=16, threshold=float("-inf"), search: PoseSearch | None = None):
