@@ -107,16 +107,33 @@ class ClockSampler:
         self.gpu_index = gpu_index
         self.proc = None
         self.path = None
+        self.mark_line = 0
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return sum(1 for _ in f)
+        except Exception:
+            return 0
 
     def start(self):
+        """Start nvidia-smi and wait (at most 5 s) for its first sample, so that a short timed region
+        that begins after this call is sampled from its start."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.gpu_index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self._lines() == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
+
+    def mark(self):
+        """Call when the timed region starts: samples written before this point are not part of it."""
+        self.mark_line = self._lines()
 
     def stop(self):
         if self.proc is None:
@@ -127,21 +144,28 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         rows = []
-        for line in open(self.path):
+        for k, line in enumerate(open(self.path)):
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                rows.append((k, float(parts[1]), float(parts[2]), parts[5:9]))
             except ValueError:
                 continue
         os.unlink(self.path)
-        if not rows:
+        region = [r for r in rows if r[0] >= self.mark_line]
+        note = None
+        if not region and rows:  # region shorter than one sampling period: the last sample before it
+            region, note = rows[-1:], "no sample fell inside the timed region; last sample before it"
+        if not region:
             return None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({names[i] for _, _, _, r in region for i, v in enumerate(r) if v.lower() == "active"})
+        out = {"sm_mhz": statistics.median(r[1] for r in region), "sm_max_mhz": max(r[2] for r in region),
+               "reasons": reasons, "samples": len(region)}
+        if note:
+            out["note"] = note
+        return out
 
 
 # ---------------------------------------------------------------------------
@@ -1167,6 +1191,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark()
     ev0.record(stream)
     for _ in range(args.steps):
         step()

@@ -62,7 +62,7 @@ CANDIDATES = [
     {"ilp": ilp, "tile": tile, "chunk_mb": chunk}
     for ilp in (1, 2, 4)
     for tile in (0, 1, 2)
-    for chunk in (256, 512)
+    for chunk in (512, 1024)
 ]
 
 

@@ -595,7 +595,7 @@ static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py
 
 // Process-wide tuning knobs (cjx_tuning_set / cjx_tuning_get).
 static std::atomic<int64_t> g_gather_ilp{2};
-static std::atomic<int64_t> g_chunk_bytes{512ll << 20};
+static std::atomic<int64_t> g_chunk_bytes{1024ll << 20};  // 16384 images 320^2 from N = 512: 4 % faster than 512 MB
 static std::atomic<int64_t> g_gather_mode{1};
 static std::atomic<int64_t> g_fft_mode{2};
 static std::atomic<int64_t> g_gather_tile{1};
@@ -653,7 +653,8 @@ size_t workspace_per_image(const SliceGeom& g) {
   return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2 + (size_t)g.ncols * g.ldh);
 }
 
-// Default chunk: about 64 MB of intermediates, so a chunk stays in L2.
+// Default chunk: CJX_TUNE_CHUNK_BYTES of intermediates (1 GiB unless set); larger
+// chunks mean fewer launches and shorter tails, at the cost of workspace.
 int64_t default_chunk(const SliceGeom& g, int64_t n_images) {
   const size_t per = workspace_per_image(g);
   int64_t c = (int64_t)((size_t)g_chunk_bytes.load() / std::max<size_t>(per, 1));

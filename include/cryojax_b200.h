@@ -366,7 +366,7 @@ CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t
 /* Process-wide tuning knobs (no counterpart in the reference; set by the
  * autotuner).  CJX_TUNE_GATHER_ILP: samples whose corner loads one lane
  * issues together in the gather (1, 2 or 4).  CJX_TUNE_CHUNK_BYTES: target
- * workspace bytes per chunk when desc->images_per_chunk is 0.
+ * workspace bytes per chunk when desc->images_per_chunk is 0 (default 1 GiB).
  * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
  * column-FFT kernel, 0 = one fused gather + column-FFT kernel.
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
