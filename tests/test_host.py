@@ -154,3 +154,19 @@ def test_gaussian_mixture_volume_shapes_and_pose():
     back = r.rotate_to_pose(pose, inverse=True)
     np.testing.assert_allclose(back.positions, p, atol=1e-12)
     np.testing.assert_allclose(S.GaussianMixtureVolume(p).translate_to_pose(pose).positions, p + [1.0, -2.0, 0.0])
+
+
+def test_host_streaming_sub_batch_plan():
+    """HostStreamingSimulator.sub_batches: sub_batch / 8, / 4, / 2, then full sub-batches, covering every
+    image once in order (the plan needs no device, so the simulator is not constructed)."""
+    from cryojax_b200.pipeline import HostStreamingSimulator
+
+    sim = object.__new__(HostStreamingSimulator)
+    sim.sub_batch = 2048
+    plan = sim.sub_batches(16384)
+    counts = [c for _, c in plan]
+    assert counts[:4] == [256, 512, 1024, 2048] and max(counts) == 2048 and sum(counts) == 16384
+    assert [s for s, _ in plan] == list(np.cumsum([0] + counts[:-1]))
+    assert sim.sub_batches(0) == [] and sim.sub_batches(100) == [(0, 100)]
+    sim.sub_batch = 3
+    assert sim.sub_batches(10) == [(0, 1), (1, 2), (3, 3), (6, 3), (9, 1)]
