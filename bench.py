@@ -24,6 +24,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -99,7 +100,14 @@ def config_dict(args, world):
 # clocks sampling
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi samples of SM clock, power and throttle reasons during the timed region.
+
+    Every sample carries nvidia-smi's own timestamp, and only samples taken at or after ``mark()``
+    count, so samples that nvidia-smi took before the region but flushed to its output file later
+    (block-buffered output) are never attributed to the region.  nvidia-smi runs line-buffered
+    through ``stdbuf -oL`` where that exists, so ``start()`` sees the first sample promptly."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -107,7 +115,7 @@ class ClockSampler:
         self.gpu_index = gpu_index
         self.proc = None
         self.path = None
-        self.mark_line = 0
+        self.mark_time = None
 
     def _lines(self):
         try:
@@ -116,15 +124,24 @@ class ClockSampler:
         except Exception:
             return 0
 
+    @staticmethod
+    def _epoch(stamp):
+        """nvidia-smi's timestamp (local time, "YYYY/MM/DD HH:MM:SS.mmm") as seconds since the epoch."""
+        import datetime
+
+        return datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+
     def start(self):
         """Start nvidia-smi and wait (at most 5 s) for its first sample, so that a short timed region
         that begins after this call is sampled from its start."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
-                 "-i", str(self.gpu_index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                   "-i", str(self.gpu_index)]
+            if shutil.which("stdbuf"):
+                cmd = ["stdbuf", "-oL"] + cmd
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
             t0 = time.time()
             while time.time() - t0 < 5.0 and self._lines() == 0 and self.proc.poll() is None:
                 time.sleep(0.02)
@@ -132,8 +149,8 @@ class ClockSampler:
             self.proc = None
 
     def mark(self):
-        """Call when the timed region starts: samples written before this point are not part of it."""
-        self.mark_line = self._lines()
+        """Call when the timed region starts: samples taken before this moment are not part of it."""
+        self.mark_time = time.time()
 
     def stop(self):
         if self.proc is None:
@@ -144,16 +161,17 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         rows = []
-        for k, line in enumerate(open(self.path)):
+        for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                rows.append((k, float(parts[1]), float(parts[2]), parts[5:9]))
+                rows.append((self._epoch(parts[0]), float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
         os.unlink(self.path)
-        region = [r for r in rows if r[0] >= self.mark_line]
+        mark = self.mark_time if self.mark_time is not None else float("-inf")
+        region = [r for r in rows if r[0] >= mark]
         note = None
         if not region and rows:  # region shorter than one sampling period: the last sample before it
             region, note = rows[-1:], "no sample fell inside the timed region; last sample before it"
@@ -161,8 +179,8 @@ class ClockSampler:
             return None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for _, _, _, r in region for i, v in enumerate(r) if v.lower() == "active"})
-        out = {"sm_mhz": statistics.median(r[1] for r in region), "sm_max_mhz": max(r[2] for r in region),
-               "reasons": reasons, "samples": len(region)}
+        out = {"sm_mhz": statistics.median(r[1] for r in region), "sm_min_mhz": min(r[1] for r in region),
+               "sm_max_mhz": max(r[2] for r in region), "reasons": reasons, "samples": len(region)}
         if note:
             out["note"] = note
         return out
@@ -251,11 +269,17 @@ def run_reference(args):
         vals.append(v)
     wall = time.perf_counter() - t_all
     value = statistics.median(vals)
+    cfg = config_dict(args, 1)
+    for key in ("volume_layout", "processing_order", "l2_flush"):  # device-side choices; the port has none
+        cfg.pop(key, None)
+    cfg["images_per_step"] = sample
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000.0 * args.images / value, "higher_is_better": True,
+        "warmup": args.warmup, "images_per_step": sample,
+        # one step is the bounded sample of `sample` images of the workload, not all args.images of it
+        "ms_per_step": 1000.0 * sample / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict(args, 1),
+        "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
                          "sample": f"{sample} images per step of the same workload (N={n}, {args.image}^2), float64 NumPy "
                                    f"oracle of the reference path, {workers} spawn workers; JAX is not installed so "

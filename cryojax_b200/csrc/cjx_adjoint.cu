@@ -582,11 +582,8 @@ static cudaError_t allow_smem_adj(K kernel) {
 }
 
 static int ensure_adjoint_smem_attrs() {
-  static std::once_flag flags[64];
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
-  int err = CJX_OK;
-  std::call_once(flags[dev & 63], [&] {
+  static PerDeviceOnce once;
+  const cudaError_t err = once.run([] {
     cudaError_t e = cudaSuccess;
 #define CJX_ADJ_ATTR(R)                                                    \
   if (e == cudaSuccess) e = allow_smem_adj(k_colfft_loss_adj<R>);          \
@@ -595,9 +592,9 @@ static int ensure_adjoint_smem_attrs() {
     CJX_ADJ_ATTR(1) CJX_ADJ_ATTR(2) CJX_ADJ_ATTR(3) CJX_ADJ_ATTR(4) CJX_ADJ_ATTR(5)
     CJX_ADJ_ATTR(6) CJX_ADJ_ATTR(8) CJX_ADJ_ATTR(10) CJX_ADJ_ATTR(12) CJX_ADJ_ATTR(16)
 #undef CJX_ADJ_ATTR
-    if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
+    return e;
   });
-  return err;
+  return err == cudaSuccess ? CJX_OK : check_cuda(err, "cudaFuncSetAttribute (adjoint kernels)");
 }
 
 __global__ void k_zero_doubles(double* p, int64_t count) {

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -823,5 +824,24 @@ Tuning current_tuning();
 void set_last_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int check_cuda(cudaError_t e, const char* what);
+
+// Per-device one-time set-up (function attributes belong to each device's
+// context).  `init` runs the first time a thread reaches this with a given
+// device current; its outcome is stored and returned to every later call on
+// that device, so a failed set-up keeps failing instead of letting kernels
+// that depend on it launch.  Device indices from kMaxDevices up are refused.
+constexpr int kMaxDevices = 64;
+struct PerDeviceOnce {
+  std::once_flag flags[kMaxDevices];
+  cudaError_t errs[kMaxDevices] = {};
+  template <typename F>
+  cudaError_t run(F&& init) {
+    int dev = 0;
+    if (cudaError_t e = cudaGetDevice(&dev)) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::call_once(flags[dev], [&] { errs[dev] = init(); });
+    return errs[dev];
+  }
+};
 
 }  // namespace cjx

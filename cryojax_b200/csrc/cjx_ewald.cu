@@ -347,11 +347,8 @@ size_t ewald_cols_smem(const SliceGeom& g) {
 }
 
 static int ensure_ewald_smem() {
-  static std::once_flag flags[64];
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
-  int err = CJX_OK;
-  std::call_once(flags[dev & 63], [&] {
+  static PerDeviceOnce once;
+  const cudaError_t err = once.run([] {
     const int kMax = 227 * 1024;
     cudaError_t e = cudaFuncSetAttribute(k_ewald_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ewald_colfft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
@@ -365,9 +362,9 @@ static int ensure_ewald_smem() {
     CJX_EW_ATTR(1) CJX_EW_ATTR(2) CJX_EW_ATTR(3) CJX_EW_ATTR(4) CJX_EW_ATTR(5)
     CJX_EW_ATTR(6) CJX_EW_ATTR(8) CJX_EW_ATTR(10) CJX_EW_ATTR(12) CJX_EW_ATTR(16)
 #undef CJX_EW_ATTR
-    if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
+    return e;
   });
-  return err;
+  return err == cudaSuccess ? CJX_OK : check_cuda(err, "cudaFuncSetAttribute (Ewald kernels)");
 }
 
 int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream,

@@ -143,15 +143,11 @@ int make_operand_map(CUtensorMap* map, const void* base, int64_t rows, int64_t k
 // Once per device (function attributes belong to each device's context).
 template <int BN>
 static cudaError_t gemm_smem_attr() {
-  static std::once_flag flags[64];
-  static cudaError_t errs[64];
-  int dev = 0;
-  if (cudaError_t e = cudaGetDevice(&dev)) return e;
-  std::call_once(flags[dev & 63], [&] {
-    errs[dev & 63] = cudaFuncSetAttribute(k_gemm_tc<BN, GemmEpilogue>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)tc::gemm_smem_bytes(BN));
+  static PerDeviceOnce once;
+  return once.run([] {
+    return cudaFuncSetAttribute(k_gemm_tc<BN, GemmEpilogue>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tc::gemm_smem_bytes(BN));
   });
-  return errs[dev & 63];
 }
 
 template <int BN>

@@ -32,17 +32,20 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CJX_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
 static std::mutex g_noalloc_mutex;
 static void* g_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of g_noalloc_scratch on the current device.  Looked up once
 // per device (the host-side symbol is only a stand-in, never a device
-// address).
+// address) and cached for the life of the process.  The cache does not
+// survive a reset of the device's primary context (cudaDeviceReset, or the
+// context being destroyed and re-created): after one, the library reloads on
+// that device and the cached address no longer names the array, so a process
+// that resets a device must not call this entry point on it again.
 static int noalloc_scratch(void** ptr) {
   int dev = 0;
   if (int e = check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return e;
-  if (dev < 0 || dev >= kMaxDevices) return fail(CJX_ERR_UNSUPPORTED, "device index beyond 64");
+  if (dev < 0 || dev >= kMaxDevices) return fail(CJX_ERR_UNSUPPORTED, "device index beyond the 64 supported");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (!g_noalloc_ptr[dev]) {
     void* p = nullptr;

@@ -320,11 +320,8 @@ __global__ void k_unpack_best(const unsigned long long* __restrict__ best, float
 // Once per device (function attributes belong to each device's context);
 // the outcome of that first attempt is returned to every later call.
 static cudaError_t search_smem_attrs() {
-  static std::once_flag flags[64];
-  static cudaError_t errs[64];
-  int dev = 0;
-  if (cudaError_t e = cudaGetDevice(&dev)) return e;
-  std::call_once(flags[dev & 63], [&] {
+  static PerDeviceOnce once;
+  return once.run([] {
     cudaError_t err = cudaSuccess;
 #define CJX_SA(R)                                                                                              \
   if (err == cudaSuccess)                                                                                      \
@@ -333,9 +330,8 @@ static cudaError_t search_smem_attrs() {
     err = cudaFuncSetAttribute(k_ewald_colfft_score_reg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     CJX_SA(1) CJX_SA(2) CJX_SA(3) CJX_SA(4) CJX_SA(5) CJX_SA(6) CJX_SA(8) CJX_SA(10) CJX_SA(12) CJX_SA(16)
 #undef CJX_SA
-    errs[dev & 63] = err;
+    return err;
   });
-  return errs[dev & 63];
 }
 
 // Workspace: per candidate the forward intermediates + a params record,

@@ -721,11 +721,8 @@ static cudaError_t allow_smem(K kernel) {
 }
 
 static int ensure_smem_attrs() {
-  static std::once_flag flags[64];
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(cudaGetLastError(), "cudaGetDevice");
-  int err = CJX_OK;
-  std::call_once(flags[dev & 63], [&] {
+  static PerDeviceOnce once;
+  const cudaError_t e = once.run([] {
     cudaError_t e = allow_smem(k_gather_colifft<1, LinearLayout>);
     if (e == cudaSuccess) e = allow_smem(k_gather_colifft<2, LinearLayout>);
     if (e == cudaSuccess) e = allow_smem(k_gather_colifft<4, LinearLayout>);
@@ -735,9 +732,9 @@ static int ensure_smem_attrs() {
     if (e == cudaSuccess) e = allow_smem(k_colifft_window);
     if (e == cudaSuccess) e = allow_smem(k_rows_c2r_r2c);
     if (e == cudaSuccess) e = allow_smem(k_colfft_epilogue);
-    if (e != cudaSuccess) err = check_cuda(e, "cudaFuncSetAttribute");
+    return e;
   });
-  return err;
+  return e == cudaSuccess ? CJX_OK : check_cuda(e, "cudaFuncSetAttribute (slice kernels)");
 }
 
 int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream,

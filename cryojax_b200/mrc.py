@@ -32,10 +32,19 @@ _HEADER_BYTES = 1024
 
 
 def _suffix(filename) -> str:
-    suffixes = pathlib.Path(filename).suffixes
-    if len(suffixes) == 0 or suffixes[0] not in (".mrc", ".mrcs"):
-        raise OSError(f"Filename should include .mrc or .mrcs suffix. Got filename {filename}.")
-    return suffixes[0]
+    """'.mrc' or '.mrcs': the first suffix of an MRC file name (anything else is an OSError)."""
+    first = (pathlib.Path(filename).suffixes or [None])[0]
+    if first not in (".mrc", ".mrcs"):
+        raise OSError(f"{str(filename)!r} is not an MRC file name: expected a '.mrc' or '.mrcs' suffix")
+    return first
+
+
+def _require_suffix(filename, wanted: str, what: str, ndim: int, array) -> None:
+    """Writers: `what` goes to a file named *`wanted` and must be an `ndim`-dimensional array."""
+    if _suffix(filename) != wanted:
+        raise OSError(f"an MRC {what} is written to a '{wanted}' file, not {str(filename)!r}")
+    if np.ndim(array) != ndim:
+        raise ValueError(f"an MRC {what} is a {ndim}-D array; got {np.ndim(array)}-D")
 
 
 def read_mrc_header(filename) -> dict:
@@ -174,28 +183,19 @@ def _no_compression(compression):
 def write_image_to_mrc(image, pixel_size, filename, overwrite: bool = False, compression=None):
     """cryojax/io/_mrc.py:103-134 (suffix .mrc, a 2-D array)."""
     _no_compression(compression)
-    if _suffix(filename) != ".mrc":
-        raise OSError(f"The suffix for an image in MRC format must be .mrc. Got {filename}.")
-    if np.ndim(image) != 2:
-        raise ValueError("image.ndim must be equal to 2.")
+    _require_suffix(filename, ".mrc", "image", 2, image)
     _write(image, pixel_size, filename, "image", overwrite)
 
 
 def write_image_stack_to_mrc(image_stack, pixel_size, filename, overwrite: bool = False, compression=None):
     """cryojax/io/_mrc.py:137-172 (suffix .mrcs, a 3-D array; written as an image stack)."""
     _no_compression(compression)
-    if _suffix(filename) != ".mrcs":
-        raise OSError(f"The suffix for an image stack in MRC format must be .mrcs. Instead, got {filename}.")
-    if np.ndim(image_stack) != 3:
-        raise ValueError("image_stack.ndim must be equal to 3.")
+    _require_suffix(filename, ".mrcs", "image stack", 3, image_stack)
     _write(image_stack, pixel_size, filename, "image_stack", overwrite)
 
 
 def write_volume_to_mrc(voxel_grid, voxel_size, filename, overwrite: bool = False, compression=None):
     """cryojax/io/_mrc.py:175-210 (suffix .mrc, a 3-D array; written as a volume)."""
     _no_compression(compression)
-    if _suffix(filename) != ".mrc":
-        raise OSError(f"The suffix for a volume in MRC format must be .mrc. Got {filename}.")
-    if np.ndim(voxel_grid) != 3:
-        raise ValueError("voxel_grid.ndim must be equal to 3.")
+    _require_suffix(filename, ".mrc", "volume", 3, voxel_grid)
     _write(voxel_grid, voxel_size, filename, "volume", overwrite)

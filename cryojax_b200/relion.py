@@ -77,46 +77,58 @@ def _empty_frame(entries):
 # ---------------------------------------------------------------------------
 
 
-def _validate_mode(mode):
-    if mode not in ("r", "w"):
-        raise ValueError(f"Passed unsupported `mode = {mode}`. Supported modes are 'r' and 'w'.")
+_MODES = {"r": "read an existing STAR file", "w": "write a new STAR file"}
+_PARAMETER_TYPES = {"image_config": BasicImageConfig, "transfer_theory": ContrastTransferTheory,
+                    "pose": EulerAnglePose}
+
+
+def _checked_mode(mode):
+    """The file mode, if it is one of _MODES."""
+    if mode not in _MODES:
+        options = "; ".join(f"{k!r} to {v}" for k, v in _MODES.items())
+        raise ValueError(f"unknown mode {mode!r}: use {options}")
     return mode
 
 
-def _validate_dataset_index(cls, index, n_rows):
-    msg = lambda i: (f"The index at which the `{cls.__name__}` was accessed was out of bounds! The number of rows "
-                     f"in the dataset is {n_rows}, but you tried to access the index {i}.")
+def _check_index(owner, index, n_rows):
+    """Accept an integer row (negative counts from the end), a slice that starts inside the table, or a
+    non-empty one-dimensional integer array; anything else is an IndexError naming the dataset class."""
+    name = owner.__name__
     if isinstance(index, (int, np.integer)):
-        if index > n_rows - 1:
-            raise IndexError(msg(index))
-    elif isinstance(index, slice):
-        if index.start is not None and index.start > n_rows - 1:
-            raise IndexError(msg(index.start))
-    elif isinstance(index, np.ndarray):
-        if index.size == 0:
-            raise IndexError("Found that the index passed to the dataset was an empty numpy array.")
-    else:
-        raise IndexError(f"Indexing with the type {type(index)} is not supported by `{cls.__name__}`. Index with an "
-                         "integer, a slice or a one-dimensional integer numpy array.")
+        if not -n_rows <= int(index) < n_rows:
+            raise IndexError(f"{name}[{int(index)}]: the STAR file holds {n_rows} particle rows")
+        return
+    if isinstance(index, slice):
+        if index.start is not None and index.start >= n_rows:
+            raise IndexError(f"{name}[{index.start}:...]: the slice starts past the {n_rows} particle rows")
+        return
+    if isinstance(index, np.ndarray):
+        if index.ndim != 1 or index.size == 0:
+            raise IndexError(f"{name}: an index array must be one-dimensional and non-empty (shape {index.shape})")
+        return
+    raise IndexError(f"{name} is indexed by an int, a slice or a 1-D integer numpy array, not {type(index).__name__}")
 
 
-def _validate_starfile_data(data):
+def _check_star_blocks(data):
+    """The particles and optics blocks exist and carry every column the reader needs."""
     for block, entries in (("particles", RELION_REQUIRED_PARTICLE_ENTRIES), ("optics", RELION_REQUIRED_OPTICS_ENTRIES)):
         if block not in data:
-            raise ValueError(f"Missing key '{block}' in the STAR file.")
-        keys = [k for k, _ in entries]
-        if not set(keys).issubset(set(data[block].columns)):
-            raise ValueError(f"Missing required keys in starfile '{block}' group. Required keys are {tuple(keys)}.")
+            raise ValueError(f"the STAR data has no '{block}' block (blocks present: {sorted(data)})")
+        missing = sorted({k for k, _ in entries} - set(data[block].columns))
+        if missing:
+            raise ValueError(f"the STAR '{block}' block lacks the required columns {missing}")
 
 
-def _validate_parameters(parameters, force_keys=False):
-    if force_keys and not {"image_config", "transfer_theory", "pose"}.issubset(parameters):
-        raise ValueError("The parameter dictionary must have keys 'pose', 'transfer_theory', and 'image_config'.")
-    for key, cls in (("image_config", BasicImageConfig), ("transfer_theory", ContrastTransferTheory),
-                     ("pose", EulerAnglePose)):
+def _check_parameter_types(parameters, require_all=False):
+    """Each of pose / transfer_theory / image_config present has the simulator type the writer converts;
+    with require_all, all three must be present."""
+    if require_all:
+        missing = sorted(set(_PARAMETER_TYPES) - set(parameters))
+        if missing:
+            raise ValueError(f"the parameters lack {missing}: appending needs {sorted(_PARAMETER_TYPES)}")
+    for key, cls in _PARAMETER_TYPES.items():
         if key in parameters and not isinstance(parameters[key], cls):
-            raise TypeError(f"Found that dict key '{key}' was not type `{cls.__name__}`. Instead, it was type "
-                            f"{type(parameters[key]).__name__}.")
+            raise TypeError(f"parameters[{key!r}] should be a {cls.__name__}, got {type(parameters[key]).__name__}")
 
 
 # ---------------------------------------------------------------------------
@@ -300,7 +312,7 @@ class RelionParticleParameterFile:
                  selection_filter: dict[str, Callable] | None = None, *, loads_metadata: bool = False,
                  broadcasts_image_config: bool = True, loads_envelope: bool = False,
                  updates_optics_group: bool = False, inverts_rotation: bool = False, pad_options: dict | None = None):
-        self._mode = _validate_mode(mode)
+        self._mode = _checked_mode(mode)
         self._pad_options = dict(pad_options or {})
         self.path_to_starfile = pathlib.Path(path_to_starfile)
         self._starfile_data = self._load(selection_filter, exists_ok)
@@ -317,7 +329,7 @@ class RelionParticleParameterFile:
                 raise FileNotFoundError(f"Set `mode = 'r'`, but STAR file {p} does not exist. To write a new STAR "
                                         "file, set `mode = 'w'`.")
             data = _star.read_starfile(p)
-            _validate_starfile_data(data)
+            _check_star_blocks(data)
             if selection_filter is not None:
                 data["particles"] = _select(data["particles"], selection_filter)
             return {"optics": data["optics"], "particles": data["particles"]}
@@ -339,7 +351,7 @@ class RelionParticleParameterFile:
 
     @starfile_data.setter
     def starfile_data(self, value):
-        _validate_starfile_data(value)
+        _check_star_blocks(value)
         self._starfile_data = {"optics": value["optics"], "particles": value["particles"]}
 
     def copy(self):
@@ -350,7 +362,7 @@ class RelionParticleParameterFile:
 
     def __getitem__(self, index):
         particles = self._starfile_data["particles"]
-        _validate_dataset_index(type(self), index, len(particles))
+        _check_index(type(self), index, len(particles))
         scalar = isinstance(index, (int, np.integer))
         rows = particles.iloc[[int(index)]] if scalar else particles.iloc[index]
         optics = _optics_group_of(rows, self._starfile_data["optics"])
@@ -364,8 +376,8 @@ class RelionParticleParameterFile:
 
     def __setitem__(self, index, value):
         particles = self._starfile_data["particles"]
-        _validate_dataset_index(type(self), index, len(particles))
-        _validate_parameters(value)
+        _check_index(type(self), index, len(particles))
+        _check_parameter_types(value)
         value = dict(value)
         if "pose" in value and self.inverts_rotation:
             value["pose"] = _invert_rotation(value["pose"])
@@ -385,7 +397,7 @@ class RelionParticleParameterFile:
 
     def append(self, value):
         """relion.py:382-419: a new optics group for the appended particles."""
-        _validate_parameters(value, force_keys=True)
+        _check_parameter_types(value, require_all=True)
         value = dict(value)
         if self.inverts_rotation:
             value["pose"] = _invert_rotation(value["pose"])
@@ -441,7 +453,7 @@ class RelionParticleStackDataset:
 
     def __init__(self, parameter_file: RelionParticleParameterFile, path_to_relion_project, mode: str = "r",
                  mrcfile_settings: dict[str, Any] | None = None, *, loads_parameters: bool = True):
-        self._mode = _validate_mode(mode)
+        self._mode = _checked_mode(mode)
         self.parameter_file = parameter_file
         self.path_to_relion_project = pathlib.Path(path_to_relion_project)
         s = dict(mrcfile_settings or {})
@@ -490,7 +502,7 @@ class RelionParticleStackDataset:
     def __getitem__(self, index):
         pf = self.parameter_file
         particles = pf.starfile_data["particles"]
-        _validate_dataset_index(type(self), index, len(particles))
+        _check_index(type(self), index, len(particles))
         scalar = isinstance(index, (int, np.integer))
         rows = particles.iloc[[int(index)]] if scalar else particles.iloc[index]
         if "rlnImageName" not in rows.columns:

@@ -19,11 +19,13 @@ import numpy as np
 import pandas as pd
 
 
-def _validate_filename(filename, mode: str):
-    suffixes = pathlib.Path(filename).suffixes
-    if not (len(suffixes) == 1 and suffixes[0] == ".star"):
-        raise OSError(f"Tried to {'write' if mode == 'w' else 'read'} STAR file, but the filename does not "
-                      f"include a '.star' suffix. Got filename '{filename}'.")
+def _check_star_path(filename, mode: str):
+    """STAR files are named *.star with no other suffix (the same rule on read and write)."""
+    path = pathlib.Path(filename)
+    if path.suffixes != [".star"]:
+        action = "write" if mode == "w" else "read"
+        raise OSError(f"cannot {action} {str(path)!r} as a STAR file: its name must end in '.star' "
+                      f"(and carry no other suffix), found {path.suffixes or 'none'}")
 
 
 def _typed(values: list[str]) -> pd.Series:
@@ -53,7 +55,7 @@ def _finish(name, columns, rows, pairs, out):
 
 def read_starfile(filename) -> dict[str, pd.DataFrame]:
     """Every block of a STAR file as {block name: DataFrame}.  cryojax/io/_starfile.py:12-20."""
-    _validate_filename(filename, "r")
+    _check_star_path(filename, "r")
     out: dict[str, pd.DataFrame] = {}
     name, columns, rows, pairs, in_loop = None, [], [], [], False
     with open(filename) as f:
@@ -98,7 +100,7 @@ def _format(v) -> str:
 
 def write_starfile(starfile_data: dict[str, pd.DataFrame], filename, **kwargs):
     """Write {block name: DataFrame} as loop_ tables.  cryojax/io/_starfile.py:23-29."""
-    _validate_filename(filename, "w")
+    _check_star_path(filename, "w")
     if kwargs.get("overwrite") is False and pathlib.Path(filename).exists():
         raise FileExistsError(str(filename))
     lines = ["# Created by cryojax_b200", ""]

@@ -286,7 +286,9 @@ CJX_API int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_gro
  * GPU that loads the library until the process exits.  Results equal
  * cjx_slice_ctf_forward's.
  *  - The first call on each device looks up that array's device address;
- *    make that first call before any stream capture.
+ *    make that first call before any stream capture.  The address is cached
+ *    for the life of the process and does not survive a reset of the
+ *    device (cudaDeviceReset): do not call this again on a reset device.
  *  - All calls on a device share the array: calls that overlap on the GPU
  *    (other streams, other host threads) race; serialise them.
  *  - Returns CJX_ERR_UNSUPPORTED if one image, or desc->images_per_chunk

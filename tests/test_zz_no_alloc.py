@@ -76,6 +76,31 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda_device):
     assert max(e2) <= IMAGE_REL_L2_TOL, e2
 
 
+def test_noalloc_leaves_free_device_memory_unchanged(cuda_device):
+    """The property the entry point is named for: after a warm-up call (which may load kernels and look up
+    the scratch address), further calls change the device's free memory (cudaMemGetInfo, which
+    torch.cuda.mem_get_info wraps) by not one byte."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    g, p, f, s = _inputs(505, 11, (32, 32))
+    py, px = s
+    desc = nat.make_desc(g.shape[0], py, px, f, images_per_chunk=3)
+    out = torch.empty((p.shape[0], py, px // 2 + 1), dtype=torch.complex64, device="cuda")
+    nat.slice_ctf_forward_noalloc(desc, g, p, out)
+    torch.cuda.synchronize()
+    first = out.clone()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        nat.slice_ctf_forward_noalloc(desc, g, p, out)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0, (free0, free1)
+    assert torch.equal(out, first)
+
+
 def test_noalloc_rejects_chunks_beyond_its_scratch(cuda_device):
     from cryojax_b200 import _native as nat
 
