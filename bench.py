@@ -244,6 +244,34 @@ def cpu_oracle_throughput(grid_c128, batch, n_images, image, pixel_size, voltage
     return done / busy, done, time.perf_counter() - t0
 
 
+PARITY_IMAGES = 8  # timed images per leg checked against the float64 oracle after all timed regions
+PARITY_TOL = 1e-5  # relative L2 per image, the tolerance of the parity tests
+
+
+def oracle_specs(batch, idx, shape, pixel_size=2.0, voltage=300.0):
+    """Oracle parameter records of images `idx` of a synthetic batch (the same pose / CTF the device saw)."""
+    from oracle import cryojax_oracle as O
+
+    return [O.ImageSpec(shape=shape, pixel_size=pixel_size, voltage_in_kilovolts=voltage, wxyz=batch.wxyz[b],
+                        offset_in_angstroms=batch.offsets[b], defocus_in_angstroms=batch.defocus[b],
+                        astigmatism_in_angstroms=batch.astigmatism[b], astigmatism_angle=batch.astigmatism_angle[b])
+            for b in idx]
+
+
+def oracle_parity(grid, got, specs, n=None, grid_source="float64 FFT of the same real volume", **kw):
+    """Per-image relative L2 of the device's images `got` (host complex64) against the float64 oracle
+    (cryojax_oracle.compute_fourier_image with keyword options `kw`) fed `grid`."""
+    from oracle import cryojax_oracle as O
+
+    n = grid.shape[0] if n is None else n
+    fs = O.make_frequency_slice((n, n), outputs_rfftfreqs=False)
+    t0 = time.perf_counter()
+    errs = [float(O.relative_l2(g, O.compute_fourier_image(grid, fs, s, **kw))) for g, s in zip(got, specs)]
+    return {"max_rel_l2": max(errs), "median_rel_l2": statistics.median(errs), "images": len(errs),
+            "tolerance": PARITY_TOL, "pass": max(errs) <= PARITY_TOL, "oracle_grid": grid_source,
+            "oracle_seconds": time.perf_counter() - t0}
+
+
 def run_reference(args):
     """Reference arm: the oracle port on all host cores, same config/metric."""
     import numpy as np
@@ -400,7 +428,11 @@ def measure_batched_uneven(dev, steps, warmup, seed):
         from cryojax_b200.batched import autotune
 
         tun.append(autotune(m))
-    return {"metric": "mixed-size slice+CTF images/s (96^3..256^3 volumes, images at box size)",
+    # the timed replay's own first images of each group, for the oracle check after all timed regions
+    parity = [{"box": box, "gaussians": ng, "volume_seed": seed + 10 + i, "batch_seed": seed + 20 + i,
+               "got": sim.outputs[i][:PARITY_IMAGES].cpu().numpy()} for i, (box, ng) in enumerate(specs)]
+    return {"_parity": parity,
+            "metric": "mixed-size slice+CTF images/s (96^3..256^3 volumes, images at box size)",
             "value": sim.n_images / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms,
             "images_per_step": sim.n_images, "groups": [f"N={2 * b} -> {b}x{b} x 4096" for b, _ in specs],
             "launch": "one CUDA graph replay per step (cjx_slice_ctf_forward_multi captured once)",
@@ -784,11 +816,16 @@ def measure_spline(dev, grid, batch, cfg, steps, warmup, n_images, cpu_images):
            "gather_us_per_image": prof["k_gather_slice"][1] * 1000.0 / n_images,
            "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()},
            "bound": "L1 data-stage wavefronts (ncu: 83 % of peak; DRAM 27 %)"}
+    got = out[:PARITY_IMAGES].cpu().numpy()
     del out, wsf, pd
     if cpu_images:
         from oracle import cryojax_oracle as O
 
         coef_h = coef.cpu().numpy().astype(np.complex128)
+        res["parity"] = oracle_parity(coef_h, got, oracle_specs(batch, range(len(got)), cfg.shape), n=n,
+                                      grid_source="the device-solved coefficients in float64 (the solve itself is "
+                                                  "checked against the oracle's banded solve in the tests)",
+                                      spline=True)
         fs = O.make_frequency_slice((n, n), outputs_rfftfreqs=False)
         t0 = time.perf_counter()
         for b in range(cpu_images):
@@ -850,7 +887,8 @@ def measure_ewald(dev, volume, batch, cfg, steps, warmup, n_images, cpu_images):
     nat.profile_enable(False)
     res = {"value": n_images / (ms / 1000.0), "unit": UNIT, "images": n_images, "ms_per_step": ms,
            "layout": "x-pair bricked grid, trilinear",
-           "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()}}
+           "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()},
+           "_parity": out[:PARITY_IMAGES].cpu().numpy()}
     del out, ws, pd
     if cpu_images:
         from oracle import cryojax_oracle as O
@@ -1232,6 +1270,7 @@ def main():
     torch.cuda.synchronize()
     prof = nat.profile_read()
     nat.profile_enable(False)
+    headline_got = out[:PARITY_IMAGES].cpu().numpy()  # the timed steps' images 0..7 (every step writes the same)
     launches_per_step = sum(c for c, _ in prof.values())
     top = max(prof.items(), key=lambda kv: kv[1][1])
     top_name, (top_count, top_ms) = top
@@ -1387,18 +1426,58 @@ def main():
         except Exception as e:
             render = {"error": repr(e)}
 
-    # ---- CPU baseline (rank 0, N=1 only)
+    # ---- CPU legs (rank 0, N=1 only): the oracle as CPU baseline and as the parity check of the timed images
     cpu = None
+    parity = None
+    batched_parity = batched.pop("_parity", None) if isinstance(batched, dict) else None
+    ewald_parity = ewald.pop("_parity", None) if isinstance(ewald, dict) else None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import cryojax_oracle as O
+
+        grid_f64 = None
         try:
-            grid_host = volume.fourier_voxel_grid.cpu().numpy().astype(np.complex128)
-            v, done, wall = cpu_oracle_throughput(grid_host, batch, args.cpu_sample, args.image, 2.0, 300.0, 1)
+            grid_f64, _ = O.fourier_voxel_grid_from_real_voxel_grid(vol_np, pad_scale=args.pad_scale)
+            v, done, wall = cpu_oracle_throughput(grid_f64, batch, args.cpu_sample, args.image, 2.0, 300.0, 1)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"{done} images of this workload through the float64 NumPy oracle of the reference "
                              f"path, 1 process ({wall:.1f} s)"}
-            del grid_host
         except Exception as e:
             cpu = {"error": str(e)}
+        parity = {}
+        try:
+            parity["headline"] = oracle_parity(grid_f64, headline_got,
+                                               oracle_specs(batch, range(len(headline_got)), cfg.shape))
+        except Exception as e:
+            parity["headline"] = {"error": repr(e)}
+        if ewald_parity is not None:
+            try:
+                ewald["parity"] = oracle_parity(grid_f64, ewald_parity,
+                                                oracle_specs(batch, range(len(ewald_parity)), cfg.shape), ewald=True)
+            except Exception as e:
+                ewald["parity"] = {"error": repr(e)}
+        del grid_f64
+        if batched_parity is not None:
+            groups = []
+            for grp in batched_parity:
+                try:
+                    v_np = synthetic.gaussian_sum_volume(grp["box"], grp["gaussians"], grp["volume_seed"],
+                                                         sigma_range=(1.0, 3.0))
+                    g64, _ = O.fourier_voxel_grid_from_real_voxel_grid(v_np, pad_scale=2.0)
+                    b = synthetic.image_batch(4096, grp["batch_seed"])
+                    r = oracle_parity(g64, grp["got"], oracle_specs(b, range(len(grp["got"])), (grp["box"],) * 2))
+                    r["group"] = f"N={2 * grp['box']} -> {grp['box']}^2"
+                    groups.append(r)
+                    del g64
+                except Exception as e:
+                    groups.append({"error": repr(e)})
+            batched["parity"] = {"groups": groups,
+                                 "max_rel_l2": max((g.get("max_rel_l2", float("inf")) for g in groups),
+                                                   default=None)}
+        parity["max_rel_l2_per_leg"] = {
+            "headline": parity["headline"].get("max_rel_l2"),
+            "batched_uneven": (batched or {}).get("parity", {}).get("max_rel_l2"),
+            "spline": ((spline or {}).get("parity") or {}).get("max_rel_l2"),
+            "ewald": ((ewald or {}).get("parity") or {}).get("max_rel_l2")}
 
     if rank == 0:
         line = {
@@ -1423,6 +1502,7 @@ def main():
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "parity": parity,
             "batched_uneven": batched,
             "gradient": gradient,
             "pose_search": pose_search,

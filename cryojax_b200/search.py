@@ -177,21 +177,29 @@ class LearnedPoseSearch:
             score[low] = ex.best_score
         return LearnedSearchResult(best, score, low if fallback else np.zeros_like(low), dirs)
 
-    def calibrate_threshold(self, image_model, observed, exhaustive_best, *, target_agreement=0.995):
-        """Lowest threshold at which the calibration images agree with the exhaustive optimum.
+    def calibrate_threshold(self, image_model, observed, exhaustive_best, *, target_agreement=0.995,
+                            min_fallback_fraction=0.02):
+        """Fallback threshold from calibration images whose exhaustive optimum is known.
 
-        Runs the learned search without fallback on calibration images whose
-        exhaustive optimum is known; images that disagree need the fallback,
+        Runs the learned search without fallback on the calibration images.
+        Images that disagree with the exhaustive optimum need the fallback,
         so the threshold is set just above the best score of the disagreeing
         images, allowing (1 - target_agreement) of the set to disagree above
-        it.  Sets and returns ``self.threshold``.
+        it.  The threshold is never below the ``min_fallback_fraction``
+        quantile of the calibration images' best scores: when (almost) no
+        calibration image disagrees, the least confident images still fall
+        back, so the fallback stays live on images unlike the calibration
+        set.  Sets and returns ``self.threshold`` (always finite).
         """
         res = self.run(image_model, observed, fallback=False)
         wrong = res.best_orientation != np.asarray(exhaustive_best)
         allowed = int(np.floor((1.0 - target_agreement) * len(wrong)))
         s = np.sort(res.best_score[wrong])[::-1]
-        self.threshold = float(np.nextafter(np.float32(s[allowed]), np.float32(np.inf))) if len(s) > allowed else \
-            float("-inf")
+        floor = float(np.quantile(res.best_score, min_fallback_fraction)) if min_fallback_fraction > 0 else -np.inf
+        thr = float(np.nextafter(np.float32(s[allowed]), np.float32(np.inf))) if len(s) > allowed else -np.inf
+        self.threshold = max(thr, floor)
+        if not np.isfinite(self.threshold):  # min_fallback_fraction = 0 and nothing disagreed
+            self.threshold = float(np.min(res.best_score))
         return self.threshold
 
 

@@ -92,12 +92,12 @@ def test_calibrated_fallback_reaches_agreement(setup):
     cal_ex = search.run(cal_model, cal_noisy)
     ls = LearnedPoseSearch(net, grid, top_k=8, search=search)
     thr = ls.calibrate_threshold(cal_model, cal_noisy, cal_ex.best_orientation, target_agreement=1.0)
-    assert np.isfinite(thr) or thr == float("-inf")
-    model, noisy = _batch(V, cfg, 96, 9, 0.1)
+    assert np.isfinite(thr)  # the fallback is always live: at least the least confident 2 % fall back
+    model, noisy = _batch(V, cfg, 256, 9, 0.1)
     ex = search.run(model, noisy)
     res = ls.run(model, noisy)
     agree = float(np.mean(res.best_orientation == ex.best_orientation))
-    assert agree >= 0.97, (agree, res.fallback.mean(), thr)
-    assert res.fallback.mean() <= 1 / 3, res.fallback.mean()
+    assert agree >= 0.99, (agree, res.fallback.mean(), thr)
+    assert 0 < res.fallback.mean() <= 1 / 3, res.fallback.mean()
     # fallback images carry the exhaustive answer exactly
     np.testing.assert_array_equal(res.best_orientation[res.fallback], ex.best_orientation[res.fallback])
