@@ -388,14 +388,50 @@ __global__ void __launch_bounds__(kWarps * 32)
 }
 
 // ---------------------------------------------------------------------------
+// Warp aggregation of atomics that hit the same address.
+// ---------------------------------------------------------------------------
+// Lanes holding the same key (a gradient element index, or kNoKey) form a
+// group (__match_any_sync).  A binary tree over the group's ranks (lanes in
+// increasing order) sums their values: at step s a lane of rank r with
+// r % 2s == 0 adds the partial sum of the lane of rank r + s, the s-th group
+// member above it.  The group's lowest lane ends with the total and returns
+// true; it alone issues the atomic.  Called by all 32 lanes together.
+constexpr unsigned kNoKey = 0xffffffffu;
+
+__device__ __forceinline__ bool peer_sum(unsigned key, float2& v, int lane) {
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  const unsigned below = peers & ((1u << lane) - 1u);
+  const unsigned above = peers & ~below & ~(1u << lane);
+  const int rank = __popc(below);
+  const int count = __popc(peers);
+  for (int s = 1; __any_sync(0xffffffffu, rank + s < count); s <<= 1) {
+    unsigned m = above;
+    for (int i = 1; i < s && m; ++i) m &= m - 1u;  // drop the s - 1 nearest members above
+    const int src = m ? __ffs(m) - 1 : lane;
+    const float tx = __shfl_sync(0xffffffffu, v.x, src);
+    const float ty = __shfl_sync(0xffffffffu, v.y, src);
+    if (m && (rank % (2 * s)) == 0) {
+      v.x += tx;
+      v.y += ty;
+    }
+  }
+  return rank == 0 && key != kNoKey;
+}
+
+// ---------------------------------------------------------------------------
 // Trilinear scatter-add of the slice gradient and d/dR.
 // ---------------------------------------------------------------------------
+// AGG (CJX_TUNE_SCATTER_VEC = 2): for each of the 8 corners, the lanes of a
+// warp whose corner lands on the same voxel sum their contributions with
+// peer_sum and one lane per voxel issues the atomic; neighbouring samples of
+// a warp's 4 x 8 patch share most of their corners (about 3.3 samples update
+// each voxel), so this cuts the atomics that serialise on one address.
 // VEC: the two x-corners of a (y, z) corner row land in one 16-byte
 // float4 atomic when both are valid, adjacent and 16-byte aligned in the
 // gradient array (about half the rows); otherwise each corner takes an
 // 8-byte float2 atomic.  The scatter is bound by the L2's atomic units, so
 // fewer atomic operations is what shortens it.
-template <typename Layout, bool VEC>
+template <typename Layout, bool VEC, bool AGG = false>
 __global__ void __launch_bounds__(256)
     k_scatter_slice(const float2* __restrict__ grid, const float2* __restrict__ gh,
                     const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
@@ -416,7 +452,45 @@ __global__ void __launch_bounds__(256)
   const int u = blockIdx.x * 16 + du;
   const int v = blockIdx.y * 16 + dv;
   float gr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (u < g.nxh && v < n) {
+  if constexpr (AGG) {
+    // every lane takes part in the warp-level grouping, so the per-corner work runs outside the bounds test
+    // with inactive lanes carrying kNoKey
+    const bool live = u < g.nxh && v < n;
+    const float2 gs = live ? gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v] : make_float2(0.f, 0.f);
+    const float ux = (float)fft_index(live ? u : 0, n), vy = (float)fft_index(live ? v : 0, n);
+    const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    const AxisNodes ax = axis_nodes(o[0], n, wrap);
+    const AxisNodes ay = axis_nodes(o[1], n, wrap);
+    const AxisNodes az = axis_nodes(o[2], n, wrap);
+    float dH[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+      const bool ok = live && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
+      const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
+      const float wx = dx ? ax.w1 : ax.w0, wy = dy ? ay.w1 : ay.w0, wz = dz ? az.w1 : az.w0;
+      const float2 val = ok ? __ldg(&grid[L.az(iz) + L.ay(iy) + L.ax(ix)]) : g.fill;
+      const float sx = dx ? 1.f : -1.f, sy = dy ? 1.f : -1.f, sz = dz ? 1.f : -1.f;
+      const float gwx = sx * wy * wz, gwy = sy * wx * wz, gwz = sz * wx * wy;
+      dH[0][0] += gwx * val.x; dH[0][1] += gwx * val.y;
+      dH[1][0] += gwy * val.x; dH[1][1] += gwy * val.y;
+      dH[2][0] += gwz * val.x; dH[2][1] += gwz * val.y;
+      if (grad_grid) {
+        const float w = (wz * wy) * wx;
+        const unsigned key = ok ? (unsigned)(((size_t)iz * n + iy) * n + ix) : kNoKey;
+        float2 c2 = make_float2(w * gs.x, w * gs.y);
+        if (peer_sum(key, c2, lane)) atomicAdd(&grad_grid[key], c2);
+      }
+    }
+    if (live) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float dLdo = gs.x * dH[a][0] + gs.y * dH[a][1];
+        gr[2 * a] = dLdo * ux;
+        gr[2 * a + 1] = dLdo * vy;
+      }
+    }
+  } else if (u < g.nxh && v < n) {
     const float2 gs = gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v];
     const float ux = (float)fft_index(u, n), vy = (float)fft_index(v, n);
     const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
@@ -661,13 +735,20 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
     prof_end("k_colfft_adj", stream);
     prof_begin(stream);
     const dim3 gs((g.nxh + 15) / 16, (g.n + 15) / 16, cnt);
-    const bool agg = tn.scatter_vec != 0;
+    const bool agg = tn.scatter_vec == 1;
+    const bool warp_agg = tn.scatter_vec == 2;
     if ((g.flags & CJX_GRID_SPLINE) && bricked) {
       k_scatter_slice_spline<SplineBrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
                                                                         k0);
     } else if (g.flags & CJX_GRID_SPLINE) {
       k_scatter_slice_spline<SplineLinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads,
                                                                          g, k0);
+    } else if (bricked && warp_agg) {
+      k_scatter_slice<BrickLayout, false, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
+                                                                         k0);
+    } else if (warp_agg) {
+      k_scatter_slice<LinearLayout, false, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
+                                                                          k0);
     } else if (bricked && agg) {
       k_scatter_slice<BrickLayout, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
     } else if (bricked) {

@@ -152,8 +152,8 @@ int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, voi
     if (gr.tuning_valid) {
       if (gr.gather_ilp != 1 && gr.gather_ilp != 2 && gr.gather_ilp != 4)
         return fail(CJX_ERR_INVALID_ARGUMENT, "group gather_ilp must be 1, 2 or 4");
-      if (gr.gather_tile < 0 || gr.gather_tile > 2)
-        return fail(CJX_ERR_INVALID_ARGUMENT, "group gather_tile must be 0, 1 or 2");
+      if (gr.gather_tile < 0 || gr.gather_tile > 3)
+        return fail(CJX_ERR_INVALID_ARGUMENT, "group gather_tile must be 0, 1, 2 or 3");
     }
   }
   const Tuning base = current_tuning();

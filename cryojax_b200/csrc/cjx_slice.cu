@@ -688,7 +688,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_GATHER_MODE) {
-    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0 or 1");
+    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0, 1 or 2");
     g_gather_mode = value;
     return CJX_OK;
   }
@@ -698,7 +698,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_GATHER_TILE) {
-    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather tile must be 0, 1 or 2");
+    if (value < 0 || value > 3) return fail(CJX_ERR_INVALID_ARGUMENT, "gather tile must be 0, 1, 2 or 3");
     g_gather_tile = value;
     return CJX_OK;
   }
@@ -708,7 +708,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_SCATTER_VEC) {
-    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "scatter vector mode must be 0 or 1");
+    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "scatter mode must be 0, 1 or 2");
     g_scatter_vec = value;
     return CJX_OK;
   }
@@ -739,6 +739,10 @@ static int ensure_smem_attrs() {
 
 int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream,
                       const Tuning& tn);
+bool fused_gather_supported(const SliceGeom& g);
+int launch_gather_colifft_fused(const SliceGeom& g, const float2* grid, const cjx_image_params* params,
+                                const int32_t* order, int64_t k0, int cnt, float2* t1, const Tuning& tn,
+                                cudaStream_t stream);
 int launch_ewald_colfft(const SliceGeom& g, const float2* t2, const cjx_image_params* params, const int32_t* order,
                         float2* out, int64_t k0, int cnt, cudaStream_t stream, const Tuning& tn);
 int launch_ewald_direct(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
@@ -751,17 +755,21 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
                          const Tuning& tn) {
   if (int e = ensure_smem_attrs()) return e;
   const int64_t ilp = (g.flags & CJX_GRID_SPLINE) ? tn.spline_ilp : tn.ilp;
-  // the fused kernel has no pair, spline or Ewald path
-  const bool split =
-      tn.gather_mode == 1 || (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE));
   const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
   const bool fast = tn.fft_mode >= 1;
+  // gather mode 2: the register-FFT fused pass (trilinear grids, N = 32 R); otherwise the split pair of
+  // kernels, or mode 0's shared-memory fused kernel, which has no pair, spline or Ewald path
+  const bool fused_reg = tn.gather_mode == 2 && fast && fused_gather_supported(g);
+  const bool split = !fused_reg && (tn.gather_mode != 0 ||
+                                    (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE)));
   const bool t512 = tn.fft_mode == 2 && rn == 16;  // 512-point column transforms through the transpose FFT
   const size_t sa = smem_a(g), sb = smem_b(g);
   const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
   const size_t sb_reg =
       sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
-    if (split) {
+    if (fused_reg) {
+      if (int e = launch_gather_colifft_fused(g, grid, params, order, k0, cnt, t1, tn, stream)) return e;
+    } else if (split) {
       const dim3 gg((g.ncols + 15) / 16, (g.n + 16 * (int)ilp - 1) / (16 * (int)ilp), cnt);
       prof_begin(stream);
       const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;

@@ -370,17 +370,24 @@ CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t
  * issues together in the gather (1, 2 or 4).  CJX_TUNE_CHUNK_BYTES: target
  * workspace bytes per chunk when desc->images_per_chunk is 0 (default 1 GiB).
  * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
- * column-FFT kernel, 0 = one fused gather + column-FFT kernel.
+ * column-FFT kernel, 0 = one fused gather + column-FFT kernel with
+ * shared-memory FFTs (C-order and bricked grids only), 2 = one fused
+ * gather + register-FFT column kernel (trilinear grids in any layout, slice
+ * or Ewald sphere, N = 32 R; other cases run as 1), which never writes the
+ * sampled plane to memory.
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
  * (R in 1-6, 8, 10, 12, 16), 2 (default) = the same, with the 512-point
  * column transforms of the resize stage done as 16 x 32 through one
  * shared-memory transpose instead of five shuffle stages, 0 = shared-memory
  * Stockham FFTs everywhere.
  * CJX_TUNE_GATHER_TILE: lanes of a gather warp cover 2 x 16 (0), 4 x 8 (1)
- * or 8 x 4 (2) samples (columns x rows) of the slice plane.
+ * or 8 x 4 (2) samples (columns x rows) of the slice plane; 3 = one column
+ * x 32 rows in gather mode 2 (the split gather takes 3 as 0).
  * CJX_TUNE_SCATTER_VEC: 1 (default) = the adjoint's grid scatter-add puts
  * the two x-corners of a corner row into one 16-byte atomic when they are
- * adjacent and aligned; 0 = one 8-byte atomic per (sample, corner).
+ * adjacent and aligned; 0 = one 8-byte atomic per (sample, corner); 2 =
+ * warp-aggregated: lanes whose corner lands on the same voxel sum their
+ * contributions with warp shuffles and one lane per voxel issues the atomic.
  * CJX_TUNE_SPLINE_ILP: samples per lane in the cubic-spline gather
  * (CJX_GRID_SPLINE; 1, 2 or 4, default 4).                                 */
 #define CJX_TUNE_GATHER_ILP 1

@@ -87,7 +87,11 @@ def test_tuning_knobs():
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(nat.CJX_TUNE_FFT_MODE, 3)
     with pytest.raises(nat.CryojaxB200Error):
-        nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, 2)
+        nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, 3)
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(nat.CJX_TUNE_GATHER_MODE, 3)
+    with pytest.raises(nat.CryojaxB200Error):
+        nat.tuning_set(nat.CJX_TUNE_GATHER_TILE, 4)
 
 
 def _search_desc(n, py, px, n_img, n_orient, k):
