@@ -220,6 +220,15 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     ),
+    "cjx_postprocess_workspace_size": (
+        ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "cjx_postprocess_real": (
+        ctypes.c_int,
+        [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+    ),
+    "cjx_rfft2": (
+        ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "cjx_tuning_set": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64]),
     "cjx_tuning_get": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]),
     "cjx_brick_volume_pairs": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -815,6 +824,65 @@ def fft_c2c(x, direction: int, out=None, stream=None):
     n = x.shape[-1]
     _check(load_library().cjx_fft_c2c(int(n), int(direction), _cuda_ptr(x, "x"), _cuda_ptr(out, "out"),
                                       int(x.numel() // n), _stream_ptr(stream)))
+    return out
+
+
+CJX_PP_NORMALIZE = 1
+
+
+def postprocess_workspace_size(n_images: int, py: int, px: int) -> int:
+    v = ctypes.c_size_t(0)
+    _check(load_library().cjx_postprocess_workspace_size(int(n_images), int(py), int(px), ctypes.byref(v)))
+    return int(v.value)
+
+
+def postprocess_real(fourier, padded_shape, shape, *, normalize=False, mask=None, out=None, workspace=None,
+                     stream=None):
+    """cjx_postprocess_real: complex64 CUDA [..., Py, Px//2+1] -> float32 [..., H, W] real-space images
+    (irfftn -> centre crop -> optional normalisation -> optional float32 [H, W] mask)."""
+    import torch
+
+    if fourier.dtype != torch.complex64:
+        raise ValueError("fourier must be complex64")
+    py, px = (int(v) for v in padded_shape)
+    h, w = (int(v) for v in shape)
+    if tuple(fourier.shape[-2:]) != (py, px // 2 + 1):
+        raise ValueError(f"fourier images must be [..., {py}, {px // 2 + 1}], got {tuple(fourier.shape)}")
+    f = fourier.contiguous()
+    lead = tuple(f.shape[:-2])
+    n = int(np.prod(lead)) if lead else 1
+    if out is None:
+        out = torch.empty(lead + (h, w), dtype=torch.float32, device=f.device)
+    if n == 0:
+        return out
+    if mask is not None:
+        mask = torch.as_tensor(mask, dtype=torch.float32, device=f.device).contiguous()
+        if tuple(mask.shape) != (h, w):
+            raise ValueError(f"mask must be [{h}, {w}], got {tuple(mask.shape)}")
+    if workspace is None or workspace.numel() * workspace.element_size() < postprocess_workspace_size(1, py, px):
+        # up to 2048 images per pass: larger batches take several passes over the same workspace
+        workspace = torch.empty(postprocess_workspace_size(min(n, 2048), py, px), dtype=torch.uint8, device=f.device)
+    wsb = workspace.numel() * workspace.element_size()
+    _check(load_library().cjx_postprocess_real(
+        n, py, px, h, w, CJX_PP_NORMALIZE if normalize else 0, _cuda_ptr(f, "fourier"),
+        _cuda_ptr(mask, "mask") if mask is not None else None, _cuda_ptr(out, "out"),
+        _cuda_ptr(workspace, "workspace"), int(wsb), _stream_ptr(stream)))
+    return out
+
+
+def rfft2(image, out=None, stream=None):
+    """cjx_rfft2: float32 CUDA [..., Py, Px] -> complex64 [..., Py, Px//2+1], rfft2 of ifftshift(image)."""
+    import torch
+
+    x = image.to(torch.float32).contiguous()
+    py, px = int(x.shape[-2]), int(x.shape[-1])
+    lead = tuple(x.shape[:-2])
+    n = int(np.prod(lead)) if lead else 1
+    if out is None:
+        out = torch.empty(lead + (py, px // 2 + 1), dtype=torch.complex64, device=x.device)
+    if n == 0:
+        return out
+    _check(load_library().cjx_rfft2(n, py, px, _cuda_ptr(x, "image"), _cuda_ptr(out, "out"), _stream_ptr(stream)))
     return out
 
 

@@ -1,42 +1,27 @@
-"""Real-space postprocessing of simulated rfft images on the device.
+"""Real-space output and post-processing of simulated rfft images, on this library's kernels.
 
 irfftn follows cryoJAX's convention (cryojax/ndimage/_fft.py:57-77): an
-inverse real FFT followed by fftshift.  Like the reference's FFT backends,
-the inverse transforms the leading axis as complex and keeps only the real
-part of the DC and (even size) Nyquist bins of the last axis; the columns
-kx = 0 and kx = Px/2 are made Hermitian in ky first so the library C2R sees
-a well-defined input.  postprocess mirrors
-cryojax/simulator/_image_model/base_image_model.py:107-158 (the filter is
-applied earlier, inside the device launch).
+inverse real FFT of the rfft half plane followed by fftshift; rfftn is
+ifftshift then rfft2 (cryojax/ndimage/_fft.py:80-99).  postprocess mirrors
+cryojax/simulator/_image_model/base_image_model.py:107-158: irfftn -> centre
+crop -> normalise -> mask, in one cjx_postprocess_real call (the Fourier
+filter is applied earlier, inside the simulation launch).  Masks that are
+cryoJAX transform objects (or arrays) are multiplied in inside that call; any
+other callable is applied to its output.
 """
 
 from __future__ import annotations
 
-
-def _hermitian_columns(f, px):
-    import torch
-
-    py = f.shape[-2]
-    idx = (-torch.arange(py, device=f.device)) % py
-    g = f.clone()
-    cols = [0] + ([px // 2] if px % 2 == 0 else [])
-    for c in cols:
-        col = f[..., :, c]
-        g[..., :, c] = 0.5 * (col + torch.conj(col[..., idx]))
-    return g
+from . import _native as nat
 
 
 def irfftn(fourier_image, shape):
-    import torch
-
-    py, px = shape
-    f = _hermitian_columns(fourier_image, px)
-    x = torch.fft.irfftn(f, s=(py, px), dim=(-2, -1))
-    return torch.fft.fftshift(x, dim=(-2, -1))
+    """float32 real-space images [..., Py, Px] of complex64 rfft half planes [..., Py, Px//2+1]."""
+    return nat.postprocess_real(fourier_image, shape, shape)
 
 
 def crop_to_shape(image, shape):
-    """Centre crop (cryojax/ndimage/_edges.py:15-62)."""
+    """Centre crop (cryojax/ndimage/_edges.py:15-62) of a real-space array (a view)."""
     ny, nx = image.shape[-2:]
     h, w = shape
     yc, xc = ny // 2, nx // 2
@@ -44,22 +29,27 @@ def crop_to_shape(image, shape):
 
 
 def rfftn(image):
-    import torch
+    """complex64 rfft half planes [..., Py, Px//2+1] of float real-space images [..., Py, Px]."""
+    return nat.rfft2(image)
 
-    return torch.fft.rfftn(torch.fft.ifftshift(image, dim=(-2, -1)), dim=(-2, -1))
+
+def _mask_array(mask):
+    """The real-space array of a mask object (AbstractMask.get()) or array; None for other callables."""
+    if mask is None:
+        return None
+    if hasattr(mask, "get"):
+        return mask.get()
+    if callable(mask):
+        return None
+    return mask
 
 
 def postprocess(fourier_image, shape, padded_shape, *, outputs_real_space=True, normalizes_signal=False,
                 mask=None):
     if mask is None and tuple(padded_shape) == tuple(shape) and not normalizes_signal:
         return irfftn(fourier_image, shape) if outputs_real_space else fourier_image
-    image = irfftn(fourier_image, padded_shape)
-    if tuple(padded_shape) != tuple(shape):
-        image = crop_to_shape(image, shape)
-    if normalizes_signal:
-        mean = image.mean(dim=(-2, -1), keepdim=True)
-        std = image.std(dim=(-2, -1), keepdim=True, unbiased=False)
-        image = (image - mean) / std
-    if mask is not None:
+    arr = _mask_array(mask)
+    image = nat.postprocess_real(fourier_image, padded_shape, shape, normalize=normalizes_signal, mask=arr)
+    if mask is not None and arr is None:
         image = mask(image)
     return image if outputs_real_space else rfftn(image)

@@ -10,8 +10,10 @@ under ``eqx.filter_jit``).
 
 ``autotune`` picks the gather kernel's choices (ILP, lane tile) and the
 workspace chunk size for one (volume side, image shape, flags) by timing
-the candidates on a sample of the caller's images.  The result is cached in
-a JSON file keyed by GPU name and shape.
+the candidates on a sample of the caller's images.  Each candidate carries
+its choices in its own call (a group record and the descriptor), so tuning
+never changes process-wide state and other threads can simulate meanwhile.
+The result is cached in a JSON file keyed by GPU name and shape.
 """
 
 from __future__ import annotations
@@ -88,33 +90,30 @@ def autotune(model, *, n_sample=1024, repeats=2, candidates=None, use_cache=True
     m = min(n_sample, params.shape[0])
     pd = torch.as_tensor(params[:m], device=vol.device)
     out = torch.empty((m, py, px // 2 + 1), dtype=torch.complex64, device=pd.device)
-    old = (nat.tuning_get(nat.CJX_TUNE_GATHER_ILP), nat.tuning_get(nat.CJX_TUNE_GATHER_TILE),
-           nat.tuning_get(nat.CJX_TUNE_CHUNK_BYTES))
+    per_image = nat.workspace_size(nat.make_desc(n, py, px, flags, integ.fill_value, 1), 1)
     best, best_ms = None, float("inf")
-    try:
-        for c in candidates or CANDIDATES:
-            nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, c["ilp"])
-            nat.tuning_set(nat.CJX_TUNE_GATHER_TILE, c["tile"])
-            nat.tuning_set(nat.CJX_TUNE_CHUNK_BYTES, c["chunk_mb"] << 20)
-            desc = nat.make_desc(n, py, px, flags, integ.fill_value)
-            ws = nat.workspace_size(desc, m)
-            wsb = torch.empty(max(ws, 1), dtype=torch.uint8, device=pd.device)
-            nat.slice_ctf_forward(desc, grid, pd, out, wsb)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(repeats):
-                nat.slice_ctf_forward(desc, grid, pd, out, wsb)
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / repeats
-            if ms < best_ms:
-                best, best_ms = dict(c), ms
-            del wsb
-    finally:
-        nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, old[0])
-        nat.tuning_set(nat.CJX_TUNE_GATHER_TILE, old[1])
-        nat.tuning_set(nat.CJX_TUNE_CHUNK_BYTES, old[2])
+    # each candidate runs through the multi-group entry point with its kernel choices in the group record
+    # and its chunk in the descriptor: the process-wide knobs are never touched, so forward calls on other
+    # threads meanwhile keep their own settings
+    for c in candidates or CANDIDATES:
+        chunk = max(1, min(m, (c["chunk_mb"] << 20) // max(per_image, 1)))
+        desc = nat.make_desc(n, py, px, flags, integ.fill_value, chunk)
+        groups = nat.make_groups([{"desc": desc, "grid": grid, "params": pd, "order": None, "out": out,
+                                   "n_images": m, "tuning": {"ilp": c["ilp"], "tile": c["tile"]}}])
+        ws = nat.multi_workspace_size(groups)
+        wsb = torch.empty(max(ws, 1), dtype=torch.uint8, device=pd.device)
+        nat.slice_ctf_forward_multi(groups, wsb)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            nat.slice_ctf_forward_multi(groups, wsb)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / repeats
+        if ms < best_ms:
+            best, best_ms = dict(c), ms
+        del wsb
     best["ms_per_image"] = best_ms / m
     if use_cache:
         with _CACHE_LOCK:

@@ -1,0 +1,328 @@
+// Real-space output and post-processing of simulated images (sm_100a).
+//
+// AbstractImageModel.postprocess (cryojax/simulator/_image_model/base_image_model.py:107-158)
+// after the Fourier image: irfftn (cryojax/ndimage/_fft.py:57-77: inverse
+// real FFT, then fftshift) -> centre crop to the image shape
+// (cryojax/ndimage/_edges.py:15-62) -> normalise ((x - mean) / std, the
+// population std) -> mask (times a real-space array); and the reference's
+// rfftn of real-space images (ifftshift, then rfft2; cryojax/ndimage/_fft.py:80-99),
+// used on observed images and on masked images whose Fourier form is wanted.
+//
+// irfft2, three passes per chunk of images:
+//   1 k_pp_colifft: per column kx of the half plane a Py-point inverse FFT
+//     (columns kx = 0 and, for even Px, kx = Px/2 made Hermitian in ky first:
+//     the part of them an inverse real FFT keeps) into the workspace T;
+//   2 k_pp_rows_c2r: two rows of T at a time, Hermitian-extended and packed as
+//     A + iB, one Px-point inverse FFT gives both real rows; the fftshift and
+//     the crop are an index map on the rows read and the columns written; the
+//     mask multiplies here unless the image is normalised, and the per-image
+//     sums for the normalisation are accumulated in double;
+//   3 k_pp_normalize (only with CJX_PP_NORMALIZE): (x - mean) / std, then the mask.
+// rfft2, two passes, in place in the output: k_pp_rows_r2c (two real rows as
+// one complex FFT, split into their half spectra) and k_pp_colfft.
+// The transforms are the library's shared-memory Stockham warp FFTs, so every
+// size up to CJX_MAX_SIDE works.
+#include <algorithm>
+
+#include "cjx_common.cuh"
+#include "cjx_profile.cuh"
+
+namespace cjx {
+
+namespace {
+
+// Result buffer of warp_fft: a after an even number of Stockham stages, b otherwise.
+inline int fft_result_offset(const FftPlan& p, int n) { return (p.nstages == 0 || (p.nstages & 1)) ? n : 0; }
+
+// Pass 1 of irfft2: column inverse FFTs of the half plane.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_colifft(const float2* __restrict__ in, float2* __restrict__ t, int py, int px, FftPlan plan, int res_off) {
+  extern __shared__ float2 smem[];
+  const int pxh = px / 2 + 1;
+  const int stride = 2 * py + 2;
+  float2* tw = smem;
+  float2* bufs = smem + py;
+  build_twiddles(tw, py);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, pxh - j0);
+  const float2* src = in + (size_t)blockIdx.y * py * pxh + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + m] = src[(size_t)m * pxh + jj];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) {
+    float2* a = bufs + warp * stride;
+    const int j = j0 + warp;
+    if (j == 0 || ((px % 2 == 0) && j == px / 2)) {
+      // (S[v] + conj(S[-v])) / 2: the pairs (v, -v) are disjoint across lanes
+      for (int i = lane; i <= py / 2; i += 32) {
+        const int i2 = (i == 0) ? 0 : py - i;
+        const float2 x = a[i], y = a[i2];
+        const float2 sv = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        a[i] = sv;
+        a[i2] = cconj(sv);
+      }
+      __syncwarp();
+    }
+    warp_fft<+1>(a, a + py, plan, tw, lane);
+  }
+  __syncthreads();
+  float2* dst = t + (size_t)blockIdx.y * py * pxh + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) dst[(size_t)m * pxh + jj] = bufs[jj * stride + res_off + m];
+  }
+}
+
+// Pass 2 of irfft2: rows (two per warp) -> fftshift -> crop -> scale (-> mask) -> float32 output,
+// plus the per-image sum and sum of squares (double) when stats != NULL.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_rows_c2r(const float2* __restrict__ t, float* __restrict__ out, int py, int px, int h, int w,
+                  const float* __restrict__ mask, double* __restrict__ stats, FftPlan plan) {
+  extern __shared__ float2 smem[];
+  const int pxh = px / 2 + 1;
+  float2* tw = smem;
+  float2* bufs = smem + px;
+  build_twiddles(tw, px);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = 2 * (blockIdx.x * kWarps + warp);
+  if (r0 >= h) return;
+  const bool has_b = r0 + 1 < h;
+  // output row r of the crop is row (r + y0 + py - py/2) mod py of the unshifted inverse transform
+  const int y0 = py / 2 - h / 2, x0 = px / 2 - w / 2;
+  const int sa = (r0 + y0 + py - py / 2) % py;
+  const int sb = (r0 + 1 + y0 + py - py / 2) % py;
+  const float2* rowA = t + ((size_t)blockIdx.y * py + sa) * pxh;
+  const float2* rowB = t + ((size_t)blockIdx.y * py + sb) * pxh;
+  float2* a = bufs + warp * (2 * px + 2);
+  float2* b = a + px;
+  // z = A + iB on the Hermitian extension; DC and (even Px) Nyquist bins keep their real parts only
+  for (int k = lane; k <= px / 2; k += 32) {
+    const float2 A = rowA[k];
+    const float2 B = has_b ? rowB[k] : make_float2(0.f, 0.f);
+    if (k == 0 || ((px % 2 == 0) && k == px / 2)) {
+      a[k] = make_float2(A.x, B.x);
+    } else {
+      a[k] = make_float2(A.x - B.y, A.y + B.x);
+      a[px - k] = make_float2(A.x + B.y, B.x - A.y);
+    }
+  }
+  __syncwarp();
+  const float2* z = warp_fft<+1>(a, b, plan, tw, lane);
+  const float scale = (float)(1.0 / ((double)py * (double)px));
+  const bool fuse_mask = mask && !stats;
+  float* oa = out + ((size_t)blockIdx.y * h + r0) * w;
+  double s = 0.0, ss = 0.0;
+  for (int c = lane; c < w; c += 32) {
+    const float2 v = z[(c + x0 + px - px / 2) % px];
+    float va = v.x * scale, vb = v.y * scale;
+    s += (double)va;
+    ss += (double)va * (double)va;
+    if (has_b) {
+      s += (double)vb;
+      ss += (double)vb * (double)vb;
+    }
+    if (fuse_mask) {
+      va *= __ldg(mask + (size_t)r0 * w + c);
+      if (has_b) vb *= __ldg(mask + (size_t)(r0 + 1) * w + c);
+    }
+    oa[c] = va;
+    if (has_b) oa[w + c] = vb;
+  }
+  if (stats) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    if (lane == 0) {
+      atomicAdd(stats + 2 * blockIdx.y, s);
+      atomicAdd(stats + 2 * blockIdx.y + 1, ss);
+    }
+  }
+}
+
+// Pass 3 of irfft2 (normalisation): (x - mean) / std with the population std, then the optional mask.
+__global__ void k_pp_normalize(float* __restrict__ out, int64_t n_img, int hw, const double* __restrict__ stats,
+                               const float* __restrict__ mask) {
+  const int64_t total = n_img * hw;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t img = e / hw;
+    const int p = (int)(e - img * hw);
+    const double mean = stats[2 * img] / hw;
+    const double var = fmax(stats[2 * img + 1] / hw - mean * mean, 0.0);
+    float v = (float)(((double)out[e] - mean) / sqrt(var));
+    if (mask) v *= __ldg(mask + p);
+    out[e] = v;
+  }
+}
+
+// rfft2 pass 1: rows (two per warp) of ifftshift(image) as one complex FFT, split into the half spectra.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_rows_r2c(const float* __restrict__ image, float2* __restrict__ out, int py, int px, FftPlan plan) {
+  extern __shared__ float2 smem[];
+  const int pxh = px / 2 + 1;
+  float2* tw = smem;
+  float2* bufs = smem + px;
+  build_twiddles(tw, px);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  if (ra >= py) return;
+  const bool has_b = ra + 1 < py;
+  // ifftshift: transform row i / column j read image row (i + py/2) mod py / column (j + px/2) mod px
+  const float* xa = image + ((size_t)blockIdx.y * py + (ra + py / 2) % py) * px;
+  const float* xb = image + ((size_t)blockIdx.y * py + (ra + 1 + py / 2) % py) * px;
+  float2* a = bufs + warp * (2 * px + 2);
+  float2* b = a + px;
+  for (int j = lane; j < px; j += 32) {
+    const int c = (j + px / 2) % px;
+    a[j] = make_float2(xa[c], has_b ? xb[c] : 0.f);
+  }
+  __syncwarp();
+  const float2* Z = warp_fft<-1>(a, b, plan, tw, lane);
+  float2* oa = out + ((size_t)blockIdx.y * py + ra) * pxh;
+  for (int k = lane; k < pxh; k += 32) {
+    const float2 Zk = Z[k];
+    const float2 Zm = Z[(px - k) % px];
+    oa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    if (has_b) oa[pxh + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+  }
+}
+
+// rfft2 pass 2: column forward FFTs, in place (each CTA owns its columns).
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_colfft(float2* __restrict__ data, int py, int px, FftPlan plan, int res_off) {
+  extern __shared__ float2 smem[];
+  const int pxh = px / 2 + 1;
+  const int stride = 2 * py + 2;
+  float2* tw = smem;
+  float2* bufs = smem + py;
+  build_twiddles(tw, py);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, pxh - j0);
+  float2* col0 = data + (size_t)blockIdx.y * py * pxh + j0;
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + m] = col0[(size_t)m * pxh + jj];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) warp_fft<-1>(bufs + warp * stride, bufs + warp * stride + py, plan, tw, lane);
+  __syncthreads();
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) col0[(size_t)m * pxh + jj] = bufs[jj * stride + res_off + m];
+  }
+}
+
+size_t smem_cols(int py) { return sizeof(float2) * (size_t)(py + kWarps * (2 * py + 2)); }
+size_t smem_rows(int px) { return sizeof(float2) * (size_t)(px + kWarps * (2 * px + 2)); }
+
+int ensure_pp_smem() {
+  static PerDeviceOnce once;
+  const cudaError_t e = once.run([] {
+    const int kMax = 227 * 1024;
+    cudaError_t r = cudaFuncSetAttribute(k_pp_colifft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_pp_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_pp_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_pp_colfft, cudaFuncAttributeMaxDynamicSharedMemorySize, kMax);
+    return r;
+  });
+  return e == cudaSuccess ? CJX_OK : check_cuda(e, "cudaFuncSetAttribute (post-processing kernels)");
+}
+
+int check_shape(int64_t n, int py, int px) {
+  if (n < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n < 0");
+  if (py < 1 || px < 2) return fail(CJX_ERR_INVALID_ARGUMENT, "need py >= 1 and px >= 2");
+  if (py > CJX_MAX_SIDE || px > CJX_MAX_SIDE) return fail(CJX_ERR_UNSUPPORTED, "image sides are limited to CJX_MAX_SIDE");
+  if (smem_cols(py) > 227 * 1024 || smem_rows(px) > 227 * 1024)
+    return fail(CJX_ERR_UNSUPPORTED, "post-processing shared-memory footprint exceeds 227 KB");
+  return CJX_OK;
+}
+
+size_t pp_bytes_per_image(int py, int px) { return sizeof(float2) * (size_t)py * (px / 2 + 1) + 2 * sizeof(double); }
+
+}  // namespace
+
+}  // namespace cjx
+
+using namespace cjx;
+
+extern "C" int cjx_postprocess_workspace_size(int64_t n_images, int py, int px, size_t* bytes) {
+  if (!bytes) return fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  if (int e = check_shape(n_images, py, px)) return e;
+  *bytes = (size_t)n_images * pp_bytes_per_image(py, px);
+  return CJX_OK;
+}
+
+extern "C" int cjx_postprocess_real(int64_t n_images, int py, int px, int h, int w, uint32_t flags,
+                                    const void* fourier, const float* mask, float* out, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+  if (int e = check_shape(n_images, py, px)) return e;
+  if (h < 1 || w < 1 || h > py || w > px)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "the image shape (h, w) must fit inside the padded shape (py, px)");
+  if (flags & ~CJX_PP_NORMALIZE) return fail(CJX_ERR_INVALID_ARGUMENT, "unknown post-processing flag bits");
+  if (n_images == 0) return CJX_OK;
+  if (!fourier || !out || !workspace)
+    return fail(CJX_ERR_INVALID_ARGUMENT, "fourier, out and workspace must be non-NULL");
+  const size_t per = pp_bytes_per_image(py, px);
+  if (workspace_bytes < per) return fail(CJX_ERR_WORKSPACE, "workspace smaller than one image's need");
+  if (int e = ensure_pp_smem()) return e;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t chunk = std::min<int64_t>({(int64_t)(workspace_bytes / per), n_images, 65535});
+  const bool normalize = (flags & CJX_PP_NORMALIZE) != 0;
+  const int pxh = px / 2 + 1;
+  float2* t = static_cast<float2*>(workspace);
+  double* stats = reinterpret_cast<double*>(static_cast<char*>(workspace) + (size_t)chunk * py * pxh * sizeof(float2));
+  const FftPlan plan_y = make_fft_plan(py), plan_x = make_fft_plan(px);
+  for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
+    const float2* src = static_cast<const float2*>(fourier) + (size_t)k0 * py * pxh;
+    float* dst = out + (size_t)k0 * h * w;
+    prof_begin(s);
+    k_pp_colifft<<<dim3((pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, smem_cols(py), s>>>(
+        src, t, py, px, plan_y, fft_result_offset(plan_y, py));
+    prof_end("k_pp_colifft", s);
+    if (normalize) {
+      if (int e = check_cuda(cudaMemsetAsync(stats, 0, sizeof(double) * 2 * cnt, s), "cudaMemsetAsync")) return e;
+    }
+    prof_begin(s);
+    k_pp_rows_c2r<<<dim3((h + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, smem_rows(px), s>>>(
+        t, dst, py, px, h, w, mask, normalize ? stats : nullptr, plan_x);
+    prof_end("k_pp_rows_c2r", s);
+    if (normalize) {
+      prof_begin(s);
+      const int64_t blocks = std::min<int64_t>(((int64_t)cnt * h * w + 255) / 256, 148 * 16);
+      k_pp_normalize<<<(unsigned)blocks, 256, 0, s>>>(dst, cnt, h * w, stats, mask);
+      prof_end("k_pp_normalize", s);
+    }
+  }
+  return check_cuda(cudaGetLastError(), "post-processing launch");
+}
+
+extern "C" int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void* out, void* stream) {
+  if (int e = check_shape(n_images, py, px)) return e;
+  if (n_images == 0) return CJX_OK;
+  if (!image || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "image and out must be non-NULL");
+  if (int e = ensure_pp_smem()) return e;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const FftPlan plan_y = make_fft_plan(py), plan_x = make_fft_plan(px);
+  const int pxh = px / 2 + 1;
+  for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
+    const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
+    float2* o = static_cast<float2*>(out) + (size_t)k0 * py * pxh;
+    prof_begin(s);
+    k_pp_rows_r2c<<<dim3((py + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, smem_rows(px), s>>>(
+        image + (size_t)k0 * py * px, o, py, px, plan_x);
+    prof_end("k_pp_rows_r2c", s);
+    prof_begin(s);
+    k_pp_colfft<<<dim3((pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, smem_cols(py), s>>>(
+        o, py, px, plan_y, fft_result_offset(plan_y, py));
+    prof_end("k_pp_colfft", s);
+  }
+  return check_cuda(cudaGetLastError(), "rfft2 launch");
+}

@@ -110,9 +110,7 @@ def observed_to_fourier(observed):
     obs = observed if isinstance(observed, torch.Tensor) else torch.as_tensor(np.asarray(observed))
     if obs.dim() == 2:
         obs = obs[None]
-    obs = obs.to(device="cuda", dtype=torch.float64)
-    f = torch.fft.rfftn(torch.fft.ifftshift(obs, dim=(-2, -1)), dim=(-2, -1))
-    return f.to(torch.complex64).contiguous()
+    return nat.rfft2(obs.to(device="cuda", dtype=torch.float32))
 
 
 def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observed_is_fourier: bool = False,

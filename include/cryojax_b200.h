@@ -365,6 +365,35 @@ CJX_API int cjx_render_gaussians(const cjx_render_desc* desc, const float* posit
 CJX_API int cjx_fft_c2c(int n, int direction, const void* in, void* out, int64_t count,
                         void* stream);
 
+/* ---- real-space output and post-processing ---------------------------- */
+/* AbstractImageModel.postprocess after the Fourier image
+ * (cryojax/simulator/_image_model/base_image_model.py:107-158): for each
+ * image b, out[b] (float32 [h][w]) = mask * normalise(crop(irfftn(
+ * fourier[b], s=(py, px)))), where
+ *  - irfftn is cryoJAX's (cryojax/ndimage/_fft.py:57-77): inverse real FFT
+ *    of the rfft half plane complex64 [py][px/2+1] (zero frequency in the
+ *    corner), scaled by 1 / (py px), then fftshift; the kx = 0 and (even px)
+ *    kx = px/2 columns count only with their Hermitian part in ky, as an
+ *    inverse real FFT reads them;
+ *  - crop is the centre crop to (h, w) <= (py, px)
+ *    (cryojax/ndimage/_edges.py:15-62), a no-op when equal;
+ *  - with CJX_PP_NORMALIZE: (x - mean) / std over the h w pixels, the
+ *    population std (cryojax/ndimage/_normalize.py:11-28);
+ *  - mask: optional float32 [h][w] multiplied in last (NULL: none).
+ * workspace: at least cjx_postprocess_workspace_size(1, ...) bytes; a
+ * larger one lets more images share a pass.  Stream-ordered.              */
+#define CJX_PP_NORMALIZE 1u
+CJX_API int cjx_postprocess_workspace_size(int64_t n_images, int py, int px, size_t* bytes);
+CJX_API int cjx_postprocess_real(int64_t n_images, int py, int px, int h, int w, uint32_t flags,
+                                 const void* fourier, const float* mask, float* out, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+/* cryoJAX's rfftn of real-space images (cryojax/ndimage/_fft.py:80-99):
+ * out[b] (complex64 [py][px/2+1]) = rfft2(ifftshift(image[b])), image
+ * float32 [n][py][px].  Used for observed images and for post-processed
+ * images whose Fourier form is requested.  Needs no workspace; image and
+ * out must not overlap.  Stream-ordered.                                   */
+CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void* out, void* stream);
+
 /* Process-wide tuning knobs (no counterpart in the reference; set by the
  * autotuner).  CJX_TUNE_GATHER_ILP: samples whose corner loads one lane
  * issues together in the gather (1, 2 or 4).  CJX_TUNE_CHUNK_BYTES: target

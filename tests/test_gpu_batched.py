@@ -73,3 +73,44 @@ def test_multi_validates_all_groups_before_launching(cuda_device):
         nat.slice_ctf_forward_multi(nat.make_groups([good, bad]))
     torch.cuda.synchronize()
     assert torch.all(out == 7.0)  # nothing ran
+
+
+def test_autotune_leaves_process_knobs_alone_while_another_thread_simulates(cuda_device, tmp_path, monkeypatch):
+    """The autotuner times its candidates through per-call choices: while it runs on one thread, forward
+    calls on another thread (process-default knobs) keep giving the same images, and the knobs are unchanged
+    afterwards."""
+    import threading
+
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.batched import autotune
+
+    monkeypatch.setenv("CRYOJAX_B200_AUTOTUNE_CACHE", str(tmp_path / "autotune.json"))
+    models, refs = _models_and_refs()
+    knobs = (nat.CJX_TUNE_GATHER_ILP, nat.CJX_TUNE_GATHER_TILE, nat.CJX_TUNE_CHUNK_BYTES, nat.CJX_TUNE_GATHER_MODE)
+    before = [nat.tuning_get(k) for k in knobs]
+    ref = models[1].compute_fourier_image().clone()
+    errors, stop = [], threading.Event()
+
+    def simulate_repeatedly():
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            while not stop.is_set():
+                got = models[1].compute_fourier_image()
+                stream.synchronize()
+                if not torch.equal(got, ref):
+                    errors.append("images changed while the autotuner ran")
+                if [nat.tuning_get(k) for k in knobs] != before:
+                    errors.append("process knobs changed while the autotuner ran")
+
+    t = threading.Thread(target=simulate_repeatedly)
+    t.start()
+    try:
+        for m in models:
+            autotune(m, n_sample=8, repeats=1, use_cache=False)
+    finally:
+        stop.set()
+        t.join()
+    assert not errors, errors[:3]
+    assert [nat.tuning_get(k) for k in knobs] == before
