@@ -309,6 +309,14 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "cjx_ncc_directions_workspace_size": (
+        ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "cjx_ncc_directions": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_size_t, ctypes.c_void_p],
+    ),
     "cjx_probe_read_bandwidth": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -691,6 +699,22 @@ def ncc_topk(num, den, n, T, oo, yinv, zinv, k, indices, stream=None) -> None:
     _check(load_library().cjx_ncc_topk(
         _cuda_ptr(num, "num"), _cuda_ptr(den, "den"), int(num.stride(0)), int(n), int(T), _cuda_ptr(oo, "oo"),
         _cuda_ptr(yinv, "yinv"), _cuda_ptr(zinv, "zinv"), int(k), _cuda_ptr(indices, "indices"), _stream_ptr(stream)))
+
+
+def ncc_directions_workspace_size(n: int, kd: int, n_dir: int) -> int:
+    v = ctypes.c_size_t(0)
+    _check(load_library().cjx_ncc_directions_workspace_size(int(n), int(kd), int(n_dir), ctypes.byref(v)))
+    return int(v.value)
+
+
+def ncc_directions(y16, z16, s16, p16, kp, dirs, n_dir, n_inplane, num, den, workspace, stream=None) -> None:
+    """cjx_ncc_directions: num / den [n, kd * n_inplane] of each image against its proposed directions'
+    templates (rows from pack_observed / pack_templates)."""
+    n, kd = int(dirs.shape[0]), int(dirs.shape[1])
+    _check(load_library().cjx_ncc_directions(
+        _cuda_ptr(y16, "y16"), _cuda_ptr(z16, "z16"), _cuda_ptr(s16, "s16"), _cuda_ptr(p16, "p16"), n, int(kp),
+        _cuda_ptr(dirs, "dirs"), kd, int(n_dir), int(n_inplane), _cuda_ptr(num, "num"), _cuda_ptr(den, "den"),
+        _cuda_ptr(workspace, "workspace"), int(workspace.numel() * workspace.element_size()), _stream_ptr(stream)))
 
 
 def selftest_bounded_wait(limit_ns: int, status, stream=None) -> None:

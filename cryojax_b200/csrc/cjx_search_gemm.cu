@@ -16,7 +16,10 @@
 // No counterpart in the reference: its grid search simulates every pair.
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "cjx_common.cuh"
+#include "cjx_profile.cuh"
 
 namespace cjx {
 
@@ -242,6 +245,129 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Candidate blocks of the learned search: each image's proposed directions
+// against the shared template rows, without simulating anything.
+// ---------------------------------------------------------------------------
+// Counting sort of the (image, slot) pairs by proposed direction, so the CTAs
+// that read one direction's n_inplane template rows run together and find
+// them in L2.  cursor: [n_dir + 1] ints (zeroed, then counts, then offsets);
+// directions outside [0, n_dir) go to the last bin.
+__device__ __forceinline__ int dir_bin(int d, int n_dir) { return (unsigned)d < (unsigned)n_dir ? d : n_dir; }
+
+__global__ void k_dir_count(const int32_t* __restrict__ dirs, int64_t pairs, int n_dir, int* __restrict__ cursor) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < pairs; p += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(cursor + dir_bin(dirs[p], n_dir), 1);
+}
+
+// exclusive prefix sum of cursor[0..bins) in place (one block of 1024 threads)
+__global__ void k_dir_scan(int* __restrict__ cursor, int bins) {
+  __shared__ int part[1024];
+  const int per = (bins + 1023) / 1024;
+  const int lo = threadIdx.x * per, hi = min(lo + per, bins);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += cursor[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = lo; i < hi; ++i) {
+    const int c = cursor[i];
+    cursor[i] = run;
+    run += c;
+  }
+}
+
+__global__ void k_dir_scatter(const int32_t* __restrict__ dirs, int64_t pairs, int n_dir, int* __restrict__ cursor,
+                              int32_t* __restrict__ sorted) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < pairs; p += (int64_t)gridDim.x * blockDim.x)
+    sorted[atomicAdd(cursor + dir_bin(dirs[p], n_dir), 1)] = (int32_t)p;
+}
+
+// FP32 dot product of 8 halves at a time
+__device__ __forceinline__ float dot8(uint4 a, uint4 b, float acc) {
+  const __half2* ha = reinterpret_cast<const __half2*>(&a);
+  const __half2* hb = reinterpret_cast<const __half2*>(&b);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float2 fa = __half22float2(ha[q]), fb = __half22float2(hb[q]);
+    acc = fmaf(fa.x, fb.x, acc);
+    acc = fmaf(fa.y, fb.y, acc);
+  }
+  return acc;
+}
+
+// One CTA per (image b, slot k) pair (in direction order): for a in
+// [0, n_inplane), template t = dirs[b][k] n_inplane + a,
+//   num[b][k n_inplane + a] = y16[b] . s16[t]   (K = 2 kp)
+//   den[b][k n_inplane + a] = z16[b] . p16[t]   (K = kp)
+// Each warp takes 3 templates at a time, so one load of the image's row
+// serves three template rows.  Rows are 16-byte aligned (kp % 8 == 0).
+constexpr int kDirTemplatesPerPass = 3;
+
+__global__ void __launch_bounds__(256)
+    k_ncc_directions(const uint4* __restrict__ y16, const uint4* __restrict__ z16, const uint4* __restrict__ s16,
+                     const uint4* __restrict__ p16, int64_t kp, const int32_t* __restrict__ dirs,
+                     const int32_t* __restrict__ sorted, int kd, int n_dir, int n_inplane, float* __restrict__ num,
+                     float* __restrict__ den) {
+  const int32_t pair = sorted[blockIdx.x];
+  const int64_t b = pair / kd;
+  const int k = pair % kd;
+  const int d = dirs[pair];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t out0 = b * (int64_t)kd * n_inplane + (int64_t)k * n_inplane;
+  if ((unsigned)d >= (unsigned)n_dir) {  // no such direction: zero sums, which score 0
+    for (int a = threadIdx.x; a < n_inplane; a += blockDim.x) {
+      num[out0 + a] = 0.f;
+      den[out0 + a] = 0.f;
+    }
+    return;
+  }
+  const int64_t vn = 2 * kp / 8, vd = kp / 8;  // 16-byte vectors per row
+  const uint4* yb = y16 + b * vn;
+  const uint4* zb = z16 + b * vd;
+  for (int a0 = warp * kDirTemplatesPerPass; a0 < n_inplane; a0 += 8 * kDirTemplatesPerPass) {
+    float accn[kDirTemplatesPerPass], accd[kDirTemplatesPerPass];
+    const uint4* srow[kDirTemplatesPerPass];
+    const uint4* prow[kDirTemplatesPerPass];
+#pragma unroll
+    for (int q = 0; q < kDirTemplatesPerPass; ++q) {
+      accn[q] = accd[q] = 0.f;
+      const int a = min(a0 + q, n_inplane - 1);  // a tail pass recomputes the last template, stored once
+      const int64_t t = (int64_t)d * n_inplane + a;
+      srow[q] = s16 + t * vn;
+      prow[q] = p16 + t * vd;
+    }
+    for (int64_t i = lane; i < vn; i += 32) {
+      const uint4 yv = __ldg(yb + i);
+#pragma unroll
+      for (int q = 0; q < kDirTemplatesPerPass; ++q) accn[q] = dot8(yv, __ldg(srow[q] + i), accn[q]);
+    }
+    for (int64_t i = lane; i < vd; i += 32) {
+      const uint4 zv = __ldg(zb + i);
+#pragma unroll
+      for (int q = 0; q < kDirTemplatesPerPass; ++q) accd[q] = dot8(zv, __ldg(prow[q] + i), accd[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < kDirTemplatesPerPass; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        accn[q] += __shfl_xor_sync(0xffffffffu, accn[q], o);
+        accd[q] += __shfl_xor_sync(0xffffffffu, accd[q], o);
+      }
+      if (lane == 0 && a0 + q < n_inplane) {
+        num[out0 + a0 + q] = accn[q];
+        den[out0 + a0 + q] = accd[q];
+      }
+    }
+  }
+}
+
 }  // namespace cjx
 
 extern "C" {
@@ -292,6 +418,53 @@ int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t n, int6
   cjx::k_ncc_topm<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(num, den, ld, T, oo, yinv, zinv, k,
                                                                             indices);
   return cjx::check_cuda(cudaGetLastError(), "ncc_topk launch");
+}
+
+
+static size_t ncc_directions_workspace_bytes(int64_t n, int kd, int n_dir) {
+  return sizeof(int) * ((size_t)n_dir + 1 + (size_t)n * kd);
+}
+
+int cjx_ncc_directions_workspace_size(int64_t n, int kd, int n_dir, size_t* bytes) {
+  if (!bytes) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "bytes is NULL");
+  if (n < 0 || kd < 1 || n_dir < 1) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_directions: bad sizes");
+  *bytes = ncc_directions_workspace_bytes(n, kd, n_dir);
+  return CJX_OK;
+}
+
+int cjx_ncc_directions(const void* y16, const void* z16, const void* s16, const void* p16, int64_t n, int64_t kp,
+                       const int32_t* dirs, int kd, int n_dir, int n_inplane, float* num, float* den,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+  if (n < 0 || kp < 8 || kp % 8 || kd < 1 || n_dir < 1 || n_inplane < 1)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT,
+                     "ncc_directions: need kp a positive multiple of 8 and kd, n_dir, n_inplane >= 1");
+  if (n * (int64_t)kd > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "ncc_directions: too many pairs");
+  if (n == 0) return CJX_OK;
+  if (!y16 || !z16 || !s16 || !p16 || !dirs || !num || !den || !workspace)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_directions: NULL pointer");
+  if (workspace_bytes < ncc_directions_workspace_bytes(n, kd, n_dir))
+    return cjx::fail(CJX_ERR_WORKSPACE, "ncc_directions: workspace smaller than cjx_ncc_directions_workspace_size");
+  for (const void* ptr : {y16, z16, s16, p16})
+    if (reinterpret_cast<uintptr_t>(ptr) % 16)
+      return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_directions: rows must be 16-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int* cursor = static_cast<int*>(workspace);
+  int32_t* sorted = cursor + n_dir + 1;
+  const int64_t pairs = n * kd;
+  if (int e = cjx::check_cuda(cudaMemsetAsync(cursor, 0, sizeof(int) * ((size_t)n_dir + 1), s), "cudaMemsetAsync"))
+    return e;
+  const int blocks = (int)std::min<int64_t>((pairs + 255) / 256, 1184);
+  cjx::prof_begin(s);
+  cjx::k_dir_count<<<blocks, 256, 0, s>>>(dirs, pairs, n_dir, cursor);
+  cjx::k_dir_scan<<<1, 1024, 0, s>>>(cursor, n_dir + 1);
+  cjx::k_dir_scatter<<<blocks, 256, 0, s>>>(dirs, pairs, n_dir, cursor, sorted);
+  cjx::prof_end("k_dir_sort", s);
+  cjx::prof_begin(s);
+  cjx::k_ncc_directions<<<(unsigned)pairs, 256, 0, s>>>(
+      static_cast<const uint4*>(y16), static_cast<const uint4*>(z16), static_cast<const uint4*>(s16),
+      static_cast<const uint4*>(p16), kp, dirs, sorted, kd, n_dir, n_inplane, num, den);
+  cjx::prof_end("k_ncc_directions", s);
+  return cjx::check_cuda(cudaGetLastError(), "ncc_directions launch");
 }
 
 }  // extern "C"

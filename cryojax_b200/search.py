@@ -144,7 +144,8 @@ class LearnedPoseSearch:
     search therefore stays both the fallback and the scorer of every result.
     """
 
-    def __init__(self, net, grid, *, top_k=16, threshold=float("-inf"), search: PoseSearch | None = None):
+    def __init__(self, net, grid, *, top_k=16, threshold=float("-inf"), search: PoseSearch | None = None,
+                 templates: "TemplateSharingSearch | None" = None, rerank_top=8):
         if net.n_classes != grid.n_dir:
             raise ValueError("the network's classes must be the grid's directions")
         self.net = net
@@ -152,6 +153,11 @@ class LearnedPoseSearch:
         self.top_k = top_k
         self.threshold = threshold
         self.search = search if search is not None else PoseSearch(grid.rotation_matrices())
+        # with `templates` (a TemplateSharingSearch over the same grid) the proposed candidates are scored
+        # from its CTF-free template rows and only the `rerank_top` best per image are simulated (FP32);
+        # the fallback is then its exhaustive search with the same re-ranking
+        self.templates = templates
+        self.rerank_top = rerank_top
 
     def run(self, image_model, observed, *, batch=None, fallback=True) -> LearnedSearchResult:
         """observed: real-space float32 CUDA images (n, P, P)."""
@@ -166,13 +172,23 @@ class LearnedPoseSearch:
                             device=obs.device)
             nat.area_downsample(obs, x)  # the network's input size
         dirs, cand = self.net.propose(x, k=self.top_k, n_inplane=self.grid.n_inplane, batch=batch)
-        res = self.search.run(image_model, obs_f, candidates=cand, observed_is_fourier=True, image_params_device=pd)
+        if self.templates is not None:
+            res = self.templates.run_directions(image_model, obs_f, dirs, self.grid.n_inplane,
+                                                rerank_top=self.rerank_top, observed_is_fourier=True,
+                                                image_params_device=pd)
+        else:
+            res = self.search.run(image_model, obs_f, candidates=cand, observed_is_fourier=True,
+                                  image_params_device=pd)
         best, score = res.best_orientation.copy(), res.best_score.copy()
         low = score < self.threshold
         if fallback and low.any():
             idx = torch.as_tensor(np.flatnonzero(low), device=obs.device)
-            ex = self.search.run(image_model, obs_f.index_select(0, idx).contiguous(), observed_is_fourier=True,
-                                 image_params_device=pd.index_select(0, idx).contiguous())
+            sub_obs, sub_pd = obs_f.index_select(0, idx).contiguous(), pd.index_select(0, idx).contiguous()
+            if self.templates is not None:
+                ex = self.templates.run(image_model, sub_obs, observed_is_fourier=True, image_params_device=sub_pd,
+                                        rerank_top=self.rerank_top)
+            else:
+                ex = self.search.run(image_model, sub_obs, observed_is_fourier=True, image_params_device=sub_pd)
             best[low] = ex.best_orientation
             score[low] = ex.best_score
         return LearnedSearchResult(best, score, low if fallback else np.zeros_like(low), dirs)
@@ -267,6 +283,66 @@ class TemplateSharingSearch:
             nat.pack_templates(out, py, px, self.s16[s:e], self.p16[s:e])
         self._key = key
 
+    def _pack_observed(self, image_model, obs_f, pd):
+        torch = _torch()
+        cfg = image_model.image_config
+        py, px = cfg.padded_shape
+        kp = py * (px // 2 + 1)
+        n = obs_f.shape[0]
+        dev = self.device
+        y16 = torch.empty((n, 2 * kp), dtype=torch.float16, device=dev)
+        z16 = torch.empty((n, kp), dtype=torch.float16, device=dev)
+        oo, yinv, zinv = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+        nat.pack_observed(obs_f, pd, py, px, image_model._flags(), y16, z16, oo, yinv, zinv)
+        return y16, z16, oo, yinv, zinv
+
+    def _rerank(self, image_model, obs_f, pd, top):
+        """FP32 scores (PoseSearch with candidate lists) of the (n, m) template indices `top`."""
+        if getattr(self, "_plain", None) is None:
+            self._plain = PoseSearch(self.rot, device=self.device)
+        return self._plain.run(image_model, obs_f, candidates=top, observed_is_fourier=True, image_params_device=pd)
+
+    def run_directions(self, image_model, observed, dirs, n_inplane, *, rerank_top=8, observed_is_fourier=False,
+                       image_params_device=None) -> SearchResult:
+        """Best orientation per image among its proposed directions' templates, with no simulation.
+
+        ``dirs`` (n, kd) int32 CUDA: each image's proposed directions; template t = dir * n_inplane + a
+        (the orientation grid's order).  Every candidate is scored from the FP16 template rows
+        (cjx_ncc_directions), the ``rerank_top`` best of each image are rescored by the FP32 scorer
+        (PoseSearch with candidate lists) and the best of those is returned: the candidate set's FP32
+        optimum whenever it is among them.
+        """
+        torch = _torch()
+        if not 1 <= rerank_top <= 16:
+            raise ValueError("rerank_top must be in [1, 16]")
+        self.build_templates(image_model)
+        cfg = image_model.image_config
+        py, px = cfg.padded_shape
+        kp = py * (px // 2 + 1)
+        obs_f = observed if observed_is_fourier else observed_to_fourier(observed)
+        n = obs_f.shape[0]
+        pd = image_params_device if image_params_device is not None else torch.as_tensor(
+            image_model.image_params(), device=self.device)
+        dirs = dirs.to(device=self.device, dtype=torch.int32).contiguous()
+        kd = dirs.shape[1]
+        K = kd * n_inplane
+        if self.n_orientations % n_inplane:
+            raise ValueError("the template count must be a multiple of n_inplane")
+        n_dir = self.n_orientations // n_inplane
+        y16, z16, oo, yinv, zinv = self._pack_observed(image_model, obs_f, pd)
+        num = torch.empty((n, K), dtype=torch.float32, device=self.device)
+        den = torch.empty((n, K), dtype=torch.float32, device=self.device)
+        ws = torch.empty(nat.ncc_directions_workspace_size(n, kd, n_dir), dtype=torch.uint8, device=self.device)
+        nat.ncc_directions(y16, z16, self.s16, self.p16, kp, dirs, n_dir, n_inplane, num, den, ws)
+        m = min(rerank_top, K)
+        pos = torch.empty((n, m), dtype=torch.int32, device=self.device)
+        nat.ncc_topk(num, den, n, K, oo, yinv, zinv, m, pos)
+        # position k n_inplane + a -> template dirs[b][k] n_inplane + a
+        pos64 = pos.long()
+        top = (dirs.long().gather(1, pos64 // n_inplane) * n_inplane + pos64 % n_inplane).to(torch.int32)
+        exact = self._rerank(image_model, obs_f, pd, top.contiguous())
+        return SearchResult(exact.best_orientation, exact.best_score, None, top)
+
     def run(self, image_model, observed, *, observed_is_fourier=False, image_params_device=None,
             return_scores=False, rerank_top=0) -> SearchResult:
         """Best orientation per image; with ``rerank_top`` = k (<= 16) the k best FP16 candidates of
@@ -283,13 +359,9 @@ class TemplateSharingSearch:
         n = obs_f.shape[0]
         pd = image_params_device if image_params_device is not None else torch.as_tensor(
             image_model.image_params(), device=self.device)
-        flags = image_model._flags()
         T = self.n_orientations
         dev = self.device
-        y16 = torch.empty((n, 2 * kp), dtype=torch.float16, device=dev)
-        z16 = torch.empty((n, kp), dtype=torch.float16, device=dev)
-        oo, yinv, zinv = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
-        nat.pack_observed(obs_f, pd, py, px, flags, y16, z16, oo, yinv, zinv)
+        y16, z16, oo, yinv, zinv = self._pack_observed(image_model, obs_f, pd)
         best_score = torch.empty(n, dtype=torch.float32, device=dev)
         best = torch.empty(n, dtype=torch.int32, device=dev)
         scores = torch.empty((n, T), dtype=torch.float32, device=dev) if return_scores else None
@@ -308,7 +380,5 @@ class TemplateSharingSearch:
                 nat.ncc_topk(num, den, m, T, oo[s:e], yinv[s:e], zinv[s:e], rerank_top, top[s:e])
         if top is None:
             return SearchResult(best.cpu().numpy().astype(np.int64), best_score.cpu().numpy(), scores, None)
-        if getattr(self, "_plain", None) is None:
-            self._plain = PoseSearch(self.rot, device=dev)
-        exact = self._plain.run(image_model, obs_f, candidates=top, observed_is_fourier=True, image_params_device=pd)
+        exact = self._rerank(image_model, obs_f, pd, top)
         return SearchResult(exact.best_orientation, exact.best_score, scores, top)

@@ -485,6 +485,23 @@ CJX_API int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t
                          const float* oo, const float* yinv, const float* zinv, int k,
                          int32_t* indices, void* stream);
 
+/* The learned search's rescoring from the same template rows: for image b
+ * and proposed-direction slot k (dirs [n][kd], int32), the n_inplane
+ * templates t = dirs[b][k] n_inplane + a (a in [0, n_inplane)) give
+ *   num[b][k n_inplane + a] = y16[b] . s16[t] (K = 2 kp),
+ *   den[b][k n_inplane + a] = z16[b] . p16[t] (K = kp),
+ * the inputs of cjx_ncc_argmax / cjx_ncc_topk over kd n_inplane columns
+ * (kp = Py (Px/2+1), a multiple of 8; rows 16-byte aligned).  The (image,
+ * slot) pairs are processed in direction order, so the images proposing
+ * one direction read its template rows from L2 together.  A direction
+ * outside [0, n_dir) gives zero sums.  workspace:
+ * cjx_ncc_directions_workspace_size bytes.  No counterpart in the reference
+ * (its search simulates every candidate).                                   */
+CJX_API int cjx_ncc_directions_workspace_size(int64_t n, int kd, int n_dir, size_t* bytes);
+CJX_API int cjx_ncc_directions(const void* y16, const void* z16, const void* s16, const void* p16, int64_t n,
+                               int64_t kp, const int32_t* dirs, int kd, int n_dir, int n_inplane, float* num,
+                               float* den, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- tensor-core GEMM (pose-proposal network) -------------------------- */
 #define CJX_GEMM_OUT_BF16 1   /* store C as BF16 (default FP32)              */
 #define CJX_GEMM_BIAS 2       /* C[:, n] += bias[n] (FP32)                    */

@@ -101,3 +101,45 @@ def test_calibrated_fallback_reaches_agreement(setup):
     assert 0 < res.fallback.mean() <= 1 / 3, res.fallback.mean()
     # fallback images carry the exhaustive answer exactly
     np.testing.assert_array_equal(res.best_orientation[res.fallback], ex.best_orientation[res.fallback])
+
+
+def test_template_row_scoring_matches_simulated_candidates(setup):
+    """The learned search with candidates scored from the shared template rows (cjx_ncc_directions) and the
+    8 best re-ranked in FP32 returns the simulate-every-candidate answer on >= 99 % of the images (exactly
+    whenever that answer is among the 8), and its FP16 candidate scores equal the template-sharing
+    exhaustive search's scores of the same templates."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.gradients import observed_to_fourier
+    from cryojax_b200.search import LearnedPoseSearch, PoseSearch, TemplateSharingSearch
+
+    V, cfg, grid, net = setup
+    model, noisy = _batch(V, cfg, 128, 13, 0.1)
+    search = PoseSearch(grid.rotation_matrices())
+    shared = TemplateSharingSearch(grid.rotation_matrices())
+    sim = LearnedPoseSearch(net, grid, top_k=8, search=search).run(model, noisy, fallback=False)
+    tmpl = LearnedPoseSearch(net, grid, top_k=8, search=search, templates=shared, rerank_top=8).run(
+        model, noisy, fallback=False)
+    agree = float(np.mean(sim.best_orientation == tmpl.best_orientation))
+    assert agree >= 0.99, agree
+    same = sim.best_orientation == tmpl.best_orientation
+    np.testing.assert_array_equal(sim.best_score[same], tmpl.best_score[same])
+
+    # FP16 candidate sums against the exhaustive template GEMM's scores of the same templates
+    obs_f = observed_to_fourier(noisy)
+    pd = torch.as_tensor(model.image_params(), device="cuda")
+    full = shared.run(model, obs_f, observed_is_fourier=True, image_params_device=pd, return_scores=True).scores
+    dirs = tmpl.proposed_directions
+    y16, z16, oo, yinv, zinv = shared._pack_observed(model, obs_f, pd)
+    py, px = cfg.padded_shape
+    kp = py * (px // 2 + 1)
+    n, kd, ni = dirs.shape[0], dirs.shape[1], grid.n_inplane
+    num = torch.empty((n, kd * ni), dtype=torch.float32, device="cuda")
+    den = torch.empty_like(num)
+    ws = torch.empty(nat.ncc_directions_workspace_size(n, kd, grid.n_dir), dtype=torch.uint8, device="cuda")
+    nat.ncc_directions(y16, z16, shared.s16, shared.p16, kp, dirs, grid.n_dir, ni, num, den, ws)
+    score = num * yinv[:, None] / torch.sqrt(den * zinv[:, None] * oo[:, None])
+    t = (dirs.long()[:, :, None] * ni + torch.arange(ni, device="cuda")).reshape(n, -1)
+    ref = full.gather(1, t)
+    torch.testing.assert_close(score, ref, rtol=2e-3, atol=2e-4)
