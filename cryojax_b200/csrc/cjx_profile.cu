@@ -52,6 +52,8 @@ void prof_end(const char* name, cudaStream_t s) {
   g_prof.pending_start = nullptr;
 }
 
+bool prof_active() { return g_prof.on; }
+
 }  // namespace cjx
 
 using namespace cjx;

@@ -5,4 +5,5 @@
 namespace cjx {
 void prof_begin(cudaStream_t s);
 void prof_end(const char* name, cudaStream_t s);
+bool prof_active();  // profiling enabled on the calling thread
 }  // namespace cjx

@@ -601,6 +601,7 @@ static std::atomic<int64_t> g_fft_mode{2};
 static std::atomic<int64_t> g_gather_tile{1};
 static std::atomic<int64_t> g_scatter_vec{1};
 static std::atomic<int64_t> g_spline_ilp{4};
+static std::atomic<int64_t> g_overlap{0};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -673,6 +674,7 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_GATHER_TILE) return g_gather_tile.load();
   if (key == CJX_TUNE_SCATTER_VEC) return g_scatter_vec.load();
   if (key == CJX_TUNE_SPLINE_ILP) return g_spline_ilp.load();
+  if (key == CJX_TUNE_OVERLAP) return g_overlap.load();
   return -1;
 }
 
@@ -705,6 +707,11 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_SPLINE_ILP) {
     if (value != 1 && value != 2 && value != 4) return fail(CJX_ERR_INVALID_ARGUMENT, "spline ILP must be 1, 2 or 4");
     g_spline_ilp = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_OVERLAP) {
+    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "overlap must be 0 or 1");
+    g_overlap = value;
     return CJX_OK;
   }
   if (key == CJX_TUNE_SCATTER_VEC) {
@@ -748,14 +755,13 @@ int launch_ewald_colfft(const SliceGeom& g, const float2* t2, const cjx_image_pa
 int launch_ewald_direct(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                         int64_t n_images, float2* out, cudaStream_t stream);
 
-// Passes up to T2 (gather, column inverse FFT + window, rows) for one chunk of
-// `cnt` images starting at processing index k0.
-int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                         int64_t k0, int cnt, float2* t1, float2* t2, float2* hb, cudaStream_t stream,
-                         const Tuning& tn) {
+// The front of the resize path for one chunk of `cnt` images starting at
+// processing index k0: gather and column inverse FFT + window, into T1.
+static int launch_front(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                        int64_t k0, int cnt, float2* t1, float2* hb, cudaStream_t stream, const Tuning& tn) {
   if (int e = ensure_smem_attrs()) return e;
   const int64_t ilp = (g.flags & CJX_GRID_SPLINE) ? tn.spline_ilp : tn.ilp;
-  const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
+  const int rn = reg_fft_radix(g.n);
   const bool fast = tn.fft_mode >= 1;
   // gather mode 2: the register-FFT fused pass (trilinear grids, N = 32 R); otherwise the split pair of
   // kernels, or mode 0's shared-memory fused kernel, which has no pair, spline or Ewald path
@@ -763,10 +769,8 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
   const bool split = !fused_reg && (tn.gather_mode != 0 ||
                                     (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE)));
   const bool t512 = tn.fft_mode == 2 && rn == 16;  // 512-point column transforms through the transpose FFT
-  const size_t sa = smem_a(g), sb = smem_b(g);
+  const size_t sa = smem_a(g);
   const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
-  const size_t sb_reg =
-      sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
     if (fused_reg) {
       if (int e = launch_gather_colifft_fused(g, grid, params, order, k0, cnt, t1, tn, stream)) return e;
     } else if (split) {
@@ -842,7 +846,18 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 #undef CJX_GC
       prof_end("k_gather_colifft", stream);
     }
-    if (g.flags & CJX_EWALD_SPHERE) return launch_ewald_rows(g, t1, t2, cnt, stream, tn);
+  return check_cuda(cudaGetLastError(), "forward launch");
+}
+
+// The row pass for one chunk: T1 -> T2.
+static int launch_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt, cudaStream_t stream,
+                       const Tuning& tn) {
+  if (g.flags & CJX_EWALD_SPHERE) return launch_ewald_rows(g, t1, t2, cnt, stream, tn);
+  const int rn = reg_fft_radix(g.n), rpx = reg_fft_radix(g.px);
+  const bool fast = tn.fft_mode >= 1;
+  const size_t sb = smem_b(g);
+  const size_t sb_reg =
+      sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
     prof_begin(stream);
     const dim3 gb((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt);
     if (fast && rn && rpx) {
@@ -860,9 +875,111 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
   return check_cuda(cudaGetLastError(), "forward launch");
 }
 
+// Passes up to T2 (gather, column inverse FFT + window, rows) for one chunk of
+// `cnt` images starting at processing index k0.
+int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
+                         int64_t k0, int cnt, float2* t1, float2* t2, float2* hb, cudaStream_t stream,
+                         const Tuning& tn) {
+  if (int e = launch_front(g, grid, params, order, k0, cnt, t1, hb, stream, tn)) return e;
+  return launch_rows(g, t1, t2, cnt, stream, tn);
+}
+
 Tuning current_tuning() {
   return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
-                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load()};
+                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load(), (int)g_overlap.load()};
+}
+
+// The last pass for one chunk: column FFT + scale, CTF, envelope, translation (and filter), T2 -> out.
+static int launch_tail(const SliceGeom& g, const float2* t2, const cjx_image_params* params, const int32_t* order,
+                       float2* out, int64_t k0, int cnt, cudaStream_t stream, const Tuning& tn) {
+  if (g.flags & CJX_EWALD_SPHERE) return launch_ewald_colfft(g, t2, params, order, out, k0, cnt, stream, tn);
+  const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
+  const int rpy = reg_fft_radix(g.py);
+  const size_t sc = smem_c(g);
+  const size_t sc_reg = sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1));
+  prof_begin(stream);
+  const dim3 gcc((g.pxh + kWarps - 1) / kWarps, cnt);
+  if (tn.fft_mode >= 1 && rpy) {
+    switch (rpy) {
+#define CJX_C_CASE(R) \
+  case R:             \
+    k_colfft_epilogue_reg<R><<<gcc, kWarps * 32, sc_reg, stream>>>(t2, params, order, out, g, k0, norm); break;
+      CJX_C_CASE(1) CJX_C_CASE(2) CJX_C_CASE(3) CJX_C_CASE(4) CJX_C_CASE(5)
+      CJX_C_CASE(6) CJX_C_CASE(8) CJX_C_CASE(10) CJX_C_CASE(12) CJX_C_CASE(16)
+#undef CJX_C_CASE
+    }
+  } else {
+    k_colfft_epilogue<<<gcc, kWarps * 32, sc, stream>>>(t2, params, order, out, g, k0, norm);
+  }
+  prof_end("k_colfft_epilogue", stream);
+  return check_cuda(cudaGetLastError(), "forward launch");
+}
+
+// Second stream and events of the overlapped chunk schedule, per host thread
+// and device, created on first use and kept for the thread's life (they are
+// not destroyed at thread exit, when the runtime may already be shut down).
+// Being per thread, two host threads never share them.
+struct OverlapCtx {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t ready[2] = {nullptr, nullptr};  // front pass of the chunk in buffer b done (caller's stream)
+  cudaEvent_t freed[2] = {nullptr, nullptr};  // row pass of the chunk in buffer b done: its T1 may be rewritten
+};
+
+static int overlap_ctx(OverlapCtx** out) {
+  static thread_local OverlapCtx ctx[kMaxDevices];
+  int dev = 0;
+  if (int e = check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return e;
+  if (dev < 0 || dev >= kMaxDevices) return fail(CJX_ERR_UNSUPPORTED, "device index beyond the 64 supported");
+  OverlapCtx& c = ctx[dev];
+  if (!c.side) {
+    OverlapCtx n;
+    cudaError_t e = cudaStreamCreateWithFlags(&n.side, cudaStreamNonBlocking);
+    cudaEvent_t* evs[] = {&n.fork, &n.join, &n.ready[0], &n.ready[1], &n.freed[0], &n.freed[1]};
+    for (cudaEvent_t* ev : evs)
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return check_cuda(e, "creating the overlap stream and events");
+    c = n;
+  }
+  *out = &c;
+  return CJX_OK;
+}
+
+// Chunks of half the workspace's images, alternating between its two halves:
+// chunk i's front pass (gather + column inverse FFT, into T1[i % 2]) runs on
+// the caller's stream while the row and column passes of chunk i - 1 run on
+// the second stream.  The front of chunk i waits until the row pass of chunk
+// i - 2 has read T1[i % 2]; the rows of chunk i wait for its front.  The
+// second stream forks from the caller's stream at the start and joins it at
+// the end, so the call stays stream-ordered (and capturable as one graph).
+static int launch_forward_overlapped(const SliceGeom& g, const float2* grid, const cjx_image_params* params,
+                                     const int32_t* order, int64_t n_images, float2* out, float2* t1, float2* t2,
+                                     float2* hb, int64_t chunk, cudaStream_t stream, const Tuning& tn) {
+  OverlapCtx* c = nullptr;
+  if (int e = overlap_ctx(&c)) return e;
+  const int64_t half = chunk / 2;
+  float2* t1b[2] = {t1, t1 + (size_t)half * g.py * g.ld1};
+  float2* t2b[2] = {t2, t2 + (size_t)half * g.py * g.ld2};
+  float2* hbb[2] = {hb, hb + (size_t)half * g.ncols * g.ldh};
+  if (int e = check_cuda(cudaEventRecord(c->fork, stream), "cudaEventRecord")) return e;
+  if (int e = check_cuda(cudaStreamWaitEvent(c->side, c->fork, 0), "cudaStreamWaitEvent")) return e;
+  int err = CJX_OK;
+  int64_t i = 0;
+  for (int64_t k0 = 0; k0 < n_images && !err; k0 += half, ++i) {
+    const int b = (int)(i & 1);
+    const int cnt = (int)std::min<int64_t>(half, n_images - k0);
+    if (i >= 2) err = check_cuda(cudaStreamWaitEvent(stream, c->freed[b], 0), "cudaStreamWaitEvent");
+    if (!err) err = launch_front(g, grid, params, order, k0, cnt, t1b[b], hbb[b], stream, tn);
+    if (!err) err = check_cuda(cudaEventRecord(c->ready[b], stream), "cudaEventRecord");
+    if (!err) err = check_cuda(cudaStreamWaitEvent(c->side, c->ready[b], 0), "cudaStreamWaitEvent");
+    if (!err) err = launch_rows(g, t1b[b], t2b[b], cnt, c->side, tn);
+    if (!err) err = check_cuda(cudaEventRecord(c->freed[b], c->side), "cudaEventRecord");
+    if (!err) err = launch_tail(g, t2b[b], params, order, out, k0, cnt, c->side, tn);
+  }
+  // join the second stream back into the caller's stream, also after an error
+  const int ej = check_cuda(cudaEventRecord(c->join, c->side), "cudaEventRecord");
+  const int ew = ej ? ej : check_cuda(cudaStreamWaitEvent(stream, c->join, 0), "cudaStreamWaitEvent");
+  return err ? err : ew;
 }
 
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
@@ -900,32 +1017,12 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   float2* t1 = static_cast<float2*>(workspace);
   float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
   float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
-  const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
-  const int rpy = reg_fft_radix(g.py);
-  const bool fast = tn.fft_mode >= 1;
-  const size_t sc_reg = sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1));
+  if (tn.overlap && !prof_active() && chunk >= 2 && n_images > chunk / 2)
+    return launch_forward_overlapped(g, grid, params, order, n_images, out, t1, t2, hb, chunk, stream, tn);
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
-    if (g.flags & CJX_EWALD_SPHERE) {
-      if (int e = launch_ewald_colfft(g, t2, params, order, out, k0, cnt, stream, tn)) return e;
-      continue;
-    }
-    prof_begin(stream);
-    const dim3 gcc((g.pxh + kWarps - 1) / kWarps, cnt);
-    if (fast && rpy) {
-      switch (rpy) {
-#define CJX_C_CASE(R) \
-  case R:             \
-    k_colfft_epilogue_reg<R><<<gcc, kWarps * 32, sc_reg, stream>>>(t2, params, order, out, g, k0, norm); break;
-        CJX_C_CASE(1) CJX_C_CASE(2) CJX_C_CASE(3) CJX_C_CASE(4) CJX_C_CASE(5)
-        CJX_C_CASE(6) CJX_C_CASE(8) CJX_C_CASE(10) CJX_C_CASE(12) CJX_C_CASE(16)
-#undef CJX_C_CASE
-      }
-    } else {
-      k_colfft_epilogue<<<gcc, kWarps * 32, sc, stream>>>(t2, params, order, out, g, k0, norm);
-    }
-    prof_end("k_colfft_epilogue", stream);
+    if (int e = launch_tail(g, t2, params, order, out, k0, cnt, stream, tn)) return e;
   }
   return check_cuda(cudaGetLastError(), "forward launch");
 }

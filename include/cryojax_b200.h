@@ -426,6 +426,15 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
 #define CJX_TUNE_GATHER_TILE 5
 #define CJX_TUNE_SCATTER_VEC 6
 #define CJX_TUNE_SPLINE_ILP 7
+/* CJX_TUNE_OVERLAP: 1 = the resize path runs its chunks as two interleaved
+ * halves, the gather pass of one on the caller's stream while the row and
+ * column passes of the previous one run on a second stream of the calling
+ * host thread (created on its first use on each device, before any stream
+ * capture that should include it; joined back into the caller's stream
+ * before the call returns, so the call stays stream-ordered); 0 = one
+ * stream.  The allocation-free entry point and calls made while profiling
+ * is enabled always use one stream.                                        */
+#define CJX_TUNE_OVERLAP 8
 CJX_API int cjx_tuning_set(int key, int64_t value);
 CJX_API int cjx_tuning_get(int key, int64_t* value);
 
