@@ -178,7 +178,7 @@ void launch_fused_rsm(const SliceGeom& g, const float2* grid, const cjx_image_pa
 template <int R, typename Layout>
 int launch_fused_r(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                    int64_t k0, int cnt, float2* t1, const Tuning& tn, cudaStream_t stream) {
-  const bool t512 = tn.fft_mode == 2;
+  const bool t512 = tn.fft_mode >= 2;
   if constexpr (R == 16 && std::is_same<Layout, PairLayout>::value) {
     const int key = 10 * tn.ilp + tn.tile;
     switch (key) {

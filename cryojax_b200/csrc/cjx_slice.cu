@@ -390,11 +390,11 @@ __global__ void __launch_bounds__(kWarps * 32)
 // R = RN), Px window, Px-point forward FFT (register form, RP), split.
 // The load of the packed pair (z = A + iB in the lane's bit-reversed order)
 // is separate, so that a kernel can issue it before its table copy.
-template <int RN>
+template <int RN, bool NATURAL = false>
 __device__ __forceinline__ void rows_pair_load(const float2* __restrict__ rowA, const float2* __restrict__ rowB,
                                                bool has_b, float2 (&z)[RN], int lane) {
   constexpr int n = 32 * RN, h = n / 2;
-  const int bl = brev5(lane);
+  const int bl = NATURAL ? lane : brev5(lane);  // natural lane order feeds the transpose FFT
 #pragma unroll
   for (int n1 = 0; n1 < RN; ++n1) {
     const int idx = 32 * n1 + bl;
@@ -414,15 +414,23 @@ __device__ __forceinline__ void rows_pair_load(const float2* __restrict__ rowA, 
   }
 }
 
-template <int RN, int RP>
+template <int RN, int RP, bool T512 = false>
 __device__ __forceinline__ void rows_pair_reg(float2 (&z)[RN], bool has_b, float2* __restrict__ outA, int ld2,
                                               float2* buf, const float2* tabN, const float2* tabP,
-                                              const LaneTwiddles& lt, int lane, const int* winx) {
+                                              const LaneTwiddles& lt, int lane, const int* winx,
+                                              const float2* w32 = nullptr) {
   constexpr int px = 32 * RP;
   const int bl = brev5(lane);
-  warp_fft_reg<RN, +1>(z, tabN, lt, lane);  // z = a + i b (the two real rows)
+  if constexpr (T512) {  // 512-point inverse as 16 x 32 through one shared-memory transpose (z in natural order)
+    static_assert(RN == 16, "the transpose FFT is 512-point");
+    warp_fft512_t<+1>(z, tabN, w32, buf, lane);
 #pragma unroll
-  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+    for (int q = 0; q < RN; ++q) buf[pad16(fft512_t_out(q, lane))] = z[q];
+  } else {
+    warp_fft_reg<RN, +1>(z, tabN, lt, lane);  // z = a + i b (the two real rows)
+#pragma unroll
+    for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+  }
   __syncwarp();
   float2 w[RP];
 #pragma unroll
@@ -443,7 +451,7 @@ __device__ __forceinline__ void rows_pair_reg(float2 (&z)[RN], bool has_b, float
   }
 }
 
-template <int RN>
+template <int RN, bool T512 = false>
 __global__ void __launch_bounds__(kWarps * 32)
     k_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
   constexpr int n = 32 * RN;
@@ -462,7 +470,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2 z[RN];
   if (ra < g.py) {
     const float2* rowA = t1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
-    rows_pair_load<RN>(rowA, rowA + g.ld1, has_b, z, lane);
+    rows_pair_load<RN, T512>(rowA, rowA + g.ld1, has_b, z, lane);
   }
   build_reg_twiddles(tabN, n);
   build_reg_twiddles(tabP, px);
@@ -475,7 +483,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   const LaneTwiddles lt = make_lane_twiddles(w32, lane);
   switch (rp) {
 #define CJX_ROWS_CASE(RPV) \
-  case RPV: rows_pair_reg<RN, RPV>(z, has_b, outA, g.ld2, buf, tabN, tabP, lt, lane, winx); break;
+  case RPV: rows_pair_reg<RN, RPV, T512>(z, has_b, outA, g.ld2, buf, tabN, tabP, lt, lane, winx, w32); break;
     CJX_ROWS_CASE(1) CJX_ROWS_CASE(2) CJX_ROWS_CASE(3) CJX_ROWS_CASE(4) CJX_ROWS_CASE(5)
     CJX_ROWS_CASE(6) CJX_ROWS_CASE(8) CJX_ROWS_CASE(10) CJX_ROWS_CASE(12) CJX_ROWS_CASE(16)
 #undef CJX_ROWS_CASE
@@ -695,7 +703,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_FFT_MODE) {
-    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "FFT mode must be 0, 1 or 2");
+    if (value < 0 || value > 3) return fail(CJX_ERR_INVALID_ARGUMENT, "FFT mode must be 0, 1, 2 or 3");
     g_fft_mode = value;
     return CJX_OK;
   }
@@ -768,7 +776,7 @@ static int launch_front(const SliceGeom& g, const float2* grid, const cjx_image_
   const bool fused_reg = tn.gather_mode == 2 && fast && fused_gather_supported(g);
   const bool split = !fused_reg && (tn.gather_mode != 0 ||
                                     (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE)));
-  const bool t512 = tn.fft_mode == 2 && rn == 16;  // 512-point column transforms through the transpose FFT
+  const bool t512 = tn.fft_mode >= 2 && rn == 16;  // 512-point column transforms through the transpose FFT
   const size_t sa = smem_a(g);
   const size_t sa_reg = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
     if (fused_reg) {
@@ -863,7 +871,12 @@ static int launch_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt
     if (fast && rn && rpx) {
       switch (rn) {
 #define CJX_B_CASE(R) \
-  case R: k_rows_reg<R><<<gb, kWarps * 32, sb_reg, stream>>>(t1, t2, g, rpx); break;
+  case R:                                                                                   \
+    if (R == 16 && tn.fft_mode == 3)                                                        \
+      k_rows_reg<16, true><<<gb, kWarps * 32, sb_reg, stream>>>(t1, t2, g, rpx);             \
+    else                                                                                    \
+      k_rows_reg<R><<<gb, kWarps * 32, sb_reg, stream>>>(t1, t2, g, rpx);                    \
+    break;
         CJX_B_CASE(1) CJX_B_CASE(2) CJX_B_CASE(3) CJX_B_CASE(4) CJX_B_CASE(5)
         CJX_B_CASE(6) CJX_B_CASE(8) CJX_B_CASE(10) CJX_B_CASE(12) CJX_B_CASE(16)
 #undef CJX_B_CASE

@@ -407,7 +407,8 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
  * (R in 1-6, 8, 10, 12, 16), 2 (default) = the same, with the 512-point
  * column transforms of the resize stage done as 16 x 32 through one
- * shared-memory transpose instead of five shuffle stages, 0 = shared-memory
+ * shared-memory transpose instead of five shuffle stages, 3 = as 2 and the
+ * row pass's 512-point inverse transforms the same way, 0 = shared-memory
  * Stockham FFTs everywhere.
  * CJX_TUNE_GATHER_TILE: lanes of a gather warp cover 2 x 16 (0), 4 x 8 (1)
  * or 8 x 4 (2) samples (columns x rows) of the slice plane; 3 = one column

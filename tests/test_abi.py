@@ -85,7 +85,7 @@ def test_tuning_knobs():
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(nat.CJX_TUNE_SPLINE_ILP, 3)
     with pytest.raises(nat.CryojaxB200Error):
-        nat.tuning_set(nat.CJX_TUNE_FFT_MODE, 3)
+        nat.tuning_set(nat.CJX_TUNE_FFT_MODE, 4)
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, 3)
     with pytest.raises(nat.CryojaxB200Error):

@@ -60,7 +60,7 @@ def test_resize_path_sizes(cuda_device, n, shape, padded):
     assert max(errs) <= IMAGE_REL_L2_TOL, errs
 
 
-@pytest.mark.parametrize("fft_mode", [0, 1, 2])
+@pytest.mark.parametrize("fft_mode", [0, 1, 2, 3])
 def test_fft_modes_at_the_benchmark_shape(cuda_device, fft_mode):
     """N = 512 -> 320^2 through each FFT implementation (Stockham, shuffle network, 512-point transpose)."""
     import torch
