@@ -157,6 +157,28 @@ int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, voi
     }
   }
   const Tuning base = current_tuning();
+  if (base.multi_waves && n_groups <= kMaxWaveGroups) {
+    // every group on the fused register-FFT path with one grid layout: one launch per pass for all of them
+    WaveInput in[kMaxWaveGroups];
+    int n_in = 0;
+    bool eligible = true;
+    const uint32_t layout_bits = CJX_GRID_BRICKED | CJX_GRID_BRICKED_PAIRS;
+    uint32_t layout = 0;
+    for (int i = 0; i < n_groups && eligible; ++i) {
+      const cjx_slice_group& gr = groups[i];
+      if (gr.n_images == 0) continue;
+      SliceGeom g;
+      int64_t chunk;
+      size_t need;
+      group_plan(gr, &g, &chunk, &need);
+      if (n_in == 0) layout = g.flags & layout_bits;
+      eligible = wave_eligible(g, base) && (g.flags & layout_bits) == layout;
+      in[n_in++] = WaveInput{g, static_cast<const float2*>(gr.grid), gr.params, gr.order,
+                             static_cast<float2*>(gr.out), gr.n_images};
+    }
+    if (eligible && n_in > 0)
+      return launch_forward_waves(in, n_in, workspace, workspace_bytes, static_cast<cudaStream_t>(stream), base);
+  }
   for (int i = 0; i < n_groups; ++i) {
     const cjx_slice_group& gr = groups[i];
     if (gr.n_images == 0) continue;

@@ -816,8 +816,55 @@ struct Tuning {
   int scatter_vec;  // 1 = adjoint grid scatter merges aligned x-corner pairs into 16-byte atomics
   int spline_ilp;   // samples per lane in the cubic-spline gather (1, 2, 4)
   int overlap;      // 1 = resize-path chunks overlap: front pass of one chunk beside the later passes of the last
+  int multi_waves;  // 1 = mixed-size batches run in waves, one launch per pass for all groups
 };
 Tuning current_tuning();
+
+// ---------------------------------------------------------------------------
+// One wave of a mixed-size batch: a slice of every group's images, each pass
+// of the resize path launched once for all of them (the CTAs of the groups
+// follow one another in the launch: group i owns CTAs [cta0[pass], next
+// group's cta0[pass]) of that pass).
+// ---------------------------------------------------------------------------
+constexpr int kMaxWaveGroups = 8;
+struct WaveGroup {
+  SliceGeom g;
+  const float2* grid;
+  const cjx_image_params* params;
+  const int32_t* order;
+  float2* t1;
+  float2* t2;
+  float2* out;
+  int64_t k0;  // processing index of the group's first image in this wave
+  int cnt;     // the group's images in this wave
+  int cta0[3]; // first CTA of the group in the front, row and column passes
+};
+struct Wave {
+  WaveGroup grp[kMaxWaveGroups];
+  int n;
+  int t512;       // 512-point column transforms of the front pass through the transpose FFT
+  int rows_t512;  // the same for the row pass
+};
+
+// One group of a mixed-size batch, as the host hands it to launch_forward_waves.
+struct WaveInput {
+  SliceGeom g;
+  const float2* grid;
+  const cjx_image_params* params;
+  const int32_t* order;
+  float2* out;
+  int64_t n;
+};
+bool wave_eligible(const SliceGeom& g, const Tuning& tn);
+int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                         const Tuning& tn);
+
+// The group that owns CTA `b` of pass `pass`.
+__device__ __forceinline__ int wave_group(const Wave& w, int pass, int b) {
+  int gi = 0;
+  while (gi + 1 < w.n && b >= w.grp[gi + 1].cta0[pass]) ++gi;
+  return gi;
+}
 
 // ---------------------------------------------------------------------------
 // Host-side error plumbing

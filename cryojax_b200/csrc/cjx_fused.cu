@@ -44,23 +44,25 @@ __device__ __forceinline__ void fused_lane_offsets(int warp, int lane, int& du, 
   }
 }
 
+// Body for the CTA at (bx, by) (column block, image of the chunk): smem is
+// the dynamic shared memory, w32 a 32-entry shared table.
 template <int R, typename Layout, int S, int MAP, bool T512>
-__global__ void __launch_bounds__(kCols * 32, 4)
-    k_gather_colifft_fused(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
-                           const int32_t* __restrict__ order, float2* __restrict__ t1, SliceGeom g, int64_t k0) {
+__device__ __forceinline__ void gather_colifft_body(const float2* __restrict__ grid,
+                                                    const cjx_image_params* __restrict__ params,
+                                                    const int32_t* __restrict__ order, float2* __restrict__ t1,
+                                                    const SliceGeom& g, int64_t k0, int bx, int by, float2* smem,
+                                                    float2* w32) {
   constexpr int n = 32 * R;
   constexpr int stride = pad16(n) + 1;
   static_assert(!T512 || R == 16, "the transpose FFT is 512-point");
-  extern __shared__ float2 smem[];
-  __shared__ float2 w32[32];
   float2* tab = smem;
   float2* tile = smem + n;  // [kCols][stride], rows in the pad16 layout
   int* winy = reinterpret_cast<int*>(tile + kCols * stride);
   const Layout L(n);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int j0 = blockIdx.x * kCols;
+  const int j0 = bx * kCols;
   const int ncols = min(kCols, g.ncols - j0);
-  const int64_t k = k0 + blockIdx.y;
+  const int64_t k = k0 + by;
   const int64_t img = order ? (int64_t)order[k] : k;
   const bool ewald = (g.flags & CJX_EWALD_SPHERE) != 0;
 
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(kCols * 32, 4)
   }
   __syncthreads();
 
-  float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
+  float2* dst = t1 + (size_t)by * g.py * g.ld1 + j0;
   for (int e = threadIdx.x; e < g.py * kCols; e += blockDim.x) {
     const int m = e / kCols, jj = e % kCols;
     if (jj < ncols) {
@@ -154,6 +156,15 @@ __global__ void __launch_bounds__(kCols * 32, 4)
       dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? tile[jj * stride + pad16(src)] : make_float2(0.f, 0.f);
     }
   }
+}
+
+template <int R, typename Layout, int S, int MAP, bool T512>
+__global__ void __launch_bounds__(kCols * 32, 4)
+    k_gather_colifft_fused(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
+                           const int32_t* __restrict__ order, float2* __restrict__ t1, SliceGeom g, int64_t k0) {
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  gather_colifft_body<R, Layout, S, MAP, T512>(grid, params, order, t1, g, k0, blockIdx.x, blockIdx.y, smem, w32);
 }
 
 template <int R, typename Layout, int S, int MAP>
@@ -210,7 +221,68 @@ int launch_fused_layout(const SliceGeom& g, const float2* grid, const cjx_image_
   }
 }
 
+// The front pass for every group of a wave in one launch (x-pair, bricked or
+// C-order grid, as the Layout), with the default sample count and lane map.
+template <typename Layout>
+__global__ void __launch_bounds__(kCols * 32, 4) k_front_wave(const __grid_constant__ Wave w) {
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int gi = wave_group(w, 0, blockIdx.x);
+  const WaveGroup& q = w.grp[gi];
+  const int local = blockIdx.x - q.cta0[0];
+  const int cx = (q.g.ncols + kCols - 1) / kCols;
+  const int bx = local % cx, by = local / cx;
+  switch (reg_fft_radix(q.g.n)) {
+#define CJX_FW(R)                                                                                              \
+  case R:                                                                                                      \
+    gather_colifft_body<R, Layout, 2, 1, false>(q.grid, q.params, q.order, q.t1, q.g, q.k0, bx, by, smem, w32); \
+    break;
+    CJX_FW(1) CJX_FW(2) CJX_FW(3) CJX_FW(4) CJX_FW(5) CJX_FW(6) CJX_FW(8) CJX_FW(10) CJX_FW(12)
+#undef CJX_FW
+    case 16:
+      if (w.t512)
+        gather_colifft_body<16, Layout, 2, 1, true>(q.grid, q.params, q.order, q.t1, q.g, q.k0, bx, by, smem, w32);
+      else
+        gather_colifft_body<16, Layout, 2, 1, false>(q.grid, q.params, q.order, q.t1, q.g, q.k0, bx, by, smem, w32);
+      break;
+    default:
+      break;
+  }
+}
+
 }  // namespace
+
+// Dynamic shared memory of the front pass for one group.
+size_t front_wave_smem(const SliceGeom& g) {
+  return sizeof(float2) * (size_t)(g.n + kCols * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
+}
+
+// CTAs of the front pass per image.
+int front_wave_ctas_per_image(const SliceGeom& g) { return (g.ncols + kCols - 1) / kCols; }
+
+int launch_front_wave(const Wave& w, int ctas, size_t smem, cudaStream_t stream) {
+  static PerDeviceOnce once;
+  const cudaError_t ea = once.run([] {
+    cudaError_t e = cudaFuncSetAttribute(k_front_wave<PairLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_front_wave<BrickLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_front_wave<LinearLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return e;
+  });
+  if (ea != cudaSuccess) return check_cuda(ea, "cudaFuncSetAttribute (wave front pass)");
+  const uint32_t flags = w.grp[0].g.flags;
+  prof_begin(stream);
+  if (flags & CJX_GRID_BRICKED_PAIRS)
+    k_front_wave<PairLayout><<<ctas, kCols * 32, smem, stream>>>(w);
+  else if (flags & CJX_GRID_BRICKED)
+    k_front_wave<BrickLayout><<<ctas, kCols * 32, smem, stream>>>(w);
+  else
+    k_front_wave<LinearLayout><<<ctas, kCols * 32, smem, stream>>>(w);
+  prof_end("k_front_wave", stream);
+  return check_cuda(cudaGetLastError(), "k_front_wave launch");
+}
 
 // True when launch_gather_colifft_fused handles this geometry: a trilinear
 // voxel grid (any of the three layouts, slice or Ewald sphere) with N of the

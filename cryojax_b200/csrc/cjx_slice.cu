@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <vector>
+#include <cmath>
 
 #include "cjx_common.cuh"
 #include "cjx_profile.cuh"
@@ -451,12 +453,12 @@ __device__ __forceinline__ void rows_pair_reg(float2 (&z)[RN], bool has_b, float
   }
 }
 
-template <int RN, bool T512 = false>
-__global__ void __launch_bounds__(kWarps * 32)
-    k_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
+// Body of the row pass for the CTA at (bx, by) of its launch: smem is the
+// dynamic shared memory, w32 a 32-entry shared table.
+template <int RN, bool T512>
+__device__ __forceinline__ void rows_reg_body(const float2* __restrict__ t1, float2* __restrict__ t2,
+                                              const SliceGeom& g, int rp, int bx, int by, float2* smem, float2* w32) {
   constexpr int n = 32 * RN;
-  extern __shared__ float2 smem[];
-  __shared__ float2 w32[32];
   const int px = g.px;
   const int stride = pad16(max(n, px)) + 1;
   float2* tabN = smem;
@@ -464,12 +466,12 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2* bufs = tabP + px;
   int* winx = reinterpret_cast<int*>(bufs + kWarps * stride);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  const int ra = 2 * (bx * kWarps + warp);
   const bool has_b = (ra + 1) < g.py;
   // the row pair is loaded first, so that its latency overlaps the table copy
   float2 z[RN];
   if (ra < g.py) {
-    const float2* rowA = t1 + ((size_t)blockIdx.y * g.py + ra) * g.ld1;
+    const float2* rowA = t1 + ((size_t)by * g.py + ra) * g.ld1;
     rows_pair_load<RN, T512>(rowA, rowA + g.ld1, has_b, z, lane);
   }
   build_reg_twiddles(tabN, n);
@@ -478,7 +480,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   for (int m = threadIdx.x; m < px; m += blockDim.x) winx[m] = win_src(m, n, px, g.pad_left_x);
   __syncthreads();
   if (ra >= g.py) return;
-  float2* outA = t2 + ((size_t)blockIdx.y * g.py + ra) * g.ld2;
+  float2* outA = t2 + ((size_t)by * g.py + ra) * g.ld2;
   float2* buf = bufs + warp * stride;
   const LaneTwiddles lt = make_lane_twiddles(w32, lane);
   switch (rp) {
@@ -491,23 +493,30 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
 }
 
-// Pass C: column forward FFT of T2 + epilogue.
-template <int R>
+template <int RN, bool T512 = false>
 __global__ void __launch_bounds__(kWarps * 32)
-    k_colfft_epilogue_reg(const float2* __restrict__ t2, const cjx_image_params* __restrict__ params,
-                          const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0,
-                          float norm) {
-  constexpr int py = 32 * R;
-  constexpr int stride = pad16(py) + 1;
+    k_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
-  __shared__ ImageConsts sc;
+  rows_reg_body<RN, T512>(t1, t2, g, rp, blockIdx.x, blockIdx.y, smem, w32);
+}
+
+// Pass C: column forward FFT of T2 + epilogue.  Body for the CTA at (bx, by):
+// smem is the dynamic shared memory, w32 and sc shared scratch.
+template <int R>
+__device__ __forceinline__ void colfft_epilogue_body(const float2* __restrict__ t2,
+                                                     const cjx_image_params* __restrict__ params,
+                                                     const int32_t* __restrict__ order, float2* __restrict__ out,
+                                                     const SliceGeom& g, int64_t k0, float norm, int bx, int by,
+                                                     float2* smem, float2* w32, ImageConsts& sc) {
+  constexpr int py = 32 * R;
+  constexpr int stride = pad16(py) + 1;
   float2* tab = smem;
   float2* row_phase = smem + py;  // exp(-2 pi i qy(i) ty)
   float2* bufs = smem + 2 * py;
-  const int j0 = blockIdx.x * kWarps;
+  const int j0 = bx * kWarps;
   const int ncols = min(kWarps, g.pxh - j0);
-  const float2* src = t2 + (size_t)blockIdx.y * py * g.ld2 + j0;
+  const float2* src = t2 + (size_t)by * py * g.ld2 + j0;
   // staging: thread t moves column t % kWarps, rows t / kWarps + 32 q; all R
   // loads are issued before the table copy and the shared-memory stores
   static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
@@ -523,7 +532,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 #pragma unroll
     for (int q = 0; q < R; ++q) bufs[sj * stride + pad16(sm0 + 32 * q)] = st[q];
   }
-  const int64_t k = k0 + blockIdx.y;
+  const int64_t k = k0 + by;
   const int64_t img = order ? (int64_t)order[k] : k;
   // the image's constants (double divisions and a sincos) once per CTA, not once per thread
   if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, g.py, g.px);
@@ -556,6 +565,65 @@ __global__ void __launch_bounds__(kWarps * 32)
   for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
     const int m = e / kWarps, jj = e % kWarps;
     if (jj < ncols) dst[(size_t)m * g.pxh + jj] = bufs[jj * stride + pad16(m)];
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_colfft_epilogue_reg(const float2* __restrict__ t2, const cjx_image_params* __restrict__ params,
+                          const int32_t* __restrict__ order, float2* __restrict__ out, SliceGeom g, int64_t k0,
+                          float norm) {
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  __shared__ ImageConsts sc;
+  colfft_epilogue_body<R>(t2, params, order, out, g, k0, norm, blockIdx.x, blockIdx.y, smem, w32, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Row and column passes for every group of a wave in one launch each.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWarps * 32) k_rows_wave(const __grid_constant__ Wave w) {
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int gi = wave_group(w, 1, blockIdx.x);
+  const WaveGroup& q = w.grp[gi];
+  const int local = blockIdx.x - q.cta0[1];
+  const int cx = (q.g.py + 2 * kWarps - 1) / (2 * kWarps);
+  const int bx = local % cx, by = local / cx;
+  const int rp = reg_fft_radix(q.g.px);
+  switch (reg_fft_radix(q.g.n)) {
+#define CJX_RW(R) \
+  case R: rows_reg_body<R, false>(q.t1, q.t2, q.g, rp, bx, by, smem, w32); break;
+    CJX_RW(1) CJX_RW(2) CJX_RW(3) CJX_RW(4) CJX_RW(5) CJX_RW(6) CJX_RW(8) CJX_RW(10) CJX_RW(12)
+#undef CJX_RW
+    case 16:
+      if (w.rows_t512)
+        rows_reg_body<16, true>(q.t1, q.t2, q.g, rp, bx, by, smem, w32);
+      else
+        rows_reg_body<16, false>(q.t1, q.t2, q.g, rp, bx, by, smem, w32);
+      break;
+    default:
+      break;
+  }
+}
+
+__global__ void __launch_bounds__(kWarps * 32) k_tail_wave(const __grid_constant__ Wave w) {
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  __shared__ ImageConsts sc;
+  const int gi = wave_group(w, 2, blockIdx.x);
+  const WaveGroup& q = w.grp[gi];
+  const int local = blockIdx.x - q.cta0[2];
+  const int cx = (q.g.pxh + kWarps - 1) / kWarps;
+  const int bx = local % cx, by = local / cx;
+  const float norm = (float)(1.0 / ((double)q.g.n * (double)q.g.n));
+  switch (reg_fft_radix(q.g.py)) {
+#define CJX_TW(R) \
+  case R: colfft_epilogue_body<R>(q.t2, q.params, q.order, q.out, q.g, q.k0, norm, bx, by, smem, w32, sc); break;
+    CJX_TW(1) CJX_TW(2) CJX_TW(3) CJX_TW(4) CJX_TW(5) CJX_TW(6) CJX_TW(8) CJX_TW(10) CJX_TW(12) CJX_TW(16)
+#undef CJX_TW
+    default:
+      break;
   }
 }
 
@@ -604,12 +672,13 @@ static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py
 // Process-wide tuning knobs (cjx_tuning_set / cjx_tuning_get).
 static std::atomic<int64_t> g_gather_ilp{2};
 static std::atomic<int64_t> g_chunk_bytes{1024ll << 20};  // 16384 images 320^2 from N = 512: 4 % faster than 512 MB
-static std::atomic<int64_t> g_gather_mode{1};
+static std::atomic<int64_t> g_gather_mode{2};  // 16384 images 320^2 from N = 512: 37.0 ms per step against 42.2 split
 static std::atomic<int64_t> g_fft_mode{2};
 static std::atomic<int64_t> g_gather_tile{1};
 static std::atomic<int64_t> g_scatter_vec{1};
 static std::atomic<int64_t> g_spline_ilp{4};
 static std::atomic<int64_t> g_overlap{0};
+static std::atomic<int64_t> g_multi_waves{0};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -683,6 +752,7 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_SCATTER_VEC) return g_scatter_vec.load();
   if (key == CJX_TUNE_SPLINE_ILP) return g_spline_ilp.load();
   if (key == CJX_TUNE_OVERLAP) return g_overlap.load();
+  if (key == CJX_TUNE_MULTI_WAVES) return g_multi_waves.load();
   return -1;
 }
 
@@ -720,6 +790,11 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_OVERLAP) {
     if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "overlap must be 0 or 1");
     g_overlap = value;
+    return CJX_OK;
+  }
+  if (key == CJX_TUNE_MULTI_WAVES) {
+    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "multi waves must be 0 or 1");
+    g_multi_waves = value;
     return CJX_OK;
   }
   if (key == CJX_TUNE_SCATTER_VEC) {
@@ -899,7 +974,8 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 
 Tuning current_tuning() {
   return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
-                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load(), (int)g_overlap.load()};
+                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load(), (int)g_overlap.load(),
+                (int)g_multi_waves.load()};
 }
 
 // The last pass for one chunk: column FFT + scale, CTF, envelope, translation (and filter), T2 -> out.
@@ -1038,6 +1114,110 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
     if (int e = launch_tail(g, t2, params, order, out, k0, cnt, stream, tn)) return e;
   }
   return check_cuda(cudaGetLastError(), "forward launch");
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-size batches in waves: one launch per pass for all groups
+// ---------------------------------------------------------------------------
+size_t front_wave_smem(const SliceGeom& g);
+int front_wave_ctas_per_image(const SliceGeom& g);
+int launch_front_wave(const Wave& w, int ctas, size_t smem, cudaStream_t stream);
+
+// A group can join the waves when it takes the fused register-FFT path end to
+// end: trilinear slice (not spline, not Ewald), resize path, N, Py, Px of the
+// register-FFT sizes, no fused filter, and the same grid layout as the others.
+bool wave_eligible(const SliceGeom& g, const Tuning& tn) {
+  return needs_resize(g) && !(g.flags & (CJX_GRID_SPLINE | CJX_EWALD_SPHERE)) && !g.filter &&
+         tn.fft_mode >= 1 && tn.gather_mode == 2 && reg_fft_radix(g.n) && reg_fft_radix(g.py) &&
+         reg_fft_radix(g.px);
+}
+
+size_t wave_bytes_per_image(const SliceGeom& g) {
+  return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2);
+}
+
+// Every group's images in waves that fit the workspace: wave v holds images
+// [v c_i, (v + 1) c_i) of group i (c_i = ceil(n_i / waves)), so all groups end
+// together; per wave the front, row and column passes are one launch each,
+// the CTAs of the groups one after another in each launch.
+int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                         const Tuning& tn) {
+  if (n_in < 1 || n_in > kMaxWaveGroups) return fail(CJX_ERR_UNSUPPORTED, "waves take 1 to 8 groups");
+  if (int e = ensure_smem_attrs()) return e;
+  static PerDeviceOnce once;
+  const cudaError_t ea = once.run([] {
+    cudaError_t e = cudaFuncSetAttribute(k_rows_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_tail_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return e;
+  });
+  if (ea != cudaSuccess) return check_cuda(ea, "cudaFuncSetAttribute (wave passes)");
+  double total = 0.0;
+  int64_t n_max = 0;
+  size_t s_front = 0, s_rows = 0, s_tail = 0;
+  for (int i = 0; i < n_in; ++i) {
+    const SliceGeom& g = in[i].g;
+    if (wave_bytes_per_image(g) > workspace_bytes) return fail(CJX_ERR_WORKSPACE, "workspace smaller than one image's need");
+    total += (double)in[i].n * (double)wave_bytes_per_image(g);
+    n_max = std::max<int64_t>(n_max, in[i].n);
+    s_front = std::max(s_front, front_wave_smem(g));
+    s_rows = std::max(s_rows, sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) +
+                                  sizeof(int) * (size_t)g.px);
+    s_tail = std::max(s_tail, sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1)));
+  }
+  if (n_max == 0) return CJX_OK;
+  int64_t waves = std::max<int64_t>(1, (int64_t)std::ceil(total / (double)workspace_bytes));
+  std::vector<int64_t> per_wave(n_in);
+  for (;; ++waves) {
+    size_t need = 0;
+    for (int i = 0; i < n_in; ++i) {
+      per_wave[i] = (in[i].n + waves - 1) / waves;
+      need += (size_t)per_wave[i] * wave_bytes_per_image(in[i].g);
+    }
+    if (need <= workspace_bytes) break;
+  }
+  Wave w{};
+  w.n = n_in;
+  w.t512 = tn.fft_mode >= 2;
+  w.rows_t512 = tn.fft_mode == 3;
+  char* base = static_cast<char*>(workspace);
+  for (int i = 0; i < n_in; ++i) {
+    WaveGroup& q = w.grp[i];
+    q.g = in[i].g;
+    q.grid = in[i].grid;
+    q.params = in[i].params;
+    q.order = in[i].order;
+    q.out = in[i].out;
+    q.t1 = reinterpret_cast<float2*>(base);
+    q.t2 = q.t1 + (size_t)per_wave[i] * q.g.py * q.g.ld1;
+    base += (size_t)per_wave[i] * wave_bytes_per_image(q.g);
+  }
+  for (int64_t v = 0; v < waves; ++v) {
+    int64_t ctas[3] = {0, 0, 0};
+    for (int i = 0; i < n_in; ++i) {
+      WaveGroup& q = w.grp[i];
+      q.k0 = std::min<int64_t>(v * per_wave[i], in[i].n);
+      q.cnt = (int)std::min<int64_t>(per_wave[i], in[i].n - q.k0);
+      const int64_t per[3] = {front_wave_ctas_per_image(q.g), (q.g.py + 2 * kWarps - 1) / (2 * kWarps),
+                              (q.g.pxh + kWarps - 1) / kWarps};
+      for (int p = 0; p < 3; ++p) {
+        q.cta0[p] = (int)ctas[p];
+        ctas[p] += per[p] * q.cnt;
+      }
+    }
+    if (ctas[0] == 0) continue;
+    if (ctas[0] > 2147483647LL || ctas[1] > 2147483647LL || ctas[2] > 2147483647LL)
+      return fail(CJX_ERR_UNSUPPORTED, "too many CTAs in one wave");
+    if (int e = launch_front_wave(w, (int)ctas[0], s_front, stream)) return e;
+    prof_begin(stream);
+    k_rows_wave<<<(unsigned)ctas[1], kWarps * 32, s_rows, stream>>>(w);
+    prof_end("k_rows_wave", stream);
+    prof_begin(stream);
+    k_tail_wave<<<(unsigned)ctas[2], kWarps * 32, s_tail, stream>>>(w);
+    prof_end("k_tail_wave", stream);
+    if (int e = check_cuda(cudaGetLastError(), "wave launch")) return e;
+  }
+  return CJX_OK;
 }
 
 // ---------------------------------------------------------------------------

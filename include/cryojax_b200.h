@@ -400,10 +400,10 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
  * workspace bytes per chunk when desc->images_per_chunk is 0 (default 1 GiB).
  * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
  * column-FFT kernel, 0 = one fused gather + column-FFT kernel with
- * shared-memory FFTs (C-order and bricked grids only), 2 = one fused
- * gather + register-FFT column kernel (trilinear grids in any layout, slice
- * or Ewald sphere, N = 32 R; other cases run as 1), which never writes the
- * sampled plane to memory.
+ * shared-memory FFTs (C-order and bricked grids only), 2 (default) = one
+ * fused gather + register-FFT column kernel (trilinear grids in any layout,
+ * slice or Ewald sphere, N = 32 R; other cases, e.g. spline volumes, run
+ * as 1), which never writes the sampled plane to memory.
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
  * (R in 1-6, 8, 10, 12, 16), 2 (default) = the same, with the 512-point
  * column transforms of the resize stage done as 16 x 32 through one
@@ -436,6 +436,14 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
  * stream.  The allocation-free entry point and calls made while profiling
  * is enabled always use one stream.                                        */
 #define CJX_TUNE_OVERLAP 8
+/* CJX_TUNE_MULTI_WAVES: 1 = cjx_slice_ctf_forward_multi runs its groups in
+ * waves, each wave holding a slice of every group's images and each pass
+ * of the resize path launched once for all groups (so small and large
+ * groups share every launch), when every group takes the fused
+ * register-FFT path (gather mode 2, trilinear slice, resize, sizes 32 R, one
+ * grid layout); the group records' gather choices are then not used.
+ * 0 = the groups one after another.                                         */
+#define CJX_TUNE_MULTI_WAVES 9
 CJX_API int cjx_tuning_set(int key, int64_t value);
 CJX_API int cjx_tuning_get(int key, int64_t* value);
 

@@ -114,3 +114,85 @@ def test_autotune_leaves_process_knobs_alone_while_another_thread_simulates(cuda
         t.join()
     assert not errors, errors[:3]
     assert [nat.tuning_get(k) for k in knobs] == before
+
+
+RESIZE_GROUPS = [(32, (32, 32), 5), (48, (64, 32), 7), (64, (64, 64), 4), (80, (96, 64), 6)]  # (box, shape, images)
+
+
+@pytest.mark.parametrize("one_image_chunks", [False, True])
+def test_waves_match_groups_one_after_another(cuda_device, one_image_chunks):
+    """CJX_TUNE_MULTI_WAVES: every pass launched once per wave for all groups gives the groups-in-turn
+    images bit for bit and the oracle's within tolerance, with one wave or (one-image chunks, so the
+    workspace holds one image of the largest group) many waves of ragged sizes."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+
+    models, refs, groups = [], [], []
+    for gi, (box, shape, nimg) in enumerate(RESIZE_GROUPS):
+        vol, grid, fs = make_volume(box, 40, seed=300 + gi)
+        specs = random_specs(nimg, seed=400 + gi, shape=shape)
+        pose, tt, cfg = specs_to_model_args(specs)
+        dvol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+        m = S.make_image_model(dvol, cfg, pose, tt)
+        models.append(m)
+        refs.append(np.stack([O.compute_fourier_image(grid, fs, s) for s in specs]))
+        integ = m.volume_integrator
+        dgrid, layout = integ.device_grid(dvol)
+        py, px = cfg.padded_shape
+        groups.append({"desc": nat.make_desc(dvol.shape[0], py, px, m._flags() | layout, 0.0,
+                                             1 if one_image_chunks else 0),
+                       "grid": dgrid, "params": torch.as_tensor(m.image_params(), device="cuda"),
+                       "order": None, "out": torch.zeros((nimg, py, px // 2 + 1), dtype=torch.complex64,
+                                                         device="cuda"),
+                       "n_images": nimg})
+    arr = nat.make_groups(groups)
+    ws = torch.empty(max(nat.multi_workspace_size(arr), 1), dtype=torch.uint8, device="cuda")
+    old = nat.tuning_get(nat.CJX_TUNE_MULTI_WAVES)
+    try:
+        nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, 0)
+        nat.slice_ctf_forward_multi(arr, ws)
+        seq = [g["out"].clone() for g in groups]
+        for g in groups:
+            g["out"].zero_()
+        nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, 1)
+        nat.profile_enable(True)
+        nat.slice_ctf_forward_multi(arr, ws)
+        torch.cuda.synchronize()
+        prof = nat.profile_read()
+        nat.profile_enable(False)
+    finally:
+        nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, old)
+    assert "k_front_wave" in prof and "k_rows_wave" in prof and "k_tail_wave" in prof, prof
+    waves = prof["k_front_wave"][0]
+    assert (waves > 1) == one_image_chunks, waves
+    assert prof["k_rows_wave"][0] == waves and prof["k_tail_wave"][0] == waves
+    for g, s, ref in zip(groups, seq, refs):
+        torch.testing.assert_close(g["out"], s, rtol=0, atol=0)
+        assert max(rel_l2_per_image(g["out"].cpu().numpy(), ref)) <= IMAGE_REL_L2_TOL
+
+
+def test_waves_fall_back_when_a_group_cannot_join(cuda_device):
+    """A group without the resize stage (Py = Px = N) cannot take the wave kernels: the call runs the groups
+    in turn instead, with the same images."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.batched import BatchedSimulator
+
+    models, refs = _models_and_refs()  # includes a no-resize group
+    old = nat.tuning_get(nat.CJX_TUNE_MULTI_WAVES)
+    try:
+        nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, 1)
+        sim = BatchedSimulator(models, tuning=None)
+        nat.profile_enable(True)
+        outs = sim.run()
+        torch.cuda.synchronize()
+        prof = nat.profile_read()
+        nat.profile_enable(False)
+    finally:
+        nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, old)
+    assert "k_front_wave" not in prof
+    for got, ref in zip(outs, refs):
+        assert max(rel_l2_per_image(got.cpu().numpy(), ref)) <= IMAGE_REL_L2_TOL
