@@ -494,7 +494,7 @@ __device__ __forceinline__ void rows_reg_body(const float2* __restrict__ t1, flo
 }
 
 template <int RN, bool T512 = false>
-__global__ void __launch_bounds__(kWarps * 32)
+__global__ void __launch_bounds__(kWarps * 32, 4)
     k_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 // ---------------------------------------------------------------------------
 // Row and column passes for every group of a wave in one launch each.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kWarps * 32) k_rows_wave(const __grid_constant__ Wave w) {
+__global__ void __launch_bounds__(kWarps * 32, 3) k_rows_wave(const __grid_constant__ Wave w) {
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
   const int gi = wave_group(w, 1, blockIdx.x);
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_rows_wave(const __grid_constant
   }
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_tail_wave(const __grid_constant__ Wave w) {
+__global__ void __launch_bounds__(kWarps * 32, 3) k_tail_wave(const __grid_constant__ Wave w) {
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
   __shared__ ImageConsts sc;
