@@ -53,7 +53,6 @@ def parse_args():
     ap.add_argument("--chunk", type=int, default=0, help="images per workspace chunk (0 = library default)")
     ap.add_argument("--ilp", type=int, default=0, help="gather ILP (1, 2, 4; 0 = library default)")
     ap.add_argument("--gather-mode", type=int, default=-1, help="CJX_TUNE_GATHER_MODE (-1 = library default)")
-    ap.add_argument("--overlap", type=int, default=-1, help="CJX_TUNE_OVERLAP (-1 = library default)")
     ap.add_argument("--scatter-mode", type=int, default=-1, help="CJX_TUNE_SCATTER_VEC (-1 = library default)")
     ap.add_argument("--layout", choices=["pairs", "bricked", "linear"], default="pairs",
                     help="device layout of the volume the gather reads")
@@ -1292,8 +1291,7 @@ def main():
     params_d = torch.as_tensor(params_h, device=dev)
     if args.ilp:
         nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, args.ilp)
-    for key, val in ((nat.CJX_TUNE_GATHER_MODE, args.gather_mode), (nat.CJX_TUNE_OVERLAP, args.overlap),
-                     (nat.CJX_TUNE_SCATTER_VEC, args.scatter_mode)):
+    for key, val in ((nat.CJX_TUNE_GATHER_MODE, args.gather_mode), (nat.CJX_TUNE_SCATTER_VEC, args.scatter_mode)):
         if val >= 0:
             nat.tuning_set(key, val)
     order_d = None

@@ -39,7 +39,6 @@ CJX_TUNE_FFT_MODE = 4
 CJX_TUNE_GATHER_TILE = 5
 CJX_TUNE_SCATTER_VEC = 6
 CJX_TUNE_SPLINE_ILP = 7
-CJX_TUNE_OVERLAP = 8
 CJX_TUNE_MULTI_WAVES = 9
 PARAMS_DOUBLES = 32  # sizeof(cjx_image_params) / 8
 

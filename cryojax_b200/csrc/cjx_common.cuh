@@ -815,7 +815,6 @@ struct Tuning {
   int fft_mode;     // 1 = register FFTs where possible
   int scatter_vec;  // 1 = adjoint grid scatter merges aligned x-corner pairs into 16-byte atomics
   int spline_ilp;   // samples per lane in the cubic-spline gather (1, 2, 4)
-  int overlap;      // 1 = resize-path chunks overlap: front pass of one chunk beside the later passes of the last
   int multi_waves;  // 1 = mixed-size batches run in waves, one launch per pass for all groups
 };
 Tuning current_tuning();

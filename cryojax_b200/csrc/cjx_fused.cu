@@ -264,11 +264,11 @@ int launch_front_wave(const Wave& w, int ctas, size_t smem, cudaStream_t stream)
   static PerDeviceOnce once;
   const cudaError_t ea = once.run([] {
     cudaError_t e = cudaFuncSetAttribute(k_front_wave<PairLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         227 * 1024);
+                                         220 * 1024);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_front_wave<BrickLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      e = cudaFuncSetAttribute(k_front_wave<BrickLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_front_wave<LinearLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      e = cudaFuncSetAttribute(k_front_wave<LinearLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     return e;
   });
   if (ea != cudaSuccess) return check_cuda(ea, "cudaFuncSetAttribute (wave front pass)");

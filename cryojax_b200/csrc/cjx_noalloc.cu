@@ -83,9 +83,6 @@ extern "C" int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const v
   chunk = std::min<int64_t>(std::min<int64_t>(chunk, n_images), 65535);
   void* scratch = nullptr;
   if (int e = noalloc_scratch(&scratch)) return e;
-  // one stream only: the overlapped schedule would create a second stream and events on first use
-  Tuning tn = current_tuning();
-  tn.overlap = 0;
   return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images, static_cast<float2*>(out),
-                        scratch, chunk, static_cast<cudaStream_t>(stream), tn);
+                        scratch, chunk, static_cast<cudaStream_t>(stream), current_tuning());
 }

@@ -671,13 +671,12 @@ static size_t smem_c(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.py
 
 // Process-wide tuning knobs (cjx_tuning_set / cjx_tuning_get).
 static std::atomic<int64_t> g_gather_ilp{2};
-static std::atomic<int64_t> g_chunk_bytes{1024ll << 20};  // 16384 images 320^2 from N = 512: 4 % faster than 512 MB
+static std::atomic<int64_t> g_chunk_bytes{2048ll << 20};  // 16384 images 320^2 from N = 512: 36.2 ms per step, 36.9 at 1 GiB
 static std::atomic<int64_t> g_gather_mode{2};  // 16384 images 320^2 from N = 512: 37.0 ms per step against 42.2 split
-static std::atomic<int64_t> g_fft_mode{2};
+static std::atomic<int64_t> g_fft_mode{3};  // 16384 images 320^2 from N = 512: row pass 7.5 ms against 7.9
 static std::atomic<int64_t> g_gather_tile{1};
 static std::atomic<int64_t> g_scatter_vec{1};
 static std::atomic<int64_t> g_spline_ilp{4};
-static std::atomic<int64_t> g_overlap{0};
 static std::atomic<int64_t> g_multi_waves{0};
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
@@ -751,7 +750,6 @@ int64_t tuning_get(int key) {
   if (key == CJX_TUNE_GATHER_TILE) return g_gather_tile.load();
   if (key == CJX_TUNE_SCATTER_VEC) return g_scatter_vec.load();
   if (key == CJX_TUNE_SPLINE_ILP) return g_spline_ilp.load();
-  if (key == CJX_TUNE_OVERLAP) return g_overlap.load();
   if (key == CJX_TUNE_MULTI_WAVES) return g_multi_waves.load();
   return -1;
 }
@@ -785,11 +783,6 @@ int tuning_set(int key, int64_t value) {
   if (key == CJX_TUNE_SPLINE_ILP) {
     if (value != 1 && value != 2 && value != 4) return fail(CJX_ERR_INVALID_ARGUMENT, "spline ILP must be 1, 2 or 4");
     g_spline_ilp = value;
-    return CJX_OK;
-  }
-  if (key == CJX_TUNE_OVERLAP) {
-    if (value != 0 && value != 1) return fail(CJX_ERR_INVALID_ARGUMENT, "overlap must be 0 or 1");
-    g_overlap = value;
     return CJX_OK;
   }
   if (key == CJX_TUNE_MULTI_WAVES) {
@@ -974,7 +967,7 @@ int launch_forward_to_t2(const SliceGeom& g, const float2* grid, const cjx_image
 
 Tuning current_tuning() {
   return Tuning{(int)g_gather_ilp.load(), (int)g_gather_tile.load(), (int)g_gather_mode.load(),
-                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load(), (int)g_overlap.load(),
+                (int)g_fft_mode.load(), (int)g_scatter_vec.load(), (int)g_spline_ilp.load(),
                 (int)g_multi_waves.load()};
 }
 
@@ -1002,73 +995,6 @@ static int launch_tail(const SliceGeom& g, const float2* t2, const cjx_image_par
   }
   prof_end("k_colfft_epilogue", stream);
   return check_cuda(cudaGetLastError(), "forward launch");
-}
-
-// Second stream and events of the overlapped chunk schedule, per host thread
-// and device, created on first use and kept for the thread's life (they are
-// not destroyed at thread exit, when the runtime may already be shut down).
-// Being per thread, two host threads never share them.
-struct OverlapCtx {
-  cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
-  cudaEvent_t ready[2] = {nullptr, nullptr};  // front pass of the chunk in buffer b done (caller's stream)
-  cudaEvent_t freed[2] = {nullptr, nullptr};  // row pass of the chunk in buffer b done: its T1 may be rewritten
-};
-
-static int overlap_ctx(OverlapCtx** out) {
-  static thread_local OverlapCtx ctx[kMaxDevices];
-  int dev = 0;
-  if (int e = check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return e;
-  if (dev < 0 || dev >= kMaxDevices) return fail(CJX_ERR_UNSUPPORTED, "device index beyond the 64 supported");
-  OverlapCtx& c = ctx[dev];
-  if (!c.side) {
-    OverlapCtx n;
-    cudaError_t e = cudaStreamCreateWithFlags(&n.side, cudaStreamNonBlocking);
-    cudaEvent_t* evs[] = {&n.fork, &n.join, &n.ready[0], &n.ready[1], &n.freed[0], &n.freed[1]};
-    for (cudaEvent_t* ev : evs)
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
-    if (e != cudaSuccess) return check_cuda(e, "creating the overlap stream and events");
-    c = n;
-  }
-  *out = &c;
-  return CJX_OK;
-}
-
-// Chunks of half the workspace's images, alternating between its two halves:
-// chunk i's front pass (gather + column inverse FFT, into T1[i % 2]) runs on
-// the caller's stream while the row and column passes of chunk i - 1 run on
-// the second stream.  The front of chunk i waits until the row pass of chunk
-// i - 2 has read T1[i % 2]; the rows of chunk i wait for its front.  The
-// second stream forks from the caller's stream at the start and joins it at
-// the end, so the call stays stream-ordered (and capturable as one graph).
-static int launch_forward_overlapped(const SliceGeom& g, const float2* grid, const cjx_image_params* params,
-                                     const int32_t* order, int64_t n_images, float2* out, float2* t1, float2* t2,
-                                     float2* hb, int64_t chunk, cudaStream_t stream, const Tuning& tn) {
-  OverlapCtx* c = nullptr;
-  if (int e = overlap_ctx(&c)) return e;
-  const int64_t half = chunk / 2;
-  float2* t1b[2] = {t1, t1 + (size_t)half * g.py * g.ld1};
-  float2* t2b[2] = {t2, t2 + (size_t)half * g.py * g.ld2};
-  float2* hbb[2] = {hb, hb + (size_t)half * g.ncols * g.ldh};
-  if (int e = check_cuda(cudaEventRecord(c->fork, stream), "cudaEventRecord")) return e;
-  if (int e = check_cuda(cudaStreamWaitEvent(c->side, c->fork, 0), "cudaStreamWaitEvent")) return e;
-  int err = CJX_OK;
-  int64_t i = 0;
-  for (int64_t k0 = 0; k0 < n_images && !err; k0 += half, ++i) {
-    const int b = (int)(i & 1);
-    const int cnt = (int)std::min<int64_t>(half, n_images - k0);
-    if (i >= 2) err = check_cuda(cudaStreamWaitEvent(stream, c->freed[b], 0), "cudaStreamWaitEvent");
-    if (!err) err = launch_front(g, grid, params, order, k0, cnt, t1b[b], hbb[b], stream, tn);
-    if (!err) err = check_cuda(cudaEventRecord(c->ready[b], stream), "cudaEventRecord");
-    if (!err) err = check_cuda(cudaStreamWaitEvent(c->side, c->ready[b], 0), "cudaStreamWaitEvent");
-    if (!err) err = launch_rows(g, t1b[b], t2b[b], cnt, c->side, tn);
-    if (!err) err = check_cuda(cudaEventRecord(c->freed[b], c->side), "cudaEventRecord");
-    if (!err) err = launch_tail(g, t2b[b], params, order, out, k0, cnt, c->side, tn);
-  }
-  // join the second stream back into the caller's stream, also after an error
-  const int ej = check_cuda(cudaEventRecord(c->join, c->side), "cudaEventRecord");
-  const int ew = ej ? ej : check_cuda(cudaStreamWaitEvent(stream, c->join, 0), "cudaStreamWaitEvent");
-  return err ? err : ew;
 }
 
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
@@ -1106,8 +1032,6 @@ int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_param
   float2* t1 = static_cast<float2*>(workspace);
   float2* t2 = t1 + (size_t)chunk * g.py * g.ld1;
   float2* hb = t2 + (size_t)chunk * g.py * g.ld2;
-  if (tn.overlap && !prof_active() && chunk >= 2 && n_images > chunk / 2)
-    return launch_forward_overlapped(g, grid, params, order, n_images, out, t1, t2, hb, chunk, stream, tn);
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
@@ -1146,9 +1070,10 @@ int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t 
   if (int e = ensure_smem_attrs()) return e;
   static PerDeviceOnce once;
   const cudaError_t ea = once.run([] {
-    cudaError_t e = cudaFuncSetAttribute(k_rows_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    // the kernels also hold static shared tables, so the dynamic limit stays below 227 KB
+    cudaError_t e = cudaFuncSetAttribute(k_rows_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_tail_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      e = cudaFuncSetAttribute(k_tail_wave, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     return e;
   });
   if (ea != cudaSuccess) return check_cuda(ea, "cudaFuncSetAttribute (wave passes)");

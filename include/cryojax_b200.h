@@ -397,7 +397,7 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
 /* Process-wide tuning knobs (no counterpart in the reference; set by the
  * autotuner).  CJX_TUNE_GATHER_ILP: samples whose corner loads one lane
  * issues together in the gather (1, 2 or 4).  CJX_TUNE_CHUNK_BYTES: target
- * workspace bytes per chunk when desc->images_per_chunk is 0 (default 1 GiB).
+ * workspace bytes per chunk when desc->images_per_chunk is 0 (default 2 GiB).
  * CJX_TUNE_GATHER_MODE: 1 = separate gather kernel (no shared memory) and
  * column-FFT kernel, 0 = one fused gather + column-FFT kernel with
  * shared-memory FFTs (C-order and bricked grids only), 2 (default) = one
@@ -405,10 +405,10 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
  * slice or Ewald sphere, N = 32 R; other cases, e.g. spline volumes, run
  * as 1), which never writes the sampled plane to memory.
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
- * (R in 1-6, 8, 10, 12, 16), 2 (default) = the same, with the 512-point
+ * (R in 1-6, 8, 10, 12, 16), 2 = the same, with the 512-point
  * column transforms of the resize stage done as 16 x 32 through one
- * shared-memory transpose instead of five shuffle stages, 3 = as 2 and the
- * row pass's 512-point inverse transforms the same way, 0 = shared-memory
+ * shared-memory transpose instead of five shuffle stages, 3 (default) = as
+ * 2 and the row pass's 512-point inverse transforms the same way, 0 = shared-memory
  * Stockham FFTs everywhere.
  * CJX_TUNE_GATHER_TILE: lanes of a gather warp cover 2 x 16 (0), 4 x 8 (1)
  * or 8 x 4 (2) samples (columns x rows) of the slice plane; 3 = one column
@@ -427,15 +427,6 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
 #define CJX_TUNE_GATHER_TILE 5
 #define CJX_TUNE_SCATTER_VEC 6
 #define CJX_TUNE_SPLINE_ILP 7
-/* CJX_TUNE_OVERLAP: 1 = the resize path runs its chunks as two interleaved
- * halves, the gather pass of one on the caller's stream while the row and
- * column passes of the previous one run on a second stream of the calling
- * host thread (created on its first use on each device, before any stream
- * capture that should include it; joined back into the caller's stream
- * before the call returns, so the call stays stream-ordered); 0 = one
- * stream.  The allocation-free entry point and calls made while profiling
- * is enabled always use one stream.                                        */
-#define CJX_TUNE_OVERLAP 8
 /* CJX_TUNE_MULTI_WAVES: 1 = cjx_slice_ctf_forward_multi runs its groups in
  * waves, each wave holding a slice of every group's images and each pass
  * of the resize path launched once for all groups (so small and large

@@ -79,7 +79,7 @@ def test_tuning_knobs():
         nat.tuning_set(nat.CJX_TUNE_GATHER_ILP, 3)
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(99, 1)
-    assert nat.tuning_get(nat.CJX_TUNE_FFT_MODE) == 2  # transpose FFT for 512-point column passes
+    assert nat.tuning_get(nat.CJX_TUNE_FFT_MODE) == 3  # transpose FFT for the 512-point column and row transforms
     assert nat.tuning_get(nat.CJX_TUNE_SCATTER_VEC) == 1
     assert nat.tuning_get(nat.CJX_TUNE_SPLINE_ILP) == 4
     with pytest.raises(nat.CryojaxB200Error):

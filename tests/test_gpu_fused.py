@@ -25,7 +25,7 @@ def tuning(**kw):
     from cryojax_b200 import _native as nat
 
     keys = {"mode": nat.CJX_TUNE_GATHER_MODE, "ilp": nat.CJX_TUNE_GATHER_ILP, "tile": nat.CJX_TUNE_GATHER_TILE,
-            "fft": nat.CJX_TUNE_FFT_MODE, "overlap": nat.CJX_TUNE_OVERLAP}
+            "fft": nat.CJX_TUNE_FFT_MODE}
     old = {k: nat.tuning_get(keys[k]) for k in kw}
     try:
         for k, v in kw.items():
@@ -137,44 +137,3 @@ def test_fused_chunked_call(cuda_device):
     np.testing.assert_array_equal(one, chunked)
     ref = np.stack([O.compute_fourier_image(grid, fs, s) for s in specs])
     assert max(rel_l2_per_image(chunked, ref)) <= IMAGE_REL_L2_TOL
-
-
-@pytest.mark.parametrize("mode", [1, 2])
-@pytest.mark.parametrize("ewald", [False, True])
-def test_overlapped_chunks_match_one_stream(cuda_device, mode, ewald):
-    """The two-stream chunk schedule (CJX_TUNE_OVERLAP) gives the one-stream images bit for bit, for odd
-    and even chunk counts and a ragged last chunk."""
-    vol, grid, fs = make_volume(32, 60, seed=31)
-    specs = random_specs(23, seed=32, shape=(40, 40))
-    for chunk in (4, 6, 22):
-        with tuning(mode=mode, overlap=0):
-            one = _run(grid, specs, chunk=chunk, ewald=ewald)
-        with tuning(mode=mode, overlap=1):
-            two = _run(grid, specs, chunk=chunk, ewald=ewald)
-        np.testing.assert_array_equal(one, two)
-    ref = np.stack([O.compute_fourier_image(grid, fs, s, ewald=ewald) for s in specs])
-    assert max(rel_l2_per_image(two, ref)) <= IMAGE_REL_L2_TOL
-
-
-def test_overlapped_chunks_in_a_cuda_graph(cuda_device):
-    """A BatchedSimulator graph captured with the overlapped schedule (its second stream forks from and
-    joins the capturing stream) replays to the oracle's images."""
-    import torch
-
-    from cryojax_b200 import simulator as S
-    from cryojax_b200.batched import BatchedSimulator
-
-    vol, grid, fs = make_volume(32, 60, seed=41)
-    specs = random_specs(9, seed=42, shape=(32, 32))
-    pose, tt, cfg = specs_to_model_args(specs)
-    dvol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
-    model = S.make_image_model(dvol, cfg, pose, tt)
-    ref = np.stack([O.compute_fourier_image(grid, fs, s) for s in specs])
-    with tuning(mode=2, overlap=1):
-        sim = BatchedSimulator([model], tuning=None)
-        sim._groups[0].desc.images_per_chunk = 2  # five chunks of 2 through both workspace halves
-        sim.capture()
-        sim.outputs[0].zero_()
-        sim.replay()
-        torch.cuda.synchronize()
-    assert max(rel_l2_per_image(sim.outputs[0].cpu().numpy(), ref)) <= IMAGE_REL_L2_TOL
