@@ -176,7 +176,8 @@ int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, voi
       in[n_in++] = WaveInput{g, static_cast<const float2*>(gr.grid), gr.params, gr.order,
                              static_cast<float2*>(gr.out), gr.n_images};
     }
-    if (eligible && n_in > 0)
+    int64_t per_wave[kMaxWaveGroups];
+    if (eligible && n_in > 0 && plan_waves(in, n_in, workspace_bytes, per_wave) > 0)
       return launch_forward_waves(in, n_in, workspace, workspace_bytes, static_cast<cudaStream_t>(stream), base);
   }
   for (int i = 0; i < n_groups; ++i) {

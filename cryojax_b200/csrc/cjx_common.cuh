@@ -855,6 +855,7 @@ struct WaveInput {
   int64_t n;
 };
 bool wave_eligible(const SliceGeom& g, const Tuning& tn);
+int64_t plan_waves(const WaveInput* in, int n_in, size_t workspace_bytes, int64_t* per_wave);
 int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t workspace_bytes, cudaStream_t stream,
                          const Tuning& tn);
 

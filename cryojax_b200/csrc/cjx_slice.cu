@@ -1060,6 +1060,30 @@ size_t wave_bytes_per_image(const SliceGeom& g) {
   return sizeof(float2) * ((size_t)g.py * g.ld1 + (size_t)g.py * g.ld2);
 }
 
+// Number of waves whose slices fit the workspace (images per wave of group i
+// in per_wave[i]), or 0 when even one image of every group does not fit (the
+// groups then run one after another).  More waves never help beyond the
+// largest group's image count, where every slice is one image.
+int64_t plan_waves(const WaveInput* in, int n_in, size_t workspace_bytes, int64_t* per_wave) {
+  double total = 0.0;
+  int64_t n_max = 0;
+  for (int i = 0; i < n_in; ++i) {
+    total += (double)in[i].n * (double)wave_bytes_per_image(in[i].g);
+    n_max = std::max<int64_t>(n_max, in[i].n);
+  }
+  if (n_max == 0) return 0;
+  for (int64_t waves = std::max<int64_t>(1, (int64_t)std::ceil(total / (double)workspace_bytes)); waves <= n_max;
+       ++waves) {
+    size_t need = 0;
+    for (int i = 0; i < n_in; ++i) {
+      per_wave[i] = (in[i].n + waves - 1) / waves;
+      need += (size_t)per_wave[i] * wave_bytes_per_image(in[i].g);
+    }
+    if (need <= workspace_bytes) return waves;
+  }
+  return 0;
+}
+
 // Every group's images in waves that fit the workspace: wave v holds images
 // [v c_i, (v + 1) c_i) of group i (c_i = ceil(n_i / waves)), so all groups end
 // together; per wave the front, row and column passes are one launch each,
@@ -1077,13 +1101,10 @@ int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t 
     return e;
   });
   if (ea != cudaSuccess) return check_cuda(ea, "cudaFuncSetAttribute (wave passes)");
-  double total = 0.0;
   int64_t n_max = 0;
   size_t s_front = 0, s_rows = 0, s_tail = 0;
   for (int i = 0; i < n_in; ++i) {
     const SliceGeom& g = in[i].g;
-    if (wave_bytes_per_image(g) > workspace_bytes) return fail(CJX_ERR_WORKSPACE, "workspace smaller than one image's need");
-    total += (double)in[i].n * (double)wave_bytes_per_image(g);
     n_max = std::max<int64_t>(n_max, in[i].n);
     s_front = std::max(s_front, front_wave_smem(g));
     s_rows = std::max(s_rows, sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) +
@@ -1091,16 +1112,9 @@ int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t 
     s_tail = std::max(s_tail, sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1)));
   }
   if (n_max == 0) return CJX_OK;
-  int64_t waves = std::max<int64_t>(1, (int64_t)std::ceil(total / (double)workspace_bytes));
   std::vector<int64_t> per_wave(n_in);
-  for (;; ++waves) {
-    size_t need = 0;
-    for (int i = 0; i < n_in; ++i) {
-      per_wave[i] = (in[i].n + waves - 1) / waves;
-      need += (size_t)per_wave[i] * wave_bytes_per_image(in[i].g);
-    }
-    if (need <= workspace_bytes) break;
-  }
+  const int64_t waves = plan_waves(in, n_in, workspace_bytes, per_wave.data());
+  if (waves <= 0) return fail(CJX_ERR_WORKSPACE, "workspace smaller than one image of every group");
   Wave w{};
   w.n = n_in;
   w.t512 = tn.fft_mode >= 2;

@@ -119,11 +119,14 @@ def test_autotune_leaves_process_knobs_alone_while_another_thread_simulates(cuda
 RESIZE_GROUPS = [(32, (32, 32), 5), (48, (64, 32), 7), (64, (64, 64), 4), (80, (96, 64), 6)]  # (box, shape, images)
 
 
-@pytest.mark.parametrize("one_image_chunks", [False, True])
-def test_waves_match_groups_one_after_another(cuda_device, one_image_chunks):
+@pytest.mark.parametrize("workspace", ["one_wave", "several_waves", "too_small"])
+def test_waves_match_groups_one_after_another(cuda_device, workspace):
     """CJX_TUNE_MULTI_WAVES: every pass launched once per wave for all groups gives the groups-in-turn
-    images bit for bit and the oracle's within tolerance, with one wave or (one-image chunks, so the
-    workspace holds one image of the largest group) many waves of ragged sizes."""
+    images bit for bit and the oracle's within tolerance: with the default chunks (one wave), with one-image
+    chunks and twice their workspace (several waves of ragged sizes), and with one-image chunks and exactly
+    their workspace, where one image of every group does not fit at once and the call runs the groups in
+    turn instead."""
+    one_image_chunks = workspace != "one_wave"
     import torch
 
     from cryojax_b200 import _native as nat
@@ -148,7 +151,8 @@ def test_waves_match_groups_one_after_another(cuda_device, one_image_chunks):
                                                          device="cuda"),
                        "n_images": nimg})
     arr = nat.make_groups(groups)
-    ws = torch.empty(max(nat.multi_workspace_size(arr), 1), dtype=torch.uint8, device="cuda")
+    factor = 2 if workspace == "several_waves" else 1
+    ws = torch.empty(max(factor * nat.multi_workspace_size(arr), 1), dtype=torch.uint8, device="cuda")
     old = nat.tuning_get(nat.CJX_TUNE_MULTI_WAVES)
     try:
         nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, 0)
@@ -164,10 +168,13 @@ def test_waves_match_groups_one_after_another(cuda_device, one_image_chunks):
         nat.profile_enable(False)
     finally:
         nat.tuning_set(nat.CJX_TUNE_MULTI_WAVES, old)
-    assert "k_front_wave" in prof and "k_rows_wave" in prof and "k_tail_wave" in prof, prof
-    waves = prof["k_front_wave"][0]
-    assert (waves > 1) == one_image_chunks, waves
-    assert prof["k_rows_wave"][0] == waves and prof["k_tail_wave"][0] == waves
+    if workspace == "too_small":
+        assert "k_front_wave" not in prof, prof
+    else:
+        assert "k_front_wave" in prof and "k_rows_wave" in prof and "k_tail_wave" in prof, prof
+        waves = prof["k_front_wave"][0]
+        assert (waves > 1) == one_image_chunks, waves
+        assert prof["k_rows_wave"][0] == waves and prof["k_tail_wave"][0] == waves
     for g, s, ref in zip(groups, seq, refs):
         torch.testing.assert_close(g["out"], s, rtol=0, atol=0)
         assert max(rel_l2_per_image(g["out"].cpu().numpy(), ref)) <= IMAGE_REL_L2_TOL
