@@ -94,15 +94,18 @@ def test_autotune_leaves_process_knobs_alone_while_another_thread_simulates(cuda
     errors, stop = [], threading.Event()
 
     def simulate_repeatedly():
-        stream = torch.cuda.Stream()
-        with torch.cuda.stream(stream):
-            while not stop.is_set():
-                got = models[1].compute_fourier_image()
-                stream.synchronize()
-                if not torch.equal(got, ref):
-                    errors.append("images changed while the autotuner ran")
-                if [nat.tuning_get(k) for k in knobs] != before:
-                    errors.append("process knobs changed while the autotuner ran")
+        try:
+            stream = torch.cuda.Stream()
+            with torch.cuda.stream(stream):
+                while not stop.is_set():
+                    got = models[1].compute_fourier_image()
+                    stream.synchronize()
+                    if not torch.equal(got, ref):
+                        errors.append("images changed while the autotuner ran")
+                    if [nat.tuning_get(k) for k in knobs] != before:
+                        errors.append("process knobs changed while the autotuner ran")
+        except Exception as e:  # a failure on this thread must fail the test
+            errors.append(repr(e))
 
     t = threading.Thread(target=simulate_repeatedly)
     t.start()
