@@ -704,6 +704,7 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
     from cryojax_b200 import synthetic
     from cryojax_b200.healpix import OrientationGrid
     from cryojax_b200.pose_net import PoseProposalNet
+    from cryojax_b200.gradients import observed_to_fourier
     from cryojax_b200.refine import refine_poses, rotation_angle_deg, with_rotations_and_defocus
     from cryojax_b200.search import LearnedPoseSearch, PoseSearch, TemplateSharingSearch
 
@@ -744,14 +745,16 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
     hist = PT.train_pose_net(net, data, epochs=12, lr=1e-3, snr=0.05, snr_start=2.0, snr_ramp=0.6, seed=seed + 53)
     del data
     torch.cuda.empty_cache()
-    learned = LearnedPoseSearch(net, grid, top_k=16, search=search)
+    tss = TemplateSharingSearch(grid.rotation_matrices())
+    # candidates simulated at full size; the fallback images take the template-sharing exhaustive search
+    learned = LearnedPoseSearch(net, grid, top_k=16, search=search, fallback_search=tss)
     cal_model, cal_obs, _, _ = batch(512, seed + 54)
-    cal_ex = TemplateSharingSearch(grid.rotation_matrices()).run(cal_model, cal_obs, rerank_top=8)
+    cal_ex = tss.run(cal_model, cal_obs, rerank_top=8)
     thr = learned.calibrate_threshold(cal_model, cal_obs, cal_ex.best_orientation, target_agreement=0.995)
     del cal_obs
     torch.cuda.empty_cache()
     model, obs, q, df = batch(n_learned, seed + 55)
-    obs_f = torch.fft.rfftn(torch.fft.ifftshift(obs.double(), dim=(-2, -1)), dim=(-2, -1)).to(torch.complex64)
+    obs_f = observed_to_fourier(obs)
 
     # starting defocus: the truth + U(-300, 300) A (a CTF-estimation error for the refinement to remove)
     df_start = df + np.random.default_rng(seed + 56).uniform(-300.0, 300.0, n_learned)
@@ -762,8 +765,6 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
                                           df_start[:len(o)])
         ref = refine_poses(init, of, steps=20, observed_is_fourier=True)
         return res, ref
-
-    tss = TemplateSharingSearch(grid.rotation_matrices())
 
     def exhaustive_arm(m, o, of):
         # exhaustive over all 36,864 orientations: the template-sharing search with its 8 best per image
@@ -784,11 +785,11 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
         return S.make_image_model(V, cfg, S.QuaternionPose(np.zeros(k), np.zeros(k), wxyz=q[:k]),
                                   S.ContrastTransferTheory(ctf, amplitude_contrast_ratio=0.1))
 
+    tss.build_templates(sub_model(64))  # the fallback's template bank, built before either arm is timed
     learned_arm(sub_model(64), obs[:64].contiguous(), obs_f[:64].contiguous())  # warm-up
     (lres, lref), t_l = timed(lambda: learned_arm(model, obs, obs_f))
     sub = sub_model(n_exhaustive)
-    tss.build_templates(sub)  # the template bank (CTF-free slices of every orientation), timed separately
-    tss._key = None
+    tss._key = None  # the template bank (CTF-free slices of every orientation), timed separately
     _, t_tmpl = timed(lambda: tss.build_templates(sub))
     (eres, eref), t_e = timed(lambda: exhaustive_arm(sub, obs[:n_exhaustive], obs_f[:n_exhaustive].contiguous()))
     n_pl = min(n_exhaustive, 32)  # the plain search (one simulation per orientation) on a small sample

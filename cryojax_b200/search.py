@@ -145,7 +145,8 @@ class LearnedPoseSearch:
     """
 
     def __init__(self, net, grid, *, top_k=16, threshold=float("-inf"), search: PoseSearch | None = None,
-                 templates: "TemplateSharingSearch | None" = None, rerank_top=8):
+                 templates: "TemplateSharingSearch | None" = None, rerank_top=8,
+                 fallback_search: "TemplateSharingSearch | None" = None):
         if net.n_classes != grid.n_dir:
             raise ValueError("the network's classes must be the grid's directions")
         self.net = net
@@ -158,6 +159,9 @@ class LearnedPoseSearch:
         # the fallback is then its exhaustive search with the same re-ranking
         self.templates = templates
         self.rerank_top = rerank_top
+        # the exhaustive search of the fallback images: the template-sharing search (with the same FP32
+        # re-ranking) when given or when the candidates are scored from templates, else PoseSearch
+        self.fallback_search = fallback_search if fallback_search is not None else templates
 
     def run(self, image_model, observed, *, batch=None, fallback=True) -> LearnedSearchResult:
         """observed: real-space float32 CUDA images (n, P, P)."""
@@ -184,9 +188,9 @@ class LearnedPoseSearch:
         if fallback and low.any():
             idx = torch.as_tensor(np.flatnonzero(low), device=obs.device)
             sub_obs, sub_pd = obs_f.index_select(0, idx).contiguous(), pd.index_select(0, idx).contiguous()
-            if self.templates is not None:
-                ex = self.templates.run(image_model, sub_obs, observed_is_fourier=True, image_params_device=sub_pd,
-                                        rerank_top=self.rerank_top)
+            if self.fallback_search is not None:
+                ex = self.fallback_search.run(image_model, sub_obs, observed_is_fourier=True,
+                                              image_params_device=sub_pd, rerank_top=self.rerank_top)
             else:
                 ex = self.search.run(image_model, sub_obs, observed_is_fourier=True, image_params_device=sub_pd)
             best[low] = ex.best_orientation
