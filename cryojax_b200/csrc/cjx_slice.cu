@@ -766,7 +766,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_GATHER_MODE) {
-    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0, 1 or 2");
+    if (value < 0 || value > 3) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0, 1, 2 or 3");
     g_gather_mode = value;
     return CJX_OK;
   }
@@ -841,7 +841,7 @@ static int launch_front(const SliceGeom& g, const float2* grid, const cjx_image_
   const bool fast = tn.fft_mode >= 1;
   // gather mode 2: the register-FFT fused pass (trilinear grids, N = 32 R); otherwise the split pair of
   // kernels, or mode 0's shared-memory fused kernel, which has no pair, spline or Ewald path
-  const bool fused_reg = tn.gather_mode == 2 && fast && fused_gather_supported(g);
+  const bool fused_reg = (tn.gather_mode == 2 || tn.gather_mode == 3) && fast && fused_gather_supported(g);
   const bool split = !fused_reg && (tn.gather_mode != 0 ||
                                     (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE)));
   const bool t512 = tn.fft_mode >= 2 && rn == 16;  // 512-point column transforms through the transpose FFT
