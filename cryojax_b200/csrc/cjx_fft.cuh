@@ -242,6 +242,20 @@ __host__ __device__ constexpr int pad16(int e) { return e + (e >> 4); }
 
 __device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
 
+// Shared-memory staging of a register FFT's outputs (lane l holds k = k1 + R l)
+// for reading back in natural order.  pad16 is conflict-free for the
+// power-of-two R; for R = 10 (the 320-point transforms) its stride-10 stores
+// meet 5-way bank conflicts within a half-warp, and k + k/16 + 14 (k/32) keeps
+// both the stores and the natural-order reads conflict-free (20 + 32
+// wavefronts per 320 outputs against 100 + 32, counted on the CPU).
+__host__ __device__ constexpr int stage_r(int R, int k) { return R == 10 ? k + (k >> 4) + (k >> 5) * 14 : pad16(k); }
+__host__ __device__ constexpr int stage_r_size(int R) { return stage_r(R, 32 * R - 1) + 1; }
+// The same for warp_fft512_t's outputs (k = fft512_t_out(q, lane)): its two
+// lane halves land 256 apart and, with pad16 alone, on the same banks; the
+// second half moves by 8 entries.  Size 551.
+__host__ __device__ constexpr int stage512(int k) { return pad16(k) + 8 * ((k >> 8) & 1); }
+constexpr int kStage512Size = 551;
+
 // Compile-time cos / sin of 2 pi m / R via Taylor series after reduction to
 // |x| <= pi/4 (enough terms for double precision); used only for the small
 // constant twiddles of the in-register DFTs.

@@ -24,6 +24,16 @@ namespace {
 
 constexpr int kCols = 8;  // slice columns per CTA (one per warp in the FFT phase)
 
+// Shared-memory layout of a column: samples at pad16(row); the transform's
+// output staged at stage_idx(k), which also moves the second half of the
+// column by 8 entries.  With a column stride of pad16(n) + 12 (12 mod 16 at
+// n = 512), the 8-byte stores of the 4 x 8 lane map, the staged outputs of the
+// transpose FFT and the window reads meet no bank conflicts within a half-warp
+// except the window's 2-way ones (about 830 shared-memory wavefronts per CTA
+// of 8 columns, counted on the CPU, against 1860 with stride pad16(n) + 1).
+__host__ __device__ constexpr int fused_stride(int n) { return pad16(n) + 12; }
+__device__ __forceinline__ int stage_idx(int k) { return stage512(k); }
+
 // Lane -> (column, row) offsets inside the CTA's 8-column x 32-row pass of the
 // plane (MAP): 0: each warp 2 columns x 16 rows, 1: 4 x 8, 2: 8 x 4, 3: one
 // column x 32 rows.
@@ -53,7 +63,7 @@ __device__ __forceinline__ void gather_colifft_body(const float2* __restrict__ g
                                                     const SliceGeom& g, int64_t k0, int bx, int by, float2* smem,
                                                     float2* w32) {
   constexpr int n = 32 * R;
-  constexpr int stride = pad16(n) + 1;
+  constexpr int stride = fused_stride(n);
   static_assert(!T512 || R == 16, "the transpose FFT is 512-point");
   float2* tab = smem;
   float2* tile = smem + n;  // [kCols][stride], rows in the pad16 layout
@@ -138,12 +148,12 @@ __device__ __forceinline__ void gather_colifft_body(const float2* __restrict__ g
     if constexpr (T512) {
       warp_fft512_t<+1>(x, tab, w32, buf, lane);
 #pragma unroll
-      for (int q = 0; q < R; ++q) buf[pad16(fft512_t_out(q, lane))] = x[q];
+      for (int q = 0; q < R; ++q) buf[stage_idx(fft512_t_out(q, lane))] = x[q];
     } else {
       const LaneTwiddles lt = make_lane_twiddles(w32, lane);
       warp_fft_reg<R, +1>(x, tab, lt, lane);
 #pragma unroll
-      for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+      for (int k1 = 0; k1 < R; ++k1) buf[stage_idx(k1 + R * lane)] = x[k1];
     }
   }
   __syncthreads();
@@ -153,135 +163,9 @@ __device__ __forceinline__ void gather_colifft_body(const float2* __restrict__ g
     const int m = e / kCols, jj = e % kCols;
     if (jj < ncols) {
       const int src = winy[m];
-      dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? tile[jj * stride + pad16(src)] : make_float2(0.f, 0.f);
+      dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? tile[jj * stride + stage_idx(src)] : make_float2(0.f, 0.f);
     }
   }
-}
-
-// Direct form (gather mode 3): each warp samples its own column straight
-// into the FFT's register layout (lane l holds rows 32 n1 + l, or + brev5(l)
-// for the shuffle FFT), two rows per step, so the samples never pass
-// through shared memory and the warp starts its transform as soon as its
-// column is in; only the Hermitian columns kx = 0 and N/2 go through the
-// warp's shared buffer to meet their mirror rows.  3 CTAs per SM (85
-// registers: the 16 complex values of the column stay live during the
-// gather).
-template <int R, typename Layout, bool T512>
-__global__ void __launch_bounds__(kCols * 32, 3)
-    k_gather_colifft_direct(const float2* __restrict__ grid, const cjx_image_params* __restrict__ params,
-                            const int32_t* __restrict__ order, float2* __restrict__ t1, SliceGeom g, int64_t k0) {
-  constexpr int n = 32 * R;
-  constexpr int stride = pad16(n) + 1;
-  static_assert(!T512 || R == 16, "the transpose FFT is 512-point");
-  extern __shared__ float2 smem[];
-  __shared__ float2 w32[32];
-  float2* tab = smem;
-  float2* tile = smem + n;  // [kCols][stride]: the warps' transform buffers, then the output staging
-  int* winy = reinterpret_cast<int*>(tile + kCols * stride);
-  const Layout L(n);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int j0 = blockIdx.x * kCols;
-  const int ncols = min(kCols, g.ncols - j0);
-  const int64_t k = k0 + blockIdx.y;
-  const int64_t img = order ? (int64_t)order[k] : k;
-  const bool ewald = (g.flags & CJX_EWALD_SPHERE) != 0;
-  build_reg_twiddles(tab, n);
-  build_w32(w32);
-  for (int m = threadIdx.x; m < g.py; m += blockDim.x) winy[m] = win_src(m, n, g.py, g.pad_left_y);
-  __syncthreads();
-
-  if (warp < ncols) {
-    const int j = j0 + warp;
-    const int bl = T512 ? lane : brev5(lane);
-    float2 x[R];
-    {
-      const double* Rm = params[img].rot;
-      const float r00 = (float)Rm[0], r01 = (float)Rm[1];
-      const float r10 = (float)Rm[3], r11 = (float)Rm[4];
-      const float r20 = (float)Rm[6], r21 = (float)Rm[7];
-      const bool wrap = !(g.flags & CJX_ZERO_FILL_NEGATIVE);
-      const float ux = (float)fft_index(j, n);
-      const float bx = r00 * ux, by = r10 * ux, bz = r20 * ux;
-      float cw = 0.f, r02 = 0.f, r12 = 0.f, r22 = 0.f;
-      if (ewald) {
-        cw = ewald_w(params + img, n);
-        r02 = (float)Rm[2];
-        r12 = (float)Rm[5];
-        r22 = (float)Rm[8];
-      }
-#pragma unroll
-      for (int p0 = 0; p0 < R; p0 += 2) {
-        constexpr int S = 2;
-        float ox[S], oy[S], oz[S];
-        bool act[S];
-        float2 val[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-          act[s] = (p0 + s) < R;
-          const float vy = (float)fft_index(act[s] ? 32 * (p0 + s) + bl : 0, n);
-          ox[s] = fmaf(r01, vy, bx);
-          oy[s] = fmaf(r11, vy, by);
-          oz[s] = fmaf(r21, vy, bz);
-          if (ewald) {
-            const float w = cw * fmaf(ux, ux, vy * vy);
-            ox[s] = fmaf(r02, w, ox[s]);
-            oy[s] = fmaf(r12, w, oy[s]);
-            oz[s] = fmaf(r22, w, oz[s]);
-          }
-        }
-        gather_samples<S>(grid, n, L, ox, oy, oz, act, wrap, g.fill, val);
-        x[p0] = val[0];
-        if (p0 + 1 < R) x[p0 + 1] = val[1];
-      }
-    }
-    float2* buf = tile + warp * stride;
-    if (!ewald && (j == 0 || j == n / 2)) {  // (S[v] + conj(S[-v])) / 2 through the warp's buffer
-#pragma unroll
-      for (int n1 = 0; n1 < R; ++n1) buf[pad16(32 * n1 + bl)] = x[n1];
-      __syncwarp();
-#pragma unroll
-      for (int n1 = 0; n1 < R; ++n1) {
-        const int idx = 32 * n1 + bl;
-        const float2 m = buf[pad16(idx == 0 ? 0 : n - idx)];
-        x[n1] = make_float2(0.5f * (x[n1].x + m.x), 0.5f * (x[n1].y - m.y));
-      }
-      __syncwarp();
-    }
-    if constexpr (T512) {
-      warp_fft512_t<+1>(x, tab, w32, buf, lane);
-#pragma unroll
-      for (int q = 0; q < R; ++q) buf[pad16(fft512_t_out(q, lane))] = x[q];
-    } else {
-      const LaneTwiddles lt = make_lane_twiddles(w32, lane);
-      warp_fft_reg<R, +1>(x, tab, lt, lane);
-#pragma unroll
-      for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
-    }
-  }
-  __syncthreads();
-
-  float2* dst = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
-  for (int e = threadIdx.x; e < g.py * kCols; e += blockDim.x) {
-    const int m = e / kCols, jj = e % kCols;
-    if (jj < ncols) {
-      const int src = winy[m];
-      dst[(size_t)m * g.ld1 + jj] = (src >= 0) ? tile[jj * stride + pad16(src)] : make_float2(0.f, 0.f);
-    }
-  }
-}
-
-template <int R, typename Layout>
-void launch_direct_r(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                     int64_t k0, int cnt, float2* t1, bool t512, cudaStream_t stream) {
-  const size_t smem = sizeof(float2) * (size_t)(32 * R + kCols * (pad16(32 * R) + 1)) + sizeof(int) * (size_t)g.py;
-  const dim3 grd((g.ncols + kCols - 1) / kCols, cnt);
-  if constexpr (R == 16) {
-    if (t512) {
-      k_gather_colifft_direct<R, Layout, true><<<grd, kCols * 32, smem, stream>>>(grid, params, order, t1, g, k0);
-      return;
-    }
-  }
-  k_gather_colifft_direct<R, Layout, false><<<grd, kCols * 32, smem, stream>>>(grid, params, order, t1, g, k0);
 }
 
 template <int R, typename Layout, int S, int MAP, bool T512>
@@ -296,7 +180,7 @@ __global__ void __launch_bounds__(kCols * 32, 4)
 template <int R, typename Layout, int S, int MAP>
 void launch_fused_rsm(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                       int64_t k0, int cnt, float2* t1, bool t512, cudaStream_t stream) {
-  const size_t smem = sizeof(float2) * (size_t)(32 * R + kCols * (pad16(32 * R) + 1)) + sizeof(int) * (size_t)g.py;
+  const size_t smem = sizeof(float2) * (size_t)(32 * R + kCols * fused_stride(32 * R)) + sizeof(int) * (size_t)g.py;
   const dim3 grd((g.ncols + kCols - 1) / kCols, cnt);
   if constexpr (R == 16) {
     if (t512) {
@@ -337,13 +221,8 @@ template <typename Layout>
 int launch_fused_layout(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                         int64_t k0, int cnt, float2* t1, const Tuning& tn, cudaStream_t stream) {
   switch (reg_fft_radix(g.n)) {
-#define CJX_FUSED_CASE(R)                                                                          \
-  case R:                                                                                          \
-    if (tn.gather_mode == 3) {                                                                     \
-      launch_direct_r<R, Layout>(g, grid, params, order, k0, cnt, t1, tn.fft_mode >= 2, stream); \
-      return CJX_OK;                                                                               \
-    }                                                                                              \
-    return launch_fused_r<R, Layout>(g, grid, params, order, k0, cnt, t1, tn, stream);
+#define CJX_FUSED_CASE(R) \
+  case R: return launch_fused_r<R, Layout>(g, grid, params, order, k0, cnt, t1, tn, stream);
     CJX_FUSED_CASE(1) CJX_FUSED_CASE(2) CJX_FUSED_CASE(3) CJX_FUSED_CASE(4) CJX_FUSED_CASE(5)
     CJX_FUSED_CASE(6) CJX_FUSED_CASE(8) CJX_FUSED_CASE(10) CJX_FUSED_CASE(12) CJX_FUSED_CASE(16)
 #undef CJX_FUSED_CASE
@@ -385,7 +264,7 @@ __global__ void __launch_bounds__(kCols * 32, 4) k_front_wave(const __grid_const
 
 // Dynamic shared memory of the front pass for one group.
 size_t front_wave_smem(const SliceGeom& g) {
-  return sizeof(float2) * (size_t)(g.n + kCols * (pad16(g.n) + 1)) + sizeof(int) * (size_t)g.py;
+  return sizeof(float2) * (size_t)(g.n + kCols * fused_stride(g.n)) + sizeof(int) * (size_t)g.py;
 }
 
 // CTAs of the front pass per image.

@@ -392,6 +392,14 @@ __global__ void __launch_bounds__(kWarps * 32)
 // R = RN), Px window, Px-point forward FFT (register form, RP), split.
 // The load of the packed pair (z = A + iB in the lane's bit-reversed order)
 // is separate, so that a kernel can issue it before its table copy.
+// Per-warp buffer of the row pass: the N-point transform's staging (stage512
+// with the transpose FFT, pad16 otherwise) and the Px-point one's (stage_r).
+__host__ __device__ inline int rows_stride(int n, int px, bool t512) {
+  const int sn = t512 ? kStage512Size : pad16(n - 1) + 1;
+  const int sp = stage_r_size(px / 32);
+  return (sn > sp ? sn : sp) + 1;
+}
+
 template <int RN, bool NATURAL = false>
 __device__ __forceinline__ void rows_pair_load(const float2* __restrict__ rowA, const float2* __restrict__ rowB,
                                                bool has_b, float2 (&z)[RN], int lane) {
@@ -427,7 +435,7 @@ __device__ __forceinline__ void rows_pair_reg(float2 (&z)[RN], bool has_b, float
     static_assert(RN == 16, "the transpose FFT is 512-point");
     warp_fft512_t<+1>(z, tabN, w32, buf, lane);
 #pragma unroll
-    for (int q = 0; q < RN; ++q) buf[pad16(fft512_t_out(q, lane))] = z[q];
+    for (int q = 0; q < RN; ++q) buf[stage512(fft512_t_out(q, lane))] = z[q];
   } else {
     warp_fft_reg<RN, +1>(z, tabN, lt, lane);  // z = a + i b (the two real rows)
 #pragma unroll
@@ -438,16 +446,16 @@ __device__ __forceinline__ void rows_pair_reg(float2 (&z)[RN], bool has_b, float
 #pragma unroll
   for (int n1 = 0; n1 < RP; ++n1) {
     const int src = winx[32 * n1 + bl];
-    w[n1] = (src >= 0) ? buf[pad16(src)] : make_float2(0.f, 0.f);
+    w[n1] = (src >= 0) ? buf[T512 ? stage512(src) : pad16(src)] : make_float2(0.f, 0.f);
   }
   __syncwarp();
   warp_fft_reg<RP, -1>(w, tabP, lt, lane);
 #pragma unroll
-  for (int k1 = 0; k1 < RP; ++k1) buf[pad16(k1 + RP * lane)] = w[k1];
+  for (int k1 = 0; k1 < RP; ++k1) buf[stage_r(RP, k1 + RP * lane)] = w[k1];
   __syncwarp();
   for (int k = lane; k <= px / 2; k += 32) {
-    const float2 Wk = buf[pad16(k)];
-    const float2 Wm = buf[pad16((px - k) % px)];
+    const float2 Wk = buf[stage_r(RP, k)];
+    const float2 Wm = buf[stage_r(RP, (px - k) % px)];
     outA[k] = make_float2(0.5f * (Wk.x + Wm.x), 0.5f * (Wk.y - Wm.y));
     if (has_b) outA[ld2 + k] = make_float2(0.5f * (Wk.y + Wm.y), -0.5f * (Wk.x - Wm.x));
   }
@@ -460,7 +468,7 @@ __device__ __forceinline__ void rows_reg_body(const float2* __restrict__ t1, flo
                                               const SliceGeom& g, int rp, int bx, int by, float2* smem, float2* w32) {
   constexpr int n = 32 * RN;
   const int px = g.px;
-  const int stride = pad16(max(n, px)) + 1;
+  const int stride = rows_stride(n, px, T512);
   float2* tabN = smem;
   float2* tabP = tabN + n;
   float2* bufs = tabP + px;
@@ -510,7 +518,7 @@ __device__ __forceinline__ void colfft_epilogue_body(const float2* __restrict__ 
                                                      const SliceGeom& g, int64_t k0, float norm, int bx, int by,
                                                      float2* smem, float2* w32, ImageConsts& sc) {
   constexpr int py = 32 * R;
-  constexpr int stride = pad16(py) + 1;
+  constexpr int stride = stage_r_size(R) + 1;
   float2* tab = smem;
   float2* row_phase = smem + py;  // exp(-2 pi i qy(i) ty)
   float2* bufs = smem + 2 * py;
@@ -556,7 +564,7 @@ __device__ __forceinline__ void colfft_epilogue_body(const float2* __restrict__ 
 #pragma unroll
     for (int k1 = 0; k1 < R; ++k1) {
       const int i = k1 + R * lane;
-      buf[pad16(i)] =
+      buf[stage_r(R, i)] =
           apply_filter(apply_column_epilogue(x[k1], i, j, py, g.px, g.flags, c, ce, row_phase), g, i, j, g.pxh);
     }
   }
@@ -564,7 +572,7 @@ __device__ __forceinline__ void colfft_epilogue_body(const float2* __restrict__ 
   float2* dst = out + (size_t)img * py * g.pxh + j0;
   for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
     const int m = e / kWarps, jj = e % kWarps;
-    if (jj < ncols) dst[(size_t)m * g.pxh + jj] = bufs[jj * stride + pad16(m)];
+    if (jj < ncols) dst[(size_t)m * g.pxh + jj] = bufs[jj * stride + stage_r(R, m)];
   }
 }
 
@@ -766,7 +774,7 @@ int tuning_set(int key, int64_t value) {
     return CJX_OK;
   }
   if (key == CJX_TUNE_GATHER_MODE) {
-    if (value < 0 || value > 3) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0, 1, 2 or 3");
+    if (value < 0 || value > 2) return fail(CJX_ERR_INVALID_ARGUMENT, "gather mode must be 0, 1 or 2");
     g_gather_mode = value;
     return CJX_OK;
   }
@@ -841,7 +849,7 @@ static int launch_front(const SliceGeom& g, const float2* grid, const cjx_image_
   const bool fast = tn.fft_mode >= 1;
   // gather mode 2: the register-FFT fused pass (trilinear grids, N = 32 R); otherwise the split pair of
   // kernels, or mode 0's shared-memory fused kernel, which has no pair, spline or Ewald path
-  const bool fused_reg = (tn.gather_mode == 2 || tn.gather_mode == 3) && fast && fused_gather_supported(g);
+  const bool fused_reg = tn.gather_mode == 2 && fast && fused_gather_supported(g);
   const bool split = !fused_reg && (tn.gather_mode != 0 ||
                                     (g.flags & (CJX_GRID_BRICKED_PAIRS | CJX_GRID_SPLINE | CJX_EWALD_SPHERE)));
   const bool t512 = tn.fft_mode >= 2 && rn == 16;  // 512-point column transforms through the transpose FFT
@@ -933,7 +941,7 @@ static int launch_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt
   const bool fast = tn.fft_mode >= 1;
   const size_t sb = smem_b(g);
   const size_t sb_reg =
-      sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * (size_t)g.px;
+      sizeof(float2) * (size_t)(g.n + g.px + kWarps * rows_stride(g.n, g.px, rn == 16)) + sizeof(int) * (size_t)g.px;
     prof_begin(stream);
     const dim3 gb((g.py + 2 * kWarps - 1) / (2 * kWarps), cnt);
     if (fast && rn && rpx) {
@@ -978,7 +986,7 @@ static int launch_tail(const SliceGeom& g, const float2* t2, const cjx_image_par
   const float norm = (float)(1.0 / ((double)g.n * (double)g.n));
   const int rpy = reg_fft_radix(g.py);
   const size_t sc = smem_c(g);
-  const size_t sc_reg = sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1));
+  const size_t sc_reg = sizeof(float2) * (size_t)(2 * g.py + kWarps * (stage_r_size(rpy) + 1));
   prof_begin(stream);
   const dim3 gcc((g.pxh + kWarps - 1) / kWarps, cnt);
   if (tn.fft_mode >= 1 && rpy) {
@@ -1107,9 +1115,9 @@ int launch_forward_waves(const WaveInput* in, int n_in, void* workspace, size_t 
     const SliceGeom& g = in[i].g;
     n_max = std::max<int64_t>(n_max, in[i].n);
     s_front = std::max(s_front, front_wave_smem(g));
-    s_rows = std::max(s_rows, sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) +
+    s_rows = std::max(s_rows, sizeof(float2) * (size_t)(g.n + g.px + kWarps * rows_stride(g.n, g.px, reg_fft_radix(g.n) == 16)) +
                                   sizeof(int) * (size_t)g.px);
-    s_tail = std::max(s_tail, sizeof(float2) * (size_t)(2 * g.py + kWarps * (pad16(g.py) + 1)));
+    s_tail = std::max(s_tail, sizeof(float2) * (size_t)(2 * g.py + kWarps * (stage_r_size(reg_fft_radix(g.py)) + 1)));
   }
   if (n_max == 0) return CJX_OK;
   std::vector<int64_t> per_wave(n_in);

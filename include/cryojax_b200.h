@@ -403,8 +403,7 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
  * shared-memory FFTs (C-order and bricked grids only), 2 (default) = one
  * fused gather + register-FFT column kernel (trilinear grids in any layout,
  * slice or Ewald sphere, N = 32 R; other cases, e.g. spline volumes, run
- * as 1), which never writes the sampled plane to memory; 3 = as 2, each
- * warp gathering its column straight into the transform's registers.
+ * as 1), which never writes the sampled plane to memory.
  * CJX_TUNE_FFT_MODE: 1 = register/shuffle FFTs where the length is 32 R
  * (R in 1-6, 8, 10, 12, 16), 2 = the same, with the 512-point
  * column transforms of the resize stage done as 16 x 32 through one

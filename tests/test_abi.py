@@ -89,7 +89,7 @@ def test_tuning_knobs():
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(nat.CJX_TUNE_SCATTER_VEC, 3)
     with pytest.raises(nat.CryojaxB200Error):
-        nat.tuning_set(nat.CJX_TUNE_GATHER_MODE, 4)
+        nat.tuning_set(nat.CJX_TUNE_GATHER_MODE, 3)
     with pytest.raises(nat.CryojaxB200Error):
         nat.tuning_set(nat.CJX_TUNE_GATHER_TILE, 4)
 

@@ -137,27 +137,3 @@ def test_fused_chunked_call(cuda_device):
     np.testing.assert_array_equal(one, chunked)
     ref = np.stack([O.compute_fourier_image(grid, fs, s) for s in specs])
     assert max(rel_l2_per_image(chunked, ref)) <= IMAGE_REL_L2_TOL
-
-
-@pytest.mark.parametrize("n,shape", [(64, (48, 40)), (128, (64, 64)), (192, (224, 200)), (512, (320, 320))])
-@pytest.mark.parametrize("layout", ["pairs", "bricked", "linear"])
-def test_direct_form_matches_split_pass(cuda_device, n, shape, layout):
-    """Gather mode 3 (each warp gathers its column straight into the FFT's registers) gives the split pass's
-    images bit for bit: the same samples through the same transform."""
-    grid = _synthetic_grid(n, seed=n + 13)
-    specs = random_specs(3, seed=n + 14, shape=shape)
-    with tuning(mode=3):
-        direct = _run(grid, specs, layout=layout)
-    with tuning(mode=1):
-        split = _run(grid, specs, layout=layout)
-    np.testing.assert_array_equal(direct, split)
-
-
-def test_direct_form_ewald_sphere(cuda_device):
-    vol, grid, fs = make_volume(48, 100, seed=15)
-    specs = random_specs(3, seed=16, shape=(64, 64))
-    with tuning(mode=3):
-        direct = _run(grid, specs, ewald=True)
-    with tuning(mode=1):
-        split = _run(grid, specs, ewald=True)
-    np.testing.assert_array_equal(direct, split)
