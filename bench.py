@@ -496,14 +496,14 @@ def measure_gradient(dev, steps, warmup, seed):
     res = squared_residual_and_grad(model, obs_f, observed_is_fourier=True, grid_grad=True)
     # device-timed loop of the library call
     integ = model.volume_integrator
-    flags = model._flags() | nat.CJX_GRID_BRICKED
+    grid_b, layout = vol.bricked_grid(), nat.CJX_GRID_BRICKED  # the layout squared_residual_and_grad takes
+    flags = model._flags() | layout
     desc = nat.make_desc(vol.shape[0], 192, 192, flags)
     pd = torch.as_tensor(model.image_params(), device=dev)
     order = torch.as_tensor(S.orientation_order(model.image_params()[:, 0:9].reshape(-1, 3, 3)), device=dev)
     grads = torch.empty((n_img, nat.GRAD_DOUBLES), dtype=torch.float64, device=dev)
     gg = torch.zeros(vol.shape, dtype=torch.complex64, device=dev)
     ws = torch.empty(nat.loss_workspace_size(desc, n_img), dtype=torch.uint8, device=dev)
-    grid_b = vol.bricked_grid()
     for _ in range(warmup):
         nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
     torch.cuda.synchronize()
@@ -522,6 +522,8 @@ def measure_gradient(dev, steps, warmup, seed):
     return {"metric": "loss + gradient images/s (192^3 volume, 192^2 images, pose/offset/defocus/grid)",
             "value": n_img / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms, "images_per_step": n_img,
             "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()},
+            "layout": "x-pair bricked grid" if layout == nat.CJX_GRID_BRICKED_PAIRS else "bricked grid",
+            "scatter_mode": nat.tuning_get(nat.CJX_TUNE_SCATTER_VEC),
             "mean_loss": float(np.mean(res["loss"])), "grid_grad_norm": float(gg.abs().pow(2).sum().sqrt())}
 
 

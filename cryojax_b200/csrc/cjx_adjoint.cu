@@ -16,11 +16,12 @@
 //                       (adjoint of the unnormalised inverse), Hermitian fix
 //                       of kx = 0, N/2 (self-adjoint);
 //   k_scatter_slice     trilinear scatter-add of the slice gradient into the
-//                       grid gradient (float2 atomics) and d/dR from the
+//                       grid gradient (float2 / float4 atomics) and d/dR from the
 //                       derivative of the interpolation weights.
 // The gradient of a real loss w.r.t. a complex value z is reported as
 // dL/dRe z + i dL/dIm z (jax.grad returns its complex conjugate).
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 
 #include "cjx_common.cuh"
@@ -421,17 +422,86 @@ __device__ __forceinline__ bool peer_sum(unsigned key, float2& v, int lane) {
 // ---------------------------------------------------------------------------
 // Trilinear scatter-add of the slice gradient and d/dR.
 // ---------------------------------------------------------------------------
-// AGG (CJX_TUNE_SCATTER_VEC = 2): for each of the 8 corners, the lanes of a
-// warp whose corner lands on the same voxel sum their contributions with
-// peer_sum and one lane per voxel issues the atomic; neighbouring samples of
-// a warp's 4 x 8 patch share most of their corners (about 3.3 samples update
-// each voxel), so this cuts the atomics that serialise on one address.
-// VEC: the two x-corners of a (y, z) corner row land in one 16-byte
-// float4 atomic when both are valid, adjacent and 16-byte aligned in the
-// gradient array (about half the rows); otherwise each corner takes an
-// 8-byte float2 atomic.  The scatter is bound by the L2's atomic units, so
-// fewer atomic operations is what shortens it.
-template <typename Layout, bool VEC, bool AGG = false>
+// The 8 corner values of one sample, corner c = 4 dz + 2 dy + dx: the fill
+// value where a corner lies outside the grid (and for lanes that are not
+// live).  Any layout: one 8-byte load per corner.
+template <typename Layout>
+__device__ __forceinline__ void load_corners(const float2* __restrict__ grid, const Layout& L, const AxisNodes& ax,
+                                             const AxisNodes& ay, const AxisNodes& az, bool live, float2 fill,
+                                             float2* v) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+    const bool ok = live && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
+    const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
+    v[c] = ok ? __ldg(&grid[L.az(iz) + L.ay(iy) + L.ax(ix)]) : fill;
+  }
+}
+
+// x-pair layout: a (dz, dy) corner row whose two x-corners are adjacent and
+// inside the grid is one 16-byte entry (g(x0), g(x0 + 1)); other corners
+// read the low half of their own entry.
+template <>
+__device__ __forceinline__ void load_corners<PairLayout>(const float2* __restrict__ grid, const PairLayout& L,
+                                                         const AxisNodes& ax, const AxisNodes& ay,
+                                                         const AxisNodes& az, bool live, float2 fill, float2* v) {
+  const float4* g4 = reinterpret_cast<const float4*>(grid);
+  const bool xpair = ax.v0 && ax.v1 && ax.i1 == ax.i0 + 1;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int dz = r >> 1, dy = r & 1;
+    const bool okr = live && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0);
+    const size_t row = (size_t)L.az(dz ? az.i1 : az.i0) + (size_t)L.ay(dy ? ay.i1 : ay.i0);
+    if (okr && xpair) {
+      const float4 q = __ldg(g4 + row + L.ax(ax.i0));
+      v[2 * r] = make_float2(q.x, q.y);
+      v[2 * r + 1] = make_float2(q.z, q.w);
+    } else {
+      v[2 * r] = (okr && ax.v0) ? __ldg(&grid[2 * (row + L.ax(ax.i0))]) : fill;
+      v[2 * r + 1] = (okr && ax.v1) ? __ldg(&grid[2 * (row + L.ax(ax.i1))]) : fill;
+    }
+  }
+}
+
+// How the grid scatter issues its atomics (CJX_TUNE_SCATTER_VEC).
+constexpr int kScatterCorner = 0;  // one 8-byte float2 atomic per valid corner
+constexpr int kScatterVec = 1;     // a corner row's two x-corners in one 16-byte float4 atomic where that is
+                                   // 16-byte aligned in the gradient array (even x0), else two float2 atomics
+constexpr int kScatterWarpAgg = 2; // lanes whose corner hits the same voxel sum first (peer_sum), float2 atomics
+
+// The scatter of one sample's corner rows (kScatterCorner, kScatterVec):
+// weight * cotangent to each valid corner of the C-order gradient array.
+template <int MODE>
+__device__ __forceinline__ void scatter_rows(float2* __restrict__ gg, int n, const AxisNodes& ax, const AxisNodes& ay,
+                                             const AxisNodes& az, float2 gs) {
+  const bool xpair = ax.v0 && ax.v1 && ax.i1 == ax.i0 + 1;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {  // corner rows (dz, dy); x-corners 0 and 1
+    const int dz = r >> 1, dy = r & 1;
+    if (!((dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0))) continue;
+    const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0;
+    const float wyz = (dz ? az.w1 : az.w0) * (dy ? ay.w1 : ay.w0);
+    const size_t row = ((size_t)iz * n + iy) * n;
+    const float2 c0 = make_float2(wyz * ax.w0 * gs.x, wyz * ax.w0 * gs.y);
+    const float2 c1 = make_float2(wyz * ax.w1 * gs.x, wyz * ax.w1 * gs.y);
+    const size_t e0 = row + ax.i0;
+    if (MODE == kScatterVec && xpair && (e0 & 1) == 0) {
+      atomicAdd(reinterpret_cast<float4*>(gg + e0), make_float4(c0.x, c0.y, c1.x, c1.y));
+    } else {
+      if (ax.v0) atomicAdd(&gg[e0], c0);
+      if (ax.v1) atomicAdd(&gg[row + ax.i1], c1);
+    }
+  }
+}
+
+// One thread per sample of the half plane (16 x 16 samples per CTA): the
+// sample's cotangent gs = g_H, its 8 corners (read for dH/d(coordinate)),
+// the scatter of w * gs to the corners (MODE above; neighbouring samples of
+// a warp's 4 x 8 patch share most of their corners, about 3.3 samples per
+// voxel), and the CTA's share of dL/dR.  The scatter is bound by the L1 and
+// the L2's atomic units, so fewer atomic instructions and sectors is what
+// shortens it.
+template <typename Layout, int MODE>
 __global__ void __launch_bounds__(256)
     k_scatter_slice(const float2* __restrict__ grid, const float2* __restrict__ gh,
                     const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
@@ -451,35 +521,44 @@ __global__ void __launch_bounds__(256)
   gather_lane_offsets<1>(warp, lane, du, dv);
   const int u = blockIdx.x * 16 + du;
   const int v = blockIdx.y * 16 + dv;
+  const bool live = u < g.nxh && v < n;
   float gr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if constexpr (AGG) {
-    // every lane takes part in the warp-level grouping, so the per-corner work runs outside the bounds test
-    // with inactive lanes carrying kNoKey
-    const bool live = u < g.nxh && v < n;
+  // the warp-aggregated form groups all 32 lanes, so there every lane runs the sample code (inactive
+  // lanes carry kNoKey)
+  if (MODE == kScatterWarpAgg || live) {
     const float2 gs = live ? gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v] : make_float2(0.f, 0.f);
     const float ux = (float)fft_index(live ? u : 0, n), vy = (float)fft_index(live ? v : 0, n);
     const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
     const AxisNodes ax = axis_nodes(o[0], n, wrap);
     const AxisNodes ay = axis_nodes(o[1], n, wrap);
     const AxisNodes az = axis_nodes(o[2], n, wrap);
-    float dH[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+    float2 val[8];
+    load_corners<Layout>(grid, L, ax, ay, az, live, g.fill, val);
+    float dH[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // dH/do_axis (complex)
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
-      const bool ok = live && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
-      const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
       const float wx = dx ? ax.w1 : ax.w0, wy = dy ? ay.w1 : ay.w0, wz = dz ? az.w1 : az.w0;
-      const float2 val = ok ? __ldg(&grid[L.az(iz) + L.ay(iy) + L.ax(ix)]) : g.fill;
       const float sx = dx ? 1.f : -1.f, sy = dy ? 1.f : -1.f, sz = dz ? 1.f : -1.f;
       const float gwx = sx * wy * wz, gwy = sy * wx * wz, gwz = sz * wx * wy;
-      dH[0][0] += gwx * val.x; dH[0][1] += gwx * val.y;
-      dH[1][0] += gwy * val.x; dH[1][1] += gwy * val.y;
-      dH[2][0] += gwz * val.x; dH[2][1] += gwz * val.y;
-      if (grad_grid) {
-        const float w = (wz * wy) * wx;
-        const unsigned key = ok ? (unsigned)(((size_t)iz * n + iy) * n + ix) : kNoKey;
-        float2 c2 = make_float2(w * gs.x, w * gs.y);
-        if (peer_sum(key, c2, lane)) atomicAdd(&grad_grid[key], c2);
+      dH[0][0] += gwx * val[c].x; dH[0][1] += gwx * val[c].y;
+      dH[1][0] += gwy * val[c].x; dH[1][1] += gwy * val[c].y;
+      dH[2][0] += gwz * val[c].x; dH[2][1] += gwz * val[c].y;
+    }
+    if (grad_grid) {
+      if constexpr (MODE == kScatterWarpAgg) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
+          const bool ok = live && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
+          const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
+          const float w = ((dz ? az.w1 : az.w0) * (dy ? ay.w1 : ay.w0)) * (dx ? ax.w1 : ax.w0);
+          const unsigned key = ok ? (unsigned)(((size_t)iz * n + iy) * n + ix) : kNoKey;
+          float2 c2 = make_float2(w * gs.x, w * gs.y);
+          if (peer_sum(key, c2, lane)) atomicAdd(&grad_grid[key], c2);
+        }
+      } else {
+        scatter_rows<MODE>(grad_grid, n, ax, ay, az, gs);
       }
     }
     if (live) {
@@ -489,56 +568,6 @@ __global__ void __launch_bounds__(256)
         gr[2 * a] = dLdo * ux;
         gr[2 * a + 1] = dLdo * vy;
       }
-    }
-  } else if (u < g.nxh && v < n) {
-    const float2 gs = gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v];
-    const float ux = (float)fft_index(u, n), vy = (float)fft_index(v, n);
-    const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
-    const AxisNodes ax = axis_nodes(o[0], n, wrap);
-    const AxisNodes ay = axis_nodes(o[1], n, wrap);
-    const AxisNodes az = axis_nodes(o[2], n, wrap);
-    float dH[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // dH/do_axis (complex)
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const int dz = c >> 2, dy = (c >> 1) & 1, dx = c & 1;
-      const bool ok = (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
-      const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
-      const float wx = dx ? ax.w1 : ax.w0, wy = dy ? ay.w1 : ay.w0, wz = dz ? az.w1 : az.w0;
-      const float2 val = ok ? __ldg(&grid[L.az(iz) + L.ay(iy) + L.ax(ix)]) : g.fill;
-      const float sx = dx ? 1.f : -1.f, sy = dy ? 1.f : -1.f, sz = dz ? 1.f : -1.f;
-      const float gwx = sx * wy * wz, gwy = sy * wx * wz, gwz = sz * wx * wy;
-      dH[0][0] += gwx * val.x; dH[0][1] += gwx * val.y;
-      dH[1][0] += gwy * val.x; dH[1][1] += gwy * val.y;
-      dH[2][0] += gwz * val.x; dH[2][1] += gwz * val.y;
-      if (!VEC && ok && grad_grid) {
-        const float w = (wz * wy) * wx;
-        atomicAdd(&grad_grid[((size_t)iz * n + iy) * n + ix], make_float2(w * gs.x, w * gs.y));
-      }
-    }
-    if (VEC && grad_grid) {
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {  // corner rows (dz, dy); x-corners 0 and 1
-        const int dz = r >> 1, dy = r & 1;
-        if (!((dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0))) continue;
-        const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0;
-        const float wyz = (dz ? az.w1 : az.w0) * (dy ? ay.w1 : ay.w0);
-        const size_t row = ((size_t)iz * n + iy) * n;
-        const float2 c0 = make_float2(wyz * ax.w0 * gs.x, wyz * ax.w0 * gs.y);
-        const float2 c1 = make_float2(wyz * ax.w1 * gs.x, wyz * ax.w1 * gs.y);
-        const size_t e0 = row + ax.i0;
-        if (ax.v0 && ax.v1 && ax.i1 == ax.i0 + 1 && (e0 & 1) == 0) {
-          atomicAdd(reinterpret_cast<float4*>(grad_grid + e0), make_float4(c0.x, c0.y, c1.x, c1.y));
-        } else {
-          if (ax.v0) atomicAdd(&grad_grid[e0], c0);
-          if (ax.v1) atomicAdd(&grad_grid[row + ax.i1], c1);
-        }
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float dLdo = gs.x * dH[a][0] + gs.y * dH[a][1];
-      gr[2 * a] = dLdo * ux;
-      gr[2 * a + 1] = dLdo * vy;
     }
   }
 #pragma unroll
@@ -676,6 +705,22 @@ __global__ void k_zero_doubles(double* p, int64_t count) {
     p[i] = 0.0;
 }
 
+template <typename Layout>
+static void launch_scatter(int mode, dim3 gs, cudaStream_t stream, const float2* grid, const float2* hb,
+                           const cjx_image_params* params, const int32_t* order, float2* grad_grid, double* grads,
+                           const SliceGeom& g, int64_t k0) {
+  switch (mode) {
+#define CJX_SC_CASE(M)                                                                                     \
+  case M:                                                                                                  \
+    k_scatter_slice<Layout, M><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0); \
+    break;
+    CJX_SC_CASE(kScatterCorner) CJX_SC_CASE(kScatterVec) CJX_SC_CASE(kScatterWarpAgg)
+#undef CJX_SC_CASE
+    default:
+      break;
+  }
+}
+
 int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                      int64_t n_images, const float2* obs, double* grads, float2* grad_grid, void* workspace,
                      int64_t chunk, cudaStream_t stream, const Tuning& tn) {
@@ -697,9 +742,13 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
   if (s_loss > 227 * 1024 || s_rows > 227 * 1024 || s_cols > 227 * 1024)
     return fail(CJX_ERR_UNSUPPORTED, "loss gradient shared-memory footprint above 227 KB for these sizes");
   if (int e = ensure_adjoint_smem_attrs()) return e;
-  if (g.flags & CJX_GRID_BRICKED_PAIRS)
-    return fail(CJX_ERR_UNSUPPORTED, "the adjoint reads the grid in the linear or bricked layout, not x-pairs");
+  const bool pairs = (g.flags & CJX_GRID_BRICKED_PAIRS) != 0;
   const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
+  if (pairs && (g.flags & CJX_GRID_SPLINE))
+    return fail(CJX_ERR_UNSUPPORTED, "the spline adjoint reads the coefficients in the linear or bricked layout");
+  // the 16-byte atomics need a 16-byte aligned gradient array
+  int mode = tn.scatter_vec;
+  if (mode == kScatterVec && (reinterpret_cast<uintptr_t>(grad_grid) & 15)) mode = kScatterCorner;
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
@@ -735,28 +784,19 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
     prof_end("k_colfft_adj", stream);
     prof_begin(stream);
     const dim3 gs((g.nxh + 15) / 16, (g.n + 15) / 16, cnt);
-    const bool agg = tn.scatter_vec == 1;
-    const bool warp_agg = tn.scatter_vec == 2;
-    if ((g.flags & CJX_GRID_SPLINE) && bricked) {
-      k_scatter_slice_spline<SplineBrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
-                                                                        k0);
-    } else if (g.flags & CJX_GRID_SPLINE) {
-      k_scatter_slice_spline<SplineLinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads,
-                                                                         g, k0);
-    } else if (bricked && warp_agg) {
-      k_scatter_slice<BrickLayout, false, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
-                                                                         k0);
-    } else if (warp_agg) {
-      k_scatter_slice<LinearLayout, false, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g,
-                                                                          k0);
-    } else if (bricked && agg) {
-      k_scatter_slice<BrickLayout, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+    if (g.flags & CJX_GRID_SPLINE) {
+      if (bricked)
+        k_scatter_slice_spline<SplineBrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads,
+                                                                          g, k0);
+      else
+        k_scatter_slice_spline<SplineLinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid,
+                                                                           grads, g, k0);
+    } else if (pairs) {
+      launch_scatter<PairLayout>(mode, gs, stream, grid, hb, params, order, grad_grid, grads, g, k0);
     } else if (bricked) {
-      k_scatter_slice<BrickLayout, false><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
-    } else if (agg) {
-      k_scatter_slice<LinearLayout, true><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+      launch_scatter<BrickLayout>(mode, gs, stream, grid, hb, params, order, grad_grid, grads, g, k0);
     } else {
-      k_scatter_slice<LinearLayout, false><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0);
+      launch_scatter<LinearLayout>(mode, gs, stream, grid, hb, params, order, grad_grid, grads, g, k0);
     }
     prof_end("k_scatter_slice", stream);
   }

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <string>
 
 #include "cjx_common.cuh"
@@ -283,6 +284,9 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
   if (!grid || !params || !observed || !image_grads)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");
+  if ((g.flags & CJX_GRID_BRICKED_PAIRS) && (reinterpret_cast<uintptr_t>(grid) & 15))
+    return fail(CJX_ERR_INVALID_ARGUMENT, "an x-pair grid must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(grid_grad) & 7) return fail(CJX_ERR_INVALID_ARGUMENT, "grid_grad must be 8-byte aligned");
   const int64_t chunk = chunk_for(g, desc, n_images);
   if (!workspace || workspace_bytes < (size_t)chunk * workspace_per_image(g))
     return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_loss_workspace_size()");

@@ -147,10 +147,14 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
             grid = vol.bricked_grid()
             flags |= nat.CJX_GRID_BRICKED
     else:
-        grid, grad_shape = vol.fourier_voxel_grid, tuple(vol.shape)
-        if integ.use_bricked_layout:
-            grid = vol.bricked_grid()
-            flags |= nat.CJX_GRID_BRICKED
+        grad_shape = tuple(vol.shape)
+        if grid_grad and integ.use_bricked_layout:
+            # with the grid scatter, the bricked layout: the x-pair copy's faster gather does not make up for
+            # the L2 room its twice larger reads take from the scatter's atomics
+            grid, layout = vol.bricked_grid(), nat.CJX_GRID_BRICKED
+        else:  # the layout the forward reads (x-pair bricked by default)
+            grid, layout = integ.device_grid(vol)
+        flags |= layout
     py, px = cfg.padded_shape
     desc = nat.make_desc(vol.shape[0], py, px, flags, integ.fill_value)
     obs_f = observed if observed_is_fourier else observed_to_fourier(observed)

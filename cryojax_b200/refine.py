@@ -75,10 +75,13 @@ def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_s
     dev = vol.device
     params = image_model.image_params().copy()
     n = params.shape[0]
-    flags = image_model._flags() | integ._base_flags() | nat.CJX_GRID_BRICKED
+    flags = image_model._flags() | integ._base_flags()
     if hasattr(vol, "spline_coefficients"):  # FourierVoxelSplineVolume: cubic-spline samples and gradients
-        flags |= nat.CJX_GRID_SPLINE
-    grid = vol.bricked_grid()
+        flags |= nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED
+        grid = vol.bricked_grid()
+    else:  # the x-pair layout: 4 vector loads per sample in the forward and the scatter
+        flags |= nat.CJX_GRID_BRICKED_PAIRS
+        grid = vol.pair_grid()
     py, px = cfg.padded_shape
     desc = nat.make_desc(vol.shape[0], py, px, flags, integ.fill_value)
     obs_f = observed if observed_is_fourier else observed_to_fourier(observed)

@@ -64,8 +64,8 @@ extern "C" {
 #define CJX_GRID_BRICKED (1u << 4)
 /* `grid` is in the x-pair layout written by cjx_brick_volume_pairs: the
  * bricked order with 16-byte entries (g(x), g(x+1)), so that an interior
- * trilinear sample reads its 8 corners with 4 vector loads.  Forward and
- * search entry points only (not cjx_slice_ctf_loss_grad).                 */
+ * trilinear sample reads its 8 corners with 4 vector loads.  Forward,
+ * search and (voxel grids) loss-gradient entry points.                    */
 #define CJX_GRID_BRICKED_PAIRS (1u << 5)
 /* `grid` holds the cubic-spline coefficients of a FourierVoxelSplineVolume
  * (side N + 2: C order, bricked on side N + 2 with CJX_GRID_BRICKED,
@@ -217,6 +217,9 @@ CJX_API int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_
  * observed: device complex64 [n_images][Py][Px/2+1], rfftn of the observed
  * real-space images in cryoJAX's convention (ifftshift, then rfft2).
  * Resize path only, with N, Py, Px of the form 32 R (R in 1-6, 8, 10, 12, 16).
+ * grid: C order, bricked, or x-pair bricked (16-byte aligned) for a voxel
+ * grid; C order or bricked for spline coefficients.  grid_grad must be
+ * 8-byte aligned (16 for the 16-byte atomics of CJX_TUNE_SCATTER_VEC 1).
  * Replaces jax.grad / eqx.filter_grad through LinearImageModel.simulate
  * (cryojax/simulator/_image_model/base_image_model.py:68-105, 297-328).      */
 CJX_API int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid,
@@ -413,11 +416,13 @@ CJX_API int cjx_rfft2(int64_t n_images, int py, int px, const float* image, void
  * CJX_TUNE_GATHER_TILE: lanes of a gather warp cover 2 x 16 (0), 4 x 8 (1)
  * or 8 x 4 (2) samples (columns x rows) of the slice plane; 3 = one column
  * x 32 rows in gather mode 2 (the split gather takes 3 as 0).
- * CJX_TUNE_SCATTER_VEC: 1 (default) = the adjoint's grid scatter-add puts
- * the two x-corners of a corner row into one 16-byte atomic when they are
- * adjacent and aligned; 0 = one 8-byte atomic per (sample, corner); 2 =
- * warp-aggregated: lanes whose corner lands on the same voxel sum their
- * contributions with warp shuffles and one lane per voxel issues the atomic.
+ * CJX_TUNE_SCATTER_VEC: how the adjoint's grid scatter-add issues its
+ * atomics.  1 (default) = the two x-corners of a corner row in one 16-byte
+ * atomic when they are adjacent and 16-byte aligned (even x0), else two
+ * 8-byte atomics (a grid_grad that is only 8-byte aligned takes 0); 0 = one
+ * 8-byte atomic per (sample, corner); 2 = warp-aggregated: lanes whose
+ * corner lands on the same voxel sum their contributions with warp shuffles
+ * and one lane per voxel issues the atomic.
  * CJX_TUNE_SPLINE_ILP: samples per lane in the cubic-spline gather
  * (CJX_GRID_SPLINE; 1, 2 or 4, default 4).                                 */
 #define CJX_TUNE_GATHER_ILP 1

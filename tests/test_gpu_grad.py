@@ -163,14 +163,18 @@ def test_grid_gradient_scatter(cuda_device):
     assert gg.shape == (n, n, n)
 
 
-def test_bricked_and_linear_layouts_give_same_gradients(cuda_device):
+@pytest.mark.parametrize("layout", ["bricked", "linear"])
+def test_grid_layouts_give_same_gradients(cuda_device, layout):
+    """The x-pair layout (the default), the bricked layout and the C-order array give the same loss and
+    gradients up to the order of the float additions."""
     from cryojax_b200.gradients import squared_residual_and_grad
 
     grid, fs, specs, obs = _setup(seed=13, n=2)
     out = []
-    for bricked in (True, False):
+    for lay in ("pairs", layout):
         model, _ = _model(grid, specs)
-        model.volume_integrator.use_bricked_layout = bricked
+        model.volume_integrator.use_bricked_layout = lay != "linear"
+        model.volume_integrator.pair_layout = lay == "pairs"
         out.append(squared_residual_and_grad(model, obs, grid_grad=True))
     for key in ("loss", "d_wxyz", "d_offset", "d_defocus"):
         np.testing.assert_allclose(out[0][key], out[1][key], rtol=1e-5, atol=1e-8 * np.abs(out[1][key]).max())
@@ -198,3 +202,49 @@ def test_vector_atomic_scatter_matches_per_corner_atomics(cuda_device, mode):
     a, b = out[0]["d_grid"].cpu().numpy(), out[1]["d_grid"].cpu().numpy()
     assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max()
     np.testing.assert_array_equal(out[0]["loss"], out[1]["loss"])
+
+
+def _raw_loss_grad(grid, specs, obs, grid_grad, pairs):
+    """One cjx_slice_ctf_loss_grad call with a caller-given grid_grad tensor."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.gradients import observed_to_fourier
+
+    model, _ = _model(grid, specs)
+    integ = model.volume_integrator
+    integ.pair_layout = pairs
+    vol = model.volume_parametrization.get_representation()
+    g, layout = integ.device_grid(vol)
+    n_img = len(specs)
+    py, px = model.image_config.padded_shape
+    desc = nat.make_desc(vol.shape[0], py, px, model._flags() | layout)
+    ws = torch.empty(nat.loss_workspace_size(desc, n_img), dtype=torch.uint8, device="cuda")
+    grads = torch.empty((n_img, nat.GRAD_DOUBLES), dtype=torch.float64, device="cuda")
+    pd = torch.as_tensor(model.image_params(), device="cuda")
+    nat.slice_ctf_loss_grad(desc, g, pd, observed_to_fourier(obs), grads, grid_grad, ws)
+    torch.cuda.synchronize()
+    return grads.cpu().numpy()
+
+
+@pytest.mark.parametrize("pairs", [False, True])
+def test_gradient_array_only_8_byte_aligned(cuda_device, pairs):
+    """A grid_grad that is only 8-byte aligned (a view one entry into a larger array) takes the 8-byte
+    atomics and gives the 16-byte-aligned result; the entry before the view stays untouched."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+
+    grid, fs, specs, obs = _setup(box=48, shape=(64, 64), seed=19, n=2)
+    n = grid.shape[0]
+    ref = torch.zeros((n, n, n), dtype=torch.complex64, device="cuda")
+    g_ref = _raw_loss_grad(grid, specs, obs, ref, pairs)
+    big = torch.zeros(n ** 3 + 1, dtype=torch.complex64, device="cuda")
+    shifted = big[1:].view(n, n, n)
+    assert shifted.data_ptr() % 16 == 8
+    g_shift = _raw_loss_grad(grid, specs, obs, shifted, pairs)
+    scale = ref.abs().max().item()
+    assert scale > 0
+    assert (shifted - ref).abs().max().item() <= 1e-5 * scale
+    np.testing.assert_array_equal(g_shift[:, nat.G_LOSS], g_ref[:, nat.G_LOSS])
+    assert big[0].item() == 0
