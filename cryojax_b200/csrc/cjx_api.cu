@@ -12,6 +12,7 @@ namespace cjx {
 int make_geom(const cjx_slice_desc* d, SliceGeom* g);
 bool needs_resize(const SliceGeom& g);
 size_t workspace_per_image(const SliceGeom& g);
+int check_alignment(uint32_t flags, const void* grid, const void* out);
 int64_t default_chunk(const SliceGeom& g, int64_t n_images);
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                    int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
@@ -55,6 +56,18 @@ static int64_t chunk_for(const SliceGeom& g, const cjx_slice_desc* d, int64_t n_
   return default_chunk(g, n_images);
 }
 
+// The kernels read a grid with 8-byte loads (16-byte loads in the x-pair
+// layout) and write complex64 outputs with 8-byte stores: reject pointers
+// that would fault those accesses.
+int check_alignment(uint32_t flags, const void* grid, const void* out) {
+  const uintptr_t g = reinterpret_cast<uintptr_t>(grid), o = reinterpret_cast<uintptr_t>(out);
+  if ((flags & CJX_GRID_BRICKED_PAIRS) && (g & 15))
+    return fail(CJX_ERR_INVALID_ARGUMENT, "an x-pair grid must be 16-byte aligned");
+  if (g & 7) return fail(CJX_ERR_INVALID_ARGUMENT, "grid must be 8-byte aligned");
+  if (o & 7) return fail(CJX_ERR_INVALID_ARGUMENT, "the output array must be 8-byte aligned");
+  return CJX_OK;
+}
+
 }  // namespace cjx
 
 using namespace cjx;
@@ -82,6 +95,7 @@ int cjx_slice_ctf_forward(const cjx_slice_desc* desc, const void* grid, const cj
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   if (n_images == 0) return CJX_OK;
   if (!grid || !params || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params and out must be non-NULL");
+  if (int e = check_alignment(g.flags, grid, out)) return e;
   int64_t chunk = 0;
   if (needs_resize(g)) {
     chunk = chunk_for(g, desc, n_images);
@@ -101,6 +115,7 @@ int cjx_slice_ctf_forward_filtered(const cjx_slice_desc* desc, const void* grid,
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   if (n_images == 0) return CJX_OK;
   if (!grid || !params || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params and out must be non-NULL");
+  if (int e = check_alignment(g.flags, grid, out)) return e;
   g.filter = filter;
   int64_t chunk = 0;
   if (needs_resize(g)) {
@@ -148,6 +163,8 @@ int cjx_slice_ctf_forward_multi(const cjx_slice_group* groups, int n_groups, voi
     if (int e = group_plan(gr, &g, &chunk, &need)) return e;
     if (gr.n_images > 0 && (!gr.grid || !gr.params || !gr.out))
       return fail(CJX_ERR_INVALID_ARGUMENT, "group grid, params and out must be non-NULL");
+    if (gr.n_images > 0)
+      if (int e = check_alignment(g.flags, gr.grid, gr.out)) return e;
     if (need && (!workspace || workspace_bytes < need))
       return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_multi_workspace_size()");
     if (gr.tuning_valid) {
@@ -284,8 +301,7 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
   if (!grid || !params || !observed || !image_grads)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");
-  if ((g.flags & CJX_GRID_BRICKED_PAIRS) && (reinterpret_cast<uintptr_t>(grid) & 15))
-    return fail(CJX_ERR_INVALID_ARGUMENT, "an x-pair grid must be 16-byte aligned");
+  if (int e = check_alignment(g.flags, grid, observed)) return e;
   if (reinterpret_cast<uintptr_t>(grid_grad) & 7) return fail(CJX_ERR_INVALID_ARGUMENT, "grid_grad must be 8-byte aligned");
   const int64_t chunk = chunk_for(g, desc, n_images);
   if (!workspace || workspace_bytes < (size_t)chunk * workspace_per_image(g))
@@ -334,6 +350,7 @@ int cjx_search(const cjx_search_desc* desc, const void* grid, const cjx_image_pa
   if (desc->n_images == 0) return CJX_OK;
   if (!grid || !image_params || !rotations || !observed)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, image_params, rotations and observed must be non-NULL");
+  if (int e = check_alignment(g.flags, grid, observed)) return e;
   if (!workspace || workspace_bytes < need) return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_search_workspace_size()");
   return launch_search(g, workspace_per_image(g), chunk, static_cast<const float2*>(grid), image_params, rotations,
                        candidates, desc->n_images, K, static_cast<const float2*>(observed), scores, best_score,

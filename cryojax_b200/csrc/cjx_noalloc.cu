@@ -26,6 +26,7 @@ namespace cjx {
 int make_geom(const cjx_slice_desc* d, SliceGeom* g);
 bool needs_resize(const SliceGeom& g);
 size_t workspace_per_image(const SliceGeom& g);
+int check_alignment(uint32_t flags, const void* grid, const void* out);
 int launch_forward(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
                    int64_t n_images, float2* out, void* workspace, int64_t chunk, cudaStream_t stream,
                    const Tuning& tn);
@@ -68,6 +69,7 @@ extern "C" int cjx_slice_ctf_forward_noalloc(const cjx_slice_desc* desc, const v
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   if (n_images == 0) return CJX_OK;
   if (!grid || !params || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params and out must be non-NULL");
+  if (int e = check_alignment(g.flags, grid, out)) return e;
   if (!needs_resize(g))  // the fused no-resize kernel uses no scratch
     return launch_forward(g, static_cast<const float2*>(grid), params, order, n_images,
                           static_cast<float2*>(out), nullptr, 0, static_cast<cudaStream_t>(stream), current_tuning());

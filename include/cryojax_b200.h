@@ -35,8 +35,12 @@ extern "C" {
 #define CJX_ABI_VERSION 1
 
 /* ---- status codes ---------------------------------------------------- */
+/* Device arrays: complex64 grids, images and outputs must be 8-byte
+ * aligned, x-pair grids (CJX_GRID_BRICKED_PAIRS) 16-byte aligned; the
+ * entry points return CJX_ERR_INVALID_ARGUMENT otherwise.                 */
 #define CJX_OK 0
-#define CJX_ERR_INVALID_ARGUMENT 1 /* bad shape, null pointer, bad flag  */
+#define CJX_ERR_INVALID_ARGUMENT 1 /* bad shape, null pointer, bad flag,
+                                      misaligned array                    */
 #define CJX_ERR_UNSUPPORTED 2      /* size beyond the compiled limits     */
 #define CJX_ERR_CUDA 3             /* a CUDA runtime call failed          */
 #define CJX_ERR_WORKSPACE 4        /* workspace too small                  */

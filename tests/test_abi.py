@@ -141,3 +141,36 @@ def test_spline_flag_validation():
     assert lib.cjx_spline_coefficients(8, None, None, None, 0, None) == nat.CJX_ERR_INVALID_ARGUMENT
     # a coefficient array (side N + 2) can be bricked up to N = CJX_MAX_SIDE
     assert nat.bricked_volume_size(nat.CJX_MAX_SIDE + 2) > 0
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(),
+                    reason="hands the library placeholder addresses: argument validation only, on a machine without a GPU")
+def test_misaligned_arrays_are_rejected_before_any_launch():
+    """An x-pair grid that is not 16-byte aligned, a grid or an output that is not 8-byte aligned: the
+    entry points return CJX_ERR_INVALID_ARGUMENT (checked on the host, before any CUDA call)."""
+    lib = nat.load_library()
+    vp = ctypes.c_void_p
+    base = 0x10000000  # placeholder addresses; never dereferenced
+    pairs = nat.make_desc(64, 32, 32, nat.CJX_APPLY_CTF | nat.CJX_GRID_BRICKED_PAIRS)
+    plain = nat.make_desc(64, 32, 32, nat.CJX_APPLY_CTF)
+    ws = vp(base + 0x100000)
+    cases = [
+        (pairs, base + 8, base + 0x2000),   # x-pair grid on an 8-byte boundary
+        (plain, base + 4, base + 0x2000),   # grid on a 4-byte boundary
+        (plain, base, base + 0x2004),       # output on a 4-byte boundary
+    ]
+    for desc, grid, out in cases:
+        rc = lib.cjx_slice_ctf_forward(ctypes.byref(desc), vp(grid), vp(base + 0x1000), None, 2, vp(out), ws,
+                                       1 << 30, None)
+        assert rc == nat.CJX_ERR_INVALID_ARGUMENT, (grid, out)
+        assert "aligned" in lib.cjx_get_last_error().decode()
+        rc = lib.cjx_slice_ctf_forward_noalloc(ctypes.byref(desc), vp(grid), vp(base + 0x1000), None, 2, vp(out),
+                                               None)
+        assert rc == nat.CJX_ERR_INVALID_ARGUMENT, (grid, out)
+    grads = vp(base + 0x3000)
+    rc = lib.cjx_slice_ctf_loss_grad(ctypes.byref(pairs), vp(base + 8), vp(base + 0x1000), None, 2,
+                                     vp(base + 0x2000), grads, None, ws, 1 << 30, None)
+    assert rc == nat.CJX_ERR_INVALID_ARGUMENT
+    rc = lib.cjx_slice_ctf_loss_grad(ctypes.byref(plain), vp(base), vp(base + 0x1000), None, 2,
+                                     vp(base + 0x2000), grads, vp(base + 0x4004), ws, 1 << 30, None)
+    assert rc == nat.CJX_ERR_INVALID_ARGUMENT
