@@ -753,6 +753,11 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
     cal_model, cal_obs, _, _ = batch(512, seed + 54)
     cal_ex = tss.run(cal_model, cal_obs, rerank_top=8)
     thr = learned.calibrate_threshold(cal_model, cal_obs, cal_ex.best_orientation, target_agreement=0.995)
+    # the same proposals scored from the template-sharing search's CTF-free rows (no simulation), the 8 best
+    # re-ranked in FP32, the same fallback; threshold calibrated on the same images
+    learned_t = LearnedPoseSearch(net, grid, top_k=16, search=search, templates=tss, rerank_top=8,
+                                  fallback_search=tss)
+    thr_t = learned_t.calibrate_threshold(cal_model, cal_obs, cal_ex.best_orientation, target_agreement=0.995)
     del cal_obs
     torch.cuda.empty_cache()
     model, obs, q, df = batch(n_learned, seed + 55)
@@ -761,8 +766,8 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
     # starting defocus: the truth + U(-300, 300) A (a CTF-estimation error for the refinement to remove)
     df_start = df + np.random.default_rng(seed + 56).uniform(-300.0, 300.0, n_learned)
 
-    def learned_arm(m, o, of):
-        res = learned.run(m, o)
+    def learned_arm(m, o, of, searcher=learned):
+        res = searcher.run(m, o)
         init = with_rotations_and_defocus(m, grid.rotation_matrices(res.best_orientation),
                                           df_start[:len(o)])
         ref = refine_poses(init, of, steps=20, observed_is_fourier=True)
@@ -790,6 +795,8 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
     tss.build_templates(sub_model(64))  # the fallback's template bank, built before either arm is timed
     learned_arm(sub_model(64), obs[:64].contiguous(), obs_f[:64].contiguous())  # warm-up
     (lres, lref), t_l = timed(lambda: learned_arm(model, obs, obs_f))
+    learned_arm(sub_model(64), obs[:64].contiguous(), obs_f[:64].contiguous(), learned_t)  # warm-up
+    (ltres, ltref), t_lt = timed(lambda: learned_arm(model, obs, obs_f, learned_t))
     sub = sub_model(n_exhaustive)
     tss._key = None  # the template bank (CTF-free slices of every orientation), timed separately
     _, t_tmpl = timed(lambda: tss.build_templates(sub))
@@ -797,7 +804,9 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
     n_pl = min(n_exhaustive, 32)  # the plain search (one simulation per orientation) on a small sample
     pl, t_pl = timed(lambda: search.run(sub_model(n_pl), obs_f[:n_pl].contiguous(), observed_is_fourier=True))
     ang = rotation_angle_deg(lref.rotations[:n_exhaustive], eref.rotations)
+    ang_t = rotation_angle_deg(ltref.rotations[:n_exhaustive], eref.rotations)
     R_true = rot.quat_to_matrix(q)
+    per_image_plain_plus_refine = 1.0 / (n_pl / t_pl) + exhaustive_times["refine"] / n_exhaustive
     return {
         "metric": "pose search + 20 refinement steps, images/s (320^2 images, N=512, 36,864 orientations)",
         "unit": "images/s",
@@ -812,8 +821,18 @@ def measure_search_and_refine(dev, seed, n_learned, n_exhaustive):
                                        "agreement_with_template_search": float(np.mean(
                                            pl.best_orientation == eres.best_orientation[:n_pl]))}},
         "speedup": (n_learned / t_l) / (n_exhaustive / t_e),
-        "speedup_vs_plain_exhaustive_plus_refine": (n_learned / t_l) * (
-            1.0 / (n_pl / t_pl) + exhaustive_times["refine"] / n_exhaustive),
+        "speedup_vs_plain_exhaustive_plus_refine": (n_learned / t_l) * per_image_plain_plus_refine,
+        "learned_template_rows_plus_refine": {
+            "value": n_learned / t_lt, "seconds": t_lt, "n_images": n_learned,
+            "scoring": "the network's 16 x 48 candidates scored from the template-sharing search's FP16 rows "
+                       "(cjx_ncc_directions), the 8 best re-ranked in FP32 (template bank prebuilt, as for the "
+                       "exhaustive arm)",
+            "fallback_fraction": float(ltres.fallback.mean()), "threshold": thr_t,
+            "speedup_vs_exhaustive_plus_refine": (n_learned / t_lt) / (n_exhaustive / t_e),
+            "speedup_vs_plain_exhaustive_plus_refine": (n_learned / t_lt) * per_image_plain_plus_refine,
+            "fraction_within_2deg_of_exhaustive": float(np.mean(ang_t < 2.0)),
+            "search_agreement_with_exhaustive": float(np.mean(ltres.best_orientation[:n_exhaustive]
+                                                              == eres.best_orientation))},
         "refine_seconds_per_image": exhaustive_times["refine"] / n_exhaustive,
         "fraction_within_2deg_of_exhaustive": float(np.mean(ang < 2.0)),
         "search_agreement_with_exhaustive": float(np.mean(lres.best_orientation[:n_exhaustive]
@@ -1112,6 +1131,17 @@ def ncu_traffic(kernel):
     try:
         d = json.load(open(path))
         return d.get(kernel, {}).get("dram_bytes_per_image")
+    except Exception:
+        return None
+
+
+def ncu_limiter(kernel):
+    """The unit that bounds `kernel` and its fraction of peak, from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        return json.load(open(path)).get(kernel, {}).get("limiter")
     except Exception:
         return None
 
@@ -1573,7 +1603,9 @@ def main():
                          # time: how close it runs to the HBM bandwidth it is bound by
                          "traffic_gbs": ((trf * images_per_launch) / (top_ms / top_count) / 1e6 if trf else None),
                          "traffic_frac": ((trf * images_per_launch) / (top_ms / top_count) / 1e6 / hbm_peak
-                                          if trf else None)},
+                                          if trf else None),
+                         # the unit ncu finds closest to its peak for this kernel (not HBM for the fused pass)
+                         "limiter": ncu_limiter(top_name)},
             "l2": l2,
             "kernels_per_step": {k: {"launches": c, "ms": ms} for k, (c, ms) in prof.items()},
             "gpu_launches": launches_per_step * args.steps,
