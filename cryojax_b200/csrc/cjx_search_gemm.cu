@@ -289,81 +289,169 @@ __global__ void k_dir_scatter(const int32_t* __restrict__ dirs, int64_t pairs, i
     sorted[atomicAdd(cursor + dir_bin(dirs[p], n_dir), 1)] = (int32_t)p;
 }
 
-// FP32 dot product of 8 halves at a time
-__device__ __forceinline__ float dot8(uint4 a, uint4 b, float acc) {
-  const __half2* ha = reinterpret_cast<const __half2*>(&a);
-  const __half2* hb = reinterpret_cast<const __half2*>(&b);
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const float2 fa = __half22float2(ha[q]), fb = __half22float2(hb[q]);
-    acc = fmaf(fa.x, fb.x, acc);
-    acc = fmaf(fa.y, fb.y, acc);
+// Tiles of the (image, slot) pairs in direction order: for each bin d in
+// [0, n_dir] (n_dir = directions outside the grid) its first pair start[d]
+// and its tiles of up to kTilePairs pairs, numbered from tile_start[d];
+// start[n_dir + 1] = pairs, tile_start[n_dir + 1] = the tile count.  One
+// block of 1024 threads; `cursor` holds the bins' exclusive offsets.
+constexpr int kTilePairs = 16;
+
+__global__ void k_dir_tiles(const int* __restrict__ cursor, int n_dir, int pairs, int* __restrict__ start,
+                            int* __restrict__ tile_start) {
+  __shared__ int part[1024];
+  const int bins = n_dir + 1;
+  const int per = (bins + 1023) / 1024;
+  const int lo = threadIdx.x * per, hi = min(lo + per, bins);
+  int s = 0;
+  for (int d = lo; d < hi; ++d) {
+    const int next = d + 1 < bins ? cursor[d + 1] : pairs;
+    start[d] = cursor[d];
+    s += (next - cursor[d] + kTilePairs - 1) / kTilePairs;
   }
-  return acc;
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int d = lo; d < hi; ++d) {
+    const int next = d + 1 < bins ? cursor[d + 1] : pairs;
+    tile_start[d] = run;
+    run += (next - cursor[d] + kTilePairs - 1) / kTilePairs;
+  }
+  if (threadIdx.x == 1023) {
+    start[bins] = pairs;
+    tile_start[bins] = part[1023];
+  }
 }
 
-// One CTA per (image b, slot k) pair (in direction order): for a in
-// [0, n_inplane), template t = dirs[b][k] n_inplane + a,
+// D (16 x 8, FP32) += A (16 x 16, FP16) B (16 x 8, FP16) on the tensor cores.
+__device__ __forceinline__ void mma16816(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Templates per pass of the tile kernel: kNTiles tensor-core column tiles of 8.
+constexpr int kNTiles = 6;
+
+// One warp's share of a tile's dot products: rows lo / hi (the tile's pairs
+// g and g + 8 of this lane's group, NULL when the tile has no such pair)
+// against the templates tmpl[j] (template of column g of column tile j,
+// NULL past n_inplane), over the warp's K steps.  A K step is 32 halves:
+// lane (g, t) loads halves [8 t, 8 t + 8) of the step from each row, and the
+// two m16n8k16 products of the step take halves {8t, 8t+1, 8t+2, 8t+3} and
+// {8t+4, .., 8t+7} as their k = {2t, 2t+1, 2t+8, 2t+9}: the same relabelling
+// of k for both operands, so the sums are the dot products.
+__device__ __forceinline__ void tile_dots(const uint4* lo, const uint4* hi, const uint4* const (&tmpl)[kNTiles],
+                                          int64_t vrow, int warp, int t, float (&acc)[kNTiles][4]) {
+  const int64_t steps = (vrow + 3) / 4;
+  for (int64_t st = warp; st < steps; st += 8) {
+    const int64_t v = 4 * st + t;
+    const bool in = v < vrow;
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    const uint4 al = (in && lo) ? __ldg(lo + v) : z;
+    const uint4 ah = (in && hi) ? __ldg(hi + v) : z;
+    uint4 b[kNTiles];
+#pragma unroll
+    for (int j = 0; j < kNTiles; ++j) b[j] = (in && tmpl[j]) ? __ldg(tmpl[j] + v) : z;
+#pragma unroll
+    for (int j = 0; j < kNTiles; ++j) {
+      mma16816(acc[j], al.x, ah.x, al.y, ah.y, b[j].x, b[j].y);
+      mma16816(acc[j], al.z, ah.z, al.w, ah.w, b[j].z, b[j].w);
+    }
+  }
+}
+
+// One CTA per tile: up to 16 (image, slot) pairs that proposed direction d,
+// against d's n_inplane templates t = d n_inplane + a:
 //   num[b][k n_inplane + a] = y16[b] . s16[t]   (K = 2 kp)
 //   den[b][k n_inplane + a] = z16[b] . p16[t]   (K = kp)
-// Each warp takes 3 templates at a time, so one load of the image's row
-// serves three template rows.  Rows are 16-byte aligned (kp % 8 == 0).
-constexpr int kDirTemplatesPerPass = 3;
-
-__global__ void __launch_bounds__(256)
-    k_ncc_directions(const uint4* __restrict__ y16, const uint4* __restrict__ z16, const uint4* __restrict__ s16,
-                     const uint4* __restrict__ p16, int64_t kp, const int32_t* __restrict__ dirs,
-                     const int32_t* __restrict__ sorted, int kd, int n_dir, int n_inplane, float* __restrict__ num,
-                     float* __restrict__ den) {
-  const int32_t pair = sorted[blockIdx.x];
-  const int64_t b = pair / kd;
-  const int k = pair % kd;
-  const int d = dirs[pair];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t out0 = b * (int64_t)kd * n_inplane + (int64_t)k * n_inplane;
-  if ((unsigned)d >= (unsigned)n_dir) {  // no such direction: zero sums, which score 0
-    for (int a = threadIdx.x; a < n_inplane; a += blockDim.x) {
-      num[out0 + a] = 0.f;
-      den[out0 + a] = 0.f;
+// FP16 operands, FP32 accumulation on the tensor cores (mma.sync m16n8k16);
+// each template row is read once per tile instead of once per pair.  The
+// 8 warps split K; their partial sums meet in shared memory.
+__global__ void __launch_bounds__(256, 2)
+    k_ncc_dir_tiles(const uint4* __restrict__ y16, const uint4* __restrict__ z16, const uint4* __restrict__ s16,
+                    const uint4* __restrict__ p16, int64_t kp, const int32_t* __restrict__ sorted,
+                    const int* __restrict__ start, const int* __restrict__ tile_start, int kd, int n_dir,
+                    int n_inplane, float* __restrict__ num, float* __restrict__ den) {
+  __shared__ float red[8][kTilePairs][kNTiles * 8];
+  __shared__ int64_t out0[kTilePairs];
+  __shared__ int64_t img[kTilePairs];
+  const int tile = blockIdx.x;
+  if (tile >= tile_start[n_dir + 1]) return;
+  // the bin holding this tile: the largest d with tile_start[d] <= tile (empty bins share their
+  // successor's value, so the largest is the non-empty one)
+  int lo_d = 0, hi_d = n_dir;
+  while (lo_d < hi_d) {
+    const int mid = (lo_d + hi_d + 1) >> 1;
+    if (tile_start[mid] <= tile) lo_d = mid;
+    else hi_d = mid - 1;
+  }
+  const int d = lo_d;
+  const int p0 = start[d] + (tile - tile_start[d]) * kTilePairs;
+  const int np = min(kTilePairs, start[d + 1] - p0);
+  if (threadIdx.x < kTilePairs) {
+    const int r = threadIdx.x;
+    const int pair = r < np ? sorted[p0 + r] : 0;
+    img[r] = pair / kd;
+    out0[r] = (int64_t)(pair / kd) * kd * n_inplane + (int64_t)(pair % kd) * n_inplane;
+  }
+  __syncthreads();
+  if (d >= n_dir) {  // no such direction: zero sums, which score 0
+    for (int e = threadIdx.x; e < np * n_inplane; e += blockDim.x) {
+      num[out0[e / n_inplane] + e % n_inplane] = 0.f;
+      den[out0[e / n_inplane] + e % n_inplane] = 0.f;
     }
     return;
   }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
   const int64_t vn = 2 * kp / 8, vd = kp / 8;  // 16-byte vectors per row
-  const uint4* yb = y16 + b * vn;
-  const uint4* zb = z16 + b * vd;
-  for (int a0 = warp * kDirTemplatesPerPass; a0 < n_inplane; a0 += 8 * kDirTemplatesPerPass) {
-    float accn[kDirTemplatesPerPass], accd[kDirTemplatesPerPass];
-    const uint4* srow[kDirTemplatesPerPass];
-    const uint4* prow[kDirTemplatesPerPass];
+  for (int a0 = 0; a0 < n_inplane; a0 += kNTiles * 8) {
+#pragma unroll 1
+    for (int part = 0; part < 2; ++part) {  // numerators, then denominators
+      const uint4* rows = part ? z16 : y16;
+      const uint4* bank = part ? p16 : s16;
+      const int64_t vrow = part ? vd : vn;
+      const uint4* lo = g < np ? rows + img[g] * vrow : nullptr;
+      const uint4* hi = g + 8 < np ? rows + img[g + 8] * vrow : nullptr;
+      const uint4* tmpl[kNTiles];
 #pragma unroll
-    for (int q = 0; q < kDirTemplatesPerPass; ++q) {
-      accn[q] = accd[q] = 0.f;
-      const int a = min(a0 + q, n_inplane - 1);  // a tail pass recomputes the last template, stored once
-      const int64_t t = (int64_t)d * n_inplane + a;
-      srow[q] = s16 + t * vn;
-      prow[q] = p16 + t * vd;
-    }
-    for (int64_t i = lane; i < vn; i += 32) {
-      const uint4 yv = __ldg(yb + i);
-#pragma unroll
-      for (int q = 0; q < kDirTemplatesPerPass; ++q) accn[q] = dot8(yv, __ldg(srow[q] + i), accn[q]);
-    }
-    for (int64_t i = lane; i < vd; i += 32) {
-      const uint4 zv = __ldg(zb + i);
-#pragma unroll
-      for (int q = 0; q < kDirTemplatesPerPass; ++q) accd[q] = dot8(zv, __ldg(prow[q] + i), accd[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < kDirTemplatesPerPass; ++q) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        accn[q] += __shfl_xor_sync(0xffffffffu, accn[q], o);
-        accd[q] += __shfl_xor_sync(0xffffffffu, accd[q], o);
+      for (int j = 0; j < kNTiles; ++j) {
+        const int a = a0 + 8 * j + g;
+        tmpl[j] = a < n_inplane ? bank + ((int64_t)d * n_inplane + a) * vrow : nullptr;
       }
-      if (lane == 0 && a0 + q < n_inplane) {
-        num[out0 + a0 + q] = accn[q];
-        den[out0 + a0 + q] = accd[q];
+      float acc[kNTiles][4];
+#pragma unroll
+      for (int j = 0; j < kNTiles; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+      tile_dots(lo, hi, tmpl, vrow, warp, t, acc);
+      // accumulator (row g / g + 8, column 2t / 2t + 1) of column tile j
+#pragma unroll
+      for (int j = 0; j < kNTiles; ++j) {
+        red[warp][g][8 * j + 2 * t] = acc[j][0];
+        red[warp][g][8 * j + 2 * t + 1] = acc[j][1];
+        red[warp][g + 8][8 * j + 2 * t] = acc[j][2];
+        red[warp][g + 8][8 * j + 2 * t + 1] = acc[j][3];
       }
+      __syncthreads();
+      float* out = part ? den : num;
+      for (int e = threadIdx.x; e < kTilePairs * kNTiles * 8; e += blockDim.x) {
+        const int r = e / (kNTiles * 8), c = e % (kNTiles * 8);
+        if (r < np && a0 + c < n_inplane) {
+          float s = 0.f;
+#pragma unroll
+          for (int w = 0; w < 8; ++w) s += red[w][r][c];
+          out[out0[r] + a0 + c] = s;
+        }
+      }
+      __syncthreads();
     }
   }
 }
@@ -421,8 +509,9 @@ int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t n, int6
 }
 
 
+// cursor [n_dir + 1], start [n_dir + 2], tile_start [n_dir + 2], sorted pairs [n kd]
 static size_t ncc_directions_workspace_bytes(int64_t n, int kd, int n_dir) {
-  return sizeof(int) * ((size_t)n_dir + 1 + (size_t)n * kd);
+  return sizeof(int) * (3 * ((size_t)n_dir + 2) + (size_t)n * kd);
 }
 
 int cjx_ncc_directions_workspace_size(int64_t n, int kd, int n_dir, size_t* bytes) {
@@ -449,7 +538,9 @@ int cjx_ncc_directions(const void* y16, const void* z16, const void* s16, const 
       return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_directions: rows must be 16-byte aligned");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int* cursor = static_cast<int*>(workspace);
-  int32_t* sorted = cursor + n_dir + 1;
+  int* start = cursor + n_dir + 2;
+  int* tile_start = start + n_dir + 2;
+  int32_t* sorted = tile_start + n_dir + 2;
   const int64_t pairs = n * kd;
   if (int e = cjx::check_cuda(cudaMemsetAsync(cursor, 0, sizeof(int) * ((size_t)n_dir + 1), s), "cudaMemsetAsync"))
     return e;
@@ -457,12 +548,15 @@ int cjx_ncc_directions(const void* y16, const void* z16, const void* s16, const 
   cjx::prof_begin(s);
   cjx::k_dir_count<<<blocks, 256, 0, s>>>(dirs, pairs, n_dir, cursor);
   cjx::k_dir_scan<<<1, 1024, 0, s>>>(cursor, n_dir + 1);
+  cjx::k_dir_tiles<<<1, 1024, 0, s>>>(cursor, n_dir, (int)pairs, start, tile_start);
   cjx::k_dir_scatter<<<blocks, 256, 0, s>>>(dirs, pairs, n_dir, cursor, sorted);
   cjx::prof_end("k_dir_sort", s);
+  // every bin has at most pairs_d / 16 + 1 tiles: a grid of pairs / 16 + n_dir + 1 CTAs covers them
+  const int64_t max_tiles = pairs / cjx::kTilePairs + n_dir + 1;
   cjx::prof_begin(s);
-  cjx::k_ncc_directions<<<(unsigned)pairs, 256, 0, s>>>(
+  cjx::k_ncc_dir_tiles<<<(unsigned)max_tiles, 256, 0, s>>>(
       static_cast<const uint4*>(y16), static_cast<const uint4*>(z16), static_cast<const uint4*>(s16),
-      static_cast<const uint4*>(p16), kp, dirs, sorted, kd, n_dir, n_inplane, num, den);
+      static_cast<const uint4*>(p16), kp, sorted, start, tile_start, kd, n_dir, n_inplane, num, den);
   cjx::prof_end("k_ncc_directions", s);
   return cjx::check_cuda(cudaGetLastError(), "ncc_directions launch");
 }

@@ -509,10 +509,12 @@ CJX_API int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t
  *   num[b][k n_inplane + a] = y16[b] . s16[t] (K = 2 kp),
  *   den[b][k n_inplane + a] = z16[b] . p16[t] (K = kp),
  * the inputs of cjx_ncc_argmax / cjx_ncc_topk over kd n_inplane columns
- * (kp = Py (Px/2+1), a multiple of 8; rows 16-byte aligned).  The (image,
- * slot) pairs are processed in direction order, so the images proposing
- * one direction read its template rows from L2 together.  A direction
- * outside [0, n_dir) gives zero sums.  workspace:
+ * (kp = Py (Px/2+1), a multiple of 8; rows 16-byte aligned; s16 / p16
+ * hold n_dir n_inplane rows).  The (image, slot) pairs are sorted by
+ * direction and taken 16 at a time with that direction's templates: FP16
+ * products, FP32 sums on the tensor cores (mma.sync m16n8k16), each
+ * template row read once per 16 pairs.  A direction outside [0, n_dir)
+ * gives zero sums.  workspace:
  * cjx_ncc_directions_workspace_size bytes.  No counterpart in the reference
  * (its search simulates every candidate).                                   */
 CJX_API int cjx_ncc_directions_workspace_size(int64_t n, int kd, int n_dir, size_t* bytes);
