@@ -36,6 +36,7 @@ def _torch():
 
 CONV_CHANNELS = (1, 32, 64, 128, 128, 256, 256)
 HIDDEN = 512
+INFER_BATCH = 2048  # largest batch of one proposal forward pass
 
 
 def _round8(x):
@@ -143,18 +144,27 @@ class PoseProposalNet:
         self.step_count = int(sd.get("step", 0))
 
     # ---- buffers ----------------------------------------------------------
-    def _alloc(self, B):
+    def _forward_buffers(self, B):
+        """Input, im2col, activation and logit buffers of a forward pass over up to B images."""
         torch = _torch()
         bf, f32 = dict(device=self.device, dtype=torch.bfloat16), dict(device=self.device, dtype=torch.float32)
         S = self.image_size
-        self.x0 = torch.empty((B, S, S), **bf)
-        self.acts, self.cols = [self.x0], []
+        x0 = torch.empty((B, S, S), **bf)
+        acts, cols = [x0], []
         for L in self.layers[:6]:
             ho = L["h"] // 2
-            self.cols.append(torch.empty((B * ho * ho, L["ldk"]), **bf))
-            self.acts.append(torch.empty((B, ho, ho, L["cout"]), **bf))
-        self.h1 = torch.empty((B, HIDDEN), **bf)
-        self.logits = torch.empty((B, self.n_classes), **f32)
+            cols.append(torch.empty((B * ho * ho, L["ldk"]), **bf))
+            acts.append(torch.empty((B, ho, ho, L["cout"]), **bf))
+        return dict(B=B, x0=x0, acts=acts, cols=cols, h1=torch.empty((B, HIDDEN), **bf),
+                    logits=torch.empty((B, self.n_classes), **f32))
+
+    def _alloc(self, B):
+        torch = _torch()
+        bf, f32 = dict(device=self.device, dtype=torch.bfloat16), dict(device=self.device, dtype=torch.float32)
+        self._fwd = self._forward_buffers(B)
+        self.x0, self.acts, self.cols = self._fwd["x0"], self._fwd["acts"], self._fwd["cols"]
+        self.h1, self.logits = self._fwd["h1"], self._fwd["logits"]
+        self._infer = None  # forward-only buffers for larger inference batches (propose)
         # backward scratch (sized for the largest layer)
         self.dlogits = torch.empty((B, self.n_classes), **bf)
         self.loss_rows = torch.empty(B, **f32)
@@ -168,26 +178,31 @@ class PoseProposalNet:
         self._B = B
 
     # ---- forward ----------------------------------------------------------
-    def forward(self, x_bf16=None, *, B=None, stream=None):
-        """Logits [B][n_classes] (FP32) for the images in self.x0[:B] (or x_bf16 copied there)."""
-        B = self._B if B is None else B
-        if B > self._B or B % 8:
-            raise ValueError(f"batch {B} must be a multiple of 8 and <= {self._B}")
+    def forward(self, x_bf16=None, *, B=None, stream=None, buffers=None):
+        """Logits [B][n_classes] (FP32) for the images in x0[:B] (or x_bf16 copied there) of `buffers`
+        (default: the training buffers, which backward reads)."""
+        buf = self._fwd if buffers is None else buffers
+        cap = buf["B"]
+        B = cap if B is None else B
+        if B > cap or B % 8:
+            raise ValueError(f"batch {B} must be a multiple of 8 and <= {cap}")
+        x0, acts, cols = buf["x0"], buf["acts"], buf["cols"]
         if x_bf16 is not None:
-            self.x0[:B].copy_(x_bf16.reshape(B, self.image_size, self.image_size))
+            x0[:B].copy_(x_bf16.reshape(B, self.image_size, self.image_size))
         for i, L in enumerate(self.layers[:6]):
             ho = L["h"] // 2
             npix = B * ho * ho
-            nat.cnn_im2col(self.acts[i], B, L["h"], L["w"], L["cin"], self.cols[i], L["ldk"], stream=stream)
-            nat.gemm(self.cols[i], L["W"], self.acts[i + 1].view(-1, L["cout"]), m=npix, n=L["cout"], k=L["K"],
+            nat.cnn_im2col(acts[i], B, L["h"], L["w"], L["cin"], cols[i], L["ldk"], stream=stream)
+            nat.gemm(cols[i], L["W"], acts[i + 1].view(-1, L["cout"]), m=npix, n=L["cout"], k=L["K"],
                      bias=self.bias(i),
                      flags=nat.CJX_GEMM_RELU | nat.CJX_GEMM_OUT_BF16, stream=stream)
         L6, L7 = self.layers[6], self.layers[7]
-        feat = self.acts[6].view(self._B, -1)
-        nat.gemm(feat, L6["W"], self.h1, m=B, n=HIDDEN, k=L6["K"], bias=self.bias(6),
+        feat = acts[6].view(cap, -1)
+        nat.gemm(feat, L6["W"], buf["h1"], m=B, n=HIDDEN, k=L6["K"], bias=self.bias(6),
                  flags=nat.CJX_GEMM_RELU | nat.CJX_GEMM_OUT_BF16, stream=stream)
-        nat.gemm(self.h1, L7["W"], self.logits, m=B, n=self.n_classes, k=L7["K"], bias=self.bias(7), stream=stream)
-        return self.logits[:B]
+        nat.gemm(buf["h1"], L7["W"], buf["logits"], m=B, n=self.n_classes, k=L7["K"], bias=self.bias(7),
+                 stream=stream)
+        return buf["logits"][:B]
 
     # ---- backward -----------------------------------------------------------
     def backward(self, labels, *, B=None, neighbours=None, smoothing=0.0, stream=None):
@@ -264,16 +279,27 @@ class PoseProposalNet:
         """
         torch = _torch()
         n = images.shape[0]
-        batch = self._B if batch is None else min(batch, self._B)
+        # batches beyond the training buffers' size use forward-only buffers of up to INFER_BATCH images
+        # (about 1.7 MB each at 128^2), allocated once: fewer, larger GEMMs per layer
+        want = _round8(min(max(n, 1), INFER_BATCH)) if batch is None else _round8(batch)
+        if want <= self._B:
+            buf = self._fwd
+        else:
+            if self._infer is None or self._infer["B"] < want:
+                self._infer = None
+                self._infer = self._forward_buffers(want)
+            buf = self._infer
+        batch = buf["B"] if batch is None else min(batch, buf["B"])
+        x0 = buf["x0"]
         dirs = torch.empty((n, k), dtype=torch.int32, device=self.device)
         cand = torch.empty((n, k * n_inplane), dtype=torch.int32, device=self.device)
         for s in range(0, n, batch):
             cnt = min(batch, n - s)
             b8 = _round8(cnt)
-            nat.cnn_noisy_normalize(images[s:s + cnt].contiguous(), self.x0, n=cnt, stream=stream)
+            nat.cnn_noisy_normalize(images[s:s + cnt].contiguous(), x0, n=cnt, stream=stream)
             if b8 > cnt:
-                self.x0[cnt:b8].zero_()
-            self.forward(B=b8, stream=stream)
-            nat.topk_candidates(self.logits, k, n_inplane, dirs=dirs[s:s + cnt], candidates=cand[s:s + cnt], B=cnt,
+                x0[cnt:b8].zero_()
+            logits = self.forward(B=b8, stream=stream, buffers=buf)
+            nat.topk_candidates(logits, k, n_inplane, dirs=dirs[s:s + cnt], candidates=cand[s:s + cnt], B=cnt,
                                 stream=stream)
         return dirs, cand
