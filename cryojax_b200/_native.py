@@ -310,6 +310,17 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "cjx_pack_observed32": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "cjx_ncc_rerank32": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "cjx_ncc_directions_workspace_size": (
         ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "cjx_ncc_directions": (
@@ -700,6 +711,23 @@ def ncc_topk(num, den, n, T, oo, yinv, zinv, k, indices, stream=None) -> None:
     _check(load_library().cjx_ncc_topk(
         _cuda_ptr(num, "num"), _cuda_ptr(den, "den"), int(num.stride(0)), int(n), int(T), _cuda_ptr(oo, "oo"),
         _cuda_ptr(yinv, "yinv"), _cuda_ptr(zinv, "zinv"), int(k), _cuda_ptr(indices, "indices"), _stream_ptr(stream)))
+
+
+def pack_observed32(observed, params, py, px, flags, y32, z32, oo, stream=None) -> None:
+    """cjx_pack_observed32: unscaled FP32 NCC terms of each observed image (complex64 y32, float z32, oo)."""
+    _check(load_library().cjx_pack_observed32(
+        _cuda_ptr(observed, "observed"), _cuda_ptr(params, "params"), int(observed.shape[0]), int(py), int(px),
+        int(flags), _cuda_ptr(y32, "y32"), _cuda_ptr(z32, "z32"), _cuda_ptr(oo, "oo"), _stream_ptr(stream)))
+
+
+def ncc_rerank32(bank, py, px, y32, z32, oo, candidates, best_score, best_orientation, *, scores=None,
+                 stream=None) -> None:
+    """cjx_ncc_rerank32: FP32 NCC of each image against its candidates [n, m] from the FP32 template bank."""
+    n, m = int(candidates.shape[0]), int(candidates.shape[1])
+    _check(load_library().cjx_ncc_rerank32(
+        _cuda_ptr(bank, "bank"), int(py), int(px), int(bank.shape[0]), _cuda_ptr(y32, "y32"), _cuda_ptr(z32, "z32"),
+        _cuda_ptr(oo, "oo"), n, _cuda_ptr(candidates, "candidates"), m, _opt_ptr(scores, "scores"),
+        _cuda_ptr(best_score, "best_score"), _cuda_ptr(best_orientation, "best_orientation"), _stream_ptr(stream)))
 
 
 def ncc_directions_workspace_size(n: int, kd: int, n_dir: int) -> int:

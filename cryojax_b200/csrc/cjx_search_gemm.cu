@@ -17,6 +17,8 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
 
 #include "cjx_common.cuh"
 #include "cjx_profile.cuh"
@@ -112,6 +114,95 @@ __global__ void k_pack_observed(const float2* __restrict__ obs, const cjx_image_
   }
 }
 
+// Most candidates per image that the top-m selection and the FP32 re-ranking take.
+constexpr int kTopMMax = 16;
+
+// Per observed image (block): the same NCC terms in FP32 and unscaled,
+//   y32 = w conj(m) O (complex), z32 = w |m|^2, oo = sum w |O|^2,
+// for the re-ranking against the FP32 template bank (k_ncc_rerank32).
+__global__ void k_pack_observed32(const float2* __restrict__ obs, const cjx_image_params* __restrict__ params,
+                                  int py, int px, uint32_t flags, float2* __restrict__ y32, float* __restrict__ z32,
+                                  float* __restrict__ oo) {
+  __shared__ float red[32];
+  const int pxh = px / 2 + 1;
+  const int kp = py * pxh;
+  const float2* o = obs + (size_t)blockIdx.x * kp;
+  float2* yo = y32 + (size_t)blockIdx.x * kp;
+  float* zo = z32 + (size_t)blockIdx.x * kp;
+  const ImageConsts c = load_image_consts(params + blockIdx.x, 1.0f, py, px);
+  float ao = 0.f;
+  for (int e = threadIdx.x; e < kp; e += blockDim.x) {
+    const int i = e / pxh, j = e - (e / pxh) * pxh;
+    const float w = (i == 0 && j == 0) ? 0.f : (self_conj_col(j, px) ? 1.f : 2.f);
+    const float2 m = apply_epilogue(make_float2(1.f, 0.f), i, j, py, px, flags, c);
+    const float2 v = o[e];
+    yo[e] = make_float2(w * (m.x * v.x + m.y * v.y), w * (m.x * v.y - m.y * v.x));
+    zo[e] = w * (m.x * m.x + m.y * m.y);
+    ao += w * (v.x * v.x + v.y * v.y);
+  }
+  const float to = block_sum_f(ao, red);
+  if (threadIdx.x == 0) oo[blockIdx.x] = to;
+}
+
+// Per observed image (block of 256; warp r takes candidates r, r + 8, ..):
+// FP32 NCC against each of its m candidate templates, read from the FP32
+// bank of CTF-free slices [T][Py][Px/2+1] with the self-conjugate columns
+// Hermitian-fixed as in the FP16 rows:
+//   num = sum y32 . S, den = sum z32 |S|^2, NCC = num / sqrt(den oo)
+// (0 when den or oo is 0; -inf for a candidate index outside [0, T)).  The
+// best (ties -> lower template index) -> best_score[b], best_orient[b];
+// every candidate's NCC -> scores[b][r] when scores is not NULL.
+__global__ void __launch_bounds__(256)
+    k_ncc_rerank32(const float2* __restrict__ bank, int py, int px, int64_t T, const float2* __restrict__ y32,
+                   const float* __restrict__ z32, const float* __restrict__ oo, const int32_t* __restrict__ cand,
+                   int m, float* __restrict__ scores, float* __restrict__ best_score,
+                   int32_t* __restrict__ best_orient) {
+  __shared__ float sc[kTopMMax];
+  const int64_t b = blockIdx.x;
+  const int pxh = px / 2 + 1;
+  const int kp = py * pxh;
+  const float2* yb = y32 + b * kp;
+  const float* zb = z32 + b * kp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = warp; r < m; r += (int)(blockDim.x >> 5)) {
+    const int32_t t = cand[b * m + r];
+    float s = -INFINITY;
+    if (t >= 0 && (int64_t)t < T) {
+      const float2* S = bank + (size_t)t * kp;
+      float num = 0.f, den = 0.f;
+      for (int e = lane; e < kp; e += 32) {
+        const int i = e / pxh, j = e - i * pxh;
+        const float2 v = sym_value(S, i, j, py, px, pxh);
+        const float2 y = yb[e];
+        num = fmaf(v.x, y.x, fmaf(v.y, y.y, num));
+        den = fmaf(zb[e], v.x * v.x + v.y * v.y, den);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, o);
+        den += __shfl_xor_sync(0xffffffffu, den, o);
+      }
+      const float o2 = oo[b];
+      s = (den > 0.f && o2 > 0.f) ? (float)((double)num / sqrt((double)den * (double)o2)) : 0.f;
+    }
+    if (lane == 0) sc[r] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float bv = -INFINITY;
+    int32_t bi = m > 0 ? cand[b * m] : 0;
+    for (int r = 0; r < m; ++r) {
+      const int32_t t = cand[b * m + r];
+      if (sc[r] > bv || (sc[r] == bv && t < bi)) {
+        bv = sc[r];
+        bi = t;
+      }
+    }
+    best_score[b] = bv;
+    best_orient[b] = bi;
+  }
+  if (scores && threadIdx.x < m) scores[b * m + threadIdx.x] = sc[threadIdx.x];
+}
+
 // Per image row (block): NCC over the T templates and its argmax (ties ->
 // lowest index); optional scores out.
 __global__ void k_ncc_argmax(const float* __restrict__ num, const float* __restrict__ den, int64_t ld,
@@ -166,7 +257,6 @@ __global__ void k_ncc_argmax(const float* __restrict__ num, const float* __restr
 // templates (descending; ties -> lower index) -> idx_out[b][0..m).  Each
 // thread keeps a sorted list of its best m, the block merges the lists in
 // shared memory and one warp selects the final m.
-constexpr int kTopMMax = 16;
 
 __device__ __forceinline__ bool key_gt(float a, int32_t ia, float b, int32_t ib) {
   return a > b || (a == b && ia < ib);
@@ -481,6 +571,39 @@ int cjx_pack_observed(const void* observed, const cjx_image_params* params, int6
       static_cast<const float2*>(observed), params, py, px, (uint32_t)flags, static_cast<__half*>(y16),
       static_cast<__half*>(z16), oo, yinv, zinv);
   return cjx::check_cuda(cudaGetLastError(), "pack_observed launch");
+}
+
+int cjx_pack_observed32(const void* observed, const cjx_image_params* params, int64_t n, int py, int px, int flags,
+                        void* y32, float* z32, float* oo, void* stream) {
+  if (n < 0 || py < 2 || px < 2) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_observed32: bad shape");
+  if (n == 0) return CJX_OK;
+  if (!observed || !params || !y32 || !z32 || !oo)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_observed32: NULL pointer");
+  if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "pack_observed32: too many images");
+  cjx::k_pack_observed32<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const float2*>(observed), params, py, px, (uint32_t)flags, static_cast<float2*>(y32), z32, oo);
+  return cjx::check_cuda(cudaGetLastError(), "pack_observed32 launch");
+}
+
+int cjx_ncc_rerank32(const void* bank, int py, int px, int64_t T, const void* y32, const float* z32, const float* oo,
+                     int64_t n, const int32_t* candidates, int m, float* scores, float* best_score,
+                     int32_t* best_orientation, void* stream) {
+  if (n < 0 || py < 2 || px < 2 || T < 1 || m < 1 || m > cjx::kTopMMax)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_rerank32: need 1 <= m <= 16, T >= 1 and a valid shape");
+  if (n == 0) return CJX_OK;
+  if (!bank || !y32 || !z32 || !oo || !candidates || !best_score || !best_orientation)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_rerank32: NULL pointer");
+  if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "ncc_rerank32: too many images");
+  for (const void* ptr : {bank, y32})
+    if (reinterpret_cast<uintptr_t>(ptr) % 8)
+      return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_rerank32: complex arrays must be 8-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cjx::prof_begin(s);
+  cjx::k_ncc_rerank32<<<(unsigned)n, 256, 0, s>>>(static_cast<const float2*>(bank), py, px, T,
+                                                  static_cast<const float2*>(y32), z32, oo, candidates, m, scores,
+                                                  best_score, best_orientation);
+  cjx::prof_end("k_ncc_rerank32", s);
+  return cjx::check_cuda(cudaGetLastError(), "ncc_rerank32 launch");
 }
 
 int cjx_ncc_argmax(const float* num, const float* den, int64_t ld, int64_t n, int64_t T, const float* oo,

@@ -233,16 +233,27 @@ class TemplateSharingSearch:
     cjx_ncc_argmax).  Exact in real arithmetic; FP16 operands make the scores
     approximate (about 1e-3 relative), so near-ties may resolve differently
     from PoseSearch.  Needs padded_shape == shape and Py a multiple of 8.
+
+    ``rerank`` chooses how the ``rerank_top`` best FP16 candidates of each
+    image are rescored in FP32: ``"bank"`` (default) from the templates' own
+    FP32 simulations, kept as a bank beside the FP16 rows (T Py (Px/2+1)
+    complex64, 2.4 GB at 128^2 for 36,864 orientations), the same NCC as
+    PoseSearch's up to FP32 rounding; ``"simulate"`` by PoseSearch with
+    candidate lists, which simulates each candidate again and returns its
+    scores bit for bit.
     """
 
-    def __init__(self, rotations, *, device="cuda", template_chunk=4096, image_chunk=4096):
+    def __init__(self, rotations, *, device="cuda", template_chunk=4096, image_chunk=4096, rerank="bank"):
         torch = _torch()
+        if rerank not in ("bank", "simulate"):
+            raise ValueError("rerank must be 'bank' or 'simulate'")
         self.rot = np.ascontiguousarray(np.asarray(rotations, np.float64).reshape(-1, 9))
         self.n_orientations = self.rot.shape[0]
         self.device = torch.device(device)
         self.template_chunk = template_chunk
         self.image_chunk = image_chunk
-        self.s16 = self.p16 = None
+        self.rerank = rerank
+        self.s16 = self.p16 = self.t32 = None
         self._key = None
 
     def build_templates(self, image_model):
@@ -278,11 +289,17 @@ class TemplateSharingSearch:
         p[:, nat.P_SCALE] = 1.0
         pd = torch.as_tensor(p, device=self.device)
         tc = min(self.template_chunk, T)
-        buf = torch.empty((tc, py, px // 2 + 1), dtype=torch.complex64, device=self.device)
+        if self.rerank == "bank":  # the simulations themselves are the FP32 bank
+            if self.t32 is None or tuple(self.t32.shape) != (T, py, px // 2 + 1):
+                self.t32 = None
+                self.t32 = torch.empty((T, py, px // 2 + 1), dtype=torch.complex64, device=self.device)
+            buf = None
+        else:
+            buf = torch.empty((tc, py, px // 2 + 1), dtype=torch.complex64, device=self.device)
         ws = None
         for s in range(0, T, tc):
             e = min(T, s + tc)
-            out = buf[:e - s]
+            out = self.t32[s:e] if buf is None else buf[:e - s]
             integ.run(vol, cfg, None, 0, params_device=pd[s:e], out=out, workspace=ws, n=e - s)
             nat.pack_templates(out, py, px, self.s16[s:e], self.p16[s:e])
         self._key = key
@@ -301,7 +318,25 @@ class TemplateSharingSearch:
         return y16, z16, oo, yinv, zinv
 
     def _rerank(self, image_model, obs_f, pd, top):
-        """FP32 scores (PoseSearch with candidate lists) of the (n, m) template indices `top`."""
+        """FP32 best of the (n, m) template indices `top` per image: from the FP32 bank, or by PoseSearch with
+        candidate lists."""
+        if self.rerank == "bank" and self.t32 is not None:
+            torch = _torch()
+            cfg = image_model.image_config
+            py, px = cfg.padded_shape
+            n = obs_f.shape[0]
+            dev = self.device
+            best_score = torch.empty(n, dtype=torch.float32, device=dev)
+            best = torch.empty(n, dtype=torch.int32, device=dev)
+            mc = min(self.image_chunk, n)
+            y32 = torch.empty((mc, py, px // 2 + 1), dtype=torch.complex64, device=dev)
+            z32 = torch.empty((mc, py, px // 2 + 1), dtype=torch.float32, device=dev)
+            oo = torch.empty(mc, dtype=torch.float32, device=dev)
+            for s in range(0, n, mc):
+                e = min(n, s + mc)
+                nat.pack_observed32(obs_f[s:e], pd[s:e], py, px, image_model._flags(), y32, z32, oo)
+                nat.ncc_rerank32(self.t32, py, px, y32, z32, oo, top[s:e], best_score[s:e], best[s:e])
+            return SearchResult(best.cpu().numpy().astype(np.int64), best_score.cpu().numpy(), None, top)
         if getattr(self, "_plain", None) is None:
             self._plain = PoseSearch(self.rot, device=self.device)
         return self._plain.run(image_model, obs_f, candidates=top, observed_is_fourier=True, image_params_device=pd)

@@ -503,6 +503,26 @@ CJX_API int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t
                          const float* oo, const float* yinv, const float* zinv, int k,
                          int32_t* indices, void* stream);
 
+/* FP32 re-ranking from a bank of the templates' FP32 simulations instead
+ * of simulating each candidate again.  cjx_pack_observed32 writes each
+ * image's unscaled FP32 terms y32 = w conj(m) O (complex64 [n][Py][Px/2+1]),
+ * z32 = w |m|^2 (float [n][Py][Px/2+1]) and oo = sum w |O|^2 (same w and m
+ * as cjx_pack_observed).  cjx_ncc_rerank32 scores image b against its m
+ * <= 16 candidates candidates[b][0..m) from bank (complex64 [T][Py][Px/2+1],
+ * the CTF-free simulations cjx_pack_templates packs):
+ *   NCC = sum y32 . S / sqrt(sum z32 |S|^2 * oo)
+ * with S the Hermitian-fixed template, FP32 sums (-inf for an index outside
+ * [0, T)); the best (ties -> lower index) goes to best_score /
+ * best_orientation and every NCC to scores[b][0..m) when scores is not
+ * NULL.  The same NCC as the simulating scorer's up to FP32 rounding.      */
+CJX_API int cjx_pack_observed32(const void* observed, const cjx_image_params* params, int64_t n,
+                                int py, int px, int flags, void* y32, float* z32, float* oo,
+                                void* stream);
+CJX_API int cjx_ncc_rerank32(const void* bank, int py, int px, int64_t T, const void* y32,
+                             const float* z32, const float* oo, int64_t n,
+                             const int32_t* candidates, int m, float* scores, float* best_score,
+                             int32_t* best_orientation, void* stream);
+
 /* The learned search's rescoring from the same template rows: for image b
  * and proposed-direction slot k (dirs [n][kd], int32), the n_inplane
  * templates t = dirs[b][k] n_inplane + a (a in [0, n_inplane)) give

@@ -117,7 +117,7 @@ def test_template_row_scoring_matches_simulated_candidates(setup):
     V, cfg, grid, net = setup
     model, noisy = _batch(V, cfg, 128, 13, 0.1)
     search = PoseSearch(grid.rotation_matrices())
-    shared = TemplateSharingSearch(grid.rotation_matrices())
+    shared = TemplateSharingSearch(grid.rotation_matrices(), rerank="simulate")
     sim = LearnedPoseSearch(net, grid, top_k=8, search=search).run(model, noisy, fallback=False)
     tmpl = LearnedPoseSearch(net, grid, top_k=8, search=search, templates=shared, rerank_top=8).run(
         model, noisy, fallback=False)
@@ -125,6 +125,13 @@ def test_template_row_scoring_matches_simulated_candidates(setup):
     assert agree >= 0.99, agree
     same = sim.best_orientation == tmpl.best_orientation
     np.testing.assert_array_equal(sim.best_score[same], tmpl.best_score[same])
+    # the re-ranking from the FP32 template bank (the default): the same answers, scores to FP32 rounding
+    bank = LearnedPoseSearch(net, grid, top_k=8, search=search, templates=TemplateSharingSearch(
+        grid.rotation_matrices()), rerank_top=8).run(model, noisy, fallback=False)
+    agree_b = float(np.mean(bank.best_orientation == tmpl.best_orientation))
+    assert agree_b >= 0.99, agree_b
+    same_b = bank.best_orientation == tmpl.best_orientation
+    np.testing.assert_allclose(bank.best_score[same_b], tmpl.best_score[same_b], rtol=1e-5, atol=1e-7)
 
     # FP16 candidate sums against the exhaustive template GEMM's scores of the same templates
     obs_f = observed_to_fourier(noisy)
