@@ -65,7 +65,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the mixed-size batch measurement")
     ap.add_argument("--no-grad", action="store_true", help="skip the loss-gradient measurement")
     ap.add_argument("--no-search", action="store_true", help="skip the pose-search (learned vs grid) measurement")
-    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline", "ewald", "render"], default=None,
+    ap.add_argument("--probe", choices=["gemm", "search", "cnn", "spline", "ewald", "render", "ncc"], default=None,
                     help="run one small workload of that kernel family (for a profiler), print its timing, exit")
     ap.add_argument("--no-refine", action="store_true",
                     help="skip the search + refinement measurement (320^2 images, N=512)")
@@ -1209,6 +1209,42 @@ def run_probe(kind, seed):
         ps = PoseSearch(grid.rotation_matrices())
         ms = ev_time(lambda: ps.run(model, obs))
         out["plain_exhaustive_8_images"] = {"ms": ms, "candidates_per_s": 8 * grid.size / (ms / 1000.0)}
+    elif kind == "ncc":
+        # the learned search's candidate sums (cjx_ncc_directions) and FP32 bank re-ranking (cjx_ncc_rerank32) at
+        # the pose-search sizes: 4096 images 128^2 (kp = 128 x 65), 16 proposed directions of 768 x 48 in-plane
+        # templates, 8 re-ranked candidates per image; random FP16 / FP32 rows (two warm-up runs, one timed)
+        g = torch.Generator(device=dev).manual_seed(seed)
+        n, kd, n_dir, ni, py, px = 4096, 16, 768, 48, 128, 128
+        kp = py * (px // 2 + 1)
+        T = n_dir * ni
+        y16 = torch.randn((n, 2 * kp), generator=g, device=dev).half()
+        z16 = torch.rand((n, kp), generator=g, device=dev).half()
+        s16 = torch.randn((T, 2 * kp), generator=g, device=dev).half()
+        p16 = torch.rand((T, kp), generator=g, device=dev).half()
+        dirs = torch.randint(0, n_dir, (n, kd), generator=g, device=dev, dtype=torch.int32)
+        num = torch.empty((n, kd * ni), device=dev)
+        den = torch.empty_like(num)
+        ws = torch.empty(nat.ncc_directions_workspace_size(n, kd, n_dir), dtype=torch.uint8, device=dev)
+        run = lambda: nat.ncc_directions(y16, z16, s16, p16, kp, dirs, n_dir, ni, num, den, ws)
+        for _ in range(2):
+            run()
+        ms = ev_time(run)
+        flop = 2.0 * n * kd * ni * 3 * kp
+        out["ncc_directions"] = {"ms": ms, "tflops": flop / ms / 1e9}
+        del s16, p16
+        bank = torch.randn((T, py, px // 2 + 1), generator=g, device=dev, dtype=torch.complex64)
+        y32 = torch.randn((n, py, px // 2 + 1), generator=g, device=dev, dtype=torch.complex64)
+        z32 = torch.rand((n, py, px // 2 + 1), generator=g, device=dev)
+        oo = torch.rand(n, generator=g, device=dev) + 1.0
+        cand = torch.randint(0, T, (n, 8), generator=g, device=dev, dtype=torch.int32)
+        bs = torch.empty(n, device=dev)
+        bo = torch.empty(n, dtype=torch.int32, device=dev)
+        run = lambda: nat.ncc_rerank32(bank, py, px, y32, z32, oo, cand, bs, bo)
+        for _ in range(2):
+            run()
+        ms = ev_time(run)
+        out["ncc_rerank32"] = {"ms": ms, "bank_bytes_read_per_run": n * 8 * kp * 8,
+                               "gbs": n * 8 * kp * 8 / ms / 1e6}
     elif kind == "render":
         # GaussianMixtureRenderFn: 50k atoms x 5 Gaussians into 256^3 at 1 A (two warm-up launches, one timed)
         rng = np.random.default_rng(seed)
