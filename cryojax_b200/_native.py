@@ -251,6 +251,11 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
          ctypes.c_void_p],
     ),
+    "cjx_cnn_conv0": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "cjx_cnn_im2col": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
@@ -633,6 +638,12 @@ def area_downsample(src, dst, stream=None) -> None:
 def cnn_im2col(x, B, H, W, C, col, ldk, stream=None) -> None:
     _check(load_library().cjx_cnn_im2col(_cuda_ptr(x, "x"), int(B), int(H), int(W), int(C), _cuda_ptr(col, "col"),
                                          int(ldk), _stream_ptr(stream)))
+
+
+def cnn_conv0(x, B, H, W, w, ldk, cout, bias, y, stream=None) -> None:
+    """cjx_cnn_conv0: first 3x3 stride-2 layer (one input channel) + bias + ReLU without im2col."""
+    _check(load_library().cjx_cnn_conv0(_cuda_ptr(x, "x"), int(B), int(H), int(W), _cuda_ptr(w, "w"), int(ldk),
+                                        int(cout), _opt_ptr(bias, "bias"), _cuda_ptr(y, "y"), _stream_ptr(stream)))
 
 
 def cnn_col2im(dcol, ldk, act, B, H, W, C, dx, stream=None) -> None:

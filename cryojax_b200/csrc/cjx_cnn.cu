@@ -8,6 +8,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "cjx_common.cuh"
 
@@ -152,6 +153,51 @@ __global__ void k_im2col_s2(const bf16* __restrict__ x, int B, int H, int W, int
       v = *reinterpret_cast<const uint4*>(h);
     }
     *reinterpret_cast<uint4*>(col + p * ldk + k0) = v;
+  }
+}
+
+// First layer at inference: 3x3 stride-2 convolution of a one-channel BF16
+// image (zero padding 1) into COUT channels, + bias, ReLU, BF16 NHWC out,
+// with no im2col matrix: what im2col + the tensor-core GEMM compute for
+// that layer (weights w [COUT][ldk], tap k = 3 dy + dx), one output pixel
+// per thread.  BF16 products are exact in FP32; the 9 taps are summed in
+// tap order, then the bias is added, as the GEMM epilogue adds it.
+template <int COUT>
+__global__ void __launch_bounds__(256, 4)
+    k_conv0_s2(const bf16* __restrict__ x, int B, int H, int W, const bf16* __restrict__ w, int ldk,
+               const float* __restrict__ bias, bf16* __restrict__ y) {
+  __shared__ float ws[9][COUT];
+  __shared__ float bs[COUT];
+  for (int e = threadIdx.x; e < 9 * COUT; e += blockDim.x) ws[e / COUT][e % COUT] = __bfloat162float(w[(e % COUT) * ldk + e / COUT]);
+  for (int c = threadIdx.x; c < COUT; c += blockDim.x) bs[c] = bias ? bias[c] : 0.f;
+  __syncthreads();
+  const int Ho = H / 2, Wo = W / 2;
+  const int64_t total = (int64_t)B * Ho * Wo;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
+    const int ox = (int)(p % Wo);
+    const int64_t t = p / Wo;
+    const int oy = (int)(t % Ho);
+    const int64_t b = t / Ho;
+    float in[9];
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const int iy = 2 * oy + tap / 3 - 1, ix = 2 * ox + tap % 3 - 1;
+      in[tap] = (iy >= 0 && ix >= 0 && iy < H && ix < W) ? __bfloat162float(x[((size_t)b * H + iy) * W + ix]) : 0.f;
+    }
+    uint4* dst = reinterpret_cast<uint4*>(y + (size_t)p * COUT);
+#pragma unroll 1
+    for (int c8 = 0; c8 < COUT / 8; ++c8) {
+      __align__(16) bf16 o[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int c = 8 * c8 + q;
+        float acc = 0.f;
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) acc = fmaf(in[tap], ws[tap][c], acc);
+        o[q] = __float2bfloat16_rn(fmaxf(acc + bs[c], 0.f));
+      }
+      dst[c8] = *reinterpret_cast<const uint4*>(o);
+    }
   }
 }
 
@@ -404,6 +450,19 @@ int cjx_cnn_im2col(const void* x, int64_t B, int H, int W, int C, void* col, int
     cjx::k_im2col_s2<false><<<cjx::grid_for(total, 256), 256, 0, st>>>(static_cast<const bf16*>(x), (int)B, H, W, C,
                                                                        static_cast<bf16*>(col), (int)ldk);
   return cjx::check_cuda(cudaGetLastError(), "im2col launch");
+}
+
+int cjx_cnn_conv0(const void* x, int64_t B, int H, int W, const void* w, int64_t ldk, int cout, const float* bias,
+                  void* y, void* stream) {
+  if (B < 0 || H < 2 || W < 2 || (H & 1) || (W & 1) || ldk < 9 || cout != 32)
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "cnn_conv0 needs even H, W >= 2, ldk >= 9 and cout = 32");
+  if (B == 0) return CJX_OK;
+  if (!x || !w || !y) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "x, w and y must be non-NULL");
+  if (reinterpret_cast<uintptr_t>(y) % 16) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "y must be 16-byte aligned");
+  const int64_t total = B * (H / 2) * (W / 2);
+  cjx::k_conv0_s2<32><<<cjx::grid_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const bf16*>(x), (int)B, H, W, static_cast<const bf16*>(w), (int)ldk, bias, static_cast<bf16*>(y));
+  return cjx::check_cuda(cudaGetLastError(), "cnn_conv0 launch");
 }
 
 int cjx_cnn_col2im(const float* dcol, int64_t ldk, const void* act, int64_t B, int H, int W, int C, void* dx,

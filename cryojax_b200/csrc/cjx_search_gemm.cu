@@ -170,7 +170,8 @@ __global__ void __launch_bounds__(256)
     if (t >= 0 && (int64_t)t < T) {
       const float2* S = bank + (size_t)t * kp;
       float num = 0.f, den = 0.f;
-      for (int e = lane; e < kp; e += 32) {
+#pragma unroll 4
+      for (int e = lane; e < kp; e += 32) {  // unrolled so that several rows' loads are in flight
         const int i = e / pxh, j = e - i * pxh;
         const float2 v = sym_value(S, i, j, py, px, pxh);
         const float2 y = yb[e];

@@ -178,9 +178,10 @@ class PoseProposalNet:
         self._B = B
 
     # ---- forward ----------------------------------------------------------
-    def forward(self, x_bf16=None, *, B=None, stream=None, buffers=None):
+    def forward(self, x_bf16=None, *, B=None, stream=None, buffers=None, direct_first_layer=False):
         """Logits [B][n_classes] (FP32) for the images in x0[:B] (or x_bf16 copied there) of `buffers`
-        (default: the training buffers, which backward reads)."""
+        (default: the training buffers, which backward reads).  ``direct_first_layer`` computes the first
+        convolution without its im2col matrix (inference only: backward reads that matrix)."""
         buf = self._fwd if buffers is None else buffers
         cap = buf["B"]
         B = cap if B is None else B
@@ -192,6 +193,10 @@ class PoseProposalNet:
         for i, L in enumerate(self.layers[:6]):
             ho = L["h"] // 2
             npix = B * ho * ho
+            if i == 0 and direct_first_layer and L["cin"] == 1 and L["cout"] == 32:
+                nat.cnn_conv0(acts[0], B, L["h"], L["w"], L["W"], L["ldk"], L["cout"], self.bias(0), acts[1],
+                              stream=stream)
+                continue
             nat.cnn_im2col(acts[i], B, L["h"], L["w"], L["cin"], cols[i], L["ldk"], stream=stream)
             nat.gemm(cols[i], L["W"], acts[i + 1].view(-1, L["cout"]), m=npix, n=L["cout"], k=L["K"],
                      bias=self.bias(i),
@@ -299,7 +304,7 @@ class PoseProposalNet:
             nat.cnn_noisy_normalize(images[s:s + cnt].contiguous(), x0, n=cnt, stream=stream)
             if b8 > cnt:
                 x0[cnt:b8].zero_()
-            logits = self.forward(B=b8, stream=stream, buffers=buf)
+            logits = self.forward(B=b8, stream=stream, buffers=buf, direct_first_layer=True)
             nat.topk_candidates(logits, k, n_inplane, dirs=dirs[s:s + cnt], candidates=cand[s:s + cnt], B=cnt,
                                 stream=stream)
         return dirs, cand

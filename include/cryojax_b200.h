@@ -590,6 +590,13 @@ CJX_API int cjx_area_downsample(const float* src, int64_t n, int H, int W, float
  * p = (b H/2 + oy) W/2 + ox, k = (3 ky + kx) C + c, zeros in [9C, ldk).    */
 CJX_API int cjx_cnn_im2col(const void* x, int64_t B, int H, int W, int C, void* col,
                            int64_t ldk, void* stream);
+/* The first layer at inference without the im2col matrix: y (BF16
+ * [B][H/2][W/2][cout], 16-byte aligned) = ReLU(conv3x3_s2(x) + bias) for a
+ * one-channel BF16 x [B][H][W], weights w (BF16 [cout][ldk], tap k = 3 ky +
+ * kx) and FP32 bias (may be NULL); cout = 32.  What cjx_cnn_im2col and the
+ * tensor-core GEMM give for that layer, summed in tap order.               */
+CJX_API int cjx_cnn_conv0(const void* x, int64_t B, int H, int W, const void* w, int64_t ldk,
+                          int cout, const float* bias, void* y, void* stream);
 /* dx (BF16 [B][H][W][C]) = col2im(dcol) (FP32 [p][ldk]), multiplied by
  * (act > 0) when act (BF16, same shape as dx) is non-NULL.                 */
 CJX_API int cjx_cnn_col2im(const float* dcol, int64_t ldk, const void* act, int64_t B, int H,

@@ -167,3 +167,30 @@ def test_noisy_normalize(cuda_device):
     np.testing.assert_allclose(r, np.sqrt(0.25 / 1.25), atol=0.03)
     nat.cnn_noisy_normalize(imgs, o2, index=idx, snr=0.25, seed=12, n=4)
     assert not torch.equal(o1, o2)
+
+
+def test_direct_first_layer_matches_im2col_gemm(cuda_device):
+    """The inference path's first layer without im2col (cjx_cnn_conv0) gives the im2col + tensor-core GEMM
+    layer's BF16 activations (equal on >= 99.9 %, else one BF16 step apart where the FP32 sums of the 9 taps
+    round differently), and the proposals of a forward pass built on either agree."""
+    import torch
+
+    from cryojax_b200.pose_net import PoseProposalNet
+
+    net = PoseProposalNet(128, 768, max_batch=64, seed=3)
+    g = torch.Generator(device="cuda").manual_seed(4)
+    x = torch.randn((64, 128, 128), generator=g, device="cuda").to(torch.bfloat16)
+    a = net.forward(x, B=64).clone()
+    act_gemm = net.acts[1].clone()
+    b = net.forward(x, B=64, direct_first_layer=True).clone()
+    act_direct = net.acts[1].clone()
+    ra, rd = act_gemm.float(), act_direct.float()
+    # one BF16 step of the larger value, or (near zero, where the ReLU cuts a sum that cancels) a tiny
+    # fraction of the layer's scale
+    tol = torch.maximum(ra.abs(), rd.abs()) * 2.0 ** -7 + 1e-4 * ra.abs().max()
+    assert ((ra - rd).abs() <= tol).all(), (ra - rd).abs().max()
+    assert (ra == rd).float().mean().item() >= 0.999
+    torch.testing.assert_close(b, a, rtol=2e-2, atol=2e-2 * a.abs().max().item())
+    top_a = torch.topk(a, 16, dim=1).indices.sort(dim=1).values
+    top_b = torch.topk(b, 16, dim=1).indices.sort(dim=1).values
+    assert (top_a == top_b).all(dim=1).float().mean().item() >= 0.9
