@@ -656,6 +656,8 @@ def measure_pose_search(dev, seed, n_obs):
                        "re-ranked in FP32 from the FP32 template bank, template-sharing exhaustive fallback "
                        "(templates prebuilt, as for the template-sharing arm's search time)",
             "fallback_fraction": float(rt.fallback.mean()), "threshold": thr_t,
+            # with the template bank's build counted, as the template-sharing arm's value counts it
+            "value_with_template_bank": n_obs / (t_tmpl + t_lt),
             "agreement_with_plain_exhaustive": float(np.mean(rt.best_orientation[:n_plain] == ex.best_orientation)),
             "agreement_with_template_exhaustive_reranked": float(np.mean(rt.best_orientation == shr.best_orientation)),
             "speedup_vs_template_exhaustive_reranked_search": t_shr / t_lt,
