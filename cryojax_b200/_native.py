@@ -251,6 +251,11 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
          ctypes.c_void_p],
     ),
+    "cjx_cnn_conv_s2": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "cjx_cnn_conv0": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
@@ -644,6 +649,13 @@ def cnn_conv0(x, B, H, W, w, ldk, cout, bias, y, stream=None) -> None:
     """cjx_cnn_conv0: first 3x3 stride-2 layer (one input channel) + bias + ReLU without im2col."""
     _check(load_library().cjx_cnn_conv0(_cuda_ptr(x, "x"), int(B), int(H), int(W), _cuda_ptr(w, "w"), int(ldk),
                                         int(cout), _opt_ptr(bias, "bias"), _cuda_ptr(y, "y"), _stream_ptr(stream)))
+
+
+def cnn_conv_s2(x, B, H, W, C, w, ldk, cout, bias, y, stream=None) -> None:
+    """cjx_cnn_conv_s2: a 3x3 stride-2 layer + bias + ReLU as an implicit GEMM on the tensor cores."""
+    _check(load_library().cjx_cnn_conv_s2(_cuda_ptr(x, "x"), int(B), int(H), int(W), int(C), _cuda_ptr(w, "w"),
+                                          int(ldk), int(cout), _opt_ptr(bias, "bias"), _cuda_ptr(y, "y"),
+                                          _stream_ptr(stream)))
 
 
 def cnn_col2im(dcol, ldk, act, B, H, W, C, dx, stream=None) -> None:

@@ -201,6 +201,99 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
+// D (16 x 8, FP32) += A (16 x 16, BF16) B (16 x 8, BF16) on the tensor cores.
+__device__ __forceinline__ void mma16816_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                              uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// A later layer at inference without the im2col matrix (implicit GEMM):
+// y (BF16 NHWC [B][H/2][W/2][64 NG]) = ReLU(conv3x3_s2(x) + bias) for x
+// (BF16 NHWC [B][H][W][CIN], zero padding 1) and weights w [64 NG][ldk]
+// with k = (3 ky + kx) CIN + c, the im2col order.  Each warp takes 16 output
+// pixels x 64 channels; a CTA's 8 warps cover 8 / NG pixel tiles x NG
+// channel groups.  A K step is one tap's 32 channels: lane (g, t) loads
+// channels [8 t, 8 t + 8) of the tap for pixels g and g + 8 and of the
+// weights for channels g of each 8-wide column tile, and the step's two
+// m16n8k16 products take them as k = {2t, 2t+1, 2t+8, 2t+9}: the same
+// relabelling for both operands, so the sums are the convolution's.  BF16
+// products, FP32 accumulation, then bias, ReLU and BF16 as the GEMM's
+// epilogue.
+template <int CIN, int NG>
+__global__ void __launch_bounds__(256)
+    k_conv_s2_mma(const bf16* __restrict__ x, int B, int H, int W, const bf16* __restrict__ w, int ldk,
+                  const float* __restrict__ bias, bf16* __restrict__ y) {
+  static_assert(CIN % 32 == 0, "one K step is 32 channels of one tap");
+  constexpr int COUT = 64 * NG;
+  constexpr int MT = 8 / NG;  // pixel tiles of 16 per CTA
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int Ho = H / 2, Wo = W / 2;
+  const int64_t total = (int64_t)B * Ho * Wo;
+  const int64_t p0 = (int64_t)blockIdx.x * (16 * MT) + 16 * (warp % MT);
+  const int n0 = 64 * (warp / MT);
+  // this lane's two output pixels (g and g + 8 of the warp's tile)
+  int oy[2], ox[2];
+  int64_t ob[2];
+  bool live[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int64_t p = p0 + g + 8 * h;
+    live[h] = p < total;
+    const int64_t pp = live[h] ? p : 0;
+    ox[h] = (int)(pp % Wo);
+    oy[h] = (int)((pp / Wo) % Ho);
+    ob[h] = pp / ((int64_t)Wo * Ho);
+  }
+  float acc[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll 1
+  for (int tap = 0; tap < 9; ++tap) {
+    const int ky = tap / 3, kx = tap % 3;
+    const bf16* src[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int iy = 2 * oy[h] + ky - 1, ix = 2 * ox[h] + kx - 1;
+      src[h] = (live[h] && iy >= 0 && ix >= 0 && iy < H && ix < W) ? x + ((ob[h] * H + iy) * W + ix) * CIN : nullptr;
+    }
+#pragma unroll 1
+    for (int c0 = 0; c0 < CIN; c0 += 32) {
+      const uint4 al = src[0] ? *reinterpret_cast<const uint4*>(src[0] + c0 + 8 * t) : z;
+      const uint4 ah = src[1] ? *reinterpret_cast<const uint4*>(src[1] + c0 + 8 * t) : z;
+      const int k = tap * CIN + c0 + 8 * t;
+      uint4 b[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = __ldg(reinterpret_cast<const uint4*>(w + (size_t)(n0 + 8 * j + g) * ldk + k));
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        mma16816_bf16(acc[j], al.x, ah.x, al.y, ah.y, b[j].x, b[j].y);
+        mma16816_bf16(acc[j], al.z, ah.z, al.w, ah.w, b[j].z, b[j].w);
+      }
+    }
+  }
+  // accumulator (pixel g / g + 8, channel 8 j + 2 t / + 1): bias, ReLU, BF16 pairs
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (!live[h]) continue;
+    bf16* dst = y + (size_t)(p0 + g + 8 * h) * COUT + n0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = 8 * j + 2 * t;
+      const float b0 = bias ? bias[n0 + c] : 0.f, b1 = bias ? bias[n0 + c + 1] : 0.f;
+      __nv_bfloat162 v;
+      v.x = __float2bfloat16_rn(fmaxf(acc[j][2 * h] + b0, 0.f));
+      v.y = __float2bfloat16_rn(fmaxf(acc[j][2 * h + 1] + b1, 0.f));
+      *reinterpret_cast<__nv_bfloat162*>(dst + c) = v;
+    }
+  }
+}
+
 // dx[b][y][x][c] = sum over the taps that read (y, x) of dcol[p][k], times
 // (act > 0) when act is given (ReLU of the layer that produced x).
 __global__ void k_col2im_s2(const float* __restrict__ dcol, int ldk, const bf16* __restrict__ act, int B, int H,
@@ -463,6 +556,34 @@ int cjx_cnn_conv0(const void* x, int64_t B, int H, int W, const void* w, int64_t
   cjx::k_conv0_s2<32><<<cjx::grid_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const bf16*>(x), (int)B, H, W, static_cast<const bf16*>(w), (int)ldk, bias, static_cast<bf16*>(y));
   return cjx::check_cuda(cudaGetLastError(), "cnn_conv0 launch");
+}
+
+int cjx_cnn_conv_s2(const void* x, int64_t B, int H, int W, int C, const void* w, int64_t ldk, int cout,
+                    const float* bias, void* y, void* stream) {
+  if (B < 0 || H < 2 || W < 2 || (H & 1) || (W & 1) || ldk < 9 * C || (ldk % 8))
+    return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "cnn_conv_s2 needs even H, W >= 2, ldk >= 9 C, ldk % 8 == 0");
+  if (B == 0) return CJX_OK;
+  if (!x || !w || !y) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "x, w and y must be non-NULL");
+  for (const void* ptr : {x, w})
+    if (reinterpret_cast<uintptr_t>(ptr) % 16)
+      return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "cnn_conv_s2: x and w must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(y) % 4) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "y must be 4-byte aligned");
+  const int64_t total = B * (H / 2) * (W / 2);
+  auto st = static_cast<cudaStream_t>(stream);
+  const bf16* xb = static_cast<const bf16*>(x);
+  const bf16* wb = static_cast<const bf16*>(w);
+  bf16* yb = static_cast<bf16*>(y);
+#define CJX_CONV_CASE(CI, NG)                                                                                      \
+  if (C == CI && cout == 64 * NG) {                                                                                \
+    const int64_t ctas = (total + 16 * (8 / NG) - 1) / (16 * (8 / NG));                                            \
+    if (ctas > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "cnn_conv_s2: too many pixels");             \
+    cjx::k_conv_s2_mma<CI, NG><<<(unsigned)ctas, 256, 0, st>>>(xb, (int)B, H, W, wb, (int)ldk, bias, yb);          \
+    return cjx::check_cuda(cudaGetLastError(), "cnn_conv_s2 launch");                                             \
+  }
+  CJX_CONV_CASE(32, 1) CJX_CONV_CASE(64, 2) CJX_CONV_CASE(128, 2) CJX_CONV_CASE(128, 4) CJX_CONV_CASE(256, 4)
+#undef CJX_CONV_CASE
+  return cjx::fail(CJX_ERR_UNSUPPORTED, "cnn_conv_s2: (C, cout) must be (32, 64), (64, 128), (128, 128), "
+                                        "(128, 256) or (256, 256)");
 }
 
 int cjx_cnn_col2im(const float* dcol, int64_t ldk, const void* act, int64_t B, int H, int W, int C, void* dx,

@@ -178,10 +178,12 @@ class PoseProposalNet:
         self._B = B
 
     # ---- forward ----------------------------------------------------------
-    def forward(self, x_bf16=None, *, B=None, stream=None, buffers=None, direct_first_layer=False):
+    def forward(self, x_bf16=None, *, B=None, stream=None, buffers=None, direct_first_layer=False,
+                implicit_convs=False):
         """Logits [B][n_classes] (FP32) for the images in x0[:B] (or x_bf16 copied there) of `buffers`
         (default: the training buffers, which backward reads).  ``direct_first_layer`` computes the first
-        convolution without its im2col matrix (inference only: backward reads that matrix)."""
+        convolution and ``implicit_convs`` the others without their im2col matrices (inference only:
+        backward reads those matrices)."""
         buf = self._fwd if buffers is None else buffers
         cap = buf["B"]
         B = cap if B is None else B
@@ -196,6 +198,10 @@ class PoseProposalNet:
             if i == 0 and direct_first_layer and L["cin"] == 1 and L["cout"] == 32:
                 nat.cnn_conv0(acts[0], B, L["h"], L["w"], L["W"], L["ldk"], L["cout"], self.bias(0), acts[1],
                               stream=stream)
+                continue
+            if i > 0 and implicit_convs:
+                nat.cnn_conv_s2(acts[i], B, L["h"], L["w"], L["cin"], L["W"], L["ldk"], L["cout"], self.bias(i),
+                                acts[i + 1], stream=stream)
                 continue
             nat.cnn_im2col(acts[i], B, L["h"], L["w"], L["cin"], cols[i], L["ldk"], stream=stream)
             nat.gemm(cols[i], L["W"], acts[i + 1].view(-1, L["cout"]), m=npix, n=L["cout"], k=L["K"],
@@ -304,7 +310,7 @@ class PoseProposalNet:
             nat.cnn_noisy_normalize(images[s:s + cnt].contiguous(), x0, n=cnt, stream=stream)
             if b8 > cnt:
                 x0[cnt:b8].zero_()
-            logits = self.forward(B=b8, stream=stream, buffers=buf, direct_first_layer=True)
+            logits = self.forward(B=b8, stream=stream, buffers=buf, direct_first_layer=True, implicit_convs=True)
             nat.topk_candidates(logits, k, n_inplane, dirs=dirs[s:s + cnt], candidates=cand[s:s + cnt], B=cnt,
                                 stream=stream)
         return dirs, cand

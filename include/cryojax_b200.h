@@ -597,6 +597,14 @@ CJX_API int cjx_cnn_im2col(const void* x, int64_t B, int H, int W, int C, void* 
  * tensor-core GEMM give for that layer, summed in tap order.               */
 CJX_API int cjx_cnn_conv0(const void* x, int64_t B, int H, int W, const void* w, int64_t ldk,
                           int cout, const float* bias, void* y, void* stream);
+/* The later layers at inference without the im2col matrix (implicit GEMM
+ * on the tensor cores, mma.sync m16n8k16 BF16 with FP32 accumulation): y
+ * (BF16 NHWC [B][H/2][W/2][cout]) = ReLU(conv3x3_s2(x) + bias) for x (BF16
+ * NHWC [B][H][W][C], 16-byte aligned), weights w (BF16 [cout][ldk], k =
+ * (3 ky + kx) C + c, the cjx_cnn_im2col order) and FP32 bias (may be NULL);
+ * (C, cout) in (32, 64), (64, 128), (128, 128), (128, 256), (256, 256).    */
+CJX_API int cjx_cnn_conv_s2(const void* x, int64_t B, int H, int W, int C, const void* w,
+                            int64_t ldk, int cout, const float* bias, void* y, void* stream);
 /* dx (BF16 [B][H][W][C]) = col2im(dcol) (FP32 [p][ldk]), multiplied by
  * (act > 0) when act (BF16, same shape as dx) is non-NULL.                 */
 CJX_API int cjx_cnn_col2im(const float* dcol, int64_t ldk, const void* act, int64_t B, int H,

@@ -194,3 +194,28 @@ def test_direct_first_layer_matches_im2col_gemm(cuda_device):
     top_a = torch.topk(a, 16, dim=1).indices.sort(dim=1).values
     top_b = torch.topk(b, 16, dim=1).indices.sort(dim=1).values
     assert (top_a == top_b).all(dim=1).float().mean().item() >= 0.9
+
+
+def test_implicit_convolutions_match_im2col_gemm(cuda_device):
+    """The inference path's later layers without im2col (cjx_cnn_conv_s2, implicit GEMM on the tensor cores)
+    give each layer's im2col + GEMM BF16 activations from the same input (equal on >= 99 %, else within one
+    BF16 step or a tiny fraction of the layer's scale), and the network's logits agree."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200.pose_net import PoseProposalNet
+
+    net = PoseProposalNet(128, 768, max_batch=64, seed=5)
+    g = torch.Generator(device="cuda").manual_seed(6)
+    x = torch.randn((64, 128, 128), generator=g, device="cuda").to(torch.bfloat16)
+    a = net.forward(x, B=64).clone()
+    ref = [t.clone() for t in net.acts]
+    for i, L in enumerate(net.layers[1:6], start=1):
+        out = torch.empty_like(ref[i + 1])
+        nat.cnn_conv_s2(ref[i], 64, L["h"], L["w"], L["cin"], L["W"], L["ldk"], L["cout"], net.bias(i), out)
+        ra, rd = ref[i + 1].float(), out.float()
+        tol = torch.maximum(ra.abs(), rd.abs()) * 2.0 ** -7 + 1e-4 * ra.abs().max()
+        assert ((ra - rd).abs() <= tol).all(), (i, (ra - rd).abs().max())
+        assert (ra == rd).float().mean().item() >= 0.99, i
+    b = net.forward(x, B=64, direct_first_layer=True, implicit_convs=True).clone()
+    torch.testing.assert_close(b, a, rtol=2e-2, atol=2e-2 * a.abs().max().item())
