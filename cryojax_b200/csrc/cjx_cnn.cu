@@ -11,6 +11,7 @@
 #include <cstdint>
 
 #include "cjx_common.cuh"
+#include "cjx_profile.cuh"
 
 namespace cjx {
 
@@ -514,8 +515,10 @@ int cjx_cnn_noisy_normalize(const float* images, const int64_t* index, int64_t n
   if (n == 0) return CJX_OK;
   if (!images || !out) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "images and out must be non-NULL");
   if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "too many images");
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_noisy_normalize<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       images, index, h * w, snr, seed, static_cast<bf16*>(out));
+  cjx::prof_end("k_noisy_normalize", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "noisy_normalize launch");
 }
 
@@ -553,8 +556,10 @@ int cjx_cnn_conv0(const void* x, int64_t B, int H, int W, const void* w, int64_t
   if (!x || !w || !y) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "x, w and y must be non-NULL");
   if (reinterpret_cast<uintptr_t>(y) % 16) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "y must be 16-byte aligned");
   const int64_t total = B * (H / 2) * (W / 2);
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_conv0_s2<32><<<cjx::grid_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const bf16*>(x), (int)B, H, W, static_cast<const bf16*>(w), (int)ldk, bias, static_cast<bf16*>(y));
+  cjx::prof_end("k_conv0_s2", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "cnn_conv0 launch");
 }
 
@@ -577,7 +582,9 @@ int cjx_cnn_conv_s2(const void* x, int64_t B, int H, int W, int C, const void* w
   if (C == CI && cout == 64 * NG) {                                                                                \
     const int64_t ctas = (total + 16 * (8 / NG) - 1) / (16 * (8 / NG));                                            \
     if (ctas > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "cnn_conv_s2: too many pixels");             \
+    cjx::prof_begin(st);                                                                                          \
     cjx::k_conv_s2_mma<CI, NG><<<(unsigned)ctas, 256, 0, st>>>(xb, (int)B, H, W, wb, (int)ldk, bias, yb);          \
+    cjx::prof_end("k_conv_s2_mma", st);                                                                           \
     return cjx::check_cuda(cudaGetLastError(), "cnn_conv_s2 launch");                                             \
   }
   CJX_CONV_CASE(32, 1) CJX_CONV_CASE(64, 2) CJX_CONV_CASE(128, 2) CJX_CONV_CASE(128, 4) CJX_CONV_CASE(256, 4)
@@ -684,8 +691,10 @@ int cjx_topk_candidates(const float* logits, int64_t B, int C, int k, int n_inpl
     return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "topk: need 1 <= k <= C <= 1024, n_inplane >= 1");
   if (B == 0) return CJX_OK;
   if (!logits) return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "logits must be non-NULL");
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_topk_candidates<<<(unsigned)((B + 7) / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       logits, B, C, k, n_inplane, dirs, candidates);
+  cjx::prof_end("k_topk_candidates", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "topk launch");
 }
 

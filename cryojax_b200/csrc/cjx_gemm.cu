@@ -12,6 +12,7 @@
 
 #include "cjx_common.cuh"
 #include "cjx_tc.cuh"
+#include "cjx_profile.cuh"
 
 namespace cjx {
 
@@ -213,7 +214,11 @@ extern "C" {
 
 int cjx_gemm(int64_t M, int64_t N, int64_t K, const void* A, int64_t lda, const void* B, int64_t ldb, void* C,
              int64_t ldc, const float* bias, int flags, int split_k, void* stream) {
-  return cjx::launch_gemm(M, N, K, A, lda, B, ldb, C, ldc, bias, flags, split_k, static_cast<cudaStream_t>(stream));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cjx::prof_begin(s);
+  const int e = cjx::launch_gemm(M, N, K, A, lda, B, ldb, C, ldc, bias, flags, split_k, s);
+  cjx::prof_end("gemm_tc", s);
+  return e;
 }
 
 int cjx_selftest_bounded_wait(uint64_t limit_ns, int* device_status, void* stream) {

@@ -568,9 +568,11 @@ int cjx_pack_observed(const void* observed, const cjx_image_params* params, int6
   if (!observed || !params || !y16 || !z16 || !oo || !yinv || !zinv)
     return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_observed: NULL pointer");
   if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "pack_observed: too many images");
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_pack_observed<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const float2*>(observed), params, py, px, (uint32_t)flags, static_cast<__half*>(y16),
       static_cast<__half*>(z16), oo, yinv, zinv);
+  cjx::prof_end("k_pack_observed", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "pack_observed launch");
 }
 
@@ -581,8 +583,10 @@ int cjx_pack_observed32(const void* observed, const cjx_image_params* params, in
   if (!observed || !params || !y32 || !z32 || !oo)
     return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "pack_observed32: NULL pointer");
   if (n > 2147483647LL) return cjx::fail(CJX_ERR_UNSUPPORTED, "pack_observed32: too many images");
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_pack_observed32<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const float2*>(observed), params, py, px, (uint32_t)flags, static_cast<float2*>(y32), z32, oo);
+  cjx::prof_end("k_pack_observed32", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "pack_observed32 launch");
 }
 
@@ -615,8 +619,10 @@ int cjx_ncc_argmax(const float* num, const float* den, int64_t ld, int64_t n, in
   if (n == 0) return CJX_OK;
   if (!num || !den || !oo || !yinv || !zinv || !best_score || !best_orientation)
     return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_argmax: NULL pointer");
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_ncc_argmax<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       num, den, ld, T, oo, yinv, zinv, t0, scores, ld_scores, best_score, best_orientation, accumulate_best);
+  cjx::prof_end("k_ncc_argmax", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "ncc_argmax launch");
 }
 
@@ -627,8 +633,10 @@ int cjx_ncc_topk(const float* num, const float* den, int64_t ld, int64_t n, int6
   if (n == 0) return CJX_OK;
   if (!num || !den || !oo || !yinv || !zinv || !indices)
     return cjx::fail(CJX_ERR_INVALID_ARGUMENT, "ncc_topk: NULL pointer");
+  cjx::prof_begin(static_cast<cudaStream_t>(stream));
   cjx::k_ncc_topm<<<(unsigned)n, 256, 0, static_cast<cudaStream_t>(stream)>>>(num, den, ld, T, oo, yinv, zinv, k,
                                                                             indices);
+  cjx::prof_end("k_ncc_topm", static_cast<cudaStream_t>(stream));
   return cjx::check_cuda(cudaGetLastError(), "ncc_topk launch");
 }
 
