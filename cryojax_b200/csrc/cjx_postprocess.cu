@@ -219,6 +219,93 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
 }
 
+// rfft2 with the register FFTs when Px and Py are 32 R (R in 1-6, 8, 10, 12,
+// 16): compile-time twiddle tables copied once per CTA instead of double
+// sin / cos per CTA, shuffles instead of the Stockham stages' shared-memory
+// passes.  Same two passes as above.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_rows_r2c_reg(const float* __restrict__ image, float2* __restrict__ out, int py) {
+  constexpr int n = 32 * R;  // Px
+  constexpr int stride = pad16(n - 1) + 1;
+  constexpr int pxh = n / 2 + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ra = 2 * (blockIdx.x * kWarps + warp);
+  if (ra >= py) return;
+  const bool has_b = ra + 1 < py;
+  // ifftshift: transform row i / column j read image row (i + py/2) mod py / column (j + n/2) mod n
+  const float* xa = image + ((size_t)blockIdx.y * py + (ra + py / 2) % py) * n;
+  const float* xb = image + ((size_t)blockIdx.y * py + (ra + 1 + py / 2) % py) * n;
+  const int bl = brev5(lane);
+  float2 z[R];
+#pragma unroll
+  for (int n1 = 0; n1 < R; ++n1) {
+    const int c = (32 * n1 + bl + n / 2) % n;
+    z[n1] = make_float2(xa[c], has_b ? xb[c] : 0.f);
+  }
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  warp_fft_reg<R, -1>(z, tab, lt, lane);
+  float2* buf = bufs + warp * stride;
+#pragma unroll
+  for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = z[k1];
+  __syncwarp();
+  float2* oa = out + ((size_t)blockIdx.y * py + ra) * pxh;
+  for (int k = lane; k < pxh; k += 32) {
+    const float2 Zk = buf[pad16(k)];
+    const float2 Zm = buf[pad16((n - k) % n)];
+    oa[k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    if (has_b) oa[pxh + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32) k_pp_colfft_reg(float2* __restrict__ data, int px) {
+  constexpr int n = 32 * R;  // Py
+  constexpr int stride = pad16(n - 1) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int pxh = px / 2 + 1;
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, pxh - j0);
+  float2* col0 = data + (size_t)blockIdx.y * n * pxh + j0;
+  for (int e = threadIdx.x; e < n * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + pad16(m)] = col0[(size_t)m * pxh + jj];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) {
+    float2* buf = bufs + warp * stride;
+    const int bl = brev5(lane);
+    float2 x[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    warp_fft_reg<R, -1>(x, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) col0[(size_t)m * pxh + jj] = bufs[jj * stride + pad16(m)];
+  }
+}
+
+size_t smem_reg(int n) { return sizeof(float2) * (size_t)(n + kWarps * (pad16(n - 1) + 1)); }
+
 size_t smem_cols(int py) { return sizeof(float2) * (size_t)(py + kWarps * (2 * py + 2)); }
 size_t smem_rows(int px) { return sizeof(float2) * (size_t)(px + kWarps * (2 * px + 2)); }
 
@@ -310,8 +397,38 @@ extern "C" int cjx_rfft2(int64_t n_images, int py, int px, const float* image, v
   if (!image || !out) return fail(CJX_ERR_INVALID_ARGUMENT, "image and out must be non-NULL");
   if (int e = ensure_pp_smem()) return e;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const FftPlan plan_y = make_fft_plan(py), plan_x = make_fft_plan(px);
   const int pxh = px / 2 + 1;
+  const int rx = reg_fft_radix(px), ry = reg_fft_radix(py);
+  if (rx && ry) {
+    for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
+      const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
+      float2* o = static_cast<float2*>(out) + (size_t)k0 * py * pxh;
+      const float* im = image + (size_t)k0 * py * px;
+      prof_begin(s);
+      switch (rx) {
+#define CJX_PPR(R)                                                                                          \
+  case R:                                                                                                   \
+    k_pp_rows_r2c_reg<R><<<dim3((py + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, smem_reg(px), s>>>( \
+        im, o, py);                                                                                         \
+    break;
+        CJX_PPR(1) CJX_PPR(2) CJX_PPR(3) CJX_PPR(4) CJX_PPR(5) CJX_PPR(6) CJX_PPR(8) CJX_PPR(10) CJX_PPR(12) CJX_PPR(16)
+#undef CJX_PPR
+      }
+      prof_end("k_pp_rows_r2c", s);
+      prof_begin(s);
+      switch (ry) {
+#define CJX_PPC(R)                                                                                                 \
+  case R:                                                                                                          \
+    k_pp_colfft_reg<R><<<dim3((pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, smem_reg(py), s>>>(o, px);           \
+    break;
+        CJX_PPC(1) CJX_PPC(2) CJX_PPC(3) CJX_PPC(4) CJX_PPC(5) CJX_PPC(6) CJX_PPC(8) CJX_PPC(10) CJX_PPC(12) CJX_PPC(16)
+#undef CJX_PPC
+      }
+      prof_end("k_pp_colfft", s);
+    }
+    return check_cuda(cudaGetLastError(), "rfft2 launch");
+  }
+  const FftPlan plan_y = make_fft_plan(py), plan_x = make_fft_plan(px);
   for (int64_t k0 = 0; k0 < n_images; k0 += 65535) {
     const int cnt = (int)std::min<int64_t>(65535, n_images - k0);
     float2* o = static_cast<float2*>(out) + (size_t)k0 * py * pxh;

@@ -14,7 +14,7 @@ from tests.helpers import IMAGE_REL_L2_TOL, rel_l2_per_image
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(32, 32), (64, 40), (33, 47), (31, 31), (96, 63), (320, 320), (41, 37), (128, 256)]
+SHAPES = [(32, 32), (64, 40), (33, 47), (31, 31), (96, 63), (320, 320), (41, 37), (128, 256), (512, 384), (192, 96)]
 
 
 def _half_planes(n, py, px, seed):
