@@ -146,17 +146,18 @@ __global__ void __launch_bounds__(kWarps * 32)
 }
 
 // Pass 3 of irfft2 (normalisation): (x - mean) / std with the population std, then the optional mask.
-__global__ void k_pp_normalize(float* __restrict__ out, int64_t n_img, int hw, const double* __restrict__ stats,
+// One image per blockIdx.y: its mean and 1 / std come once per thread from the double sums.
+__global__ void k_pp_normalize(float* __restrict__ out, int hw, const double* __restrict__ stats,
                                const float* __restrict__ mask) {
-  const int64_t total = n_img * hw;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t img = e / hw;
-    const int p = (int)(e - img * hw);
-    const double mean = stats[2 * img] / hw;
-    const double var = fmax(stats[2 * img + 1] / hw - mean * mean, 0.0);
-    float v = (float)(((double)out[e] - mean) / sqrt(var));
+  const int64_t img = blockIdx.y;
+  const double mean_d = stats[2 * img] / hw;
+  const double var = fmax(stats[2 * img + 1] / hw - mean_d * mean_d, 0.0);
+  const float mean = (float)mean_d, istd = (float)(1.0 / sqrt(var));
+  float* o = out + img * hw;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < hw; p += gridDim.x * blockDim.x) {
+    float v = (o[p] - mean) * istd;
     if (mask) v *= __ldg(mask + p);
-    out[e] = v;
+    o[p] = v;
   }
 }
 
@@ -306,6 +307,146 @@ __global__ void __launch_bounds__(kWarps * 32) k_pp_colfft_reg(float2* __restric
 
 size_t smem_reg(int n) { return sizeof(float2) * (size_t)(n + kWarps * (pad16(n - 1) + 1)); }
 
+// irfft2 passes 1 and 2 on the register FFTs (Py, Px = 32 R): the column
+// inverse FFTs with the self-conjugate columns' Hermitian fix, and two rows
+// per warp as one complex inverse FFT of their Hermitian extensions, then
+// the same fftshift, crop, scale, statistics and mask as k_pp_rows_c2r.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_colifft_reg(const float2* __restrict__ in, float2* __restrict__ t, int px) {
+  constexpr int n = 32 * R;  // Py
+  constexpr int stride = pad16(n - 1) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int pxh = px / 2 + 1;
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, pxh - j0);
+  const float2* src = in + (size_t)blockIdx.y * n * pxh + j0;
+  for (int e = threadIdx.x; e < n * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) bufs[jj * stride + pad16(m)] = src[(size_t)m * pxh + jj];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < ncols) {
+    float2* buf = bufs + warp * stride;
+    const int j = j0 + warp;
+    if (j == 0 || ((px % 2 == 0) && j == px / 2)) {
+      // (S[v] + conj(S[-v])) / 2: the pairs (v, -v) are disjoint across lanes
+      for (int i = lane; i <= n / 2; i += 32) {
+        const int i2 = (i == 0) ? 0 : n - i;
+        const float2 x = buf[pad16(i)], y = buf[pad16(i2)];
+        const float2 sv = make_float2(0.5f * (x.x + y.x), 0.5f * (x.y - y.y));
+        buf[pad16(i)] = sv;
+        buf[pad16(i2)] = cconj(sv);
+      }
+      __syncwarp();
+    }
+    const int bl = brev5(lane);
+    float2 x[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) x[n1] = buf[pad16(32 * n1 + bl)];
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    warp_fft_reg<R, +1>(x, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = x[k1];
+  }
+  __syncthreads();
+  float2* dst = t + (size_t)blockIdx.y * n * pxh + j0;
+  for (int e = threadIdx.x; e < n * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) dst[(size_t)m * pxh + jj] = bufs[jj * stride + pad16(m)];
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_pp_rows_c2r_reg(const float2* __restrict__ t, float* __restrict__ out, int py, int h, int w,
+                      const float* __restrict__ mask, double* __restrict__ stats) {
+  constexpr int n = 32 * R;  // Px
+  constexpr int stride = pad16(n - 1) + 1;
+  constexpr int hx = n / 2, pxh = n / 2 + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = 2 * (blockIdx.x * kWarps + warp);
+  if (r0 >= h) return;
+  const bool has_b = r0 + 1 < h;
+  // output row r of the crop is row (r + y0 + py - py/2) mod py of the unshifted inverse transform
+  const int y0 = py / 2 - h / 2, x0 = hx - w / 2;
+  const int sa = (r0 + y0 + py - py / 2) % py;
+  const int sb = (r0 + 1 + y0 + py - py / 2) % py;
+  const float2* rowA = t + ((size_t)blockIdx.y * py + sa) * pxh;
+  const float2* rowB = t + ((size_t)blockIdx.y * py + sb) * pxh;
+  // z = A + iB on the Hermitian extension, in the lane's bit-reversed input order; the DC and Nyquist
+  // bins keep their real parts only
+  const int bl = brev5(lane);
+  float2 z[R];
+#pragma unroll
+  for (int n1 = 0; n1 < R; ++n1) {
+    const int k = 32 * n1 + bl;
+    if (k == 0 || k == hx) {
+      const float2 A = rowA[k], B = has_b ? rowB[k] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x, B.x);
+    } else if (k < hx) {
+      const float2 A = rowA[k], B = has_b ? rowB[k] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x - B.y, A.y + B.x);
+    } else {
+      const float2 A = rowA[n - k], B = has_b ? rowB[n - k] : make_float2(0.f, 0.f);
+      z[n1] = make_float2(A.x + B.y, B.x - A.y);
+    }
+  }
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  warp_fft_reg<R, +1>(z, tab, lt, lane);
+  float2* buf = bufs + warp * stride;
+#pragma unroll
+  for (int k1 = 0; k1 < R; ++k1) buf[pad16(k1 + R * lane)] = z[k1];
+  __syncwarp();
+  const float scale = (float)(1.0 / ((double)py * (double)n));
+  const bool fuse_mask = mask && !stats;
+  float* oa = out + ((size_t)blockIdx.y * h + r0) * w;
+  double s = 0.0, ss = 0.0;
+  for (int c = lane; c < w; c += 32) {
+    const float2 v = buf[pad16((c + x0 + n - hx) % n)];
+    float va = v.x * scale, vb = v.y * scale;
+    s += (double)va;
+    ss += (double)va * (double)va;
+    if (has_b) {
+      s += (double)vb;
+      ss += (double)vb * (double)vb;
+    }
+    if (fuse_mask) {
+      va *= __ldg(mask + (size_t)r0 * w + c);
+      if (has_b) vb *= __ldg(mask + (size_t)(r0 + 1) * w + c);
+    }
+    oa[c] = va;
+    if (has_b) oa[w + c] = vb;
+  }
+  if (stats) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    if (lane == 0) {
+      atomicAdd(stats + 2 * blockIdx.y, s);
+      atomicAdd(stats + 2 * blockIdx.y + 1, ss);
+    }
+  }
+}
+
+
+
 size_t smem_cols(int py) { return sizeof(float2) * (size_t)(py + kWarps * (2 * py + 2)); }
 size_t smem_rows(int px) { return sizeof(float2) * (size_t)(px + kWarps * (2 * px + 2)); }
 
@@ -366,25 +507,46 @@ extern "C" int cjx_postprocess_real(int64_t n_images, int py, int px, int h, int
   float2* t = static_cast<float2*>(workspace);
   double* stats = reinterpret_cast<double*>(static_cast<char*>(workspace) + (size_t)chunk * py * pxh * sizeof(float2));
   const FftPlan plan_y = make_fft_plan(py), plan_x = make_fft_plan(px);
+  const int rx = reg_fft_radix(px), ry = reg_fft_radix(py);  // register FFTs when both are 32 R
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     const float2* src = static_cast<const float2*>(fourier) + (size_t)k0 * py * pxh;
     float* dst = out + (size_t)k0 * h * w;
+    const dim3 gcol((pxh + kWarps - 1) / kWarps, cnt), grow((h + 2 * kWarps - 1) / (2 * kWarps), cnt);
     prof_begin(s);
-    k_pp_colifft<<<dim3((pxh + kWarps - 1) / kWarps, cnt), kWarps * 32, smem_cols(py), s>>>(
-        src, t, py, px, plan_y, fft_result_offset(plan_y, py));
+    if (ry && rx) {
+      switch (ry) {
+#define CJX_PPCI(R) \
+  case R: k_pp_colifft_reg<R><<<gcol, kWarps * 32, smem_reg(py), s>>>(src, t, px); break;
+        CJX_PPCI(1) CJX_PPCI(2) CJX_PPCI(3) CJX_PPCI(4) CJX_PPCI(5) CJX_PPCI(6) CJX_PPCI(8) CJX_PPCI(10)
+        CJX_PPCI(12) CJX_PPCI(16)
+#undef CJX_PPCI
+      }
+    } else {
+      k_pp_colifft<<<gcol, kWarps * 32, smem_cols(py), s>>>(src, t, py, px, plan_y, fft_result_offset(plan_y, py));
+    }
     prof_end("k_pp_colifft", s);
     if (normalize) {
       if (int e = check_cuda(cudaMemsetAsync(stats, 0, sizeof(double) * 2 * cnt, s), "cudaMemsetAsync")) return e;
     }
+    double* st = normalize ? stats : nullptr;
     prof_begin(s);
-    k_pp_rows_c2r<<<dim3((h + 2 * kWarps - 1) / (2 * kWarps), cnt), kWarps * 32, smem_rows(px), s>>>(
-        t, dst, py, px, h, w, mask, normalize ? stats : nullptr, plan_x);
+    if (ry && rx) {
+      switch (rx) {
+#define CJX_PPRC(R) \
+  case R: k_pp_rows_c2r_reg<R><<<grow, kWarps * 32, smem_reg(px), s>>>(t, dst, py, h, w, mask, st); break;
+        CJX_PPRC(1) CJX_PPRC(2) CJX_PPRC(3) CJX_PPRC(4) CJX_PPRC(5) CJX_PPRC(6) CJX_PPRC(8) CJX_PPRC(10)
+        CJX_PPRC(12) CJX_PPRC(16)
+#undef CJX_PPRC
+      }
+    } else {
+      k_pp_rows_c2r<<<grow, kWarps * 32, smem_rows(px), s>>>(t, dst, py, px, h, w, mask, st, plan_x);
+    }
     prof_end("k_pp_rows_c2r", s);
     if (normalize) {
       prof_begin(s);
-      const int64_t blocks = std::min<int64_t>(((int64_t)cnt * h * w + 255) / 256, 148 * 16);
-      k_pp_normalize<<<(unsigned)blocks, 256, 0, s>>>(dst, cnt, h * w, stats, mask);
+      const int bx = std::min((h * w + 255) / 256, 32);
+      k_pp_normalize<<<dim3(bx, cnt), 256, 0, s>>>(dst, h * w, stats, mask);
       prof_end("k_pp_normalize", s);
     }
   }
