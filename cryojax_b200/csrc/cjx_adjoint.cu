@@ -471,9 +471,9 @@ constexpr int kScatterWarpAgg = 2; // lanes whose corner hits the same voxel sum
 
 // The scatter of one sample's corner rows (kScatterCorner, kScatterVec):
 // weight * cotangent to each valid corner of the C-order gradient array.
-template <int MODE>
-__device__ __forceinline__ void scatter_rows(float2* __restrict__ gg, int n, const AxisNodes& ax, const AxisNodes& ay,
-                                             const AxisNodes& az, float2 gs) {
+template <int MODE, typename GL>
+__device__ __forceinline__ void scatter_rows(float2* __restrict__ gg, const GL& G, const AxisNodes& ax,
+                                             const AxisNodes& ay, const AxisNodes& az, float2 gs) {
   const bool xpair = ax.v0 && ax.v1 && ax.i1 == ax.i0 + 1;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {  // corner rows (dz, dy); x-corners 0 and 1
@@ -481,16 +481,35 @@ __device__ __forceinline__ void scatter_rows(float2* __restrict__ gg, int n, con
     if (!((dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0))) continue;
     const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0;
     const float wyz = (dz ? az.w1 : az.w0) * (dy ? ay.w1 : ay.w0);
-    const size_t row = ((size_t)iz * n + iy) * n;
+    const size_t row = (size_t)G.az(iz) + (size_t)G.ay(iy);
     const float2 c0 = make_float2(wyz * ax.w0 * gs.x, wyz * ax.w0 * gs.y);
     const float2 c1 = make_float2(wyz * ax.w1 * gs.x, wyz * ax.w1 * gs.y);
-    const size_t e0 = row + ax.i0;
-    if (MODE == kScatterVec && xpair && (e0 & 1) == 0) {
+    const size_t e0 = row + G.ax(ax.i0), e1 = row + G.ax(ax.i1);
+    if (MODE == kScatterVec && xpair && (e0 & 1) == 0 && e1 == e0 + 1) {
       atomicAdd(reinterpret_cast<float4*>(gg + e0), make_float4(c0.x, c0.y, c1.x, c1.y));
     } else {
       if (ax.v0) atomicAdd(&gg[e0], c0);
-      if (ax.v1) atomicAdd(&gg[row + ax.i1], c1);
+      if (ax.v1) atomicAdd(&gg[e1], c1);
     }
+  }
+}
+
+// grid_grad (C order [z][y][x]) += acc (the bricked accumulator of the
+// scatter), two x-neighbours per thread: for even x both are one 16-byte
+// entry pair in either layout.
+__global__ void k_unbrick_add(float2* __restrict__ gg, const float2* __restrict__ acc, int n) {
+  const BrickLayout L(n);
+  const int half = n / 2;
+  const int64_t total = (int64_t)n * n * half;
+  float4* g4 = reinterpret_cast<float4*>(gg);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int x = 2 * (int)(e % half);
+    const int64_t t = e / half;
+    const int y = (int)(t % n), z = (int)(t / n);
+    const float4 a = *reinterpret_cast<const float4*>(acc + (size_t)L.az(z) + L.ay(y) + L.ax(x));
+    float4 v = g4[e];
+    v.x += a.x; v.y += a.y; v.z += a.z; v.w += a.w;
+    g4[e] = v;
   }
 }
 
@@ -501,12 +520,13 @@ __device__ __forceinline__ void scatter_rows(float2* __restrict__ gg, int n, con
 // voxel), and the CTA's share of dL/dR.  The scatter is bound by the L1 and
 // the L2's atomic units, so fewer atomic instructions and sectors is what
 // shortens it.
-template <typename Layout, int MODE>
+template <typename Layout, int MODE, typename GL>
 __global__ void __launch_bounds__(256)
     k_scatter_slice(const float2* __restrict__ grid, const float2* __restrict__ gh,
                     const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
                     float2* __restrict__ grad_grid, double* __restrict__ grads, SliceGeom g, int64_t k0) {
   const Layout L(g.n);
+  const GL G(g.n);  // the gradient array's layout: C order, or the bricked accumulator
   __shared__ float red[8][6];
   const int n = g.n;
   const int64_t k = k0 + blockIdx.z;
@@ -553,12 +573,12 @@ __global__ void __launch_bounds__(256)
           const bool ok = live && (dz ? az.v1 : az.v0) && (dy ? ay.v1 : ay.v0) && (dx ? ax.v1 : ax.v0);
           const int iz = dz ? az.i1 : az.i0, iy = dy ? ay.i1 : ay.i0, ix = dx ? ax.i1 : ax.i0;
           const float w = ((dz ? az.w1 : az.w0) * (dy ? ay.w1 : ay.w0)) * (dx ? ax.w1 : ax.w0);
-          const unsigned key = ok ? (unsigned)(((size_t)iz * n + iy) * n + ix) : kNoKey;
+          const unsigned key = ok ? (unsigned)((size_t)G.az(iz) + G.ay(iy) + G.ax(ix)) : kNoKey;
           float2 c2 = make_float2(w * gs.x, w * gs.y);
           if (peer_sum(key, c2, lane)) atomicAdd(&grad_grid[key], c2);
         }
       } else {
-        scatter_rows<MODE>(grad_grid, n, ax, ay, az, gs);
+        scatter_rows<MODE>(grad_grid, G, ax, ay, az, gs);
       }
     }
     if (live) {
@@ -705,14 +725,14 @@ __global__ void k_zero_doubles(double* p, int64_t count) {
     p[i] = 0.0;
 }
 
-template <typename Layout>
+template <typename Layout, typename GL>
 static void launch_scatter(int mode, dim3 gs, cudaStream_t stream, const float2* grid, const float2* hb,
                            const cjx_image_params* params, const int32_t* order, float2* grad_grid, double* grads,
                            const SliceGeom& g, int64_t k0) {
   switch (mode) {
-#define CJX_SC_CASE(M)                                                                                     \
-  case M:                                                                                                  \
-    k_scatter_slice<Layout, M><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0); \
+#define CJX_SC_CASE(M)                                                                                         \
+  case M:                                                                                                      \
+    k_scatter_slice<Layout, M, GL><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0); \
     break;
     CJX_SC_CASE(kScatterCorner) CJX_SC_CASE(kScatterVec) CJX_SC_CASE(kScatterWarpAgg)
 #undef CJX_SC_CASE
@@ -721,9 +741,15 @@ static void launch_scatter(int mode, dim3 gs, cudaStream_t stream, const float2*
   }
 }
 
+size_t bricked_elements(int n);
+
+// Bytes of the bricked accumulator of the grid scatter (voxel grids), which
+// follows the per-chunk scratch in the loss workspace at a 256-byte boundary.
+size_t loss_accumulator_bytes(int n) { return 256 + sizeof(float2) * bricked_elements(n); }
+
 int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                     int64_t n_images, const float2* obs, double* grads, float2* grad_grid, void* workspace,
-                     int64_t chunk, cudaStream_t stream, const Tuning& tn) {
+                     int64_t n_images, const float2* obs, double* grads, float2* grad_grid, float2* acc,
+                     void* workspace, int64_t chunk, cudaStream_t stream, const Tuning& tn) {
   const int rn = reg_fft_radix(g.n), rpy = reg_fft_radix(g.py), rpx = reg_fft_radix(g.px);
   if (!rn || !rpy || !rpx)
     return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs N, Py, Px = 32 R with R in {1-6, 8, 10, 12, 16}");
@@ -748,7 +774,17 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
     return fail(CJX_ERR_UNSUPPORTED, "the spline adjoint reads the coefficients in the linear or bricked layout");
   // the 16-byte atomics need a 16-byte aligned gradient array
   int mode = tn.scatter_vec;
-  if (mode == kScatterVec && (reinterpret_cast<uintptr_t>(grad_grid) & 15)) mode = kScatterCorner;
+  const bool aligned16 = (reinterpret_cast<uintptr_t>(grad_grid) & 15) == 0;
+  if (mode == kScatterVec && !aligned16) mode = kScatterCorner;
+  // voxel grids scatter into a zeroed bricked accumulator: a warp's corner rows then touch about 12 instead of
+  // about 20 distinct 128-byte lines; it is added into grid_grad (C order) at the end
+  const bool use_acc = grad_grid && acc && aligned16 && !(g.flags & CJX_GRID_SPLINE);
+  float2* target = use_acc ? acc : grad_grid;
+  if (use_acc) {
+    if (int e = check_cuda(cudaMemsetAsync(acc, 0, sizeof(float2) * bricked_elements(g.n), stream),
+                           "zero the gradient accumulator"))
+      return e;
+  }
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
@@ -791,14 +827,27 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
       else
         k_scatter_slice_spline<SplineLinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid,
                                                                            grads, g, k0);
-    } else if (pairs) {
-      launch_scatter<PairLayout>(mode, gs, stream, grid, hb, params, order, grad_grid, grads, g, k0);
-    } else if (bricked) {
-      launch_scatter<BrickLayout>(mode, gs, stream, grid, hb, params, order, grad_grid, grads, g, k0);
+    } else if (use_acc) {
+      if (pairs)
+        launch_scatter<PairLayout, BrickLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+      else if (bricked)
+        launch_scatter<BrickLayout, BrickLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+      else
+        launch_scatter<LinearLayout, BrickLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
     } else {
-      launch_scatter<LinearLayout>(mode, gs, stream, grid, hb, params, order, grad_grid, grads, g, k0);
+      if (pairs)
+        launch_scatter<PairLayout, LinearLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+      else if (bricked)
+        launch_scatter<BrickLayout, LinearLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+      else
+        launch_scatter<LinearLayout, LinearLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
     }
     prof_end("k_scatter_slice", stream);
+  }
+  if (use_acc) {
+    prof_begin(stream);
+    k_unbrick_add<<<148 * 8, 256, 0, stream>>>(grad_grid, acc, g.n);
+    prof_end("k_unbrick_add", stream);
   }
   return check_cuda(cudaGetLastError(), "loss gradient launch");
 }

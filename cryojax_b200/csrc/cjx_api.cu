@@ -25,8 +25,9 @@ int launch_search(const SliceGeom& g, size_t per_fwd, int64_t chunk, const float
                   int64_t n_images, int K, const float2* obs, float* scores, float* best_score, int32_t* best_orient,
                   void* workspace, cudaStream_t stream, const Tuning& tn);
 int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_params* params, const int32_t* order,
-                     int64_t n_images, const float2* obs, double* grads, float2* grad_grid, void* workspace,
-                     int64_t chunk, cudaStream_t stream, const Tuning& tn);
+                     int64_t n_images, const float2* obs, double* grads, float2* grad_grid, float2* acc,
+                     void* workspace, int64_t chunk, cudaStream_t stream, const Tuning& tn);
+size_t loss_accumulator_bytes(int n);
 int tuning_set(int key, int64_t value);
 int launch_read_probe(const void* buf, size_t bytes, int passes, void* sink, cudaStream_t stream);
 size_t bricked_elements(int n);
@@ -286,7 +287,8 @@ int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_imag
   if (int e = make_geom(desc, &g)) return e;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
   if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
-  *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) : 0;
+  const size_t acc = (g.flags & CJX_GRID_SPLINE) ? 0 : loss_accumulator_bytes(g.n);
+  *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) + acc : 0;
   return CJX_OK;
 }
 
@@ -304,10 +306,17 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (int e = check_alignment(g.flags, grid, observed)) return e;
   if (reinterpret_cast<uintptr_t>(grid_grad) & 7) return fail(CJX_ERR_INVALID_ARGUMENT, "grid_grad must be 8-byte aligned");
   const int64_t chunk = chunk_for(g, desc, n_images);
-  if (!workspace || workspace_bytes < (size_t)chunk * workspace_per_image(g))
+  const size_t scratch = (size_t)chunk * workspace_per_image(g);
+  if (!workspace || workspace_bytes < scratch)
     return fail(CJX_ERR_WORKSPACE, "workspace smaller than cjx_slice_ctf_loss_workspace_size()");
+  // the grid scatter's bricked accumulator, when the workspace has room for it (voxel grids)
+  float2* acc = nullptr;
+  if (grid_grad && !(g.flags & CJX_GRID_SPLINE) && workspace_bytes >= scratch + loss_accumulator_bytes(g.n)) {
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(workspace) + scratch + 255) & ~(uintptr_t)255;
+    acc = reinterpret_cast<float2*>(a);
+  }
   return launch_loss_grad(g, static_cast<const float2*>(grid), params, order, n_images,
-                          static_cast<const float2*>(observed), image_grads, static_cast<float2*>(grid_grad),
+                          static_cast<const float2*>(observed), image_grads, static_cast<float2*>(grid_grad), acc,
                           workspace, chunk, static_cast<cudaStream_t>(stream), current_tuning());
 }
 

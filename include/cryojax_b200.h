@@ -206,8 +206,11 @@ CJX_API int cjx_slice_ctf_forward_filtered(const cjx_slice_desc* desc, const voi
                                            int64_t n_images, const float* filter, void* out,
                                            void* workspace, size_t workspace_bytes, void* stream);
 
-/* Workspace for cjx_slice_ctf_loss_grad (same per-image need as the
- * forward's resize path).                                                  */
+/* Workspace for cjx_slice_ctf_loss_grad: the forward's resize-path scratch
+ * per chunk of images, then (voxel grids) a bricked N^3 complex64
+ * accumulator into which the grid scatter adds before the result goes into
+ * grid_grad (its atomics then touch fewer cache lines).  A workspace of only
+ * the first part is accepted and scatters into grid_grad directly.        */
 CJX_API int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_images,
                                               size_t* bytes);
 /* Loss L_b = sum_pixels (simulate_b() - obs_b)^2 in real space (the
