@@ -174,3 +174,28 @@ def test_misaligned_arrays_are_rejected_before_any_launch():
     rc = lib.cjx_slice_ctf_loss_grad(ctypes.byref(plain), vp(base), vp(base + 0x1000), None, 2,
                                      vp(base + 0x2000), grads, vp(base + 0x4004), ws, 1 << 30, None)
     assert rc == nat.CJX_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(),
+                    reason="hands the library placeholder addresses: argument validation only, on a machine without a GPU")
+def test_search_and_network_entry_points_validate_arguments():
+    """The re-ranking, candidate-sum and convolution entry points reject bad sizes before any launch."""
+    lib = nat.load_library()
+    vp = ctypes.c_void_p
+    base = 0x10000000  # placeholder addresses; never dereferenced
+    p = [vp(base + 0x1000 * i) for i in range(8)]
+    # re-ranking: m must be in [1, 16]
+    assert lib.cjx_ncc_rerank32(p[0], 64, 64, 100, p[1], p[2], p[3], 4, p[4], 17, None, p[5], p[6], None) \
+        == nat.CJX_ERR_INVALID_ARGUMENT
+    assert lib.cjx_ncc_rerank32(p[0], 64, 64, 100, p[1], p[2], p[3], 4, p[4], 0, None, p[5], p[6], None) \
+        == nat.CJX_ERR_INVALID_ARGUMENT
+    # candidate sums: kp must be a positive multiple of 8
+    ws = ctypes.c_size_t(0)
+    assert lib.cjx_ncc_directions_workspace_size(4, 2, 10, ctypes.byref(ws)) == nat.CJX_OK
+    assert ws.value == 4 * (3 * 12 + 8)
+    assert lib.cjx_ncc_directions(p[0], p[1], p[2], p[3], 4, 12, p[4], 2, 10, 48, p[5], p[6], p[7], ws.value,
+                                  None) == nat.CJX_ERR_INVALID_ARGUMENT
+    # implicit convolution: only the network's (C, cout) pairs are compiled
+    assert lib.cjx_cnn_conv_s2(p[0], 2, 16, 16, 48, p[1], 9 * 48, 64, None, p[2], None) == nat.CJX_ERR_UNSUPPORTED
+    assert lib.cjx_cnn_conv_s2(p[0], 2, 15, 16, 32, p[1], 288, 64, None, p[2], None) == nat.CJX_ERR_INVALID_ARGUMENT
+    assert lib.cjx_cnn_conv0(p[0], 2, 16, 16, p[1], 16, 64, None, p[2], None) == nat.CJX_ERR_INVALID_ARGUMENT
