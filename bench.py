@@ -1331,6 +1331,16 @@ def run_probe(kind, seed):
             step()
         ms = ev_time(step)
         out["train_step_batch256"] = {"ms": ms, "images_per_s": 256 / (ms / 1000.0)}
+        # proposals (inference): first layer without im2col, the others as implicit GEMMs on mma.sync tiles
+        x = torch.randn((2048, 128, 128), generator=g, device=dev)
+
+        def prop():
+            net.propose(x, k=16, n_inplane=48)
+
+        for _ in range(2):
+            prop()
+        ms = ev_time(prop)
+        out["proposals_batch2048"] = {"ms": ms, "images_per_s": 2048 / (ms / 1000.0)}
     out["device_status"] = nat.device_status()
     print(json.dumps(out))
     return 0
