@@ -210,16 +210,16 @@ __global__ void __launch_bounds__(kWarps * 32)
   sty = warp_sum(sty);
   sdf = warp_sum(sdf);
   if (lane == 0) {
-    red[warp][0] = sl;
-    red[warp][1] = stx;
-    red[warp][2] = sty;
-    red[warp][3] = sdf;
+    red[warp][kGradLoss] = sl;
+    red[warp][kGradTx] = stx;
+    red[warp][kGradTy] = sty;
+    red[warp][kGradDf] = sdf;
   }
   __syncthreads();
-  if (threadIdx.x < 4) {
+  if (threadIdx.x < 4) {  // loss, d/d shift_x, d/d shift_y, d/d defocus
     double acc = 0.0;
     for (int w = 0; w < kWarps; ++w) acc += (double)red[w][threadIdx.x];
-    atomicAdd(&grads[img * 16 + threadIdx.x], acc);
+    atomicAdd(&grads[img * 16 + kGradLoss + threadIdx.x], acc);
   }
   for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
     const int m = e / kWarps, jj = e % kWarps;
