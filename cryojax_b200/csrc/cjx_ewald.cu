@@ -113,21 +113,30 @@ __global__ void __launch_bounds__(kEwWarps * 32)
 // ---------------------------------------------------------------------------
 // z holds the row in the lane's bit-reversed order, loaded by the caller
 // before its table copy.
-template <int RN, int RP>
+// With T512 (N = 512) the N-point transform is the 16 x 32 transpose FFT
+// (z in natural lane order, output staged with stage512).
+template <int RN, int RP, bool T512>
 __device__ __forceinline__ void ewald_row_reg(float2 (&z)[RN], float2* __restrict__ dst, float2* buf,
                                               const float2* tabN, const float2* tabP, const LaneTwiddles& lt,
-                                              int lane, const int* winx) {
+                                              int lane, const int* winx, const float2* w32) {
   constexpr int px = 32 * RP;
   const int bl = brev5(lane);
-  warp_fft_reg<RN, +1>(z, tabN, lt, lane);
+  if constexpr (T512) {
+    static_assert(RN == 16, "the transpose FFT is 512-point");
+    warp_fft512_t<+1>(z, tabN, w32, buf, lane);
 #pragma unroll
-  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+    for (int q = 0; q < RN; ++q) buf[stage512(fft512_t_out(q, lane))] = z[q];
+  } else {
+    warp_fft_reg<RN, +1>(z, tabN, lt, lane);
+#pragma unroll
+    for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+  }
   __syncwarp();
   float2 w[RP];
 #pragma unroll
   for (int n1 = 0; n1 < RP; ++n1) {
     const int src = winx[32 * n1 + bl];
-    w[n1] = (src >= 0) ? buf[pad16(src)] : make_float2(0.f, 0.f);
+    w[n1] = (src >= 0) ? buf[T512 ? stage512(src) : pad16(src)] : make_float2(0.f, 0.f);
   }
   __syncwarp();
   warp_fft_reg<RP, -1>(w, tabP, lt, lane);
@@ -137,14 +146,21 @@ __device__ __forceinline__ void ewald_row_reg(float2 (&z)[RN], float2* __restric
   for (int k = lane; k < px; k += 32) dst[k] = buf[pad16(k)];
 }
 
-template <int RN>
-__global__ void __launch_bounds__(kWarps * 32)
+// Per-warp buffer of the Ewald row pass: the N-point transform's staging
+// (stage512 with the transpose FFT, pad16 otherwise) and the Px-point one's.
+__host__ __device__ inline int ewald_rows_stride(int n, int px, bool t512) {
+  const int s = (n > px ? pad16(n) : pad16(px)) + 1;
+  return (t512 && kStage512Size + 1 > s) ? kStage512Size + 1 : s;
+}
+
+template <int RN, bool T512 = false>
+__global__ void __launch_bounds__(kWarps * 32, 4)
     k_ewald_rows_reg(const float2* __restrict__ t1, float2* __restrict__ t2, SliceGeom g, int rp) {
   constexpr int n = 32 * RN;
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
   const int px = g.px;
-  const int stride = pad16(max(n, px)) + 1;
+  const int stride = ewald_rows_stride(n, px, T512);
   float2* tabN = smem;
   float2* tabP = tabN + n;
   float2* bufs = tabP + px;
@@ -154,7 +170,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   float2 z[RN];  // loaded first, so that the load latency overlaps the table copy
   if (r < g.py) {
     const float2* row = t1 + ((size_t)blockIdx.y * g.py + r) * g.ld1;
-    const int bl = brev5(lane);
+    const int bl = T512 ? lane : brev5(lane);  // the transpose FFT takes natural lane order
 #pragma unroll
     for (int n1 = 0; n1 < RN; ++n1) z[n1] = row[32 * n1 + bl];
   }
@@ -169,7 +185,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   const LaneTwiddles lt = make_lane_twiddles(w32, lane);
   switch (rp) {
 #define CJX_EROW_CASE(RPV) \
-  case RPV: ewald_row_reg<RN, RPV>(z, dst, buf, tabN, tabP, lt, lane, winx); break;
+  case RPV: ewald_row_reg<RN, RPV, T512>(z, dst, buf, tabN, tabP, lt, lane, winx, w32); break;
     CJX_EROW_CASE(1) CJX_EROW_CASE(2) CJX_EROW_CASE(3) CJX_EROW_CASE(4) CJX_EROW_CASE(5)
     CJX_EROW_CASE(6) CJX_EROW_CASE(8) CJX_EROW_CASE(10) CJX_EROW_CASE(12) CJX_EROW_CASE(16)
 #undef CJX_EROW_CASE
@@ -362,6 +378,8 @@ static int ensure_ewald_smem() {
     CJX_EW_ATTR(1) CJX_EW_ATTR(2) CJX_EW_ATTR(3) CJX_EW_ATTR(4) CJX_EW_ATTR(5)
     CJX_EW_ATTR(6) CJX_EW_ATTR(8) CJX_EW_ATTR(10) CJX_EW_ATTR(12) CJX_EW_ATTR(16)
 #undef CJX_EW_ATTR
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_ewald_rows_reg<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxReg);
     return e;
   });
   return err == cudaSuccess ? CJX_OK : check_cuda(err, "cudaFuncSetAttribute (Ewald kernels)");
@@ -374,8 +392,14 @@ int launch_ewald_rows(const SliceGeom& g, const float2* t1, float2* t2, int cnt,
   const int rn = reg_fft_radix(g.n), rp = reg_fft_radix(g.px);
   prof_begin(stream);
   if (tn.fft_mode >= 1 && rn && rp) {
-    const size_t sm = sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) +
+    const bool t512 = rn == 16 && tn.fft_mode >= 3;  // the 512-point transform through one transpose
+    const size_t sm = sizeof(float2) * (size_t)(g.n + g.px + kWarps * ewald_rows_stride(g.n, g.px, t512)) +
                       sizeof(int) * (size_t)g.px;
+    if (t512) {
+      k_ewald_rows_reg<16, true><<<gd, kWarps * 32, sm, stream>>>(t1, t2, g, rp);
+      prof_end("k_ewald_rows", stream);
+      return check_cuda(cudaGetLastError(), "k_ewald_rows launch");
+    }
     switch (rn) {
 #define CJX_ER_CASE(R) \
   case R: k_ewald_rows_reg<R><<<gd, kWarps * 32, sm, stream>>>(t1, t2, g, rp); break;

@@ -167,7 +167,8 @@ def test_register_fft_passes_match_oracle(cuda_device, spline):
 
 
 def test_fft_modes_agree_at_the_benchmark_shape(cuda_device):
-    """N = 512 -> 320^2: register-FFT passes (default) against the shared-memory Stockham passes."""
+    """N = 512 -> 320^2: register-FFT passes (mode 2; mode 3, the default, with the 512-point transpose FFT in
+    the row pass) against the shared-memory Stockham passes (mode 0)."""
     import torch
 
     from cryojax_b200 import _native as nat
@@ -184,10 +185,11 @@ def test_fft_modes_agree_at_the_benchmark_shape(cuda_device):
     old = nat.tuning_get(nat.CJX_TUNE_FFT_MODE)
     try:
         outs = {}
-        for mode in (0, 2):
+        for mode in (0, 2, 3):
             nat.tuning_set(nat.CJX_TUNE_FFT_MODE, mode)
             outs[mode] = model.compute_fourier_image().cpu().numpy()
     finally:
         nat.tuning_set(nat.CJX_TUNE_FFT_MODE, old)
     torch.cuda.synchronize()
     assert max(rel_l2_per_image(outs[2], outs[0])) <= 1e-5
+    assert max(rel_l2_per_image(outs[3], outs[0])) <= 1e-5  # the transpose FFT in the row pass
