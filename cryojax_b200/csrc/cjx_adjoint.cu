@@ -520,14 +520,17 @@ __global__ void k_unbrick_add(float2* __restrict__ gg, const float2* __restrict_
 // voxel), and the CTA's share of dL/dR.  The scatter is bound by the L1 and
 // the L2's atomic units, so fewer atomic instructions and sectors is what
 // shortens it.
-template <typename Layout, int MODE, typename GL>
+// EW: the Ewald sphere's full surface (N columns; the third coordinate
+// w = cw (u^2 + v^2) along R's third column, so dL/dR gains that column).
+template <typename Layout, int MODE, typename GL, bool EW>
 __global__ void __launch_bounds__(256)
     k_scatter_slice(const float2* __restrict__ grid, const float2* __restrict__ gh,
                     const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
                     float2* __restrict__ grad_grid, double* __restrict__ grads, SliceGeom g, int64_t k0) {
   const Layout L(g.n);
   const GL G(g.n);  // the gradient array's layout: C order, or the bricked accumulator
-  __shared__ float red[8][6];
+  constexpr int NR = EW ? 9 : 6;  // dL/dR entries: columns 0 and 1 (as (row, column) pairs), then column 2
+  __shared__ float red[8][NR];
   const int n = g.n;
   const int64_t k = k0 + blockIdx.z;
   const int64_t img = order ? (int64_t)order[k] : k;
@@ -541,14 +544,23 @@ __global__ void __launch_bounds__(256)
   gather_lane_offsets<1>(warp, lane, du, dv);
   const int u = blockIdx.x * 16 + du;
   const int v = blockIdx.y * 16 + dv;
-  const bool live = u < g.nxh && v < n;
-  float gr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const bool live = u < g.ncols && v < n;
+  float gr[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) gr[q] = 0.f;
   // the warp-aggregated form groups all 32 lanes, so there every lane runs the sample code (inactive
   // lanes carry kNoKey)
   if (MODE == kScatterWarpAgg || live) {
-    const float2 gs = live ? gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v] : make_float2(0.f, 0.f);
+    const float2 gs = live ? gh[((size_t)blockIdx.z * g.ncols + u) * g.ldh + v] : make_float2(0.f, 0.f);
     const float ux = (float)fft_index(live ? u : 0, n), vy = (float)fft_index(live ? v : 0, n);
-    const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    float ew = 0.f;  // the surface's third coordinate
+    if constexpr (EW) {
+      ew = ewald_w(params + img, n) * fmaf(ux, ux, vy * vy);
+      o[0] = fmaf((float)Rm[2], ew, o[0]);
+      o[1] = fmaf((float)Rm[5], ew, o[1]);
+      o[2] = fmaf((float)Rm[8], ew, o[2]);
+    }
     const AxisNodes ax = axis_nodes(o[0], n, wrap);
     const AxisNodes ay = axis_nodes(o[1], n, wrap);
     const AxisNodes az = axis_nodes(o[2], n, wrap);
@@ -587,15 +599,16 @@ __global__ void __launch_bounds__(256)
         const float dLdo = gs.x * dH[a][0] + gs.y * dH[a][1];
         gr[2 * a] = dLdo * ux;
         gr[2 * a + 1] = dLdo * vy;
+        if constexpr (EW) gr[6 + a] = dLdo * ew;
       }
     }
   }
 #pragma unroll
-  for (int q = 0; q < 6; ++q) gr[q] = warp_sum(gr[q]);
+  for (int q = 0; q < NR; ++q) gr[q] = warp_sum(gr[q]);
   if (lane == 0)
-    for (int q = 0; q < 6; ++q) red[warp][q] = gr[q];
+    for (int q = 0; q < NR; ++q) red[warp][q] = gr[q];
   __syncthreads();
-  if (threadIdx.x < 6) {
+  if (threadIdx.x < NR) {
     double acc = 0.0;
     for (int w = 0; w < 8; ++w) acc += (double)red[w][threadIdx.x];
     atomicAdd(&grads[img * 16 + kGradRot + threadIdx.x], acc);
@@ -619,13 +632,14 @@ __device__ __forceinline__ void spline_dweights(float f, float* dw) {
   dw[3] = 3.0f * f * f;
 }
 
-template <typename Layout>
+template <typename Layout, bool EW>
 __global__ void __launch_bounds__(256)
     k_scatter_slice_spline(const float2* __restrict__ coef, const float2* __restrict__ gh,
                            const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
                            float2* __restrict__ grad_coef, double* __restrict__ grads, SliceGeom g, int64_t k0) {
   const Layout L(g.n);
-  __shared__ float red[8][6];
+  constexpr int NR = EW ? 9 : 6;
+  __shared__ float red[8][NR];
   const int n = g.n, m = n + 2;
   const int64_t k = k0 + blockIdx.z;
   const int64_t img = order ? (int64_t)order[k] : k;
@@ -639,11 +653,20 @@ __global__ void __launch_bounds__(256)
   gather_lane_offsets<1>(warp, lane, du, dv);
   const int u = blockIdx.x * 16 + du;
   const int v = blockIdx.y * 16 + dv;
-  float gr[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (u < g.nxh && v < n) {
-    const float2 gs = gh[((size_t)blockIdx.z * g.nxh + u) * g.ldh + v];
+  float gr[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) gr[q] = 0.f;
+  if (u < g.ncols && v < n) {
+    const float2 gs = gh[((size_t)blockIdx.z * g.ncols + u) * g.ldh + v];
     const float ux = (float)fft_index(u, n), vy = (float)fft_index(v, n);
-    const float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    float o[3] = {fmaf(r01, vy, r00 * ux), fmaf(r11, vy, r10 * ux), fmaf(r21, vy, r20 * ux)};
+    float ew = 0.f;  // the surface's third coordinate
+    if constexpr (EW) {
+      ew = ewald_w(params + img, n) * fmaf(ux, ux, vy * vy);
+      o[0] = fmaf((float)params[img].rot[2], ew, o[0]);
+      o[1] = fmaf((float)params[img].rot[5], ew, o[1]);
+      o[2] = fmaf((float)params[img].rot[8], ew, o[2]);
+    }
     const SplineAxis ax = spline_axis(o[0], n, wrap);
     const SplineAxis ay = spline_axis(o[1], n, wrap);
     const SplineAxis az = spline_axis(o[2], n, wrap);
@@ -678,19 +701,285 @@ __global__ void __launch_bounds__(256)
       const float dLdo = gs.x * dH[a][0] + gs.y * dH[a][1];
       gr[2 * a] = dLdo * ux;
       gr[2 * a + 1] = dLdo * vy;
+      if constexpr (EW) gr[6 + a] = dLdo * ew;
     }
   }
 #pragma unroll
-  for (int q = 0; q < 6; ++q) gr[q] = warp_sum(gr[q]);
+  for (int q = 0; q < NR; ++q) gr[q] = warp_sum(gr[q]);
   if (lane == 0)
-    for (int q = 0; q < 6; ++q) red[warp][q] = gr[q];
+    for (int q = 0; q < NR; ++q) red[warp][q] = gr[q];
   __syncthreads();
-  if (threadIdx.x < 6) {
+  if (threadIdx.x < NR) {
     double acc = 0.0;
     for (int w = 0; w < 8; ++w) acc += (double)red[w][threadIdx.x];
     atomicAdd(&grads[img * 16 + kGradRot + threadIdx.x], acc);
   }
 }
+
+// ---------------------------------------------------------------------------
+// Ewald sphere (CJX_EWALD_SPHERE with CJX_APPLY_CTF): the transposes of
+// k_ewald_colfft (column FFTs of x and -x, the contrast pairing of +q with
+// -q), k_ewald_rows (complex rows: N-point inverse, Px window, Px-point
+// forward) and the column inverse FFT + Py window of the full surface (no
+// Hermitian fix), on the shared-memory FFTs.
+// ---------------------------------------------------------------------------
+constexpr int kEwAdjWarps = 4;  // warps per CTA in the Ewald loss kernel (one output column, two T2 columns each)
+
+// Cotangents of one output entry F(i, j) = T (V(pos, neg)) of ewald_epilogue,
+// given E = dL/dF: ga, gb for its inputs a = A[i] and b = B[-i] (before the
+// scale), and Re(conj(E) dF/d defocus).  With P = (w2 sin - w1 cos) / 2 and
+// Q = (w1 sin + w2 cos) / 2 of the aberration phase,
+//   V = (P (pos + neg).re + Q (pos + neg).im,  P (pos - neg).im + Q (neg - pos).re),
+// T the envelope times the translation phase; conj(T) E is dL/dV.
+struct EwaldAdj {
+  float2 ga, gb;
+  float ddf;
+};
+
+__device__ __forceinline__ EwaldAdj ewald_epilogue_adj(float2 a, float2 b, float2 E, int i, int j, int py, int px,
+                                                      uint32_t flags, const ImageConsts& c) {
+  a.x *= c.scale; a.y *= c.scale;
+  b.x *= c.scale; b.y *= c.scale;
+  const double qy = (double)fft_index(i, py) * c.qy_step;
+  const double qx = (double)j * c.qx_step;
+  const double k2 = qx * qx + qy * qy;
+  const double arg = aberration_cycles(qx, qy, k2, c) - c.ps_cycles;
+  const float r = (float)(arg - rint(arg));
+  float s, co;
+  sincospif(2.0f * r, &s, &co);
+  const int kNone = 0, kNyqCol = 1, kZeroColNyqRow = 2;
+  int rule = kNone;
+  float2 pos = a, neg = b;
+  if ((px % 2 == 0) && j == px / 2) {
+    rule = kNyqCol;
+    pos = cconj(b);
+  } else if (j == 0 && (py % 2 == 0) && i == py / 2) {
+    rule = kZeroColNyqRow;
+    pos = cconj(a);
+    neg = a;
+  }
+  const float P = 0.5f * (c.w2 * s - c.w1 * co), Q = 0.5f * (c.w1 * s + c.w2 * co);
+  const float Pd = 0.5f * (c.w2 * co + c.w1 * s), Qd = 0.5f * (c.w1 * co - c.w2 * s);  // d/d(2 pi arg)
+  const float sr = pos.x + neg.x, si = pos.y + neg.y;
+  const float dr = neg.x - pos.x, di = pos.y - neg.y;
+  float2 dv = make_float2(Pd * sr + Qd * si, Pd * di + Qd * dr);
+  if (rule == kZeroColNyqRow) dv.y = -dv.y;
+  // T: envelope and translation (zero at the self-conjugate entries)
+  float2 T = make_float2(1.f, 0.f);
+  if (flags & CJX_APPLY_ENVELOPE) {
+    const float e = c.env_amp * expf(-c.env_quarter_b * (float)k2);
+    T = make_float2(e, 0.f);
+  }
+  if (flags & CJX_APPLY_TRANSLATION) {
+    const bool ey = (py % 2 == 0), ex = (px % 2 == 0);
+    const bool self_conj = (ey && i == py / 2 && j == 0) || (ex && i == 0 && j == px / 2) ||
+                           (ey && ex && i == py / 2 && j == px / 2);
+    if (self_conj) {
+      T = make_float2(0.f, 0.f);
+    } else {
+      const double ph = qx * c.tx + qy * c.ty;
+      const float rp = (float)(ph - rint(ph));
+      float sp, cp;
+      sincospif(2.0f * rp, &sp, &cp);
+      T = cmul(T, make_float2(cp, -sp));
+    }
+  }
+  EwaldAdj out;
+  // dF/d defocus = T dV/d(2 pi arg) * 2 pi c_def k^2
+  const float dth = (float)(6.283185307179586 * c.c_def * k2);
+  const float2 dF = cmul(T, make_float2(dv.x * dth, dv.y * dth));
+  out.ddf = E.x * dF.x + E.y * dF.y;
+  float2 G = cmul(cconj(T), E);
+  if (rule == kZeroColNyqRow) G.y = -G.y;
+  const float2 dpos = make_float2(G.x * P - G.y * Q, G.x * Q + G.y * P);
+  const float2 dneg = make_float2(G.x * P + G.y * Q, G.x * Q - G.y * P);
+  float2 ga = dpos, gb = dneg;
+  if (rule == kNyqCol) {
+    ga = make_float2(0.f, 0.f);
+    gb = make_float2(dpos.x + dneg.x, dneg.y - dpos.y);
+  } else if (rule == kZeroColNyqRow) {
+    ga = make_float2(dpos.x + dneg.x, dneg.y - dpos.y);
+    gb = make_float2(0.f, 0.f);
+  }
+  out.ga = make_float2(c.scale * ga.x, c.scale * ga.y);
+  out.gb = make_float2(c.scale * gb.x, c.scale * gb.y);
+  return out;
+}
+
+// Loss and the adjoint of the Ewald column pass.  One warp per output column
+// x in [0, Px/2]: T2 columns x and (Px - x) mod Px are transformed, the
+// contrast formed, the loss taken on the Hermitian part of the x = 0 and
+// Nyquist columns (what irfftn reads), and the cotangents of both T2
+// columns (inverse FFT: the adjoint of the forward FFT) written back over them.
+__global__ void __launch_bounds__(kEwAdjWarps * 32)
+    k_ewald_loss_adj(float2* __restrict__ t2, const float2* __restrict__ obs, const cjx_image_params* __restrict__ params,
+                     const int32_t* __restrict__ order, double* __restrict__ grads, SliceGeom g, int64_t k0,
+                     float norm) {
+  extern __shared__ float2 smem[];
+  __shared__ float red[kEwAdjWarps][4];
+  const int py = g.py, px = g.px;
+  const int stride = 2 * py + 2;
+  float2* tw = smem;
+  float2* bufs = smem + py;  // per warp: A ping-pong, B ping-pong, F, gA, gB
+  build_twiddles(tw, py);
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  const ImageConsts c = load_image_consts(params + img, norm, py, px);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int x = blockIdx.x * kEwAdjWarps + warp;
+  float sl = 0.f, stx = 0.f, sty = 0.f, sdf = 0.f;
+  if (x < g.pxh) {
+    const int xm = (px - x) % px;
+    const bool pair = xm != x;
+    float2* a = bufs + warp * (2 * stride + 3 * py);
+    float2* b = a + stride;
+    float2* F = b + stride;
+    float2* gA = F + py;
+    float2* gB = gA + py;
+    float2* col = t2 + (size_t)blockIdx.y * py * g.ld2;
+    for (int i = lane; i < py; i += 32) {
+      a[i] = col[(size_t)i * g.ld2 + x];
+      if (pair) b[i] = col[(size_t)i * g.ld2 + xm];
+    }
+    __syncwarp();
+    const float2* A = warp_fft<-1>(a, a + py, g.plan_py, tw, lane);
+    const float2* B = pair ? warp_fft<-1>(b, b + py, g.plan_py, tw, lane) : A;
+    __syncwarp();
+    for (int i = lane; i < py; i += 32) F[i] = ewald_epilogue(A[i], B[(py - i) % py], i, x, py, px, g.flags, c);
+    __syncwarp();
+    const bool self_col = (x == 0) || ((px % 2 == 0) && x == px / 2);
+    const float wj = self_col ? 1.f : 2.f;
+    const float inv_pp = 1.0f / ((float)py * (float)px);
+    const float2* ocol = obs + (size_t)img * py * g.pxh + x;
+    for (int i = lane; i < py; i += 32) {
+      const float2 f = F[i];
+      float2 fh = f;
+      if (self_col) {
+        const float2 fm = F[(py - i) % py];
+        fh = make_float2(0.5f * (f.x + fm.x), 0.5f * (f.y - fm.y));
+      }
+      const float2 o = ocol[(size_t)i * g.pxh];
+      const float2 d = make_float2(fh.x - o.x, fh.y - o.y);
+      sl += wj * inv_pp * (d.x * d.x + d.y * d.y);
+      const float2 E = make_float2(2.f * wj * inv_pp * d.x, 2.f * wj * inv_pp * d.y);
+      const float zim = E.x * f.y - E.y * f.x;  // Im(conj(E) F): dL/dt = 2 pi q Im(conj(E) F)
+      stx += 6.283185307179586f * (float)((double)x * c.qx_step) * zim;
+      sty += 6.283185307179586f * (float)((double)fft_index(i, py) * c.qy_step) * zim;
+      const EwaldAdj ad = ewald_epilogue_adj(A[i], B[(py - i) % py], E, i, x, py, px, g.flags, c);
+      sdf += ad.ddf;
+      gA[i] = ad.ga;
+      gB[(py - i) % py] = ad.gb;
+    }
+    __syncwarp();
+    if (!pair) {
+      for (int i = lane; i < py; i += 32) gA[i] = make_float2(gA[i].x + gB[i].x, gA[i].y + gB[i].y);
+      __syncwarp();
+    }
+    // adjoint of the forward column FFTs (unnormalised inverse), into the ping-pong buffers
+    for (int i = lane; i < py; i += 32) {
+      a[i] = gA[i];
+      if (pair) b[i] = gB[i];
+    }
+    __syncwarp();
+    const float2* GA = warp_fft<+1>(a, a + py, g.plan_py, tw, lane);
+    const float2* GB = pair ? warp_fft<+1>(b, b + py, g.plan_py, tw, lane) : GA;
+    __syncwarp();
+    for (int i = lane; i < py; i += 32) {
+      col[(size_t)i * g.ld2 + x] = GA[i];
+      if (pair) col[(size_t)i * g.ld2 + xm] = GB[i];
+    }
+  }
+  sl = warp_sum(sl);
+  stx = warp_sum(stx);
+  sty = warp_sum(sty);
+  sdf = warp_sum(sdf);
+  if (lane == 0) {
+    red[warp][kGradLoss] = sl;
+    red[warp][kGradTx] = stx;
+    red[warp][kGradTy] = sty;
+    red[warp][kGradDf] = sdf;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (int w = 0; w < kEwAdjWarps; ++w) acc += (double)red[w][threadIdx.x];
+    atomicAdd(&grads[img * 16 + kGradLoss + threadIdx.x], acc);
+  }
+}
+
+// Adjoint of k_ewald_rows, one warp per row: g_T2 row -> Px-point inverse
+// (adjoint of the forward FFT) -> transpose of the Px window -> N-point
+// forward FFT (adjoint of the unnormalised inverse) -> g_T1 row.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_rows_adj(const float2* __restrict__ t2, float2* __restrict__ t1, SliceGeom g) {
+  extern __shared__ float2 smem[];
+  const int n = g.n, px = g.px;
+  const int L = max(n, px);
+  float2* twn = smem;
+  float2* twp = twn + n;
+  float2* bufs = twp + px;
+  build_twiddles(twn, n);
+  build_twiddles(twp, px);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kWarps + warp;
+  if (r >= g.py) return;
+  float2* a = bufs + warp * (2 * L + 2);
+  float2* b = a + L;
+  const float2* row = t2 + ((size_t)blockIdx.y * g.py + r) * g.ld2;
+  for (int m = lane; m < px; m += 32) a[m] = row[m];
+  __syncwarp();
+  float2* w = warp_fft<+1>(a, b, g.plan_px, twp, lane);
+  float2* z = (w == a) ? b : a;
+  for (int k = lane; k < n; k += 32) z[k] = make_float2(0.f, 0.f);
+  __syncwarp();
+  for (int m = lane; m < px; m += 32) {
+    const int src = win_src(m, n, px, g.pad_left_x);
+    if (src >= 0) z[src] = w[m];
+  }
+  __syncwarp();
+  const float2* Z = warp_fft<-1>(z, w, g.plan_n, twn, lane);
+  float2* dst = t1 + ((size_t)blockIdx.y * g.py + r) * g.ld1;
+  for (int k = lane; k < n; k += 32) dst[k] = Z[k];
+}
+
+// Adjoint of the column inverse FFT + Py window over the full surface, one
+// warp per column j in [0, N): g_T1 column -> transpose of the window ->
+// N-point forward FFT -> the surface cotangent H[j][*].
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_colfft_adj(const float2* __restrict__ t1, float2* __restrict__ hb, SliceGeom g) {
+  extern __shared__ float2 smem[];
+  const int n = g.n;
+  float2* tw = smem;
+  float2* bufs = smem + n;
+  build_twiddles(tw, n);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.x * kWarps + warp;
+  if (j >= g.ncols) return;
+  float2* a = bufs + warp * (2 * n + 2);
+  float2* b = a + n;
+  for (int k = lane; k < n; k += 32) a[k] = make_float2(0.f, 0.f);
+  __syncwarp();
+  const float2* col = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j;
+  for (int m = lane; m < g.py; m += 32) {
+    const int src = win_src(m, n, g.py, g.pad_left_y);
+    if (src >= 0) a[src] = col[(size_t)m * g.ld1];
+  }
+  __syncwarp();
+  const float2* Z = warp_fft<-1>(a, b, g.plan_n, tw, lane);
+  float2* dst = hb + ((size_t)blockIdx.y * g.ncols + j) * g.ldh;
+  for (int k = lane; k < n; k += 32) dst[k] = Z[k];
+}
+
+size_t ewald_loss_smem(const SliceGeom& g) {
+  return sizeof(float2) * (size_t)(g.py + kEwAdjWarps * (2 * (2 * g.py + 2) + 3 * g.py));
+}
+size_t ewald_rows_adj_smem(const SliceGeom& g) {
+  return sizeof(float2) * (size_t)(g.n + g.px + kWarps * (2 * std::max(g.n, g.px) + 2));
+}
+size_t ewald_colfft_adj_smem(const SliceGeom& g) { return sizeof(float2) * (size_t)(g.n + kWarps * (2 * g.n + 2)); }
 
 // ---------------------------------------------------------------------------
 // Host launcher
@@ -715,6 +1004,9 @@ static int ensure_adjoint_smem_attrs() {
     CJX_ADJ_ATTR(1) CJX_ADJ_ATTR(2) CJX_ADJ_ATTR(3) CJX_ADJ_ATTR(4) CJX_ADJ_ATTR(5)
     CJX_ADJ_ATTR(6) CJX_ADJ_ATTR(8) CJX_ADJ_ATTR(10) CJX_ADJ_ATTR(12) CJX_ADJ_ATTR(16)
 #undef CJX_ADJ_ATTR
+    if (e == cudaSuccess) e = allow_smem_adj(k_ewald_loss_adj);
+    if (e == cudaSuccess) e = allow_smem_adj(k_ewald_rows_adj);
+    if (e == cudaSuccess) e = allow_smem_adj(k_ewald_colfft_adj);
     return e;
   });
   return err == cudaSuccess ? CJX_OK : check_cuda(err, "cudaFuncSetAttribute (adjoint kernels)");
@@ -725,19 +1017,51 @@ __global__ void k_zero_doubles(double* p, int64_t count) {
     p[i] = 0.0;
 }
 
-template <typename Layout, typename GL>
+template <typename Layout, typename GL, bool EW>
 static void launch_scatter(int mode, dim3 gs, cudaStream_t stream, const float2* grid, const float2* hb,
                            const cjx_image_params* params, const int32_t* order, float2* grad_grid, double* grads,
                            const SliceGeom& g, int64_t k0) {
   switch (mode) {
-#define CJX_SC_CASE(M)                                                                                         \
-  case M:                                                                                                      \
-    k_scatter_slice<Layout, M, GL><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0); \
+#define CJX_SC_CASE(M)                                                                                             \
+  case M:                                                                                                          \
+    k_scatter_slice<Layout, M, GL, EW><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads, g, k0); \
     break;
     CJX_SC_CASE(kScatterCorner) CJX_SC_CASE(kScatterVec) CJX_SC_CASE(kScatterWarpAgg)
 #undef CJX_SC_CASE
     default:
       break;
+  }
+}
+
+// The grid scatter for one chunk: spline coefficients (C order or bricked), or voxel grids in any layout
+// scattering into the bricked accumulator (use_acc) or straight into grid_grad.
+template <bool EW>
+static void dispatch_scatter(dim3 gs, cudaStream_t stream, const float2* grid, const float2* hb,
+                             const cjx_image_params* params, const int32_t* order, float2* grad_grid, float2* target,
+                             double* grads, const SliceGeom& g, int64_t k0, int mode, bool use_acc) {
+  const bool pairs = (g.flags & CJX_GRID_BRICKED_PAIRS) != 0;
+  const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
+  if (g.flags & CJX_GRID_SPLINE) {
+    if (bricked)
+      k_scatter_slice_spline<SplineBrickLayout, EW><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads,
+                                                                            g, k0);
+    else
+      k_scatter_slice_spline<SplineLinearLayout, EW><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid,
+                                                                             grads, g, k0);
+  } else if (use_acc) {
+    if (pairs)
+      launch_scatter<PairLayout, BrickLayout, EW>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+    else if (bricked)
+      launch_scatter<BrickLayout, BrickLayout, EW>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+    else
+      launch_scatter<LinearLayout, BrickLayout, EW>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+  } else {
+    if (pairs)
+      launch_scatter<PairLayout, LinearLayout, EW>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+    else if (bricked)
+      launch_scatter<BrickLayout, LinearLayout, EW>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
+    else
+      launch_scatter<LinearLayout, LinearLayout, EW>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
   }
 }
 
@@ -751,7 +1075,11 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
                      int64_t n_images, const float2* obs, double* grads, float2* grad_grid, float2* acc,
                      void* workspace, int64_t chunk, cudaStream_t stream, const Tuning& tn) {
   const int rn = reg_fft_radix(g.n), rpy = reg_fft_radix(g.py), rpx = reg_fft_radix(g.px);
-  if (!rn || !rpy || !rpx)
+  const bool ewald = (g.flags & CJX_EWALD_SPHERE) != 0;
+  if (ewald && !(g.flags & CJX_APPLY_CTF))
+    return fail(CJX_ERR_UNSUPPORTED, "loss gradient on the Ewald sphere needs the contrast transfer (CJX_APPLY_CTF)");
+  // the Ewald adjoint runs on the shared-memory FFTs (any size the forward takes)
+  if (!ewald && (!rn || !rpy || !rpx))
     return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs N, Py, Px = 32 R with R in {1-6, 8, 10, 12, 16}");
   prof_begin(stream);
   k_zero_doubles<<<64, 256, 0, stream>>>(grads, n_images * 16);
@@ -765,11 +1093,12 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
                         sizeof(int) * (size_t)g.n;
   const size_t s_cols = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(std::max(g.n, g.py)) + 1)) +
                         sizeof(int) * (size_t)g.n;
-  if (s_loss > 227 * 1024 || s_rows > 227 * 1024 || s_cols > 227 * 1024)
+  const size_t e_loss = ewald_loss_smem(g), e_rows = ewald_rows_adj_smem(g), e_cols = ewald_colfft_adj_smem(g);
+  if (ewald ? (e_loss > 227 * 1024 || e_rows > 227 * 1024 || e_cols > 227 * 1024)
+            : (s_loss > 227 * 1024 || s_rows > 227 * 1024 || s_cols > 227 * 1024))
     return fail(CJX_ERR_UNSUPPORTED, "loss gradient shared-memory footprint above 227 KB for these sizes");
   if (int e = ensure_adjoint_smem_attrs()) return e;
   const bool pairs = (g.flags & CJX_GRID_BRICKED_PAIRS) != 0;
-  const bool bricked = (g.flags & CJX_GRID_BRICKED) != 0;
   if (pairs && (g.flags & CJX_GRID_SPLINE))
     return fail(CJX_ERR_UNSUPPORTED, "the spline adjoint reads the coefficients in the linear or bricked layout");
   // the 16-byte atomics need a 16-byte aligned gradient array
@@ -788,6 +1117,18 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
   for (int64_t k0 = 0; k0 < n_images; k0 += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_images - k0);
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
+    if (ewald) {
+      prof_begin(stream);
+      k_ewald_loss_adj<<<dim3((g.pxh + kEwAdjWarps - 1) / kEwAdjWarps, cnt), kEwAdjWarps * 32, e_loss, stream>>>(
+          t2, obs, params, order, grads, g, k0, norm);
+      prof_end("k_ewald_loss_adj", stream);
+      prof_begin(stream);
+      k_ewald_rows_adj<<<dim3((g.py + kWarps - 1) / kWarps, cnt), kWarps * 32, e_rows, stream>>>(t2, t1, g);
+      prof_end("k_ewald_rows_adj", stream);
+      prof_begin(stream);
+      k_ewald_colfft_adj<<<dim3((g.ncols + kWarps - 1) / kWarps, cnt), kWarps * 32, e_cols, stream>>>(t1, hb, g);
+      prof_end("k_ewald_colfft_adj", stream);
+    } else {
     prof_begin(stream);
     const dim3 gl((g.pxh + kWarps - 1) / kWarps, cnt);
     switch (rpy) {
@@ -818,30 +1159,13 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
 #undef CJX_CA_CASE
     }
     prof_end("k_colfft_adj", stream);
-    prof_begin(stream);
-    const dim3 gs((g.nxh + 15) / 16, (g.n + 15) / 16, cnt);
-    if (g.flags & CJX_GRID_SPLINE) {
-      if (bricked)
-        k_scatter_slice_spline<SplineBrickLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid, grads,
-                                                                          g, k0);
-      else
-        k_scatter_slice_spline<SplineLinearLayout><<<gs, 256, 0, stream>>>(grid, hb, params, order, grad_grid,
-                                                                           grads, g, k0);
-    } else if (use_acc) {
-      if (pairs)
-        launch_scatter<PairLayout, BrickLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
-      else if (bricked)
-        launch_scatter<BrickLayout, BrickLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
-      else
-        launch_scatter<LinearLayout, BrickLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
-    } else {
-      if (pairs)
-        launch_scatter<PairLayout, LinearLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
-      else if (bricked)
-        launch_scatter<BrickLayout, LinearLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
-      else
-        launch_scatter<LinearLayout, LinearLayout>(mode, gs, stream, grid, hb, params, order, target, grads, g, k0);
     }
+    prof_begin(stream);
+    const dim3 gs((g.ncols + 15) / 16, (g.n + 15) / 16, cnt);
+    if (ewald)
+      dispatch_scatter<true>(gs, stream, grid, hb, params, order, grad_grid, target, grads, g, k0, mode, use_acc);
+    else
+      dispatch_scatter<false>(gs, stream, grid, hb, params, order, grad_grid, target, grads, g, k0, mode, use_acc);
     prof_end("k_scatter_slice", stream);
   }
   if (use_acc) {

@@ -286,7 +286,8 @@ int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_t n_imag
   SliceGeom g;
   if (int e = make_geom(desc, &g)) return e;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
-  if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
+  if ((g.flags & CJX_EWALD_SPHERE) && !(g.flags & CJX_APPLY_CTF))
+    return fail(CJX_ERR_UNSUPPORTED, "loss gradient on the Ewald sphere needs the contrast transfer (CJX_APPLY_CTF)");
   const size_t acc = (g.flags & CJX_GRID_SPLINE) ? 0 : loss_accumulator_bytes(g.n);
   *bytes = n_images > 0 ? (size_t)chunk_for(g, desc, n_images) * workspace_per_image(g) + acc : 0;
   return CJX_OK;
@@ -300,7 +301,8 @@ int cjx_slice_ctf_loss_grad(const cjx_slice_desc* desc, const void* grid, const 
   if (n_images < 0) return fail(CJX_ERR_INVALID_ARGUMENT, "n_images < 0");
   if (n_images == 0) return CJX_OK;
   if (!needs_resize(g)) return fail(CJX_ERR_UNSUPPORTED, "loss gradient needs the resize path ((Py, Px) != (N, N))");
-  if (g.flags & CJX_EWALD_SPHERE) return fail(CJX_ERR_UNSUPPORTED, "loss gradient of the Ewald sphere is not implemented");
+  if ((g.flags & CJX_EWALD_SPHERE) && !(g.flags & CJX_APPLY_CTF))
+    return fail(CJX_ERR_UNSUPPORTED, "loss gradient on the Ewald sphere needs the contrast transfer (CJX_APPLY_CTF)");
   if (!grid || !params || !observed || !image_grads)
     return fail(CJX_ERR_INVALID_ARGUMENT, "grid, params, observed and image_grads must be non-NULL");
   if (int e = check_alignment(g.flags, grid, observed)) return e;

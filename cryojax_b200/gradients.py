@@ -123,8 +123,11 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
     Returns a dict with ``loss`` (n,), the pose gradient under the pose's own
     parameter name (``d_wxyz`` (n, 4), ``d_euler_angles`` (n, 3) in degrees,
     or ``d_euler_vector`` (n, 3)), ``d_offset`` (n, 2), ``d_defocus`` (n,),
-    ``d_rotation`` (n, 3, 2) and, with ``grid_grad``, ``d_grid`` (complex64,
-    shape of the grid, summed over the images).
+    ``d_rotation`` (n, 3, 2) (dL/dR for R's first two columns; (n, 3, 3) on the
+    Ewald sphere, whose surface has a third coordinate) and, with ``grid_grad``,
+    ``d_grid`` (complex64, shape of the grid, summed over the images).
+    Volume integrators: FourierSliceExtraction and EwaldSphereExtraction (with
+    a ContrastTransferTheory).
     """
     torch = _torch()
     from .simulator import orientation_order
@@ -136,8 +139,7 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
     integ = model.volume_integrator
     params = model.image_params()
     n = params.shape[0]
-    if not integ.is_projection_approximation:
-        raise NotImplementedError("gradients through the Ewald sphere are not implemented on the device")
+    ewald = not integ.is_projection_approximation  # EwaldSphereExtraction: R's third column enters too
     dev = vol.device
     flags = model._flags() | integ._base_flags()
     if hasattr(vol, "spline_coefficients"):  # gradient with respect to the spline coefficients
@@ -170,11 +172,13 @@ def squared_residual_and_grad(model, observed, *, grid_grad: bool = True, observ
     nat.slice_ctf_loss_grad(desc, grid, pd, obs_f, grads, gg, ws, order=order)
     g = grads.cpu().numpy()
     d_rot = g[:, nat.G_ROT:nat.G_ROT + 6].reshape(n, 3, 2)
+    if ewald:  # the third column's entries follow the first two columns'
+        d_rot = np.concatenate([d_rot, g[:, nat.G_ROT + 6:nat.G_ROT + 9, None]], axis=2)
     # chain dL/dR -> pose parameters (float64 autograd on the host)
     pvals, pname = _pose_param_array(model.pose, n)
     p_t = torch.tensor(np.ascontiguousarray(pvals), dtype=torch.float64, requires_grad=True)
     R = _pose_rotation_t(model.pose, p_t)
-    (R[:, :, 0:2] * torch.as_tensor(d_rot)).sum().backward()
+    (R[:, :, 0:d_rot.shape[2]] * torch.as_tensor(d_rot)).sum().backward()
     out = {
         "loss": g[:, nat.G_LOSS].copy(),
         pname: p_t.grad.numpy().copy(),

@@ -95,8 +95,8 @@ extern "C" {
  * Without CJX_APPLY_CTF the output is the integrator's full spectrum
  * [Py][Px] (scale applied; no envelope or translation allowed).  Any grid
  * layout, trilinear or spline.  Forward, multi and no-alloc entry points,
- * and cjx_search with CJX_APPLY_CTF (the scores are the contrast images'
- * NCC); not loss_grad.                                                    */
+ * cjx_search with CJX_APPLY_CTF (the scores are the contrast images'
+ * NCC) and cjx_slice_ctf_loss_grad with CJX_APPLY_CTF.                    */
 #define CJX_EWALD_SPHERE (1u << 7)
 
 /* ---- per-image parameters (one record per image, device memory) ------
@@ -190,7 +190,9 @@ typedef struct cjx_image_grads {
   double d_rot[6];    /* dL / dR[i][j] for j = 0, 1 (the columns that span
                          the slice plane), row-major [3][2]; chain to the
                          pose parameters on the host                         */
-  double reserved[6];
+  double d_rot_z[3];  /* dL / dR[i][2] (CJX_EWALD_SPHERE: the surface's third
+                         coordinate); zero for the slice                     */
+  double reserved[3];
 } cjx_image_grads;
 
 /* cjx_slice_ctf_forward with a Fourier-space filter fused into the output
@@ -223,7 +225,10 @@ CJX_API int cjx_slice_ctf_loss_workspace_size(const cjx_slice_desc* desc, int64_
  *    conjugate).  The caller zeroes it.
  * observed: device complex64 [n_images][Py][Px/2+1], rfftn of the observed
  * real-space images in cryoJAX's convention (ifftshift, then rfft2).
- * Resize path only, with N, Py, Px of the form 32 R (R in 1-6, 8, 10, 12, 16).
+ * Resize path only, with N, Py, Px of the form 32 R (R in 1-6, 8, 10, 12, 16)
+ * for the slice; on the Ewald sphere (CJX_EWALD_SPHERE, which needs
+ * CJX_APPLY_CTF: the loss is on the contrast image) any size the forward
+ * takes, on the shared-memory FFTs.
  * grid: C order, bricked, or x-pair bricked (16-byte aligned) for a voxel
  * grid; C order or bricked for spline coefficients.  grid_grad must be
  * 8-byte aligned (16 for the 16-byte atomics of CJX_TUNE_SCATTER_VEC 1).

@@ -126,10 +126,12 @@ def test_spline_flag_validation():
     d = nat.make_desc(64, 32, 32, nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED)
     assert nat.workspace_size(d, 2) == nat.workspace_size(nat.make_desc(64, 32, 32, 0), 2)
     assert nat.workspace_size(nat.make_desc(64, 32, 32, nat.CJX_GRID_SPLINE | nat.CJX_GRID_BRICKED_PAIRS), 1) > 0
-    # spline volumes have loss gradients; the Ewald sphere has none
+    # spline volumes and the Ewald sphere's contrast have loss gradients; the Ewald sphere's bare spectrum
+    # (no contrast transfer) has none
     assert nat.loss_workspace_size(nat.make_desc(64, 32, 32, nat.CJX_GRID_SPLINE), 1) > 0
+    assert nat.loss_workspace_size(nat.make_desc(64, 32, 32, nat.CJX_EWALD_SPHERE | nat.CJX_APPLY_CTF), 1) > 0
     with pytest.raises(nat.CryojaxB200Error) as e:
-        nat.loss_workspace_size(nat.make_desc(64, 32, 32, nat.CJX_EWALD_SPHERE | nat.CJX_APPLY_CTF), 1)
+        nat.loss_workspace_size(nat.make_desc(64, 32, 32, nat.CJX_EWALD_SPHERE), 1)
     assert e.value.code == nat.CJX_ERR_UNSUPPORTED
     # coefficient solve: N in [4, CJX_MAX_SIDE], scratch N (N + 2)^2 complex64
     assert nat.spline_coefficients_workspace_size(64) == 8 * 64 * 66 * 66
