@@ -70,8 +70,7 @@ def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_s
         raise NotImplementedError("refinement needs padded_shape == shape")
     vol = image_model.volume_parametrization.get_representation()
     integ = image_model.volume_integrator
-    if not integ.is_projection_approximation:
-        raise NotImplementedError("refinement through the Ewald sphere is not implemented on the device")
+    ewald = not integ.is_projection_approximation  # the surface's third coordinate: R's third column enters
     dev = vol.device
     params = image_model.image_params().copy()
     n = params.shape[0]
@@ -107,7 +106,10 @@ def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_s
         hist[it] = loss
         R = cur[:, 0:9].reshape(n, 3, 3)
         dR = g[:, nat.G_ROT:nat.G_ROT + 6].reshape(n, 3, 2)
+        # dL/dw for R -> exp([w]x) R: the sum over R's columns of column x dL/dcolumn
         gw = np.cross(R[:, :, 0], dR[:, :, 0]) + np.cross(R[:, :, 1], dR[:, :, 1])
+        if ewald:
+            gw += np.cross(R[:, :, 2], g[:, nat.G_ROT + 6:nat.G_ROT + 9])
         better = loss < best_loss
         if it > 0:
             accepted += better

@@ -148,9 +148,11 @@ def test_ewald_rejections(cuda_device):
     with pytest.raises(nat.CryojaxB200Error) as e:
         nat.workspace_size(nat.make_desc(32, 16, 16, nat.CJX_EWALD_SPHERE | nat.CJX_APPLY_TRANSLATION), 1)
     assert e.value.code == nat.CJX_ERR_INVALID_ARGUMENT
+    # the loss gradient is on the contrast image: the bare spectrum has none
     with pytest.raises(nat.CryojaxB200Error) as e:
-        nat.loss_workspace_size(nat.make_desc(32, 16, 16, nat.CJX_EWALD_SPHERE | nat.CJX_APPLY_CTF), 1)
+        nat.loss_workspace_size(nat.make_desc(32, 16, 16, nat.CJX_EWALD_SPHERE), 1)
     assert e.value.code == nat.CJX_ERR_UNSUPPORTED
+    assert nat.loss_workspace_size(nat.make_desc(32, 16, 16, nat.CJX_EWALD_SPHERE | nat.CJX_APPLY_CTF), 1) > 0
     torch.cuda.synchronize()
 
 

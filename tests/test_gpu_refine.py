@@ -126,3 +126,38 @@ def test_refinement_on_a_spline_volume(cuda_device):
     err = rotation_angle_deg(res.rotations, rot.quat_to_matrix(q_true))
     assert np.all(res.loss <= res.loss_history[0] + 1e-9)
     assert np.sum(err < 0.5) >= 7, err
+
+
+def test_refinement_on_the_ewald_sphere(cuda_device):
+    """The same refinement through EwaldSphereExtraction at 40 kV (the surface leaves the plane by up to about a
+    voxel at its corners), against the oracle's Ewald contrast simulations of the truth."""
+    import torch
+
+    from cryojax_b200 import rotations as rot
+    from cryojax_b200 import simulator as S
+    from cryojax_b200.refine import refine_poses, rotation_angle_deg
+
+    n = 8
+    _, grid, fs = make_volume(64, 150, seed=10)
+    q_true, _ = O.uniform_poses(n, 11, 0.0)
+    rng = np.random.default_rng(12)
+    specs, obs = [], []
+    for b in range(n):
+        s = O.ImageSpec(shape=(64, 64), pixel_size=2.0, voltage_in_kilovolts=40.0, wxyz=q_true[b],
+                        offset_in_angstroms=(0.0, 0.0), defocus_in_angstroms=rng.uniform(8000, 15000),
+                        astigmatism_in_angstroms=100.0, astigmatism_angle=20.0, amplitude_contrast_ratio=0.1)
+        img = O.simulate(grid, fs, s, ewald=True)
+        obs.append(img + rng.standard_normal(img.shape) * np.sqrt(img.var() / 5.0))
+        s2 = copy.deepcopy(s)
+        axis = rng.standard_normal(3)
+        axis /= np.linalg.norm(axis)
+        s2.wxyz = O.quat_compose(O.so3_exp(np.deg2rad(rng.uniform(2, 4)) * axis), q_true[b])
+        specs.append(s2)
+    pose, tt, cfg = specs_to_model_args(specs)
+    vol = S.FourierVoxelGridVolume(torch.as_tensor(grid.astype(np.complex64)).cuda())
+    integ = S.EwaldSphereExtraction(outputs_integral=False)
+    res = refine_poses(S.make_image_model(vol, cfg, pose, tt, volume_integrator=integ), np.stack(obs), steps=20,
+                       rot_step_deg=2.0, defocus_step=150.0)
+    err = rotation_angle_deg(res.rotations, rot.quat_to_matrix(q_true))
+    assert np.all(res.loss <= res.loss_history[0] + 1e-9)
+    assert np.sum(err < 0.5) >= 7, err
