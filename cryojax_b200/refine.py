@@ -54,6 +54,18 @@ def _exp_so3(w):
     return rot.quat_to_matrix(q)
 
 
+def rotation_step_gradient(R, g, ewald=False):
+    """dL/dw at w = 0 for the rotation step R -> exp([w]x) R, from the per-image gradient records g (n, 16):
+    the sum over R's columns c of R[:, c] x dL/dR[:, c] (columns 0 and 1; column 2 too on the Ewald sphere,
+    whose surface has a third coordinate)."""
+    n = g.shape[0]
+    dR = g[:, nat.G_ROT:nat.G_ROT + 6].reshape(n, 3, 2)
+    gw = np.cross(R[:, :, 0], dR[:, :, 0]) + np.cross(R[:, :, 1], dR[:, :, 1])
+    if ewald:
+        gw = gw + np.cross(R[:, :, 2], g[:, nat.G_ROT + 6:nat.G_ROT + 9])
+    return gw
+
+
 def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_step=200.0, grow=1.25, shrink=0.5,
                  observed_is_fourier=False, min_rot_step_deg=1e-3, min_defocus_step=0.1) -> RefineResult:
     """Refine every image's rotation and defocus starting from the image model's pose and CTF.
@@ -104,12 +116,7 @@ def refine_poses(image_model, observed, *, steps=20, rot_step_deg=2.0, defocus_s
         g = grads.cpu().numpy()
         loss = g[:, nat.G_LOSS]
         hist[it] = loss
-        R = cur[:, 0:9].reshape(n, 3, 3)
-        dR = g[:, nat.G_ROT:nat.G_ROT + 6].reshape(n, 3, 2)
-        # dL/dw for R -> exp([w]x) R: the sum over R's columns of column x dL/dcolumn
-        gw = np.cross(R[:, :, 0], dR[:, :, 0]) + np.cross(R[:, :, 1], dR[:, :, 1])
-        if ewald:
-            gw += np.cross(R[:, :, 2], g[:, nat.G_ROT + 6:nat.G_ROT + 9])
+        gw = rotation_step_gradient(cur[:, 0:9].reshape(n, 3, 3), g, ewald)
         better = loss < best_loss
         if it > 0:
             accepted += better

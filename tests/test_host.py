@@ -170,3 +170,29 @@ def test_host_streaming_sub_batch_plan():
     assert sim.sub_batches(0) == [] and sim.sub_batches(100) == [(0, 100)]
     sim.sub_batch = 3
     assert sim.sub_batches(10) == [(0, 1), (1, 2), (3, 3), (6, 3), (9, 1)]
+
+
+@pytest.mark.parametrize("ewald", [False, True])
+def test_rotation_step_gradient_is_the_derivative_along_the_step(ewald):
+    """refine's rotation step R -> exp([w]x) R: for a loss linear in R with dL/dR = G (the columns the gradient
+    record holds: 0 and 1, and 2 on the Ewald sphere), dL/dw at w = 0 equals central differences of
+    L(exp([w]x) R)."""
+    from cryojax_b200.refine import _exp_so3, rotation_step_gradient
+
+    rng = np.random.default_rng(3)
+    n = 4
+    R = rot.quat_to_matrix(rot.quat_normalize(rng.standard_normal((n, 4))))
+    G = rng.standard_normal((n, 3, 3))
+    if not ewald:
+        G[:, :, 2] = 0.0
+    g = np.zeros((n, nat.GRAD_DOUBLES))
+    g[:, nat.G_ROT:nat.G_ROT + 6] = G[:, :, 0:2].reshape(n, 6)
+    g[:, nat.G_ROT + 6:nat.G_ROT + 9] = G[:, :, 2]
+    gw = rotation_step_gradient(R, g, ewald)
+    h = 1e-6
+    for a in range(3):
+        w = np.zeros((n, 3))
+        w[:, a] = h
+        lp = np.einsum("nij,nij->n", G, _exp_so3(w) @ R)
+        lm = np.einsum("nij,nij->n", G, _exp_so3(-w) @ R)
+        np.testing.assert_allclose(gw[:, a], (lp - lm) / (2 * h), rtol=1e-6, atol=1e-8)
