@@ -18,6 +18,10 @@
 //   k_scatter_slice     trilinear scatter-add of the slice gradient into the
 //                       grid gradient (float2 / float4 atomics) and d/dR from the
 //                       derivative of the interpolation weights.
+// On the Ewald sphere (CJX_EWALD_SPHERE with CJX_APPLY_CTF) the first three
+// are k_ewald_loss_adj (contrast pairing of +q with -q), k_ewald_rows_adj
+// (complex rows) and k_ewald_colfft_adj (all N surface columns), and the
+// scatter samples the curved surface and adds R's third column to d/dR.
 // The gradient of a real loss w.r.t. a complex value z is reported as
 // dL/dRe z + i dL/dIm z (jax.grad returns its complex conjugate).
 #include <algorithm>
