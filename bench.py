@@ -519,12 +519,57 @@ def measure_gradient(dev, steps, warmup, seed):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    gnorm = float(gg.abs().pow(2).sum().sqrt())
+    ewald = measure_gradient_ewald(vol, model, obs_f, grid_b, gg, steps, warmup)
     return {"metric": "loss + gradient images/s (192^3 volume, 192^2 images, pose/offset/defocus/grid)",
             "value": n_img / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms, "images_per_step": n_img,
             "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()},
             "layout": "x-pair bricked grid" if layout == nat.CJX_GRID_BRICKED_PAIRS else "bricked grid",
             "scatter_mode": nat.tuning_get(nat.CJX_TUNE_SCATTER_VEC),
-            "mean_loss": float(np.mean(res["loss"])), "grid_grad_norm": float(gg.abs().pow(2).sum().sqrt())}
+            "mean_loss": float(np.mean(res["loss"])), "grid_grad_norm": gnorm, "ewald_sphere": ewald}
+
+
+def measure_gradient_ewald(vol, model, obs_f, grid_b, gg, steps, warmup):
+    """The same loss + gradients through EwaldSphereExtraction (300 kV contrast), same volume, poses, CTFs
+    and observed images; one step = one cjx_slice_ctf_loss_grad call over the 1024 images."""
+    import torch
+
+    from cryojax_b200 import _native as nat
+    from cryojax_b200 import simulator as S
+
+    try:
+        n_img = obs_f.shape[0]
+        integ = S.EwaldSphereExtraction()
+        em = S.make_image_model(vol, model.image_config, model.pose, model.transfer_theory, volume_integrator=integ)
+        params = em.image_params()
+        desc = nat.make_desc(vol.shape[0], 192, 192, em._flags() | integ._base_flags() | nat.CJX_GRID_BRICKED)
+        dev = obs_f.device
+        pd = torch.as_tensor(params, device=dev)
+        order = torch.as_tensor(S.orientation_order(params[:, 0:9].reshape(-1, 3, 3)), device=dev)
+        grads = torch.empty((n_img, nat.GRAD_DOUBLES), dtype=torch.float64, device=dev)
+        ws = torch.empty(nat.loss_workspace_size(desc, n_img), dtype=torch.uint8, device=dev)
+        gg.zero_()
+        for _ in range(warmup):
+            nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
+        torch.cuda.synchronize()
+        nat.profile_enable(True)
+        nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
+        torch.cuda.synchronize()
+        prof = nat.profile_read()
+        nat.profile_enable(False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            nat.slice_ctf_loss_grad(desc, grid_b, pd, obs_f, grads, gg, ws, order=order)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        return {"value": n_img / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms,
+                "kernels_per_step": {k: {"launches": c, "ms": t} for k, (c, t) in prof.items()},
+                "mean_loss": float(grads[:, nat.G_LOSS].mean())}
+    except Exception as exc:  # reported in the line; the slice figures above stand
+        nat.profile_enable(False)
+        return {"error": f"{type(exc).__name__}: {exc}"}
 
 
 def measure_pose_search(dev, seed, n_obs):
