@@ -977,6 +977,128 @@ __global__ void __launch_bounds__(kWarps * 32)
   for (int k = lane; k < n; k += 32) dst[k] = Z[k];
 }
 
+// Register-FFT forms (N, Px = 32 R): the transforms in registers
+// (cjx_fft.cuh), shared memory for the tables, the window's inverse map
+// winv[k] (the m with win_src(m) = k, or -1; win_src is one-to-one) and the
+// per-warp staging that keeps the row loads and stores coalesced.
+template <int RN, int RP>
+__device__ __forceinline__ void ewald_row_adj_reg(float2 (&w)[RP], float2* __restrict__ dst, float2* buf,
+                                                  const float2* tabN, const float2* tabP, const LaneTwiddles& lt,
+                                                  int lane, const int* winv) {
+  constexpr int n = 32 * RN;
+  const int bl = brev5(lane);
+  warp_fft_reg<RP, +1>(w, tabP, lt, lane);  // adjoint of the forward Px-point FFT
+#pragma unroll
+  for (int k1 = 0; k1 < RP; ++k1) buf[pad16(k1 + RP * lane)] = w[k1];
+  __syncwarp();
+  float2 z[RN];
+#pragma unroll
+  for (int n1 = 0; n1 < RN; ++n1) {
+    const int m = winv[32 * n1 + bl];
+    z[n1] = (m >= 0) ? buf[pad16(m)] : make_float2(0.f, 0.f);
+  }
+  __syncwarp();
+  warp_fft_reg<RN, -1>(z, tabN, lt, lane);  // adjoint of the unnormalised N-point inverse
+#pragma unroll
+  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+  __syncwarp();
+  for (int k = lane; k < n; k += 32) dst[k] = buf[pad16(k)];
+}
+
+template <int RN>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_rows_adj_reg(const float2* __restrict__ t2, float2* __restrict__ t1, SliceGeom g, int rp) {
+  constexpr int n = 32 * RN;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  const int px = g.px;
+  const int stride = pad16(max(n, px)) + 1;
+  float2* tabN = smem;
+  float2* tabP = tabN + n;
+  float2* bufs = tabP + px;
+  int* winv = reinterpret_cast<int*>(bufs + kWarps * stride);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kWarps + warp;
+  const int bl = brev5(lane);
+  build_reg_twiddles(tabN, n);
+  build_reg_twiddles(tabP, px);
+  build_w32(w32);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) winv[k] = -1;
+  __syncthreads();
+  for (int m = threadIdx.x; m < px; m += blockDim.x) {
+    const int s = win_src(m, n, px, g.pad_left_x);
+    if (s >= 0) winv[s] = m;
+  }
+  __syncthreads();
+  if (r >= g.py) return;
+  const float2* row = t2 + ((size_t)blockIdx.y * g.py + r) * g.ld2;
+  float2* dst = t1 + ((size_t)blockIdx.y * g.py + r) * g.ld1;
+  float2* buf = bufs + warp * stride;
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  switch (rp) {
+#define CJX_ERADJ_CASE(RPV)                                                  \
+  case RPV: {                                                                \
+    float2 v[RPV];                                                           \
+    for (int q = 0; q < RPV; ++q) v[q] = row[32 * q + bl];                   \
+    ewald_row_adj_reg<RN, RPV>(v, dst, buf, tabN, tabP, lt, lane, winv);     \
+  } break;
+    CJX_ERADJ_CASE(1) CJX_ERADJ_CASE(2) CJX_ERADJ_CASE(3) CJX_ERADJ_CASE(4) CJX_ERADJ_CASE(5)
+    CJX_ERADJ_CASE(6) CJX_ERADJ_CASE(8) CJX_ERADJ_CASE(10) CJX_ERADJ_CASE(12) CJX_ERADJ_CASE(16)
+#undef CJX_ERADJ_CASE
+    default: break;
+  }
+}
+
+// Column adjoint in registers: the window transpose reads g_T1 straight into
+// the lane's bit-reversed inputs; the N-point FFT's output is staged so that
+// the surface column is stored contiguously.
+template <int RN>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_colfft_adj_reg(const float2* __restrict__ t1, float2* __restrict__ hb, SliceGeom g) {
+  constexpr int n = 32 * RN;
+  constexpr int stride = pad16(n) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  float2* tab = smem;
+  float2* bufs = smem + n;
+  int* winv = reinterpret_cast<int*>(bufs + kWarps * stride);
+  build_reg_twiddles(tab, n);
+  build_w32(w32);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) winv[k] = -1;
+  __syncthreads();
+  for (int m = threadIdx.x; m < g.py; m += blockDim.x) {
+    const int s = win_src(m, n, g.py, g.pad_left_y);
+    if (s >= 0) winv[s] = m;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.x * kWarps + warp;
+  if (j >= g.ncols) return;
+  const int bl = brev5(lane);
+  const float2* col = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j;
+  float2 z[RN];
+#pragma unroll
+  for (int n1 = 0; n1 < RN; ++n1) {
+    const int m = winv[32 * n1 + bl];
+    z[n1] = (m >= 0) ? col[(size_t)m * g.ld1] : make_float2(0.f, 0.f);
+  }
+  const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+  warp_fft_reg<RN, -1>(z, tab, lt, lane);
+  float2* buf = bufs + warp * stride;
+#pragma unroll
+  for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
+  __syncwarp();
+  float2* dst = hb + ((size_t)blockIdx.y * g.ncols + j) * g.ldh;
+  for (int k = lane; k < n; k += 32) dst[k] = buf[pad16(k)];
+}
+
+size_t ewald_rows_adj_reg_smem(const SliceGeom& g) {
+  return sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * g.n;
+}
+size_t ewald_colfft_adj_reg_smem(const SliceGeom& g) {
+  return sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * g.n;
+}
+
 size_t ewald_loss_smem(const SliceGeom& g) {
   return sizeof(float2) * (size_t)(g.py + kEwAdjWarps * (2 * (2 * g.py + 2) + 3 * g.py));
 }
@@ -1011,6 +1133,12 @@ static int ensure_adjoint_smem_attrs() {
     if (e == cudaSuccess) e = allow_smem_adj(k_ewald_loss_adj);
     if (e == cudaSuccess) e = allow_smem_adj(k_ewald_rows_adj);
     if (e == cudaSuccess) e = allow_smem_adj(k_ewald_colfft_adj);
+#define CJX_EADJ_ATTR(R)                                                         \
+  if (e == cudaSuccess) e = allow_smem_adj(k_ewald_rows_adj_reg<R>);             \
+  if (e == cudaSuccess) e = allow_smem_adj(k_ewald_colfft_adj_reg<R>);
+    CJX_EADJ_ATTR(1) CJX_EADJ_ATTR(2) CJX_EADJ_ATTR(3) CJX_EADJ_ATTR(4) CJX_EADJ_ATTR(5)
+    CJX_EADJ_ATTR(6) CJX_EADJ_ATTR(8) CJX_EADJ_ATTR(10) CJX_EADJ_ATTR(12) CJX_EADJ_ATTR(16)
+#undef CJX_EADJ_ATTR
     return e;
   });
   return err == cudaSuccess ? CJX_OK : check_cuda(err, "cudaFuncSetAttribute (adjoint kernels)");
@@ -1097,7 +1225,12 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
                         sizeof(int) * (size_t)g.n;
   const size_t s_cols = sizeof(float2) * (size_t)(g.n + kWarps * (pad16(std::max(g.n, g.py)) + 1)) +
                         sizeof(int) * (size_t)g.n;
-  const size_t e_loss = ewald_loss_smem(g), e_rows = ewald_rows_adj_smem(g), e_cols = ewald_colfft_adj_smem(g);
+  // the Ewald row and column adjoints run on register FFTs where N and Px (rows) or N (columns) are 32 R
+  const bool ew_reg_rows = ewald && tn.fft_mode >= 1 && rn && rpx;
+  const bool ew_reg_cols = ewald && tn.fft_mode >= 1 && rn;
+  const size_t e_loss = ewald_loss_smem(g);
+  const size_t e_rows = ew_reg_rows ? ewald_rows_adj_reg_smem(g) : ewald_rows_adj_smem(g);
+  const size_t e_cols = ew_reg_cols ? ewald_colfft_adj_reg_smem(g) : ewald_colfft_adj_smem(g);
   if (ewald ? (e_loss > 227 * 1024 || e_rows > 227 * 1024 || e_cols > 227 * 1024)
             : (s_loss > 227 * 1024 || s_rows > 227 * 1024 || s_cols > 227 * 1024))
     return fail(CJX_ERR_UNSUPPORTED, "loss gradient shared-memory footprint above 227 KB for these sizes");
@@ -1127,10 +1260,32 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
           t2, obs, params, order, grads, g, k0, norm);
       prof_end("k_ewald_loss_adj", stream);
       prof_begin(stream);
-      k_ewald_rows_adj<<<dim3((g.py + kWarps - 1) / kWarps, cnt), kWarps * 32, e_rows, stream>>>(t2, t1, g);
+      const dim3 gr((g.py + kWarps - 1) / kWarps, cnt);
+      if (ew_reg_rows) {
+        switch (rn) {
+#define CJX_ERA_CASE(R) \
+  case R: k_ewald_rows_adj_reg<R><<<gr, kWarps * 32, e_rows, stream>>>(t2, t1, g, rpx); break;
+          CJX_ERA_CASE(1) CJX_ERA_CASE(2) CJX_ERA_CASE(3) CJX_ERA_CASE(4) CJX_ERA_CASE(5)
+          CJX_ERA_CASE(6) CJX_ERA_CASE(8) CJX_ERA_CASE(10) CJX_ERA_CASE(12) CJX_ERA_CASE(16)
+#undef CJX_ERA_CASE
+        }
+      } else {
+        k_ewald_rows_adj<<<gr, kWarps * 32, e_rows, stream>>>(t2, t1, g);
+      }
       prof_end("k_ewald_rows_adj", stream);
       prof_begin(stream);
-      k_ewald_colfft_adj<<<dim3((g.ncols + kWarps - 1) / kWarps, cnt), kWarps * 32, e_cols, stream>>>(t1, hb, g);
+      const dim3 gc((g.ncols + kWarps - 1) / kWarps, cnt);
+      if (ew_reg_cols) {
+        switch (rn) {
+#define CJX_ECA_CASE(R) \
+  case R: k_ewald_colfft_adj_reg<R><<<gc, kWarps * 32, e_cols, stream>>>(t1, hb, g); break;
+          CJX_ECA_CASE(1) CJX_ECA_CASE(2) CJX_ECA_CASE(3) CJX_ECA_CASE(4) CJX_ECA_CASE(5)
+          CJX_ECA_CASE(6) CJX_ECA_CASE(8) CJX_ECA_CASE(10) CJX_ECA_CASE(12) CJX_ECA_CASE(16)
+#undef CJX_ECA_CASE
+        }
+      } else {
+        k_ewald_colfft_adj<<<gc, kWarps * 32, e_cols, stream>>>(t1, hb, g);
+      }
       prof_end("k_ewald_colfft_adj", stream);
     } else {
     prof_begin(stream);
