@@ -1092,6 +1092,163 @@ __global__ void __launch_bounds__(kWarps * 32)
   for (int k = lane; k < n; k += 32) dst[k] = buf[pad16(k)];
 }
 
+// k_ewald_loss_adj with register FFTs (Py = 32 R): a CTA takes kWarps
+// consecutive output columns; T2 columns x, their mirrors and the observed
+// columns are staged with coalesced row loads, and the cotangents stored
+// back the same way.  Shared memory per warp: the column (then its
+// cotangent), the mirror (then its cotangent), the observed column, F.
+template <int R>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_ewald_loss_adj_reg(float2* __restrict__ t2, const float2* __restrict__ obs,
+                         const cjx_image_params* __restrict__ params, const int32_t* __restrict__ order,
+                         double* __restrict__ grads, SliceGeom g, int64_t k0, float norm) {
+  constexpr int py = 32 * R;
+  constexpr int stride = pad16(py) + 1;
+  extern __shared__ float2 smem[];
+  __shared__ float2 w32[32];
+  __shared__ float red[kWarps][4];
+  __shared__ ImageConsts sc;
+  float2* tab = smem;
+  float2* bufs = smem + py;
+  const int px = g.px;
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.pxh - j0);
+  const int64_t k = k0 + blockIdx.y;
+  const int64_t img = order ? (int64_t)order[k] : k;
+  float2* src = t2 + (size_t)blockIdx.y * py * g.ld2;
+  const float2* ocol0 = obs + (size_t)img * py * g.pxh + j0;
+  static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
+  const int sj = threadIdx.x % kWarps, sm0 = threadIdx.x / kWarps;
+  {
+    const int cj = j0 + sj, cm = (px - j0 - sj) % px;
+    float2 st[R], sb[R], so[R];
+    if (sj < ncols) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        st[q] = src[(size_t)(sm0 + 32 * q) * g.ld2 + cj];
+        sb[q] = src[(size_t)(sm0 + 32 * q) * g.ld2 + cm];
+        so[q] = ocol0[(size_t)(sm0 + 32 * q) * g.pxh + sj];
+      }
+    }
+    build_reg_twiddles(tab, py);
+    build_w32(w32);
+    if (sj < ncols) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        bufs[sj * stride + pad16(sm0 + 32 * q)] = st[q];
+        bufs[(kWarps + sj) * stride + pad16(sm0 + 32 * q)] = sb[q];
+        bufs[(2 * kWarps + sj) * stride + pad16(sm0 + 32 * q)] = so[q];
+      }
+    }
+  }
+  if (threadIdx.x == 0) sc = load_image_consts(params + img, norm, py, px);  // once per CTA
+  __syncthreads();
+  const ImageConsts& c = sc;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float sl = 0.f, stx = 0.f, sty = 0.f, sdf = 0.f;
+  if (warp < ncols) {
+    const int x = j0 + warp;
+    const bool pair = (px - x) % px != x;
+    float2* A = bufs + warp * stride;
+    float2* B = bufs + (kWarps + warp) * stride;
+    const float2* O = bufs + (2 * kWarps + warp) * stride;
+    float2* F = bufs + (3 * kWarps + warp) * stride;
+    const LaneTwiddles lt = make_lane_twiddles(w32, lane);
+    const int bl = brev5(lane);
+    float2 v[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) v[n1] = A[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(v, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) A[pad16(k1 + R * lane)] = v[k1];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) v[n1] = B[pad16(32 * n1 + bl)];
+    warp_fft_reg<R, -1>(v, tab, lt, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) B[pad16(k1 + R * lane)] = v[k1];
+    __syncwarp();
+    for (int i = lane; i < py; i += 32)
+      F[pad16(i)] = ewald_epilogue(A[pad16(i)], B[pad16((py - i) % py)], i, x, py, px, g.flags, c);
+    __syncwarp();
+    const bool self_col = (x == 0) || ((px % 2 == 0) && x == px / 2);
+    const float wj = self_col ? 1.f : 2.f;
+    const float inv_pp = 1.0f / ((float)py * (float)px);
+    // lane i alone reads A[i] and B[-i] here, so it may overwrite them with their cotangents
+    for (int i = lane; i < py; i += 32) {
+      const float2 f = F[pad16(i)];
+      float2 fh = f;
+      if (self_col) {
+        const float2 fm = F[pad16((py - i) % py)];
+        fh = make_float2(0.5f * (f.x + fm.x), 0.5f * (f.y - fm.y));
+      }
+      const float2 o = O[pad16(i)];
+      const float2 d = make_float2(fh.x - o.x, fh.y - o.y);
+      sl += wj * inv_pp * (d.x * d.x + d.y * d.y);
+      const float2 E = make_float2(2.f * wj * inv_pp * d.x, 2.f * wj * inv_pp * d.y);
+      const float zim = E.x * f.y - E.y * f.x;
+      stx += 6.283185307179586f * (float)((double)x * c.qx_step) * zim;
+      sty += 6.283185307179586f * (float)((double)fft_index(i, py) * c.qy_step) * zim;
+      const int im = (py - i) % py;
+      const EwaldAdj ad = ewald_epilogue_adj(A[pad16(i)], B[pad16(im)], E, i, x, py, px, g.flags, c);
+      sdf += ad.ddf;
+      A[pad16(i)] = ad.ga;
+      B[pad16(im)] = ad.gb;
+    }
+    __syncwarp();
+    if (!pair) {  // one column: its two cotangent shares add
+      for (int i = lane; i < py; i += 32) {
+        const float2 a = A[pad16(i)], b = B[pad16(i)];
+        A[pad16(i)] = make_float2(a.x + b.x, a.y + b.y);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) v[n1] = A[pad16(32 * n1 + bl)];
+    __syncwarp();
+    warp_fft_reg<R, +1>(v, tab, lt, lane);  // adjoint of the forward column FFT
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) A[pad16(k1 + R * lane)] = v[k1];
+    if (pair) {
+#pragma unroll
+      for (int n1 = 0; n1 < R; ++n1) v[n1] = B[pad16(32 * n1 + bl)];
+      __syncwarp();
+      warp_fft_reg<R, +1>(v, tab, lt, lane);
+#pragma unroll
+      for (int k1 = 0; k1 < R; ++k1) B[pad16(k1 + R * lane)] = v[k1];
+    }
+  }
+  sl = warp_sum(sl);
+  stx = warp_sum(stx);
+  sty = warp_sum(sty);
+  sdf = warp_sum(sdf);
+  if (lane == 0) {
+    red[warp][kGradLoss] = sl;
+    red[warp][kGradTx] = stx;
+    red[warp][kGradTy] = sty;
+    red[warp][kGradDf] = sdf;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (int w = 0; w < kWarps; ++w) acc += (double)red[w][threadIdx.x];
+    atomicAdd(&grads[img * 16 + kGradLoss + threadIdx.x], acc);
+  }
+  for (int e = threadIdx.x; e < py * kWarps; e += blockDim.x) {
+    const int m = e / kWarps, jj = e % kWarps;
+    if (jj < ncols) {
+      const int x = j0 + jj, xm = (px - x) % px;
+      src[(size_t)m * g.ld2 + x] = bufs[jj * stride + pad16(m)];
+      if (xm != x) src[(size_t)m * g.ld2 + xm] = bufs[(kWarps + jj) * stride + pad16(m)];
+    }
+  }
+}
+
+size_t ewald_loss_adj_reg_smem(const SliceGeom& g) {
+  return sizeof(float2) * (size_t)(g.py + 4 * kWarps * (pad16(g.py) + 1));
+}
+
 size_t ewald_rows_adj_reg_smem(const SliceGeom& g) {
   return sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * g.n;
 }
@@ -1135,7 +1292,8 @@ static int ensure_adjoint_smem_attrs() {
     if (e == cudaSuccess) e = allow_smem_adj(k_ewald_colfft_adj);
 #define CJX_EADJ_ATTR(R)                                                         \
   if (e == cudaSuccess) e = allow_smem_adj(k_ewald_rows_adj_reg<R>);             \
-  if (e == cudaSuccess) e = allow_smem_adj(k_ewald_colfft_adj_reg<R>);
+  if (e == cudaSuccess) e = allow_smem_adj(k_ewald_colfft_adj_reg<R>);          \
+  if (e == cudaSuccess) e = allow_smem_adj(k_ewald_loss_adj_reg<R>);
     CJX_EADJ_ATTR(1) CJX_EADJ_ATTR(2) CJX_EADJ_ATTR(3) CJX_EADJ_ATTR(4) CJX_EADJ_ATTR(5)
     CJX_EADJ_ATTR(6) CJX_EADJ_ATTR(8) CJX_EADJ_ATTR(10) CJX_EADJ_ATTR(12) CJX_EADJ_ATTR(16)
 #undef CJX_EADJ_ATTR
@@ -1228,7 +1386,8 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
   // the Ewald row and column adjoints run on register FFTs where N and Px (rows) or N (columns) are 32 R
   const bool ew_reg_rows = ewald && tn.fft_mode >= 1 && rn && rpx;
   const bool ew_reg_cols = ewald && tn.fft_mode >= 1 && rn;
-  const size_t e_loss = ewald_loss_smem(g);
+  const bool ew_reg_loss = ewald && tn.fft_mode >= 1 && rpy;
+  const size_t e_loss = ew_reg_loss ? ewald_loss_adj_reg_smem(g) : ewald_loss_smem(g);
   const size_t e_rows = ew_reg_rows ? ewald_rows_adj_reg_smem(g) : ewald_rows_adj_smem(g);
   const size_t e_cols = ew_reg_cols ? ewald_colfft_adj_reg_smem(g) : ewald_colfft_adj_smem(g);
   if (ewald ? (e_loss > 227 * 1024 || e_rows > 227 * 1024 || e_cols > 227 * 1024)
@@ -1256,8 +1415,19 @@ int launch_loss_grad(const SliceGeom& g, const float2* grid, const cjx_image_par
     if (int e = launch_forward_to_t2(g, grid, params, order, k0, cnt, t1, t2, hb, stream, tn)) return e;
     if (ewald) {
       prof_begin(stream);
-      k_ewald_loss_adj<<<dim3((g.pxh + kEwAdjWarps - 1) / kEwAdjWarps, cnt), kEwAdjWarps * 32, e_loss, stream>>>(
-          t2, obs, params, order, grads, g, k0, norm);
+      if (ew_reg_loss) {
+        const dim3 gl((g.pxh + kWarps - 1) / kWarps, cnt);
+        switch (rpy) {
+#define CJX_ELA_CASE(R) \
+  case R: k_ewald_loss_adj_reg<R><<<gl, kWarps * 32, e_loss, stream>>>(t2, obs, params, order, grads, g, k0, norm); break;
+          CJX_ELA_CASE(1) CJX_ELA_CASE(2) CJX_ELA_CASE(3) CJX_ELA_CASE(4) CJX_ELA_CASE(5)
+          CJX_ELA_CASE(6) CJX_ELA_CASE(8) CJX_ELA_CASE(10) CJX_ELA_CASE(12) CJX_ELA_CASE(16)
+#undef CJX_ELA_CASE
+        }
+      } else {
+        k_ewald_loss_adj<<<dim3((g.pxh + kEwAdjWarps - 1) / kEwAdjWarps, cnt), kEwAdjWarps * 32, e_loss, stream>>>(
+            t2, obs, params, order, grads, g, k0, norm);
+      }
       prof_end("k_ewald_loss_adj", stream);
       prof_begin(stream);
       const dim3 gr((g.py + kWarps - 1) / kWarps, cnt);

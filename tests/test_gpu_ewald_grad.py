@@ -109,6 +109,7 @@ def _check_parameter_gradients(res, og, fs, specs, obs, spline):
     (32, (40, 24), 60.0),   # non-square crop
     (32, (70, 66), 40.0),   # pad 64 -> 70 x 66
     (31, (31, 31), 30.0),   # N = 62, odd image (no Nyquist column or row)
+    (64, (64, 64), 40.0),   # crop 128 -> 64: register transforms of 64 and 128 points in all three adjoint passes
 ])
 def test_ewald_loss_and_parameter_gradients(cuda_device, box, shape, kv):
     from cryojax_b200.gradients import squared_residual_and_grad
