@@ -1049,19 +1049,28 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
 }
 
-// Column adjoint in registers: the window transpose reads g_T1 straight into
-// the lane's bit-reversed inputs; the N-point FFT's output is staged so that
-// the surface column is stored contiguously.
+// Column adjoint in registers: a CTA takes kWarps consecutive surface
+// columns, stages their g_T1 entries with coalesced row loads, and each warp
+// reads its column through the window transpose into the lane's
+// bit-reversed inputs; the N-point FFT's output is staged so that the
+// surface column is stored contiguously.
 template <int RN>
 __global__ void __launch_bounds__(kWarps * 32)
     k_ewald_colfft_adj_reg(const float2* __restrict__ t1, float2* __restrict__ hb, SliceGeom g) {
   constexpr int n = 32 * RN;
-  constexpr int stride = pad16(n) + 1;
   extern __shared__ float2 smem[];
   __shared__ float2 w32[32];
+  const int stride = pad16(max(n, g.py)) + 1;
   float2* tab = smem;
   float2* bufs = smem + n;
   int* winv = reinterpret_cast<int*>(bufs + kWarps * stride);
+  const int j0 = blockIdx.x * kWarps;
+  const int ncols = min(kWarps, g.ncols - j0);
+  static_assert(kWarps * 32 == 256, "the staging map assumes 256 threads");
+  const int sj = threadIdx.x % kWarps, sm0 = threadIdx.x / kWarps;
+  const float2* blk = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j0;
+  if (sj < ncols)
+    for (int m = sm0; m < g.py; m += 32) bufs[sj * stride + pad16(m)] = blk[(size_t)m * g.ld1 + sj];
   build_reg_twiddles(tab, n);
   build_w32(w32);
   for (int k = threadIdx.x; k < n; k += blockDim.x) winv[k] = -1;
@@ -1072,23 +1081,22 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int j = blockIdx.x * kWarps + warp;
-  if (j >= g.ncols) return;
+  if (warp >= ncols) return;
   const int bl = brev5(lane);
-  const float2* col = t1 + (size_t)blockIdx.y * g.py * g.ld1 + j;
+  float2* buf = bufs + warp * stride;
   float2 z[RN];
 #pragma unroll
   for (int n1 = 0; n1 < RN; ++n1) {
     const int m = winv[32 * n1 + bl];
-    z[n1] = (m >= 0) ? col[(size_t)m * g.ld1] : make_float2(0.f, 0.f);
+    z[n1] = (m >= 0) ? buf[pad16(m)] : make_float2(0.f, 0.f);
   }
+  __syncwarp();
   const LaneTwiddles lt = make_lane_twiddles(w32, lane);
   warp_fft_reg<RN, -1>(z, tab, lt, lane);
-  float2* buf = bufs + warp * stride;
 #pragma unroll
   for (int k1 = 0; k1 < RN; ++k1) buf[pad16(k1 + RN * lane)] = z[k1];
   __syncwarp();
-  float2* dst = hb + ((size_t)blockIdx.y * g.ncols + j) * g.ldh;
+  float2* dst = hb + ((size_t)blockIdx.y * g.ncols + j0 + warp) * g.ldh;
   for (int k = lane; k < n; k += 32) dst[k] = buf[pad16(k)];
 }
 
@@ -1253,7 +1261,7 @@ size_t ewald_rows_adj_reg_smem(const SliceGeom& g) {
   return sizeof(float2) * (size_t)(g.n + g.px + kWarps * (pad16(std::max(g.n, g.px)) + 1)) + sizeof(int) * g.n;
 }
 size_t ewald_colfft_adj_reg_smem(const SliceGeom& g) {
-  return sizeof(float2) * (size_t)(g.n + kWarps * (pad16(g.n) + 1)) + sizeof(int) * g.n;
+  return sizeof(float2) * (size_t)(g.n + kWarps * (pad16(std::max(g.n, g.py)) + 1)) + sizeof(int) * g.n;
 }
 
 size_t ewald_loss_smem(const SliceGeom& g) {
